@@ -1,0 +1,348 @@
+"""Benchmark: cell-updates/s of the cubed-sphere finite-volume step on B200.
+
+Workload (default): the exo3 dry ideal-gas atmosphere, 6 panels x 96 x 96 x
+64 levels, FP64, WENO5 + LMARS + the 5x5 implicit vertical solver
+(implicit_flag 9), SSPRK(3,3), CFL time step -- a seeded synthetic state
+(isothermal 250 K hydrostatic column, 1 K temperature noise, 5 m/s winds).
+A "step" is one SSPRK(3,3) step of the whole atmosphere; one cell-update is
+one interior cell advanced one step (6*N*N*L per step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU; every rank advances its own atmosphere (an
+independent ensemble member), so there is no data-path collective and the
+scaling is weak.  Timing: CUDA events on the library's stream, barrier +
+synchronize on both sides, max over ranks.
+
+--impl reference times the reference's CPU algorithm on this host's cores.
+The reference itself cannot be built here (its Athena++ fork, MPI, NetCDF
+and Eigen are not available), so the C++ restatement in oracle/ stands in
+for it ("kind": "port").
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL_UPDATE = 320  # 8 registers x 5 vars x 8 B per SSPRK(3,3) step
+
+
+def workload_config(name):
+    from exocubed_b200 import workloads as W
+    if name == "c2":
+        return (W.dry_atmosphere_config(N=96, L=64, rsolver=1),
+                "exo3 dry ideal gas 6x96x96x64 FP64 WENO5+LMARS+implicit(9), SSPRK3, CFL 0.4")
+    if name == "c1":
+        return (W.shallow_water_config(N=48),
+                "exo2 shallow water 6x48x48x3 FP64 WENO5+Roe, SSPRK3, CFL 0.4")
+    if name == "c3":
+        return (W.dry_atmosphere_config(N=192, L=96, rsolver=1),
+                "exo3 dry ideal gas 6x192x192x96 FP64 WENO5+LMARS+implicit(9), SSPRK3, CFL 0.4")
+    raise ValueError(name)
+
+
+def make_state(cfg, seed):
+    from exocubed_b200 import workloads as W
+    if cfg["eqn"] == 0:
+        return W.shallow_water_state(cfg, seed=seed)
+    return W.dry_atmosphere_state(cfg, seed=seed)
+
+
+def cells_of(cfg):
+    return 6 * cfg["N"] * cfg["N"] * cfg["L"]
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed --
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------- CPU baseline --
+def cpu_worker(args):
+    """Runs in a fresh process: times the oracle on all host cores."""
+    import numpy as np  # noqa: F401
+    from oracle import oracle
+    cfg, _ = workload_config(args.workload)
+    o = oracle.Oracle(cfg)
+    o.set_primitive(make_state(cfg, 0))
+    o.step(args.cpu_warmup)
+    t0 = time.perf_counter()
+    o.step(args.cpu_steps)
+    el = time.perf_counter() - t0
+    print(json.dumps({"seconds": el, "steps": args.cpu_steps,
+                      "cells": cells_of(cfg), "threads": os.cpu_count()}))
+
+
+def run_cpu(workload, steps, warmup):
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(os.cpu_count())
+    env.pop("CUDA_VISIBLE_DEVICES", None)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--workload", workload,
+           "--cpu-steps", str(steps), "--cpu-warmup", str(warmup)]
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+# -------------------------------------------------------------- our arm --
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from exocubed_b200 import _native as nat
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    cfg, desc = workload_config(args.workload)
+    state = make_state(cfg, seed=rank)
+    g = CubedSphereAtmosphere(cfg)
+    g.set_primitive(state)
+    stream = torch.cuda.ExternalStream(g.stream)
+    cells = cells_of(cfg)
+
+    g.step(args.warmup)
+    g.synchronize()
+
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+    launches0 = g.launch_count()
+    g.profile(True)
+    barrier(pg)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(pg)
+    ms = e0.elapsed_time(e1)
+    prof = g.profile_read()
+    g.profile(False)
+    launches = g.launch_count() - launches0
+    clk = clocks.stop() if rank == 0 else None
+    ms_max = max_over_ranks(pg, ms)
+    invalid = g.invalid()
+
+    # end to end through the public API: pinned host state in, K steps,
+    # pinned host state out
+    nbytes = state.nbytes
+    h_in = torch.from_numpy(state).pin_memory()
+    h_out = torch.empty(state.shape, dtype=torch.float64).pin_memory()
+    g2 = CubedSphereAtmosphere(cfg)
+    s2 = torch.cuda.ExternalStream(g2.stream)
+    g2.set_primitive_ptr(h_in.data_ptr())
+    g2.step(1)
+    g2.synchronize()
+    barrier(pg)
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(s2)
+    g2.set_primitive_ptr(h_in.data_ptr())
+    g2.step(args.steps)
+    g2.conserved_ptr(h_out.data_ptr())
+    f1.record(s2)
+    f1.synchronize()
+    barrier(pg)
+    ms_e2e = max_over_ranks(pg, f0.elapsed_time(f1))
+    g2.close()
+
+    value = world * cells * args.steps / (ms_max / 1e3)
+    e2e_value = world * cells * args.steps / (ms_e2e / 1e3)
+
+    # dominant kernel and its roofline (algorithmic bytes per launch)
+    per_cell_alg = {"flux_x1": 10, "flux_x23": 15, "update": 35, "implicit": 20,
+                    "prim_ghost": 10, "other": 0}  # doubles moved once per cell
+    dom = max((k for k in prof if k != "other"), key=lambda k: prof[k][1])
+    n_l, t_l = prof[dom]
+    avg_ms = t_l / max(n_l, 1)
+    alg_bytes = per_cell_alg[dom] * 8 * cells
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_c2.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+    shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
+
+    if rank != 0:
+        g.close()
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        r = run_cpu(args.workload, args.cpu_steps, 1)
+        cpu = {"value": r["cells"] * r["steps"] / r["seconds"], "unit": "cell-updates/s",
+               "cores": r["threads"], "kind": "port",
+               "sample": f"oracle/ C++ restatement, OpenMP on {r['threads']} threads, "
+                         f"{r['steps']} steps of the same workload after 1 warm-up step"}
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "cells_per_step": cells, "replicas": world,
+                   "l2": "state arrays of 175 MB each exceed the 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": dom,
+                     "peak_kind": peak_kind,
+                     "step_frac": value / world * BYTES_PER_CELL_UPDATE / 1e9 / peak},
+        "kernel_share": shares,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+                "steps_per_request": args.steps},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "state_valid": invalid == 0,
+    }
+    print(json.dumps(line))
+    g.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg, desc = workload_config(args.workload)
+    r = run_cpu(args.workload, args.steps, args.warmup)
+    v = r["cells"] * r["steps"] / r["seconds"]
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["seconds"] / r["steps"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "cells_per_step": r["cells"]},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": r["threads"],
+                         "kind": "port",
+                         "sample": f"{r['steps']} full steps after {args.warmup} warm-up steps; "
+                                   "the reference cannot be built here, its C++ restatement "
+                                   "(oracle/) runs with OpenMP on all host threads"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-warmup", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-worker", action="store_true")
+    args = ap.parse_args()
+    if args.cpu_worker:
+        cpu_worker(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+"""ctypes binding of libexo_b200.so (the C ABI declared in include/exo_b200.h).
+
+The shared library is built in-tree by exocubed_b200/csrc/Makefile.  Loading
+fails loudly when it is missing: there is no CPU fallback for the product
+path.
+"""
+import ctypes
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libexo_b200.so")
+
+EXO_OK = 0
+EXO_EQN_SHALLOW_YZ, EXO_EQN_IDEAL = 0, 1
+EXO_RS_ROE_SHALLOW, EXO_RS_LMARS, EXO_RS_HLLC, EXO_RS_LMARS_SHALLOW = 0, 1, 2, 3
+EXO_PREC_FP64, EXO_PREC_MIXED = 0, 1
+EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92 = 0, 1
+NGHOST = 3
+
+# every symbol include/exo_b200.h declares
+EXPORTED = [
+    "exo_config_default", "exo_create", "exo_destroy", "exo_cell_geometry", "exo_mesh",
+    "exo_shape", "exo_last_error", "exo_set_primitive", "exo_get_conserved",
+    "exo_get_primitive", "exo_device_state", "exo_step", "exo_get_dt",
+    "exo_get_time", "exo_check_state", "exo_synchronize",
+    "exo_calculate_fluxes", "exo_get_flux", "exo_riemann", "exo_weno5",
+    "exo_get_stream", "exo_profile", "exo_profile_read", "exo_launch_count",
+]
+KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
+
+
+class ExoConfig(ctypes.Structure):
+    """exo_config of include/exo_b200.h."""
+    _fields_ = [
+        ("N", ctypes.c_int), ("L", ctypes.c_int), ("eqn", ctypes.c_int),
+        ("rsolver", ctypes.c_int), ("implicit_flag", ctypes.c_int),
+        ("precision", ctypes.c_int), ("coriolis", ctypes.c_int),
+        ("reserved0", ctypes.c_int),
+        ("x1min", ctypes.c_double), ("x1max", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("Rd", ctypes.c_double),
+        ("grav", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("omega", ctypes.c_double), ("reserved1", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ExoError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"exo error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def build():
+    """Compile the library in-tree (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "csrc")], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with "
+                          "`make -C exocubed_b200/csrc` (or __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    i, d, p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    cfgp = ctypes.POINTER(ExoConfig)
+    L.exo_last_error.restype = ctypes.c_char_p
+    L.exo_last_error.argtypes = []
+    L.exo_config_default.argtypes = [cfgp, i]
+    L.exo_create.argtypes = [cfgp, ctypes.POINTER(p)]
+    L.exo_destroy.argtypes = [p]
+    L.exo_destroy.restype = None
+    L.exo_cell_geometry.argtypes = [cfgp, dp, dp, dp, dp]
+    L.exo_mesh.argtypes = [cfgp, i, dp, dp, dp]
+    L.exo_shape.argtypes = [p] + [ctypes.POINTER(i)] * 4
+    L.exo_set_primitive.argtypes = [p, dp]
+    L.exo_get_conserved.argtypes = [p, dp]
+    L.exo_get_primitive.argtypes = [p, dp]
+    L.exo_device_state.argtypes = [p, ctypes.POINTER(p), ctypes.POINTER(p)]
+    L.exo_step.argtypes = [p, i, d]
+    L.exo_get_dt.argtypes = [p, dp]
+    L.exo_get_time.argtypes = [p, dp, ctypes.POINTER(ctypes.c_int64)]
+    L.exo_check_state.argtypes = [p, ctypes.POINTER(i)]
+    L.exo_synchronize.argtypes = [p]
+    L.exo_calculate_fluxes.argtypes = [p]
+    L.exo_get_flux.argtypes = [p, i, dp]
+    L.exo_riemann.argtypes = [i, i, i, i, d, p, p, p, p, p, p, p, p]
+    L.exo_weno5.argtypes = [i, p, p, p, p, p, p, p]
+    L.exo_get_stream.argtypes = [p, ctypes.POINTER(p)]
+    L.exo_profile.argtypes = [p, i]
+    L.exo_profile_read.argtypes = [p, i, ctypes.POINTER(ctypes.c_int64), dp]
+    L.exo_launch_count.argtypes = [p, ctypes.POINTER(ctypes.c_int64)]
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != EXO_OK:
+        raise ExoError(rc, lib().exo_last_error().decode())
+    return rc
+
+
+def dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))

@@ -1,0 +1,537 @@
+// capi.cpp -- the extern "C" boundary (include/exo_b200.h): context
+// lifecycle, device memory, the stage sequence and the operator hooks.
+//
+// The stage sequence is ImplicitHydroTasks / TimeIntegratorTaskList of the
+// reference (src/tasklist/implicit_hydro_tasks.cpp:40-102,
+// patches/24.time_integrator.patch:22-60) with every MPI exchange replaced by
+// a device read of the neighbour panel:
+//   CALC_HYDFLX -> INT_HYD -> SRC_TERM -> IMPLICIT_CORR -> UPDATE_ALLCONS ->
+//   ghost exchange -> CONS2PRIM -> PHY_BVAL -> NEW_DT
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "exo_internal.h"
+
+using exo::DevScalars;
+using exo::DevView;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return EXO_ERR_CUDA;
+}
+
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+#define RK(call)                                               \
+  do {                                                         \
+    int r_ = (call);                                           \
+    if (r_) {                                                  \
+      cudaError_t e_ = cudaGetLastError();                     \
+      return cuda_fail(e_ == cudaSuccess ? cudaErrorUnknown : e_, #call); \
+    }                                                          \
+  } while (0)
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& src, std::vector<void*>& owned) {
+  size_t bytes = src.size() * sizeof(T);
+  if (bytes == 0) bytes = sizeof(T);
+  CK(cudaMalloc((void**)dst, bytes));
+  owned.push_back(*dst);
+  if (!src.empty()) CK(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+}  // namespace
+
+struct ProfEvent {
+  cudaEvent_t a, b;
+  int kernel;
+};
+
+struct exo_ctx {
+  exo_config cfg;
+  bool profiling = false;
+  std::vector<ProfEvent> prof_used;
+  std::vector<ProfEvent> prof_pool;
+  int64_t launches = 0;
+  exo::HostTables tab;
+  DevView v;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> owned;
+  size_t state_elems = 0;  // 6*nv*cells
+  bool has_state = false;
+  int device = 0;
+};
+
+// Run one launch, bracketed by events when profiling.  `nlaunch` is the
+// number of kernels the launcher issues.
+template <typename F>
+static int timed(exo_ctx* c, int kernel, int nlaunch, F&& f) {
+  ProfEvent ev;
+  if (c->profiling) {
+    if (c->prof_pool.empty()) {
+      ProfEvent n;
+      CK(cudaEventCreate(&n.a));
+      CK(cudaEventCreate(&n.b));
+      c->prof_pool.push_back(n);
+    }
+    ev = c->prof_pool.back();
+    c->prof_pool.pop_back();
+    ev.kernel = kernel;
+    CK(cudaEventRecord(ev.a, c->stream));
+  }
+  int rc = f();
+  if (rc) {
+    cudaError_t e = cudaGetLastError();
+    return cuda_fail(e == cudaSuccess ? cudaErrorUnknown : e, "kernel launch");
+  }
+  c->launches += nlaunch;
+  if (c->profiling) {
+    CK(cudaEventRecord(ev.b, c->stream));
+    c->prof_used.push_back(ev);
+  }
+  return 0;
+}
+
+// ghost exchange + ConservedToPrimitive + x1 boundary (+ CFL candidate)
+static int boundary_and_prim(exo_ctx* c, bool dt) {
+  int rc;
+  if (dt && (rc = timed(c, EXO_K_OTHER, 1, [&] { return exo::launch_dt_reset(c->v, c->stream); })))
+    return rc;
+  return timed(c, EXO_K_PRIM_GHOST, 1,
+               [&] { return exo::launch_prim_ghost(c->v, dt, c->stream); });
+}
+
+static int one_step(exo_ctx* c, double dt_fixed) {
+  const DevView& v = c->v;
+  bool shallow = v.eqn == EXO_EQN_SHALLOW_YZ;
+  bool implicit = !shallow && (v.implicit_flag & 1);
+  int rc;
+  if (dt_fixed > 0. &&
+      (rc = timed(c, EXO_K_OTHER, 1, [&] { return exo::launch_set_dt(v, dt_fixed, c->stream); })))
+    return rc;
+  for (int s = 0; s < 3; ++s) {
+    if (!shallow &&
+        (rc = timed(c, EXO_K_FLUX_X1, 1, [&] { return exo::launch_flux_x1(v, c->stream); })))
+      return rc;
+    if ((rc = timed(c, EXO_K_FLUX_X23, 1, [&] { return exo::launch_flux_x23(v, c->stream); })))
+      return rc;
+    int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
+    if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return exo::launch_update(v, s, c->stream); })))
+      return rc;
+    if (implicit &&
+        (rc = timed(c, EXO_K_IMPLICIT, 1, [&] { return exo::launch_implicit(v, s, c->stream); })))
+      return rc;
+    if ((rc = boundary_and_prim(c, s == 2 && dt_fixed <= 0.))) return rc;
+  }
+  return timed(c, EXO_K_OTHER, 1,
+               [&] { return exo::launch_dt_finalize(v, dt_fixed, true, c->stream); });
+}
+
+extern "C" {
+
+const char* exo_last_error(void) { return g_err.c_str(); }
+
+int exo_config_default(exo_config* cfg, int eqn) {
+  if (!cfg) return fail(EXO_ERR_ARG, "cfg is NULL");
+  std::memset(cfg, 0, sizeof(*cfg));
+  if (eqn == EXO_EQN_SHALLOW_YZ) {
+    // exo2 shallow water: examples/2023-Chen-exo3/W92.inp
+    cfg->N = 48;
+    cfg->L = 3;
+    cfg->eqn = EXO_EQN_SHALLOW_YZ;
+    cfg->rsolver = EXO_RS_ROE_SHALLOW;
+    cfg->implicit_flag = 0;
+    cfg->coriolis = EXO_CORIOLIS_W92;
+    cfg->x1min = 6371000.;
+    cfg->x1max = 6371001.;
+    cfg->gamma = 1.4;
+    cfg->Rd = 287.;
+    cfg->grav = 0.;
+    cfg->cfl = 0.4;
+    cfg->omega = 7.292e-5;
+  } else if (eqn == EXO_EQN_IDEAL) {
+    // exo3 dry ideal gas: 96^2 x 64, LMARS, implicit_flag 9
+    cfg->N = 96;
+    cfg->L = 64;
+    cfg->eqn = EXO_EQN_IDEAL;
+    cfg->rsolver = EXO_RS_LMARS;
+    cfg->implicit_flag = 9;
+    cfg->coriolis = EXO_CORIOLIS_NONE;
+    cfg->gamma = 1.4;
+    cfg->Rd = 287.;
+    cfg->grav = -9.81;
+    cfg->x1min = 6.371e6;
+    cfg->x1max = 6.371e6 + 287. * 250. / 9.81 * 4.605170185988092;  // 1e5 -> 1e3 Pa
+    cfg->cfl = 0.4;
+    cfg->omega = 0.;
+  } else {
+    return fail(EXO_ERR_ARG, "unknown equation set");
+  }
+  return EXO_OK;
+}
+
+int exo_create(const exo_config* cfg, exo_ctx** out) {
+  if (!cfg || !out) return fail(EXO_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  if (cfg->eqn != EXO_EQN_SHALLOW_YZ && cfg->eqn != EXO_EQN_IDEAL)
+    return fail(EXO_ERR_ARG, "unknown equation set");
+  bool shallow = cfg->eqn == EXO_EQN_SHALLOW_YZ;
+  if (shallow && cfg->rsolver != EXO_RS_ROE_SHALLOW && cfg->rsolver != EXO_RS_LMARS_SHALLOW)
+    return fail(EXO_ERR_ARG, "shallow water needs the Roe or LMARS shallow-water solver");
+  if (!shallow && cfg->rsolver != EXO_RS_LMARS && cfg->rsolver != EXO_RS_HLLC)
+    return fail(EXO_ERR_ARG, "the ideal gas needs the LMARS or HLLC solver");
+  if (cfg->precision != EXO_PREC_FP64)
+    return fail(EXO_ERR_ARG, "only EXO_PREC_FP64 is available in this build");
+  if (!shallow && (cfg->implicit_flag & ~9))
+    return fail(EXO_ERR_ARG, "implicit_flag: only bits 1 (x1) and 8 (full 5x5) are supported");
+  if (!shallow && (cfg->implicit_flag & 1) && !(cfg->implicit_flag & 8))
+    return fail(EXO_ERR_ARG, "implicit_flag 1 (partial 3x3 correction) is not available; use 9");
+  if (!(cfg->cfl > 0.) || !(cfg->gamma > 1.) || !(cfg->x1max > cfg->x1min))
+    return fail(EXO_ERR_ARG, "cfl, gamma or x1 range out of range");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(EXO_ERR_NOGPU, "no CUDA device");
+
+  exo_ctx* c = new exo_ctx();
+  c->cfg = *cfg;
+  std::string err;
+  if (!exo::build_tables(*cfg, c->tab, &err)) {
+    delete c;
+    return fail(EXO_ERR_ARG, err);
+  }
+  cudaGetDevice(&c->device);
+  auto cleanup = [&](int rc) {
+    for (void* p : c->owned) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(EXO_ERR_CUDA, "cudaStreamCreate failed"));
+
+  DevView& v = c->v;
+  std::memset(&v, 0, sizeof(v));
+  const exo::HostTables& t = c->tab;
+  v.N = cfg->N;
+  v.L = cfg->L;
+  v.nv = shallow ? 4 : 5;
+  v.nc1 = t.nc1;
+  v.nc2 = t.nc2;
+  v.nc3 = t.nc3;
+  v.is = v.js = v.ks = exo::G;
+  v.ie = exo::G + cfg->L - 1;
+  v.je = v.ke = exo::G + cfg->N - 1;
+  v.eqn = cfg->eqn;
+  v.rsolver = cfg->rsolver;
+  v.implicit_flag = shallow ? 0 : cfg->implicit_flag;
+  v.coriolis = cfg->coriolis;
+  v.precision = cfg->precision;
+  v.gamma = cfg->gamma;
+  v.Rd = cfg->Rd;
+  v.grav = shallow ? 0. : cfg->grav;
+  v.cfl = cfg->cfl;
+  v.cells = (size_t)t.nc3 * t.nc2 * t.nc1;
+  c->state_elems = (size_t)6 * v.nv * v.cells;
+  size_t bytes = c->state_elems * sizeof(double);
+
+  double** arrays[] = {&v.u, &v.w, &v.u1, &v.flux[1], &v.flux[2]};
+  for (double** a : arrays) {
+    cudaError_t e = cudaMalloc((void**)a, bytes);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(state)"));
+    c->owned.push_back(*a);
+    cudaMemset(*a, 0, bytes);
+  }
+  if (!shallow) {
+    double** more[] = {&v.du, &v.flux[0]};
+    for (double** a : more) {
+      cudaError_t e = cudaMalloc((void**)a, bytes);
+      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(state)"));
+      c->owned.push_back(*a);
+      cudaMemset(*a, 0, bytes);
+    }
+    if (v.implicit_flag & 1) {
+      size_t sbytes = (size_t)6 * cfg->N * cfg->N * cfg->L * 30 * sizeof(double);
+      cudaError_t e = cudaMalloc((void**)&v.scratch, sbytes);
+      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(implicit scratch)"));
+      c->owned.push_back(v.scratch);
+    }
+  }
+  double *x1f, *x1v, *dx1f, *geo;
+  int* gmap;
+  exo::GhostEntry* gh;
+  exo::EdgeEntry* ed;
+  if (upload(&x1f, t.x1f, c->owned) || upload(&x1v, t.x1v, c->owned) ||
+      upload(&dx1f, t.dx1f, c->owned) || upload(&geo, t.geo, c->owned) ||
+      upload(&gmap, t.ghost_map, c->owned) || upload(&gh, t.ghost, c->owned) ||
+      upload(&ed, t.edge, c->owned))
+    return cleanup(EXO_ERR_CUDA);
+  v.x1f = x1f;
+  v.x1v = x1v;
+  v.dx1f = dx1f;
+  v.geo = geo;
+  v.ghost_map = gmap;
+  v.ghost = gh;
+  v.edge = ed;
+  cudaError_t e = cudaMalloc((void**)&v.sc, sizeof(DevScalars));
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(scalars)"));
+  c->owned.push_back(v.sc);
+  cudaMemset(v.sc, 0, sizeof(DevScalars));
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "exo_create"));
+  *out = c;
+  return EXO_OK;
+}
+
+void exo_destroy(exo_ctx* c) {
+  if (!c) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& e : c->prof_used) c->prof_pool.push_back(e);
+  for (auto& e : c->prof_pool) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  for (void* p : c->owned) cudaFree(p);
+  cudaStreamDestroy(c->stream);
+  cudaSetDevice(prev);
+  delete c;
+}
+
+int exo_cell_geometry(const exo_config* cfg, double* lat, double* lon, double* uv_to_v23,
+                      double* x1v) {
+  if (!cfg) return fail(EXO_ERR_ARG, "cfg is NULL");
+  exo::HostTables t;
+  std::string err;
+  if (!exo::build_tables(*cfg, t, &err)) return fail(EXO_ERR_ARG, err);
+  int N = cfg->N;
+  for (int p = 0; p < 6; ++p)
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j) {
+        size_t q = ((size_t)p * N + k) * N + j;
+        double dX = tan(t.x2v[p][exo::G + j]), dY = tan(t.x3v[p][exo::G + k]);
+        double la, lo;
+        exo::rll_from_xyp(dY, -dX, p, lo, la);
+        if (lat) lat[q] = la;
+        if (lon) lon[q] = 2.0 * 3.1415926535897932 - lo;
+        if (uv_to_v23) {
+          double c[4];
+          exo::abp_from_rll_coef(dX, dY, p + 1, c);
+          uv_to_v23[4 * q + 0] = -c[0];
+          uv_to_v23[4 * q + 1] = c[1];
+          uv_to_v23[4 * q + 2] = -c[2];
+          uv_to_v23[4 * q + 3] = c[3];
+        }
+      }
+  if (x1v)
+    for (int i = 0; i < cfg->L; ++i) x1v[i] = t.x1v[exo::G + i];
+  return EXO_OK;
+}
+
+int exo_mesh(const exo_config* cfg, int panel, double* x1f, double* x2f, double* x3f) {
+  if (!cfg) return fail(EXO_ERR_ARG, "cfg is NULL");
+  if (panel < 0 || panel > 5) return fail(EXO_ERR_ARG, "panel must be 0..5");
+  exo::HostTables t;
+  std::string err;
+  if (!exo::build_tables(*cfg, t, &err)) return fail(EXO_ERR_ARG, err);
+  if (x1f) std::memcpy(x1f, t.x1f.data(), t.x1f.size() * sizeof(double));
+  if (x2f) std::memcpy(x2f, t.x2f[panel].data(), t.x2f[panel].size() * sizeof(double));
+  if (x3f) std::memcpy(x3f, t.x3f[panel].data(), t.x3f[panel].size() * sizeof(double));
+  return EXO_OK;
+}
+
+int exo_shape(const exo_ctx* c, int* nvar, int* nc3, int* nc2, int* nc1) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (nvar) *nvar = c->v.nv;
+  if (nc3) *nc3 = c->v.nc3;
+  if (nc2) *nc2 = c->v.nc2;
+  if (nc1) *nc1 = c->v.nc1;
+  return EXO_OK;
+}
+
+int exo_set_primitive(exo_ctx* c, const double* w_host) {
+  if (!c || !w_host) return fail(EXO_ERR_ARG, "NULL argument");
+  size_t bytes = c->state_elems * sizeof(double);
+  // stage through the w array, then P2C of the interior into u
+  CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  RK(exo::launch_p2c_interior(c->v, c->v.w, c->stream));
+  int rc = boundary_and_prim(c, true);
+  if (rc) return rc;
+  RK(exo::launch_dt_finalize(c->v, 0., false, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->has_state = true;
+  return EXO_OK;
+}
+
+int exo_get_conserved(exo_ctx* c, double* u_host) {
+  if (!c || !u_host) return fail(EXO_ERR_ARG, "NULL argument");
+  CK(cudaMemcpyAsync(u_host, c->v.u, c->state_elems * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_get_primitive(exo_ctx* c, double* w_host) {
+  if (!c || !w_host) return fail(EXO_ERR_ARG, "NULL argument");
+  CK(cudaMemcpyAsync(w_host, c->v.w, c->state_elems * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_device_state(exo_ctx* c, double** u_dev, double** w_dev) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (u_dev) *u_dev = c->v.u;
+  if (w_dev) *w_dev = c->v.w;
+  return EXO_OK;
+}
+
+int exo_step(exo_ctx* c, int nsteps, double dt_fixed) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
+  if (nsteps < 0) return fail(EXO_ERR_ARG, "nsteps < 0");
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = one_step(c, dt_fixed);
+    if (rc) return rc;
+  }
+  return EXO_OK;
+}
+
+int exo_get_dt(exo_ctx* c, double* dt) {
+  if (!c || !dt) return fail(EXO_ERR_ARG, "NULL argument");
+  DevScalars s;
+  CK(cudaMemcpyAsync(&s, c->v.sc, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *dt = s.dt;
+  return EXO_OK;
+}
+
+int exo_get_time(exo_ctx* c, double* time, int64_t* ncycle) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  DevScalars s;
+  CK(cudaMemcpyAsync(&s, c->v.sc, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (time) *time = s.time;
+  if (ncycle) *ncycle = s.ncycle;
+  return EXO_OK;
+}
+
+int exo_check_state(exo_ctx* c, int* invalid) {
+  if (!c || !invalid) return fail(EXO_ERR_ARG, "NULL argument");
+  DevScalars s;
+  CK(cudaMemcpyAsync(&s, c->v.sc, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *invalid = s.invalid;
+  int zero = 0;
+  CK(cudaMemcpyAsync(&c->v.sc->invalid, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_synchronize(exo_ctx* c) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_get_stream(exo_ctx* c, void** stream) {
+  if (!c || !stream) return fail(EXO_ERR_ARG, "NULL argument");
+  *stream = (void*)c->stream;
+  return EXO_OK;
+}
+
+int exo_profile(exo_ctx* c, int enable) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto& e : c->prof_used) c->prof_pool.push_back(e);
+  c->prof_used.clear();
+  c->profiling = enable != 0;
+  return EXO_OK;
+}
+
+int exo_profile_read(exo_ctx* c, int kernel, int64_t* launches, double* total_ms) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (kernel < 0 || kernel >= EXO_K_COUNT) return fail(EXO_ERR_ARG, "unknown kernel id");
+  CK(cudaStreamSynchronize(c->stream));
+  int64_t n = 0;
+  double ms = 0.;
+  for (auto& e : c->prof_used) {
+    if (e.kernel != kernel) continue;
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e.a, e.b));
+    ms += t;
+    ++n;
+  }
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
+  return EXO_OK;
+}
+
+int exo_launch_count(exo_ctx* c, int64_t* launches) {
+  if (!c || !launches) return fail(EXO_ERR_ARG, "NULL argument");
+  *launches = c->launches;
+  return EXO_OK;
+}
+
+int exo_calculate_fluxes(exo_ctx* c) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
+  RK(exo::launch_flux_x1(c->v, c->stream));
+  RK(exo::launch_flux_x23(c->v, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_get_flux(exo_ctx* c, int dir, double* flux_host) {
+  if (!c || !flux_host) return fail(EXO_ERR_ARG, "NULL argument");
+  if (dir < 0 || dir > 2) return fail(EXO_ERR_ARG, "dir must be 0, 1 or 2");
+  size_t bytes = c->state_elems * sizeof(double);
+  if (!c->v.flux[dir]) {
+    std::memset(flux_host, 0, bytes);
+    return EXO_OK;
+  }
+  CK(cudaMemcpyAsync(flux_host, c->v.flux[dir], bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_riemann(int rsolver, int eqn, int ivx, int n, double gamma, const double* wl,
+                const double* wr, double* flx, const double* cos_face, const double* sin_face,
+                const double* cth_proj, const double* cth_cell, void* stream) {
+  if (n < 0 || !wl || !wr || !flx) return fail(EXO_ERR_ARG, "bad argument");
+  if (ivx < exo::IVX || ivx > exo::IVZ) return fail(EXO_ERR_ARG, "ivx must be 1, 2 or 3");
+  if (rsolver < EXO_RS_ROE_SHALLOW || rsolver > EXO_RS_LMARS_SHALLOW)
+    return fail(EXO_ERR_ARG, "unknown Riemann solver");
+  RK(exo::launch_riemann_rows(rsolver, eqn, ivx, n, gamma, wl, wr, flx, cos_face, sin_face,
+                              cth_proj, cth_cell, stream));
+  return EXO_OK;
+}
+
+int exo_weno5(int n, const double* a, const double* b, const double* c, const double* d,
+              const double* e, double* out, void* stream) {
+  if (n < 0 || !a || !b || !c || !d || !e || !out) return fail(EXO_ERR_ARG, "bad argument");
+  RK(exo::launch_weno5(n, a, b, c, d, e, out, stream));
+  return EXO_OK;
+}
+
+}  // extern "C"

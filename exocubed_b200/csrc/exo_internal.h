@@ -1,0 +1,136 @@
+// exo_internal.h -- shared definitions of the host geometry builder, the
+// CUDA kernels and the C ABI layer.
+#ifndef EXO_INTERNAL_H_
+#define EXO_INTERNAL_H_
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/exo_b200.h"
+
+namespace exo {
+
+constexpr int G = EXO_NGHOST;
+constexpr int IDN = 0, IVX = 1, IVY = 2, IVZ = 3, IPR = 4, IEN = 4;
+enum Side { UP = 0, DOWN = 1, LEFT = 2, RIGHT = 3 };
+
+// Fields of the per-panel (k,j) metric table, each nc3*nc2 doubles per panel.
+enum Geo2D {
+  GCOSC = 0, GSINC, GCOSF2, GSINF2, GCOSF3, GSINF3,  // cell / face metric
+  GDX2A, GDX3A, GDX2A_F3, GDX3A_F2,                // angular widths
+  GCTHP1, GCTHP2, GCTHP3,                          // flux projection angles
+  GFCOR,                                           // Coriolis parameter 2*Omega*sin(lat)
+  GCR0, GCR1, GCR2, GCR3,                          // cell (V2,V3) -> (U,V)
+  GCQ0, GCQ1, GCQ2, GCQ3,                          // cell (U,V) -> (V2,V3)
+  NGEO2D
+};
+
+// One ghost-band cell of a receiving panel (independent of i and n).  Its
+// value is interpolated along the shared edge from two interior cells of
+// the neighbour panel: (A*v0 + B*v1)/C, and momenta are rotated through
+// latitude-longitude (cubed_sphere_utility.cpp:92-369).
+struct GhostEntry {
+  int src_panel;
+  int k0, j0, k1, j1;        // the two source cells
+  int pad;
+  double A, B, C;
+  double ss, cs;             // source-point metric (raise to contravariant)
+  double r[4];               // (V2,V3) -> (U,V) at the source point
+  double q[4];               // (U,V) -> (V2,V3) at the target point
+  double ct;                 // target-point metric (lower to covariant)
+};
+
+// One edge face of a receiving panel: the outer face state comes from the
+// neighbour's interior-side reconstruction at its own edge face, rotated into
+// this panel's basis (cubed_sphere.cpp:326-688).
+struct EdgeEntry {
+  int src_panel;
+  int src_side;
+  int src_along;
+  int pad;
+  double r[4];               // (V2,V3) -> (U,V) at the sender's edge point
+  double q[4];               // (U,V) -> (V2,V3) in the receiver's basis
+};
+
+// Everything the host computes once per context.
+struct HostTables {
+  int N, L, nc1, nc2, nc3;
+  std::vector<double> x1f, x1v, dx1f;             // nc1+1, nc1, nc1
+  std::vector<double> x2f[6], x2v[6], x3f[6], x3v[6];
+  std::vector<double> geo;                        // [NGEO2D][6][nc3][nc2]
+  std::vector<int> ghost_map;                     // [6][nc3][nc2] -> entry or -1
+  std::vector<GhostEntry> ghost;
+  std::vector<EdgeEntry> edge;                    // [6][4][N]
+  size_t g2(int f, int p, int k, int j) const {
+    return (((size_t)f * 6 + p) * nc3 + k) * nc2 + j;
+  }
+};
+
+// geometry.cpp
+bool build_tables(const exo_config& cfg, HostTables& t, std::string* err);
+
+// Device-side scalars of one atmosphere (time step bookkeeping and flags).
+struct DevScalars {
+  double dt;                       // step in use
+  double time;                     // simulated time
+  unsigned long long dtmin_bits;   // running min of the CFL candidate (bits of a positive double)
+  int invalid;                     // sticky: rho/p negative or NaN
+  int pad;
+  long long ncycle;
+};
+
+// Sizes, parameters and device pointers of one atmosphere; passed by value
+// to every kernel.
+struct DevView {
+  int N, L, nv, nc1, nc2, nc3;
+  int is, ie, js, je, ks, ke;
+  int eqn, rsolver, implicit_flag, coriolis;
+  int precision;
+  double gamma, Rd, grav, cfl;
+  size_t cells;                    // nc3*nc2*nc1 (one variable of one panel)
+  // state
+  double* u;
+  double* w;
+  double* u1;
+  double* du;
+  double* flux[3];                 // face fluxes, same layout as u
+  double* scratch;                 // implicit solver: per column L*(25+5) doubles
+  // tables
+  const double* x1f;
+  const double* x1v;
+  const double* dx1f;
+  const double* geo;               // [NGEO2D][6][nc3][nc2]
+  const int* ghost_map;            // [6][nc3][nc2]
+  const GhostEntry* ghost;
+  const EdgeEntry* edge;           // [6][4][N]
+  DevScalars* sc;
+};
+
+// kernels.cu
+int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream);
+int launch_flux_x1(const DevView& v, void* stream);
+int launch_flux_x23(const DevView& v, void* stream);
+int launch_update(const DevView& v, int stage, void* stream);
+int launch_implicit(const DevView& v, int stage, void* stream);
+int launch_dt_reset(const DevView& v, void* stream);
+int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream);
+int launch_set_dt(const DevView& v, double dt, void* stream);
+int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);
+int launch_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
+                        const double* wl, const double* wr, double* flx,
+                        const double* cosf, const double* sinf, const double* cthp,
+                        const double* cthc, void* stream);
+int launch_weno5(int n, const double* a, const double* b, const double* c,
+                 const double* d, const double* e, double* out, void* stream);
+
+// cell (U,V) <-> panel vector transforms of cubed_sphere_transform.cpp:11-61
+// written as coefficient quadruples: out0 = c0*in0 + c1*in1, out1 = c2*in0 + c3*in1
+void rll_from_abp_coef(double X, double Y, int blockID, double c[4]);
+void abp_from_rll_coef(double X, double Y, int blockID, double c[4]);
+void rll_from_xyp(double dX, double dY, int nP, double& lon, double& lat);
+
+}  // namespace exo
+
+#endif  // EXO_INTERNAL_H_

@@ -1,0 +1,123 @@
+"""Seeded synthetic initial states for the benchmark configurations.
+
+The reference has no published benchmark inputs for this path; these stand
+in for its problem generators (examples/2023-Chen-exo3/W92.cpp:72-113 for
+the shallow-water sphere, hs94.cpp:251-291 for the dry atmosphere) with the
+shapes, sizes and value distributions of the configurations:
+
+  shallow_water   exo2, 6 x N x N x 3 layers: geopotential 2.94e4 m^2/s^2
+                  plus a random real spherical-harmonic field of degree <= 8
+                  with RMS 1 % of the base; solid-body rotation of 20-40 m/s
+                  about a random axis.
+  dry_atmosphere  exo3, 6 x N x N x L: isothermal 250 K hydrostatic column,
+                  1e5 Pa at the surface, 1e3 Pa at the top; per-cell
+                  temperature noise sigma 1 K at fixed pressure; horizontal
+                  winds sigma 5 m/s per lat-lon component.
+
+Every generator takes a numpy PCG64 seed and returns the primitive array
+(6, nvar, N+6, N+6, L+6) with the interior filled (ghosts are zero).
+"""
+import math
+
+import numpy as np
+from scipy.special import lpmv
+
+from . import _native as nat
+from .atmosphere import cell_geometry, make_config
+
+G = nat.NGHOST
+
+
+def shallow_water_config(N=48, **kw):
+    cfg = dict(N=N, L=3, eqn=nat.EXO_EQN_SHALLOW_YZ, rsolver=nat.EXO_RS_ROE_SHALLOW,
+               implicit_flag=0, coriolis=nat.EXO_CORIOLIS_W92, x1min=6371000.,
+               x1max=6371001., gamma=1.4, Rd=287., grav=0., cfl=0.4, omega=7.292e-5)
+    cfg.update(kw)
+    return cfg
+
+
+def dry_atmosphere_config(N=96, L=64, rsolver=nat.EXO_RS_LMARS, T0=250., g=9.81,
+                          Rd=287., gamma=1.4, ps=1e5, ptop=1e3, **kw):
+    ztop = Rd * T0 / g * math.log(ps / ptop)
+    cfg = dict(N=N, L=L, eqn=nat.EXO_EQN_IDEAL, rsolver=rsolver, implicit_flag=9,
+               coriolis=nat.EXO_CORIOLIS_NONE, x1min=6.371e6, x1max=6.371e6 + ztop,
+               gamma=gamma, Rd=Rd, grav=-g, cfl=0.4, omega=0.)
+    cfg.update(kw)
+    return cfg
+
+
+def _real_sph_harm_field(lat, lon, lmax, rng):
+    """sum_{l<=lmax, m} a_lm Y_lm(lat, lon) with a_lm ~ N(0, 1), real basis."""
+    x = np.sin(lat)
+    out = np.zeros_like(lat)
+    for l in range(lmax + 1):
+        for m in range(0, l + 1):
+            norm = math.sqrt((2 * l + 1) / (4 * math.pi) *
+                             math.factorial(l - m) / math.factorial(l + m))
+            P = lpmv(m, l, x) * norm
+            if m == 0:
+                out += rng.standard_normal() * P
+            else:
+                out += rng.standard_normal() * math.sqrt(2) * P * np.cos(m * lon)
+                out += rng.standard_normal() * math.sqrt(2) * P * np.sin(m * lon)
+    return out
+
+
+def _solid_body_uv(lat, lon, u0, axis):
+    """East/north components of u0 * (axis x r_hat)."""
+    cl, sl = np.cos(lat), np.sin(lat)
+    co, so = np.cos(lon), np.sin(lon)
+    r = np.stack([cl * co, cl * so, sl])
+    v = u0 * np.cross(axis, r, axis=0)
+    east = np.stack([-so, co, np.zeros_like(lon)])
+    north = np.stack([-sl * co, -sl * so, cl])
+    return (v * east).sum(0), (v * north).sum(0)
+
+
+def shallow_water_state(cfg, seed=0):
+    cfg = make_config(**cfg) if isinstance(cfg, dict) else cfg
+    N, L = cfg.N, cfg.L
+    lat, lon, m, _ = cell_geometry(cfg)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    base = 2.94e4
+    d = _real_sph_harm_field(lat, lon, 8, rng)
+    d *= 0.01 * base / math.sqrt(np.mean(d * d))
+    u0 = rng.uniform(20., 40.)
+    axis = rng.standard_normal(3)
+    axis /= np.linalg.norm(axis)
+    U, V = _solid_body_uv(lat, lon, u0, axis)
+    v2 = m[..., 0] * U + m[..., 1] * V
+    v3 = m[..., 2] * U + m[..., 3] * V
+    w = np.zeros((6, 4, N + 2 * G, N + 2 * G, L + 2 * G))
+    sl = (slice(G, G + N), slice(G, G + N), slice(G, G + L))
+    w[:, 0][(slice(None),) + sl] = (base + d)[..., None]
+    w[:, 2][(slice(None),) + sl] = v2[..., None]
+    w[:, 3][(slice(None),) + sl] = v3[..., None]
+    return w
+
+
+def dry_atmosphere_state(cfg, seed=0, T0=250., ps=1e5, temp_sigma=1.0, wind_sigma=5.0):
+    cfg = make_config(**cfg) if isinstance(cfg, dict) else cfg
+    N, L = cfg.N, cfg.L
+    Rd, g = cfg.Rd, -cfg.grav
+    lat, lon, m, x1v = cell_geometry(cfg)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    z = x1v - cfg.x1min
+    p = ps * np.exp(-g * z / (Rd * T0))
+    T = T0 + temp_sigma * rng.standard_normal((6, N, N, L))
+    U = wind_sigma * rng.standard_normal((6, N, N, L))
+    V = wind_sigma * rng.standard_normal((6, N, N, L))
+    v2 = m[..., 0, None] * U + m[..., 1, None] * V
+    v3 = m[..., 2, None] * U + m[..., 3, None] * V
+    w = np.zeros((6, 5, N + 2 * G, N + 2 * G, L + 2 * G))
+    sl = (slice(None), slice(G, G + N), slice(G, G + N), slice(G, G + L))
+    w[:, 4][sl] = p[None, None, None, :]
+    w[:, 0][sl] = p[None, None, None, :] / (Rd * T)
+    w[:, 2][sl] = v2
+    w[:, 3][sl] = v3
+    return w
+
+
+def interior(a):
+    """View of the interior cells of a (6, nvar, nc3, nc2, nc1) array."""
+    return a[:, :, G:-G, G:-G, G:-G]

@@ -1,0 +1,219 @@
+/*
+ * exo_b200.h -- C ABI of the B200-native finite-volume step on the cubed sphere.
+ *
+ * This library re-implements, for NVIDIA B200 (sm_100a), the hot path of
+ * ExoCubed's cubed-sphere dynamical core: Hydro::CalculateFluxes with WENO5
+ * sweeps, the RiemannSolver hooks (Roe shallow water, LMARS, HLLC), the exo3
+ * panel ghost-zone interpolation and panel-edge face-state exchange, the snap
+ * hydrostatic pressure decomposition, the ImplicitSolver vertical correction
+ * and the SSPRK(3,3) stage update.  All six panels of one atmosphere live on
+ * one GPU.  Everything crosses this boundary as plain pointers and sizes.
+ *
+ * Array layout (host and device): one AthenaArray<Real>(n,k,j,i) per panel,
+ * i (x1, radial) fastest, six panels back to back:
+ *     a[((((p*nvar + n)*nc3 + k)*nc2 + j)*nc1 + i]
+ * with nc1 = L + 2*EXO_NGHOST, nc2 = nc3 = N + 2*EXO_NGHOST, p = panel id - 1
+ * (panel ids follow CubedSphere::FindBlockID, src/exo3/cs_find_block_id.cpp:11).
+ *
+ * Error convention: every entry point returns an int status, 0 on success;
+ * no C++ exception crosses the boundary.  exo_last_error() gives the text of
+ * the most recent failure on the calling thread.  A context is single-stream
+ * and not thread safe: use one context per host thread.
+ */
+#ifndef EXO_B200_H_
+#define EXO_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXO_NGHOST 3
+#define EXO_NPANEL 6
+
+/* status codes */
+enum {
+  EXO_OK = 0,
+  EXO_ERR_ARG = 1,        /* bad argument or configuration */
+  EXO_ERR_SHAPE = 2,      /* array shape does not match the context */
+  EXO_ERR_CUDA = 3,       /* CUDA runtime error (text in exo_last_error) */
+  EXO_ERR_NONFINITE = 4,  /* state became invalid: rho<0, p<0 or NaN */
+  EXO_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+  EXO_ERR_NOGPU = 6,      /* no CUDA device is usable */
+  EXO_ERR_CAPACITY = 7    /* a request does not fit the slots or memory */
+};
+
+/* equation sets: the reference's EOS choice (src/snap/CMakeLists.txt:23) */
+enum { EXO_EQN_SHALLOW_YZ = 0, EXO_EQN_IDEAL = 1 };
+
+/* Riemann solvers: the reference's RSOLVER choice (src/snap/CMakeLists.txt:26) */
+enum {
+  EXO_RS_ROE_SHALLOW = 0,   /* src/snap/riemann/roe_shallow_yz.cpp   */
+  EXO_RS_LMARS = 1,         /* src/snap/riemann/lmars.cpp            */
+  EXO_RS_HLLC = 2,          /* src/snap/riemann/hllc_transform.cpp   */
+  EXO_RS_LMARS_SHALLOW = 3  /* src/snap/riemann/lmars_shallow_yz.cpp */
+};
+
+/* arithmetic of the flux path */
+enum {
+  EXO_PREC_FP64 = 0,  /* everything in FP64 */
+  EXO_PREC_MIXED = 1  /* FP32 reconstruction, Riemann flux and flux divergence;
+                         FP64 decomposition, implicit solve and RK accumulation */
+};
+
+/* source terms */
+enum { EXO_CORIOLIS_NONE = 0, EXO_CORIOLIS_W92 = 1 };
+
+typedef struct exo_config {
+  int N;              /* cells along a panel edge (meshblock nx2 = nx3)          */
+  int L;              /* radial levels (nx1)                                      */
+  int eqn;            /* EXO_EQN_*                                                */
+  int rsolver;        /* EXO_RS_*                                                 */
+  int implicit_flag;  /* <hydro> implicit_flag bits: 1 = x1, 8 = full 5x5 solve  */
+  int precision;      /* EXO_PREC_*                                               */
+  int coriolis;       /* EXO_CORIOLIS_*                                           */
+  int reserved0;
+  double x1min;       /* inner radius [m]                                         */
+  double x1max;       /* outer radius [m]                                         */
+  double gamma;       /* <hydro> gamma                                            */
+  double Rd;          /* <thermodynamics> Rd [J/kg/K]                             */
+  double grav;        /* <hydro> grav_acc1 (negative points down) [m/s^2]         */
+  double cfl;         /* <time> cfl_number                                        */
+  double omega;       /* planetary rotation rate for the Coriolis source [1/s]    */
+  double reserved1;
+} exo_config;
+
+typedef struct exo_ctx exo_ctx;
+
+/* -------------------------------------------------------------- lifecycle */
+
+/* Fill *cfg with the defaults of an equation set (C1 for shallow water, C2
+   for the ideal gas).  Replaces the <mesh>/<hydro>/<time> blocks of an
+   Athena++ input file (examples/2023-Chen-exo3/W92.inp, hs94.inp). */
+int exo_config_default(exo_config* cfg, int eqn);
+
+/* Create a context on the current CUDA device: geometry tables, panel
+   interpolation tables and device state are allocated here, never later.
+   Replaces Mesh/MeshBlock construction (src/mesh_setup.cpp:66) and the
+   GnomonicEquiangle constructor (src/exo3/gnomonic_equiangle.cpp:24). */
+int exo_create(const exo_config* cfg, exo_ctx** out);
+void exo_destroy(exo_ctx* ctx);
+
+/* Cell-centre geometry of a configuration, computed on the host (no GPU
+   needed): lat, lon [6][N][N] in radians (CubedSphere::GetLatLon,
+   src/exo3/cubed_sphere.cpp:78-91); uv_to_v23 [6][N][N][4] the map of a
+   latitude-longitude vector (U east, V north) to the panel's contravariant
+   components, V2 = c0*U + c1*V, V3 = c2*U + c3*V (CubedSphere::GetVyVz,
+   cubed_sphere.cpp:149-162); x1v [L] the radial cell centres.  Any output
+   pointer may be NULL. */
+int exo_cell_geometry(const exo_config* cfg, double* lat, double* lon,
+                      double* uv_to_v23, double* x1v);
+
+/* Face coordinates of one panel (host, no GPU): x1f [L+7], x2f [N+7],
+   x3f [N+7] in the reference's units (x1 radius in m; x2, x3 equiangular
+   angles in rad) -- patches/27.coordinates.patch:21,40. */
+int exo_mesh(const exo_config* cfg, int panel, double* x1f, double* x2f, double* x3f);
+
+/* Number of variables and cell counts of one panel array. */
+int exo_shape(const exo_ctx* ctx, int* nvar, int* nc3, int* nc2, int* nc1);
+
+/* Text of the last error on this thread ("" if none). */
+const char* exo_last_error(void);
+
+/* ---------------------------------------------------------- state access */
+
+/* Load an initial state given as primitive variables (interior cells are
+   read, ghosts ignored) from host memory.  Runs what Mesh::Initialize does
+   after ProblemGenerator: PrimitiveToConserved on the interior, the panel
+   ghost exchange, ConservedToPrimitive, the physical x1 boundary and the
+   first time step (patches/29.mesh.patch:19-86). */
+int exo_set_primitive(exo_ctx* ctx, const double* w_host);
+
+/* Copy the full conserved / primitive arrays (ghosts included) to host. */
+int exo_get_conserved(exo_ctx* ctx, double* u_host);
+int exo_get_primitive(exo_ctx* ctx, double* w_host);
+
+/* Device pointers of the resident state (valid until exo_destroy). */
+int exo_device_state(exo_ctx* ctx, double** u_dev, double** w_dev);
+
+/* --------------------------------------------------------------- stepping */
+
+/* Advance nsteps SSPRK(3,3) steps.  dt_fixed <= 0 selects the CFL time step
+   of Hydro::NewBlockTimeStep (patches/21.new_blockdt.patch:23-35), recomputed
+   on the device after every step; dt_fixed > 0 uses that step throughout.
+   Replaces the main loop's DoTaskListOneStage calls (main.cpp.in:139-141). */
+int exo_step(exo_ctx* ctx, int nsteps, double dt_fixed);
+
+/* Current time step, simulated time and step count. */
+int exo_get_dt(exo_ctx* ctx, double* dt);
+int exo_get_time(exo_ctx* ctx, double* time, int64_t* ncycle);
+
+/* Sticky device-side validity flag (MeshBlock::Impl::SetStateInvalid,
+   src/snap/eos/ideal_moist_hydro.cpp:108,150): 1 if a density or pressure
+   went negative or NaN since the last call; the flag is cleared. */
+int exo_check_state(exo_ctx* ctx, int* invalid);
+
+/* Block until the context's stream is idle. */
+int exo_synchronize(exo_ctx* ctx);
+
+/* The cudaStream_t every launch of this context goes to. */
+int exo_get_stream(exo_ctx* ctx, void** stream);
+
+/* ------------------------------------------------------------- profiling */
+
+/* kernels of one stage, for exo_profile_read */
+enum {
+  EXO_K_FLUX_X1 = 0,    /* decomposition + WENO5 + Riemann, x1 (per column)  */
+  EXO_K_FLUX_X23 = 1,   /* WENO5 + edge exchange + Riemann, x2/x3 (per face)  */
+  EXO_K_UPDATE = 2,     /* RK average + divergence + sources (per cell)       */
+  EXO_K_IMPLICIT = 3,   /* 5x5 block-tridiagonal vertical solve (per column)  */
+  EXO_K_PRIM_GHOST = 4, /* ghost bands + ConservedToPrimitive + CFL (per cell) */
+  EXO_K_OTHER = 5,      /* time-step bookkeeping                              */
+  EXO_K_COUNT = 6
+};
+
+/* enable != 0 brackets every launch with CUDA events on the context's
+   stream and clears the counters; 0 stops recording.  exo_profile_read
+   synchronizes and returns the launches and the summed device time (ms) of
+   one kernel since profiling was enabled. */
+int exo_profile(exo_ctx* ctx, int enable);
+int exo_profile_read(exo_ctx* ctx, int kernel, int64_t* launches, double* total_ms);
+
+/* Kernel launches issued by this context since it was created. */
+int exo_launch_count(exo_ctx* ctx, int64_t* launches);
+
+/* ------------------------------------------------------ operator hooks */
+
+/* Hydro::CalculateFluxes (patches/19.calculate_fluxes.patch:22-158) on the
+   current primitive state; the three flux arrays stay on the device and can
+   be copied out with exo_get_flux (dir = 0,1,2 for x1,x2,x3; layout as the
+   state arrays, face index in place of cell index). */
+int exo_calculate_fluxes(exo_ctx* ctx);
+int exo_get_flux(exo_ctx* ctx, int dir, double* flux_host);
+
+/* Hydro::RiemannSolver(k,j,il,iu,ivx,wl,wr,flx,dxw) over n faces stored as
+   device arrays wl[NHYDRO][n], wr[NHYDRO][n] -> flx[NHYDRO][n] (all FP64).
+   The face geometry enters as per-face arrays: cos_face/sin_face are the
+   face metric (Face2Metric/Face3Metric, gnomonic_equiangle.cpp:494-569),
+   cth_proj the covariant projection angle and cth_cell the cell-centred
+   metric used by HLLC in x1 (hllc_transform.cpp:95-110); pass NULL where the
+   solver does not use them.  Replaces src/snap/riemann/{roe_shallow_yz,
+   lmars,hllc_transform,lmars_shallow_yz}.cpp. */
+int exo_riemann(int rsolver, int eqn, int ivx, int n, double gamma,
+                const double* wl, const double* wr, double* flx,
+                const double* cos_face, const double* sin_face,
+                const double* cth_proj, const double* cth_cell,
+                void* stream);
+
+/* interp_weno5 on device: out[m] = weno5(a[m],b[m],c[m],d[m],e[m]), the
+   face value between the 2nd and 3rd argument (tests/test_weno.cpp:20-29). */
+int exo_weno5(int n, const double* a, const double* b, const double* c,
+              const double* d, const double* e, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EXO_B200_H_ */

@@ -1,0 +1,185 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker of the GPU path.  The oracle is a
+C++ restatement of ExoCubed's cubed-sphere step (see exo_oracle.cpp's header
+for the file:line of every piece it follows and the choices it makes where
+the reference's Athena++ fork is not available).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+NGHOST = 3
+
+
+class ExoConfig(ctypes.Structure):
+    """Mirror of exo_config in include/exo_b200.h."""
+    _fields_ = [
+        ("N", ctypes.c_int), ("L", ctypes.c_int), ("eqn", ctypes.c_int),
+        ("rsolver", ctypes.c_int), ("implicit_flag", ctypes.c_int),
+        ("precision", ctypes.c_int), ("coriolis", ctypes.c_int),
+        ("reserved0", ctypes.c_int),
+        ("x1min", ctypes.c_double), ("x1max", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("Rd", ctypes.c_double),
+        ("grav", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("omega", ctypes.c_double), ("reserved1", ctypes.c_double),
+    ]
+
+
+def build():
+    """Compile liboracle.so with its Makefile (gcc, no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        d, p, i = ctypes.c_double, ctypes.c_void_p, ctypes.c_int
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.ora_interp_weno5.restype = d
+        L.ora_interp_weno5.argtypes = [d] * 5
+        L.ora_interp_weno3.restype = d
+        L.ora_interp_weno3.argtypes = [d] * 3
+        L.ora_cov_to_contra.argtypes = [dp, d]
+        L.ora_contra_to_cov.argtypes = [dp, d]
+        L.ora_create.restype = p
+        L.ora_create.argtypes = [ctypes.POINTER(ExoConfig)]
+        L.ora_destroy.argtypes = [p]
+        L.ora_set_primitive.argtypes = [p, dp]
+        L.ora_set_conserved.argtypes = [p, dp]
+        L.ora_get_conserved.argtypes = [p, dp]
+        L.ora_get_primitive.argtypes = [p, dp]
+        L.ora_get_flux.argtypes = [p, i, dp]
+        L.ora_get_dt.restype = d
+        L.ora_get_dt.argtypes = [p]
+        L.ora_get_time.restype = d
+        L.ora_get_time.argtypes = [p]
+        L.ora_get_invalid.restype = i
+        L.ora_get_invalid.argtypes = [p]
+        L.ora_calculate_fluxes.argtypes = [p]
+        L.ora_step.argtypes = [p, i, d]
+        L.ora_get_mesh.argtypes = [p, i, dp, dp, dp]
+        L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def to_struct(cfg):
+    """dict (or ExoConfig) -> ExoConfig."""
+    if isinstance(cfg, ExoConfig):
+        return cfg
+    s = ExoConfig()
+    for k, v in cfg.items():
+        setattr(s, k, v)
+    return s
+
+
+class Oracle:
+    """Six-panel cubed-sphere state advanced on the CPU."""
+
+    def __init__(self, cfg):
+        self.cfg = to_struct(cfg)
+        self._h = lib().ora_create(ctypes.byref(self.cfg))
+        if not self._h:
+            raise ValueError("oracle rejected the configuration")
+        c = self.cfg
+        self.nvar = 4 if c.eqn == 0 else 5
+        self.shape = (6, self.nvar, c.N + 2 * NGHOST, c.N + 2 * NGHOST, c.L + 2 * NGHOST)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ora_destroy(self._h)
+            self._h = None
+
+    def set_primitive(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        assert w.shape == self.shape
+        lib().ora_set_primitive(self._h, _ptr(w))
+
+    def set_conserved(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.shape == self.shape
+        lib().ora_set_conserved(self._h, _ptr(u))
+
+    def conserved(self):
+        a = np.empty(self.shape)
+        lib().ora_get_conserved(self._h, _ptr(a))
+        return a
+
+    def primitive(self):
+        a = np.empty(self.shape)
+        lib().ora_get_primitive(self._h, _ptr(a))
+        return a
+
+    def flux(self, d):
+        a = np.empty(self.shape)
+        lib().ora_get_flux(self._h, d, _ptr(a))
+        return a
+
+    def calculate_fluxes(self):
+        lib().ora_calculate_fluxes(self._h)
+
+    def step(self, nsteps, dt_fixed=0.0):
+        lib().ora_step(self._h, int(nsteps), float(dt_fixed))
+
+    @property
+    def dt(self):
+        return lib().ora_get_dt(self._h)
+
+    @property
+    def time(self):
+        return lib().ora_get_time(self._h)
+
+    def invalid(self):
+        return lib().ora_get_invalid(self._h)
+
+    def mesh(self, panel):
+        c = self.cfg
+        x1f = np.empty(c.L + 2 * NGHOST + 1)
+        x2f = np.empty(c.N + 2 * NGHOST + 1)
+        x3f = np.empty(c.N + 2 * NGHOST + 1)
+        lib().ora_get_mesh(self._h, panel, _ptr(x1f), _ptr(x2f), _ptr(x3f))
+        return x1f, x2f, x3f
+
+
+def interp_weno5(a, b, c, d, e):
+    return lib().ora_interp_weno5(a, b, c, d, e)
+
+
+def interp_weno3(a, b, c):
+    return lib().ora_interp_weno3(a, b, c)
+
+
+def cov_to_contra(w, cth):
+    w = np.ascontiguousarray(w, dtype=np.float64).copy()
+    lib().ora_cov_to_contra(_ptr(w), cth)
+    return w
+
+
+def contra_to_cov(w, cth):
+    w = np.ascontiguousarray(w, dtype=np.float64).copy()
+    lib().ora_contra_to_cov(_ptr(w), cth)
+    return w
+
+
+def riemann_face(rsolver, eqn, ivx, gamma, wl, wr, cosf=0.0, sinf=1.0, cthp=0.0, cthc=0.0):
+    wl = np.ascontiguousarray(wl, dtype=np.float64).copy()
+    wr = np.ascontiguousarray(wr, dtype=np.float64).copy()
+    f = np.zeros(5)
+    lib().ora_riemann_face(rsolver, eqn, ivx, gamma, _ptr(wl), _ptr(wr), _ptr(f),
+                           cosf, sinf, cthp, cthc)
+    return f
