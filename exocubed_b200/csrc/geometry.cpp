@@ -400,6 +400,33 @@ bool build_tables(const exo_config& cfg, HostTables& t, std::string* err) {
   build_metric(cfg, t);
   build_ghost_table(t);
   build_edge_table(t);
+  // every ghost-band cell is mapped once and every source cell is interior
+  // (the kernels index with these values unchecked)
+  int lo = G, hi = G + cfg.N - 1;
+  for (int p = 0; p < 6; ++p)
+    for (int k = 0; k < t.nc3; ++k)
+      for (int j = 0; j < t.nc2; ++j) {
+        bool kin = k >= lo && k <= hi, jin = j >= lo && j <= hi;
+        int e = t.ghost_map[((size_t)p * t.nc3 + k) * t.nc2 + j];
+        bool band = kin != jin;
+        if (band != (e >= 0) || e >= (int)t.ghost.size()) {
+          if (err) *err = "internal: ghost table does not cover the ghost bands";
+          return false;
+        }
+        if (e < 0) continue;
+        const GhostEntry& g = t.ghost[e];
+        if (g.src_panel < 0 || g.src_panel > 5 || g.k0 < lo || g.k0 > hi || g.k1 < lo ||
+            g.k1 > hi || g.j0 < lo || g.j0 > hi || g.j1 < lo || g.j1 > hi || !(g.C != 0.)) {
+          if (err) *err = "internal: ghost source cell outside the neighbour's interior";
+          return false;
+        }
+      }
+  for (const EdgeEntry& e : t.edge)
+    if (e.src_panel < 0 || e.src_panel > 5 || e.src_side < 0 || e.src_side > 3 ||
+        e.src_along < 0 || e.src_along >= cfg.N) {
+      if (err) *err = "internal: edge table entry out of range";
+      return false;
+    }
   return true;
 }
 
