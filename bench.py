@@ -40,6 +40,9 @@ def workload_config(name):
     if name == "c2":
         return (W.dry_atmosphere_config(N=96, L=64, rsolver=1),
                 "exo3 dry ideal gas 6x96x96x64 FP64 WENO5+LMARS+implicit(9), SSPRK3, CFL 0.4")
+    if name == "c2s":  # profiling size: 6x64x64x64, state arrays 63 MB each
+        return (W.dry_atmosphere_config(N=64, L=64, rsolver=1),
+                "exo3 dry ideal gas 6x64x64x64 FP64 WENO5+LMARS+implicit(9), SSPRK3, CFL 0.4")
     if name == "c1":
         return (W.shallow_water_config(N=48),
                 "exo2 shallow water 6x48x48x3 FP64 WENO5+Roe, SSPRK3, CFL 0.4")
@@ -330,7 +333,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")

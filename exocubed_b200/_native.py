@@ -26,6 +26,7 @@ EXPORTED = [
     "exo_get_time", "exo_check_state", "exo_synchronize",
     "exo_calculate_fluxes", "exo_get_flux", "exo_riemann", "exo_weno5",
     "exo_get_stream", "exo_profile", "exo_profile_read", "exo_launch_count",
+    "exo_implicit_columns",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
 
@@ -94,6 +95,7 @@ def lib():
     L.exo_get_flux.argtypes = [p, i, dp]
     L.exo_riemann.argtypes = [i, i, i, i, d, p, p, p, p, p, p, p, p]
     L.exo_weno5.argtypes = [i, p, p, p, p, p, p, p]
+    L.exo_implicit_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
     L.exo_get_stream.argtypes = [p, ctypes.POINTER(p)]
     L.exo_profile.argtypes = [p, i]
     L.exo_profile_read.argtypes = [p, i, ctypes.POINTER(ctypes.c_int64), dp]

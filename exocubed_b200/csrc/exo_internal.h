@@ -115,6 +115,9 @@ int launch_flux_x23(const DevView& v, void* stream);
 int launch_update(const DevView& v, int stage, void* stream);
 int launch_implicit(const DevView& v, int stage, void* stream);
 int launch_dt_reset(const DevView& v, void* stream);
+int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
+                            const double* x1f, const double* x1v, const double* dx1f, double dt,
+                            double gamma, double grav, double* scratch, void* stream);
 int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream);
 int launch_set_dt(const DevView& v, double dt, void* stream);
 int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);

@@ -862,44 +862,36 @@ __device__ M5 flux_jacobian(double gm1, const double* w) {
   return J;
 }
 
-// Primitive column entry i with the velocity projected on the local
-// orthogonal frame (solve_implicit_3d.cpp:115-128)
-__device__ __forceinline__ void load_wcol(const DevView& v, int p, int k, int j, int i,
-                                          double cth, double sth, double* out) {
-  for (int n = 0; n < 5; ++n) out[n] = v.w[idx(v, p, n, k, j, i)];
-  out[IVY] += out[IVZ] * cth;
-  out[IVZ] *= sth;
-}
-
-// The vertical 5x5 block-tridiagonal correction of one column
-// (ImplicitSolver::SolveImplicit3D X1 branch + FullCorrection), then
-// u += du and, on the last stage, the AirParcel round trip.
-// scratch: per column L entries of (A*c) [25] and delta [5], interleaved
-// over columns so neighbouring threads touch neighbouring words.
-__global__ void k_implicit(DevView v, int stage, double* scratch) {
-  int ncol = 6 * v.N * v.N;
-  int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncol) return;
-  int j = v.js + col % v.N;
-  int k = v.ks + (col / v.N) % v.N;
-  int p = col / (v.N * v.N);
-  const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
-  double dt = kBeta[stage] * v.sc->dt;
-  double gamma = v.gamma, grav = v.grav;
-  int is = v.is, ie = v.ie;
-  double cos_theta = geo(v, GCOSC, p, k, j), sin_theta = geo(v, GSINC, p, k, j);
-  double s = sin_theta, d2 = geo(v, GDX2A, p, k, j), d3 = geo(v, GDX3A, p, k, j);
-  auto SCR = [&](int lev, int e) -> double& {
-    return scratch[((size_t)lev * 30 + e) * ncol + col];
+// The vertical 5x5 block-tridiagonal correction of one radial column
+// (ImplicitSolver::SolveImplicit3D X1 branch, solve_implicit_3d.cpp:102-179,
+// with FullCorrection, full_correction.cpp:32-165, and ForwardSweep /
+// BackwardSubstitution, forward_backward.hpp:15-126).
+//   W(i, w5)      loads the primitive state of level i (i in [is-2, ie+1])
+//   DU(i, n)      the explicit update of level i, variable n (read)
+//   SCR(lev, e)   30 scratch doubles per level: the forward-sweep products
+//                 A_i*c_i (25) and delta_i (5), read back by the back substitution
+//   OUT(i, dl)    receives the corrected update of level i (ie down to is)
+// geo: cos/sin of the cell metric and the angular widths dx2f_ang, dx3f_ang.
+template <class WF, class DUF, class SCRF, class OUTF>
+__device__ __forceinline__ void implicit_column(WF W, DUF DU, SCRF SCR, OUTF OUT, double cos_theta,
+                                                double sin_theta, double d2, double d3,
+                                                const double* x1f, const double* x1v,
+                                                const double* dx1f, int is, int ie, double dt,
+                                                double gamma, double grav) {
+  double s = sin_theta;
+  auto load = [&](int i, double* out) {
+    W(i, out);
+    out[IVY] += out[IVZ] * cos_theta;
+    out[IVZ] *= sin_theta;
   };
   double fsig = 1., feps = 1.;
-  double gmm1 = (gamma - 1.) * feps / fsig;  // same for every level (NVAPOR = 0)
+  double gmm1 = (gamma - 1.) * feps / fsig;  // the same for every level (NVAPOR = 0)
   double wl[5], wr[5], prim[5];
   double gm1 = 0.5 * (gmm1 + gmm1);
   double cs;
   // window at i = is: Am on the face between is-1 and is, dfdq[is-1], dfdq[is]
-  load_wcol(v, p, k, j, is - 1, cos_theta, sin_theta, wl);
-  load_wcol(v, p, k, j, is, cos_theta, sin_theta, wr);
+  load(is - 1, wl);
+  load(is, wr);
   M5 dfm = flux_jacobian(gmm1, wl);
   M5 df0 = flux_jacobian(gmm1, wr);
   roe_average(prim, gm1, wl, wr);
@@ -908,15 +900,15 @@ __global__ void k_implicit(DevView v, int stage, double* scratch) {
   M5 Aprev;
   V5 dprev;
   for (int i = is; i <= ie; ++i) {
-    load_wcol(v, p, k, j, i, cos_theta, sin_theta, wl);
-    load_wcol(v, p, k, j, i + 1, cos_theta, sin_theta, wr);
+    load(i, wl);
+    load(i + 1, wr);
     M5 dfp = flux_jacobian(gmm1, wr);
     roe_average(prim, gm1, wl, wr);
     cs = sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
     M5 Ap = abs_jacobian(prim, cs, gm1);
-    double aleft = d2 * d3 * v.x1f[i] * v.x1f[i] * s;
-    double aright = d2 * d3 * v.x1f[i + 1] * v.x1f[i + 1] * s;
-    double vol = v.dx1f[i] * d2 * d3 * v.x1v[i] * v.x1v[i] * s;
+    double aleft = d2 * d3 * x1f[i] * x1f[i] * s;
+    double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
+    double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
     M5 a, b, c;
 #pragma unroll
     for (int r = 0; r < 5; ++r)
@@ -950,12 +942,12 @@ __global__ void k_implicit(DevView v, int stage, double* scratch) {
         for (int q = 0; q < 5; ++q) a.a[r][q] += t.a[r][q];
     }
     V5 rhs;
-    rhs.a[0] = v.du[idx(v, p, IDN, k, j, i)];
+    rhs.a[0] = DU(i, IDN);
     rhs.a[0] /= dt;
-    rhs.a[1] = v.du[idx(v, p, IVX, k, j, i)] / dt;
-    rhs.a[2] = v.du[idx(v, p, IVY, k, j, i)] / dt;
-    rhs.a[3] = v.du[idx(v, p, IVZ, k, j, i)] / dt;
-    rhs.a[4] = v.du[idx(v, p, IEN, k, j, i)] / dt;
+    rhs.a[1] = DU(i, IVX) / dt;
+    rhs.a[2] = DU(i, IVY) / dt;
+    rhs.a[3] = DU(i, IVZ) / dt;
+    rhs.a[4] = DU(i, IEN) / dt;
     M5 A;
     V5 dl;
     if (i == is) {
@@ -983,17 +975,10 @@ __global__ void k_implicit(DevView v, int stage, double* scratch) {
       for (int q = 0; q < 5; ++q) SCR(lev, r * 5 + q) = Aprev.a[r][q];
 #pragma unroll
     for (int r = 0; r < 5; ++r) SCR(lev, 25 + r) = dl.a[r];
-    // shift the window
     Am = Ap;
     dfm = df0;
     df0 = dfp;
   }
-  // BackwardSubstitution, then u += du and the last-stage round trip
-  const double Rgas = 8.314462;  // src/constants.hpp:5
-  double Rd = v.Rd, gammad = v.gamma;
-  double mu0 = Rgas / Rd;
-  double inv_mu0 = 1. / (mu0 * 1.);
-  double cv0 = 1. * (Rd / (gammad - 1.));
   V5 dnext;
   for (int i = ie; i >= is; --i) {
     int lev = i - is;
@@ -1011,71 +996,21 @@ __global__ void k_implicit(DevView v, int stage, double* scratch) {
       for (int r = 0; r < 5; ++r) dl.a[r] -= ad.a[r];
     }
     dnext = dl;
-    double uu[5];
-#pragma unroll
-    for (int n = 0; n < 5; ++n) {
-      size_t q = idx(v, p, n, k, j, i);
-      uu[n] = v.u[q] + 1. * dl.a[n];
-    }
-    if (stage == 2) {
-      // GatherFromConserved -> MoleFrac -> MassConc -> DistributeToConserved
-      double w[5];
-#pragma unroll
-      for (int n = 0; n < 5; ++n) w[n] = uu[n];
-      double rho = 0., cvt = 0.;
-      rho += w[0];
-      cvt += w[0] * cv0;
-      double KE = 0.5 / rho * (sqr(w[IVX]) + sqr(w[IVY]) + sqr(w[IVZ]));
-      double tem = (w[IEN] - KE) / cvt;
-      w[IEN] = cvt * tem;
-      {
-        double r2 = 0., cv = 0., rhoR = 0.;
-        r2 += w[0];
-        cv += w[0] * cv0;
-        rhoR += w[0] * Rgas * inv_mu0;
-        double di = 1. / r2;
-        w[IDN] = w[IEN] / cv;
-        w[IPR] = rhoR * w[IDN];
-        w[IVX] *= di; w[IVY] *= di; w[IVZ] *= di;
-      }
-      {
-        double tt = w[IDN], sum = 1., gg = 1.;
-        double r2 = w[IPR] * sum / (Rd * tt * gg);
-        w[IDN] = r2;
-        w[IEN] = 0.;
-        w[IEN] += w[IDN] * cv0 * tt;
-        w[IVX] *= r2; w[IVY] *= r2; w[IVZ] *= r2;
-      }
-#pragma unroll
-      for (int n = 0; n < 5; ++n) uu[n] = w[n];
-      double r2 = 0.;
-      r2 += w[0];
-      double vx = w[IVX] / r2, vy = w[IVY] / r2, vz = w[IVZ] / r2;
-      uu[IEN] += 0.5 * w[0] * (sqr(vx) + sqr(vy) + sqr(vz));
-    }
-#pragma unroll
-    for (int n = 0; n < 5; ++n) v.u[idx(v, p, n, k, j, i)] = uu[n];
+    OUT(i, dl.a);
   }
 }
 
-// last-stage round trip when the implicit solver is off
-__global__ void k_roundtrip(DevView v) {
-  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  size_t total = (size_t)6 * v.N * v.N * v.L;
-  if (tid >= total) return;
-  int i = v.is + (int)(tid % v.L);
-  size_t r = tid / v.L;
-  int j = v.js + (int)(r % v.N);
-  r /= v.N;
-  int k = v.ks + (int)(r % v.N);
-  int p = (int)(r / v.N);
-  const double Rgas = 8.314462;
-  double Rd = v.Rd, gammad = v.gamma;
+// UpdateAllConserved on the last stage with NVAPOR = NCLOUD = 0: the
+// AirParcel round trip MassConc -> MoleFrac -> MassConc of one cell
+// (impl.cpp:138-304, air_parcel.cpp:190-278)
+__device__ __forceinline__ void airparcel_round_trip(double* uu, double Rd, double gammad) {
+  const double Rgas = 8.314462;  // src/constants.hpp:5
   double mu0 = Rgas / Rd;
   double inv_mu0 = 1. / (mu0 * 1.);
   double cv0 = 1. * (Rd / (gammad - 1.));
   double w[5];
-  for (int n = 0; n < 5; ++n) w[n] = v.u[idx(v, p, n, k, j, i)];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) w[n] = uu[n];
   double rho = 0., cvt = 0.;
   rho += w[0];
   cvt += w[0] * cv0;
@@ -1104,8 +1039,83 @@ __global__ void k_roundtrip(DevView v) {
   r2 += w[0];
   double vx = w[IVX] / r2, vy = w[IVY] / r2, vz = w[IVZ] / r2;
   double e = w[IEN] + 0.5 * w[0] * (sqr(vx) + sqr(vy) + sqr(vz));
-  for (int n = 0; n < 4; ++n) v.u[idx(v, p, n, k, j, i)] = w[n];
-  v.u[idx(v, p, IEN, k, j, i)] = e;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) uu[n] = w[n];
+  uu[IEN] = e;
+}
+
+// One radial column of the stepping context: solve, then u += du and, on
+// the last stage, the AirParcel round trip.  scratch is interleaved over
+// columns so neighbouring threads touch neighbouring words.
+__global__ void k_implicit(DevView v, int stage, double* scratch) {
+  int ncol = 6 * v.N * v.N;
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  int j = v.js + col % v.N;
+  int k = v.ks + (col / v.N) % v.N;
+  int p = col / (v.N * v.N);
+  const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
+  double dt = kBeta[stage] * v.sc->dt;
+  auto W = [&](int i, double* out) {
+    for (int n = 0; n < 5; ++n) out[n] = v.w[idx(v, p, n, k, j, i)];
+  };
+  auto DU = [&](int i, int n) { return v.du[idx(v, p, n, k, j, i)]; };
+  auto SCR = [&](int lev, int e) -> double& { return scratch[((size_t)lev * 30 + e) * ncol + col]; };
+  auto OUT = [&](int i, const double* dl) {
+    double uu[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uu[n] = v.u[idx(v, p, n, k, j, i)] + 1. * dl[n];
+    if (stage == 2) airparcel_round_trip(uu, v.Rd, v.gamma);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) v.u[idx(v, p, n, k, j, i)] = uu[n];
+  };
+  implicit_column(W, DU, SCR, OUT, geo(v, GCOSC, p, k, j), geo(v, GSINC, p, k, j),
+                  geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), v.x1f, v.x1v, v.dx1f, v.is,
+                  v.ie, dt, v.gamma, v.grav);
+}
+
+// ImplicitSolver::FullCorrection over a batch of independent columns given
+// as plain arrays: w [ncol][5][L+6] primitives with ghosts, du [ncol][5][L]
+// explicit update (overwritten by the corrected one), colgeo [ncol][4] =
+// (cos, sin, dx2f_ang, dx3f_ang), scratch ncol*L*30 doubles.
+__global__ void k_implicit_columns(int ncol, int L, const double* w, double* du,
+                                   const double* colgeo, const double* x1f, const double* x1v,
+                                   const double* dx1f, double dt, double gamma, double grav,
+                                   double* scratch) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  int nc1 = L + 2 * G;
+  const double* wc = w + (size_t)col * 5 * nc1;
+  double* duc = du + (size_t)col * 5 * L;
+  auto W = [&](int i, double* out) {
+    for (int n = 0; n < 5; ++n) out[n] = wc[n * nc1 + i];
+  };
+  auto DU = [&](int i, int n) { return duc[n * L + (i - G)]; };
+  auto SCR = [&](int lev, int e) -> double& { return scratch[((size_t)lev * 30 + e) * ncol + col]; };
+  auto OUT = [&](int i, const double* dl) {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) duc[n * L + (i - G)] = dl[n];
+  };
+  const double* g4 = colgeo + (size_t)col * 4;
+  implicit_column(W, DU, SCR, OUT, g4[0], g4[1], g4[2], g4[3], x1f, x1v, dx1f, G, G + L - 1, dt,
+                  gamma, grav);
+}
+
+// last-stage round trip when the implicit solver is off
+__global__ void k_roundtrip(DevView v) {
+  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t total = (size_t)6 * v.N * v.N * v.L;
+  if (tid >= total) return;
+  int i = v.is + (int)(tid % v.L);
+  size_t r = tid / v.L;
+  int j = v.js + (int)(r % v.N);
+  r /= v.N;
+  int k = v.ks + (int)(r % v.N);
+  int p = (int)(r / v.N);
+  double uu[5];
+  for (int n = 0; n < 5; ++n) uu[n] = v.u[idx(v, p, n, k, j, i)];
+  airparcel_round_trip(uu, v.Rd, v.gamma);
+  for (int n = 0; n < 5; ++n) v.u[idx(v, p, n, k, j, i)] = uu[n];
 }
 
 __global__ void k_p2c(DevView v, const double* wsrc) {
@@ -1211,6 +1221,15 @@ int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   int ncol = 6 * v.N * v.N;
   k_implicit<<<nblk(ncol, 64), 64, 0, (cudaStream_t)stream>>>(v, stage, v.scratch);
+  return check_launch();
+}
+
+int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
+                            const double* x1f, const double* x1v, const double* dx1f, double dt,
+                            double gamma, double grav, double* scratch, void* stream) {
+  if (ncol <= 0) return 0;
+  k_implicit_columns<<<nblk(ncol, 64), 64, 0, (cudaStream_t)stream>>>(
+      ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
   return check_launch();
 }
 

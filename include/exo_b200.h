@@ -207,6 +207,21 @@ int exo_riemann(int rsolver, int eqn, int ivx, int n, double gamma,
                 const double* cth_proj, const double* cth_cell,
                 void* stream);
 
+/* ImplicitSolver::FullCorrection with SolveImplicit3D's velocity projection
+   (src/snap/implicit/solve_implicit_3d.cpp:102-179, full_correction.cpp:32-165,
+   forward_backward.hpp:15-126) over ncol independent radial columns, all
+   arrays on the device:
+     w       [ncol][5][L+6]  primitives incl. the 3+3 radial ghosts
+     du      [ncol][5][L]    explicit update in, corrected update out
+     colgeo  [ncol][4]       cos and sin of the cell metric, dx2f_ang, dx3f_ang
+     x1f [L+7], x1v [L+6], dx1f [L+6]  radial faces, centres and widths
+     scratch ncol*L*30 doubles of caller-owned device memory
+   Reflecting radial boundaries at both ends; dt is the stage's beta*dt. */
+int exo_implicit_columns(int ncol, int L, const double* w, double* du,
+                         const double* colgeo, const double* x1f, const double* x1v,
+                         const double* dx1f, double dt, double gamma, double grav,
+                         double* scratch, void* stream);
+
 /* interp_weno5 on device: out[m] = weno5(a[m],b[m],c[m],d[m],e[m]), the
    face value between the 2nd and 3rd argument (tests/test_weno.cpp:20-29). */
 int exo_weno5(int n, const double* a, const double* b, const double* c,

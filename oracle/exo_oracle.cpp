@@ -1306,104 +1306,120 @@ M5 flux_jacobian(double gm1, const double* w) {
   return J;
 }
 
+// One radial column of SolveImplicit3D's X1 branch with FullCorrection:
+// wcol [5][nc1] primitives (velocities projected here, on a copy), ducol
+// [5][nc1] explicit update on entry and corrected update on exit (levels
+// is..ie), geometry of the column's (k,j): cos/sin of the cell metric and
+// the angular widths.
+void implicit_column(const double* wcol_in, double* ducol, int nc1, int is, int ie,
+                     double cos_theta, double sin_theta, double dx2a, double dx3a,
+                     const double* x1f, const double* x1v, const double* dx1f, double dt,
+                     double gamma, double grav) {
+  std::vector<double> wc(wcol_in, wcol_in + (size_t)5 * nc1), gmm1(nc1);
+  std::vector<M5> a(nc1), b(nc1), c(nc1), dfdq(nc1);
+  std::vector<V5> delta(nc1);
+  for (int i = 0; i < nc1; ++i) {
+    wc[IVY * nc1 + i] += wc[IVZ * nc1 + i] * cos_theta;
+    wc[IVZ * nc1 + i] *= sin_theta;
+  }
+  auto W = [&](int i, double* out) { for (int n = 0; n < 5; ++n) out[n] = wc[(size_t)n * nc1 + i]; };
+  auto area1 = [&](int i) { return dx2a * dx3a * x1f[i] * x1f[i] * sin_theta; };
+  auto volume = [&](int i) { return dx1f[i] * dx2a * dx3a * x1v[i] * x1v[i] * sin_theta; };
+  M5 Phi = mzero();
+  Phi.a[IVX][IDN] = grav;
+  Phi.a[IEN][IVX] = grav;
+  double wl[5], wr[5], prim[5];
+  for (int i = is - 2; i <= ie + 1; ++i) {
+    W(i, wr);
+    double fsig = 1., feps = 1.;
+    gmm1[i] = (gamma - 1.) * feps / fsig;
+    dfdq[i] = flux_jacobian(gmm1[i], wr);
+  }
+  W(is - 2, wl); W(is - 1, wr);
+  double gm1 = 0.5 * (gmm1[is - 2] + gmm1[is - 1]);
+  roe_average(prim, gm1, wl, wr);
+  double fsig = 1., feps = 1.;
+  double cs = std::sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
+  M5 Am = abs_jacobian(prim, cs, gm1), Ap;
+  for (int i = is - 1; i <= ie; ++i) {
+    W(i, wl); W(i + 1, wr);
+    gm1 = 0.5 * (gmm1[i] + gmm1[i + 1]);
+    roe_average(prim, gm1, wl, wr);
+    cs = std::sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
+    Ap = abs_jacobian(prim, cs, gm1);
+    double aleft = area1(i), aright = area1(i + 1);
+    double vol = volume(i);
+    for (int r = 0; r < 5; ++r)
+      for (int q = 0; q < 5; ++q) {
+        double Dt = (r == q) ? 1. / dt : 0.;
+        a[i].a[r][q] = (Am.a[r][q] * aleft + Ap.a[r][q] * aright +
+                        (aright - aleft) * dfdq[i].a[r][q]) / (2. * vol) + Dt - Phi.a[r][q];
+        b[i].a[r][q] = -(Am.a[r][q] + dfdq[i - 1].a[r][q]) * aleft / (2. * vol);
+        c[i].a[r][q] = -(Ap.a[r][q] - dfdq[i + 1].a[r][q]) * aright / (2. * vol);
+      }
+    Am = Ap;
+  }
+  // reflecting boundaries: Bnds = Bnde = diag(1,-1,1,1,1)
+  M5 B = mzero();
+  for (int r = 0; r < 5; ++r) B.a[r][r] = 1.;
+  B.a[IVX][IVX] = -1;
+  {
+    M5 t = mmul(b[is], B);
+    for (int r = 0; r < 5; ++r) for (int q = 0; q < 5; ++q) a[is].a[r][q] += t.a[r][q];
+    t = mmul(c[ie], B);
+    for (int r = 0; r < 5; ++r) for (int q = 0; q < 5; ++q) a[ie].a[r][q] += t.a[r][q];
+  }
+  // ForwardSweep / BackwardSubstitution (forward_backward.hpp:15-126)
+  for (int i = is; i <= ie; ++i) {
+    V5 rhs;
+    rhs.a[0] = ducol[IDN * nc1 + i];
+    rhs.a[0] /= dt;
+    rhs.a[1] = ducol[IVX * nc1 + i] / dt;
+    rhs.a[2] = ducol[IVY * nc1 + i] / dt;
+    rhs.a[3] = ducol[IVZ * nc1 + i] / dt;
+    rhs.a[4] = ducol[IEN * nc1 + i] / dt;
+    if (i == is) {
+      a[i] = minv(a[i]);
+      delta[i] = mvmul(a[i], rhs);
+    } else {
+      M5 ba = mmul(b[i], a[i - 1]);
+      M5 t;
+      for (int r = 0; r < 5; ++r) for (int q = 0; q < 5; ++q) t.a[r][q] = a[i].a[r][q] - ba.a[r][q];
+      a[i] = minv(t);
+      V5 bd = mvmul(b[i], delta[i - 1]), x;
+      for (int r = 0; r < 5; ++r) x.a[r] = rhs.a[r] - bd.a[r];
+      delta[i] = mvmul(a[i], x);
+    }
+    a[i] = mmul(a[i], c[i]);
+  }
+  for (int i = ie - 1; i >= is; --i) {
+    V5 ad = mvmul(a[i], delta[i + 1]);
+    for (int r = 0; r < 5; ++r) delta[i].a[r] -= ad.a[r];
+  }
+  for (int i = is; i <= ie; ++i)
+    for (int n = 0; n < 5; ++n) ducol[n * nc1 + i] = delta[i].a[n];
+}
+
 // SolveImplicit3D, X1 branch with FullCorrection (flag bit 3)
 void implicit_x1(Oracle& o, double dt) {
-  int nc1 = o.nc1, is = o.is, ie = o.ie;
-  double gamma = o.cfg.gamma, grav = o.cfg.grav;
+  int nc1 = o.nc1;
 #pragma omp parallel for collapse(2)
   for (int p = 0; p < 6; ++p)
     for (int k = o.ks; k <= o.ke; ++k) {
-      std::vector<double> wc((size_t)5 * nc1), gmm1(nc1);
-      std::vector<M5> a(nc1), b(nc1), c(nc1), dfdq(nc1);
-      std::vector<V5> delta(nc1);
+      std::vector<double> wc((size_t)5 * nc1), dc((size_t)5 * nc1);
       for (int j = o.js; j <= o.je; ++j) {
         const PanelGeo& g = o.pg[p];
-        double cos_theta = g.cosc[o.kj(k, j)], sin_theta = g.sinc[o.kj(k, j)];
+        size_t q = o.kj(k, j);
         for (int n = 0; n < 5; ++n)
-          for (int i = 0; i < nc1; ++i) wc[(size_t)n * nc1 + i] = o.w[o.at(p, n, k, j, i)];
-        for (int i = 0; i < nc1; ++i) {
-          wc[IVY * nc1 + i] += wc[IVZ * nc1 + i] * cos_theta;
-          wc[IVZ * nc1 + i] *= sin_theta;
-        }
-        auto W = [&](int i, double* out) { for (int n = 0; n < 5; ++n) out[n] = wc[(size_t)n * nc1 + i]; };
-        M5 Phi = mzero();
-        Phi.a[IVX][IDN] = grav;
-        Phi.a[IEN][IVX] = grav;
-        double wl[5], wr[5], prim[5];
-        for (int i = is - 2; i <= ie + 1; ++i) {
-          W(i, wr);
-          double fsig = 1., feps = 1.;
-          gmm1[i] = (gamma - 1.) * feps / fsig;
-          dfdq[i] = flux_jacobian(gmm1[i], wr);
-        }
-        W(is - 2, wl); W(is - 1, wr);
-        double gm1 = 0.5 * (gmm1[is - 2] + gmm1[is - 1]);
-        roe_average(prim, gm1, wl, wr);
-        double fsig = 1., feps = 1.;
-        double cs = std::sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
-        M5 Am = abs_jacobian(prim, cs, gm1), Ap;
-        for (int i = is - 1; i <= ie; ++i) {
-          W(i, wl); W(i + 1, wr);
-          gm1 = 0.5 * (gmm1[i] + gmm1[i + 1]);
-          roe_average(prim, gm1, wl, wr);
-          cs = std::sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
-          Ap = abs_jacobian(prim, cs, gm1);
-          double aleft = face1_area(o, g, k, j, i), aright = face1_area(o, g, k, j, i + 1);
-          double vol = cell_volume(o, g, k, j, i);
-          for (int r = 0; r < 5; ++r)
-            for (int q = 0; q < 5; ++q) {
-              double Dt = (r == q) ? 1. / dt : 0.;
-              a[i].a[r][q] = (Am.a[r][q] * aleft + Ap.a[r][q] * aright +
-                              (aright - aleft) * dfdq[i].a[r][q]) / (2. * vol) + Dt - Phi.a[r][q];
-              b[i].a[r][q] = -(Am.a[r][q] + dfdq[i - 1].a[r][q]) * aleft / (2. * vol);
-              c[i].a[r][q] = -(Ap.a[r][q] - dfdq[i + 1].a[r][q]) * aright / (2. * vol);
-            }
-          Am = Ap;
-        }
-        // reflecting boundaries: Bnds = Bnde = diag(1,-1,1,1,1)
-        M5 B = mzero();
-        for (int r = 0; r < 5; ++r) B.a[r][r] = 1.;
-        B.a[IVX][IVX] = -1;
-        {
-          M5 t = mmul(b[is], B);
-          for (int r = 0; r < 5; ++r) for (int q = 0; q < 5; ++q) a[is].a[r][q] += t.a[r][q];
-          t = mmul(c[ie], B);
-          for (int r = 0; r < 5; ++r) for (int q = 0; q < 5; ++q) a[ie].a[r][q] += t.a[r][q];
-        }
-        // ForwardSweep / BackwardSubstitution (forward_backward.hpp:15-126)
-        for (int i = is; i <= ie; ++i) {
-          V5 rhs;
-          rhs.a[0] = o.du[o.at(p, IDN, k, j, i)];
-          rhs.a[0] /= dt;
-          rhs.a[1] = o.du[o.at(p, IVX, k, j, i)] / dt;
-          rhs.a[2] = o.du[o.at(p, IVY, k, j, i)] / dt;
-          rhs.a[3] = o.du[o.at(p, IVZ, k, j, i)] / dt;
-          rhs.a[4] = o.du[o.at(p, IEN, k, j, i)] / dt;
-          if (i == is) {
-            a[i] = minv(a[i]);
-            delta[i] = mvmul(a[i], rhs);
-          } else {
-            M5 ba = mmul(b[i], a[i - 1]);
-            M5 t;
-            for (int r = 0; r < 5; ++r) for (int q = 0; q < 5; ++q) t.a[r][q] = a[i].a[r][q] - ba.a[r][q];
-            a[i] = minv(t);
-            V5 bd = mvmul(b[i], delta[i - 1]), x;
-            for (int r = 0; r < 5; ++r) x.a[r] = rhs.a[r] - bd.a[r];
-            delta[i] = mvmul(a[i], x);
+          for (int i = 0; i < nc1; ++i) {
+            wc[(size_t)n * nc1 + i] = o.w[o.at(p, n, k, j, i)];
+            dc[(size_t)n * nc1 + i] = o.du[o.at(p, n, k, j, i)];
           }
-          a[i] = mmul(a[i], c[i]);
-        }
-        for (int i = ie - 1; i >= is; --i) {
-          V5 ad = mvmul(a[i], delta[i + 1]);
-          for (int r = 0; r < 5; ++r) delta[i].a[r] -= ad.a[r];
-        }
-        for (int i = is; i <= ie; ++i) {
-          o.du[o.at(p, IDN, k, j, i)] = delta[i].a[0];
-          o.du[o.at(p, IVX, k, j, i)] = delta[i].a[1];
-          o.du[o.at(p, IVY, k, j, i)] = delta[i].a[2];
-          o.du[o.at(p, IVZ, k, j, i)] = delta[i].a[3];
-          o.du[o.at(p, IEN, k, j, i)] = delta[i].a[4];
-        }
+        implicit_column(wc.data(), dc.data(), nc1, o.is, o.ie, g.cosc[q], g.sinc[q], g.dx2a[q],
+                        g.dx3a[q], o.x1f.data(), o.x1v.data(), o.dx1f.data(), dt, o.cfg.gamma,
+                        o.cfg.grav);
+        for (int n = 0; n < 5; ++n)
+          for (int i = o.is; i <= o.ie; ++i) o.du[o.at(p, n, k, j, i)] = dc[(size_t)n * nc1 + i];
       }
     }
 }
@@ -1671,6 +1687,25 @@ void ora_get_mesh(void* h, int panel, double* x1f, double* x2f, double* x3f) {
   std::memcpy(x1f, o.x1f.data(), o.x1f.size() * sizeof(double));
   std::memcpy(x2f, o.pg[panel].x2f.data(), o.pg[panel].x2f.size() * sizeof(double));
   std::memcpy(x3f, o.pg[panel].x3f.data(), o.pg[panel].x3f.size() * sizeof(double));
+}
+
+// FullCorrection over a batch of columns: w [ncol][5][L+6], du [ncol][5][L]
+// (in/out), colgeo [ncol][4] = (cos, sin, dx2f_ang, dx3f_ang)
+void ora_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
+                          const double* x1f, const double* x1v, const double* dx1f, double dt,
+                          double gamma, double grav) {
+  int nc1 = L + 2 * G;
+#pragma omp parallel for
+  for (int c = 0; c < ncol; ++c) {
+    std::vector<double> dc((size_t)5 * nc1, 0.);
+    for (int n = 0; n < 5; ++n)
+      for (int i = 0; i < L; ++i) dc[(size_t)n * nc1 + G + i] = du[((size_t)c * 5 + n) * L + i];
+    const double* g4 = colgeo + (size_t)c * 4;
+    implicit_column(w + (size_t)c * 5 * nc1, dc.data(), nc1, G, G + L - 1, g4[0], g4[1], g4[2],
+                    g4[3], x1f, x1v, dx1f, dt, gamma, grav);
+    for (int n = 0; n < 5; ++n)
+      for (int i = 0; i < L; ++i) du[((size_t)c * 5 + n) * L + i] = dc[(size_t)n * nc1 + G + i];
+  }
 }
 
 // one Riemann face through the oracle (for row-level parity)
