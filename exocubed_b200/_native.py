@@ -17,6 +17,7 @@ EXO_RS_ROE_SHALLOW, EXO_RS_LMARS, EXO_RS_HLLC, EXO_RS_LMARS_SHALLOW = 0, 1, 2, 3
 EXO_PREC_FP64, EXO_PREC_MIXED = 0, 1
 EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92 = 0, 1
 NGHOST = 3
+NOALLOC_SCRATCH_DOUBLES = 1048576  # EXO_NOALLOC_SCRATCH_DOUBLES
 
 # every symbol include/exo_b200.h declares
 EXPORTED = [
@@ -26,7 +27,7 @@ EXPORTED = [
     "exo_get_time", "exo_check_state", "exo_synchronize",
     "exo_calculate_fluxes", "exo_get_flux", "exo_riemann", "exo_weno5",
     "exo_get_stream", "exo_profile", "exo_profile_read", "exo_launch_count",
-    "exo_implicit_columns",
+    "exo_implicit_columns", "exo_implicit_columns_noalloc",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
 
@@ -96,6 +97,7 @@ def lib():
     L.exo_riemann.argtypes = [i, i, i, i, d, p, p, p, p, p, p, p, p]
     L.exo_weno5.argtypes = [i, p, p, p, p, p, p, p]
     L.exo_implicit_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
+    L.exo_implicit_columns_noalloc.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p]
     L.exo_get_stream.argtypes = [p, ctypes.POINTER(p)]
     L.exo_profile.argtypes = [p, i]
     L.exo_profile_read.argtypes = [p, i, ctypes.POINTER(ctypes.c_int64), dp]

@@ -540,6 +540,21 @@ int exo_implicit_columns(int ncol, int L, const double* w, double* du, const dou
   return EXO_OK;
 }
 
+int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
+                                 const double* colgeo, const double* x1f, const double* x1v,
+                                 const double* dx1f, double dt, double gamma, double grav,
+                                 void* stream) {
+  if (ncol < 0 || L < 1) return fail(EXO_ERR_ARG, "ncol must be >= 0 and L >= 1");
+  if (ncol > 0 && (!w || !du || !colgeo || !x1f || !x1v || !dx1f))
+    return fail(EXO_ERR_ARG, "NULL array");
+  if (!(dt > 0.) || !(gamma > 1.)) return fail(EXO_ERR_ARG, "dt must be > 0 and gamma > 1");
+  std::string err;
+  int rc = exo::launch_implicit_columns_noalloc(ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma,
+                                                grav, stream, &err);
+  if (rc) return fail(rc, err);
+  return EXO_OK;
+}
+
 int exo_weno5(int n, const double* a, const double* b, const double* c, const double* d,
               const double* e, double* out, void* stream) {
   if (n < 0 || !a || !b || !c || !d || !e || !out) return fail(EXO_ERR_ARG, "bad argument");

@@ -125,6 +125,10 @@ int launch_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
                         const double* wl, const double* wr, double* flx,
                         const double* cosf, const double* sinf, const double* cthp,
                         const double* cthc, void* stream);
+int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
+                                    const double* colgeo, const double* x1f, const double* x1v,
+                                    const double* dx1f, double dt, double gamma, double grav,
+                                    void* stream, std::string* err);
 int launch_weno5(int n, const double* a, const double* b, const double* c,
                  const double* d, const double* e, double* out, void* stream);
 

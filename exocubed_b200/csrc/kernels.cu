@@ -19,6 +19,8 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
+#include <string>
 
 #include <cuda_runtime.h>
 
@@ -1231,6 +1233,61 @@ int launch_implicit_columns(int ncol, int L, const double* w, double* du, const 
   k_implicit_columns<<<nblk(ncol, 64), 64, 0, (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
   return check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of exo_implicit_columns.  Its scratch is this
+// file-scope device array instead of caller memory, so the entry point never
+// calls cudaMalloc or cudaFree.  Every GPU that loads the library holds the
+// 8 MiB until the process exits.  The array name is only a host-side handle:
+// kernels get the device address that cudaGetSymbolAddress returns, looked up
+// once per device with that device current (on the first call made there).
+static __device__ __align__(256) double g_noalloc_scratch[EXO_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[64] = {};
+}  // namespace
+
+int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
+                                    const double* colgeo, const double* x1f, const double* x1v,
+                                    const double* dx1f, double dt, double gamma, double grav,
+                                    void* stream, std::string* err) {
+  if ((size_t)ncol * (size_t)L * 30 > (size_t)EXO_NOALLOC_SCRATCH_DOUBLES) {
+    *err = "ncol*L*30 = " + std::to_string((size_t)ncol * (size_t)L * 30) +
+           " exceeds the fixed scratch of " + std::to_string((size_t)EXO_NOALLOC_SCRATCH_DOUBLES) +
+           " doubles (ncol*L must be <= " + std::to_string(EXO_NOALLOC_SCRATCH_DOUBLES / 30) + ")";
+    return EXO_ERR_CAPACITY;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    *err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
+  double* scratch;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr) {
+        *err = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e);
+        return EXO_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = static_cast<double*>(ptr);
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  if (ncol <= 0) return 0;
+  k_implicit_columns<<<nblk(ncol, 64), 64, 0, (cudaStream_t)stream>>>(
+      ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    *err = std::string("k_implicit_columns: ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
+  return 0;
 }
 
 int launch_dt_reset(const DevView& v, void* stream) {

@@ -222,6 +222,30 @@ int exo_implicit_columns(int ncol, int L, const double* w, double* du,
                          const double* dx1f, double dt, double gamma, double grav,
                          double* scratch, void* stream);
 
+/* Allocation-free form of exo_implicit_columns.  This entry point has no
+   counterpart in the reference: it exists for callers that cannot allocate
+   device memory at the moment they advance the solution -- a host
+   application whose memory pool reserved the GPU up front (cudaMalloc would
+   fail or fragment it), a time-stepping or serving loop that must not stall
+   on the device-wide synchronization cudaMalloc/cudaFree can cause, or a
+   caller held to a fixed memory budget.  The caller passes inputs and
+   outputs exactly as for exo_implicit_columns; the 30 scratch doubles per
+   column level live in one fixed device array of EXO_NOALLOC_SCRATCH_DOUBLES
+   (8 MiB) that the library holds on every GPU it is loaded on, so
+   ncol * L must not exceed EXO_NOALLOC_SCRATCH_DOUBLES / 30 = 34952 (e.g.
+   546 columns of 64 levels); larger batches return EXO_ERR_CAPACITY.
+   The first call on each device looks up the array's device address (with
+   that device current); make that first call before any stream capture.
+   All calls share the one array and nothing in it needs to start at zero
+   (every word a column reads was written earlier in the same call), but
+   calls that overlap on the GPU -- other streams, other threads -- race on
+   it: issue them in order on one stream. */
+#define EXO_NOALLOC_SCRATCH_DOUBLES 1048576
+int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
+                                 const double* colgeo, const double* x1f,
+                                 const double* x1v, const double* dx1f, double dt,
+                                 double gamma, double grav, void* stream);
+
 /* interp_weno5 on device: out[m] = weno5(a[m],b[m],c[m],d[m],e[m]), the
    face value between the 2nd and 3rd argument (tests/test_weno.cpp:20-29). */
 int exo_weno5(int n, const double* a, const double* b, const double* c,
