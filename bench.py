@@ -35,7 +35,15 @@ sys.path.insert(0, ROOT)
 BYTES_PER_CELL_UPDATE = 320  # 8 registers x 5 vars x 8 B per SSPRK(3,3) step
 
 
-def workload_config(name):
+def workload_config(name, precision=0):
+    cfg, desc = _workload(name)
+    if precision == 1:
+        cfg = dict(cfg, precision=1)
+        desc = desc.replace("FP64", "mixed FP32/FP64")
+    return cfg, desc
+
+
+def _workload(name):
     from exocubed_b200 import workloads as W
     if name == "c2":
         return (W.dry_atmosphere_config(N=96, L=64, rsolver=1),
@@ -188,7 +196,7 @@ def run_ours(args):
 
     world, rank, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    cfg, desc = workload_config(args.workload)
+    cfg, desc = workload_config(args.workload, args.precision)
     state = make_state(cfg, seed=rank)
     g = CubedSphereAtmosphere(cfg)
     g.set_primitive(state)
@@ -279,7 +287,8 @@ def run_ours(args):
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f32+f64",
+        "data": "synthetic",
         "config": {"workload": desc, "cells_per_step": cells, "replicas": world,
                    "l2": "state arrays of 175 MB each exceed the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
@@ -300,6 +309,45 @@ def run_ours(args):
     g.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def run_accuracy(args):
+    """Mixed precision against the FP64 path on the same seeded state: both
+    advance args.accuracy steps with the FP64 path's first CFL step held
+    fixed, then relative L2 and Linf errors per field are reported."""
+    import numpy as np
+    import torch  # noqa: F401  (CUDA context)
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
+    cfg, desc = workload_config(args.workload, 0)
+    state = make_state(cfg, seed=0)
+    ref = CubedSphereAtmosphere(cfg)
+    ref.set_primitive(state)
+    dt = ref.dt
+    ref.step(args.accuracy, dt)
+    wr = W.interior(ref.primitive())
+    ref.close()
+    mix = CubedSphereAtmosphere(dict(cfg, precision=1))
+    mix.set_primitive(state)
+    mix.step(args.accuracy, dt)
+    wm = W.interior(mix.primitive())
+    invalid = mix.invalid()
+    mix.close()
+    names = ["rho", "v1", "v2", "v3", "p"] if cfg["eqn"] == 1 else ["phi", "v1", "v2", "v3"]
+    err = {}
+    for n, name in enumerate(names):
+        if name == "v1" and cfg["eqn"] == 0:
+            continue
+        d = wm[:, n] - wr[:, n]
+        scale = np.linalg.norm(wr[:, n])
+        err[name] = {"rel_l2": float(np.linalg.norm(d) / scale) if scale > 0 else float(np.linalg.norm(d)),
+                     "linf": float(np.abs(d).max()),
+                     "rel_linf": float(np.abs(d).max() / max(np.abs(wr[:, n]).max(), 1e-300))}
+    print(json.dumps({"accuracy": {"workload": desc.replace("FP64", "mixed vs FP64"),
+                                   "steps": args.accuracy, "dt": dt,
+                                   "simulated_seconds": dt * args.accuracy,
+                                   "fields": err, "state_valid": invalid == 0}}))
 
 
 def run_reference(args):
@@ -334,13 +382,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3"])
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+                    help="0: FP64; 1: FP32 reconstruction/Riemann/divergence, FP64 rest")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-worker", action="store_true")
+    ap.add_argument("--accuracy", type=int, default=0,
+                    help="run N steps mixed vs FP64 and report the field errors")
     args = ap.parse_args()
     if args.cpu_worker:
         cpu_worker(args)
+    elif args.accuracy > 0:
+        run_accuracy(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

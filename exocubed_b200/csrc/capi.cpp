@@ -20,6 +20,10 @@
 using exo::DevScalars;
 using exo::DevView;
 
+// the step launchers of the context's arithmetic build
+#define STEP(name, ...) \
+  (c->v.precision == EXO_PREC_MIXED ? exo::mixed::name(__VA_ARGS__) : exo::fp64::name(__VA_ARGS__))
+
 namespace {
 
 thread_local std::string g_err;
@@ -114,10 +118,10 @@ static int timed(exo_ctx* c, int kernel, int nlaunch, F&& f) {
 // ghost exchange + ConservedToPrimitive + x1 boundary (+ CFL candidate)
 static int boundary_and_prim(exo_ctx* c, bool dt) {
   int rc;
-  if (dt && (rc = timed(c, EXO_K_OTHER, 1, [&] { return exo::launch_dt_reset(c->v, c->stream); })))
+  if (dt && (rc = timed(c, EXO_K_OTHER, 1, [&] { return STEP(launch_dt_reset, c->v, c->stream); })))
     return rc;
   return timed(c, EXO_K_PRIM_GHOST, 1,
-               [&] { return exo::launch_prim_ghost(c->v, dt, c->stream); });
+               [&] { return STEP(launch_prim_ghost, c->v, dt, c->stream); });
 }
 
 static int one_step(exo_ctx* c, double dt_fixed) {
@@ -126,24 +130,24 @@ static int one_step(exo_ctx* c, double dt_fixed) {
   bool implicit = !shallow && (v.implicit_flag & 1);
   int rc;
   if (dt_fixed > 0. &&
-      (rc = timed(c, EXO_K_OTHER, 1, [&] { return exo::launch_set_dt(v, dt_fixed, c->stream); })))
+      (rc = timed(c, EXO_K_OTHER, 1, [&] { return STEP(launch_set_dt, v, dt_fixed, c->stream); })))
     return rc;
   for (int s = 0; s < 3; ++s) {
     if (!shallow &&
-        (rc = timed(c, EXO_K_FLUX_X1, 1, [&] { return exo::launch_flux_x1(v, c->stream); })))
+        (rc = timed(c, EXO_K_FLUX_X1, 1, [&] { return STEP(launch_flux_x1, v, c->stream); })))
       return rc;
-    if ((rc = timed(c, EXO_K_FLUX_X23, 1, [&] { return exo::launch_flux_x23(v, c->stream); })))
+    if ((rc = timed(c, EXO_K_FLUX_X23, 1, [&] { return STEP(launch_flux_x23, v, c->stream); })))
       return rc;
     int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
-    if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return exo::launch_update(v, s, c->stream); })))
+    if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return STEP(launch_update, v, s, c->stream); })))
       return rc;
     if (implicit &&
-        (rc = timed(c, EXO_K_IMPLICIT, 1, [&] { return exo::launch_implicit(v, s, c->stream); })))
+        (rc = timed(c, EXO_K_IMPLICIT, 1, [&] { return STEP(launch_implicit, v, s, c->stream); })))
       return rc;
     if ((rc = boundary_and_prim(c, s == 2 && dt_fixed <= 0.))) return rc;
   }
   return timed(c, EXO_K_OTHER, 1,
-               [&] { return exo::launch_dt_finalize(v, dt_fixed, true, c->stream); });
+               [&] { return STEP(launch_dt_finalize, v, dt_fixed, true, c->stream); });
 }
 
 extern "C" {
@@ -199,8 +203,8 @@ int exo_create(const exo_config* cfg, exo_ctx** out) {
     return fail(EXO_ERR_ARG, "shallow water needs the Roe or LMARS shallow-water solver");
   if (!shallow && cfg->rsolver != EXO_RS_LMARS && cfg->rsolver != EXO_RS_HLLC)
     return fail(EXO_ERR_ARG, "the ideal gas needs the LMARS or HLLC solver");
-  if (cfg->precision != EXO_PREC_FP64)
-    return fail(EXO_ERR_ARG, "only EXO_PREC_FP64 is available in this build");
+  if (cfg->precision != EXO_PREC_FP64 && cfg->precision != EXO_PREC_MIXED)
+    return fail(EXO_ERR_ARG, "precision must be EXO_PREC_FP64 or EXO_PREC_MIXED");
   if (!shallow && (cfg->implicit_flag & ~9))
     return fail(EXO_ERR_ARG, "implicit_flag: only bits 1 (x1) and 8 (full 5x5) are supported");
   if (!shallow && (cfg->implicit_flag & 1) && !(cfg->implicit_flag & 8))
@@ -273,6 +277,17 @@ int exo_create(const exo_config* cfg, exo_ctx** out) {
       cudaError_t e = cudaMalloc((void**)&v.scratch, sbytes);
       if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(implicit scratch)"));
       c->owned.push_back(v.scratch);
+    }
+  }
+  if (cfg->precision == EXO_PREC_MIXED) {
+    size_t fbytes = c->state_elems * sizeof(float);
+    float** f32[] = {&v.w32, &v.flux32[0], &v.flux32[1], &v.flux32[2]};
+    for (float** a : f32) {
+      if (a == &v.flux32[0] && shallow) continue;
+      cudaError_t e = cudaMalloc((void**)a, fbytes);
+      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(fp32 arrays)"));
+      c->owned.push_back(*a);
+      cudaMemset(*a, 0, fbytes);
     }
   }
   double *x1f, *x1v, *dx1f, *geo;
@@ -374,10 +389,10 @@ int exo_set_primitive(exo_ctx* c, const double* w_host) {
   size_t bytes = c->state_elems * sizeof(double);
   // stage through the w array, then P2C of the interior into u
   CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
-  RK(exo::launch_p2c_interior(c->v, c->v.w, c->stream));
+  RK(STEP(launch_p2c_interior, c->v, c->v.w, c->stream));
   int rc = boundary_and_prim(c, true);
   if (rc) return rc;
-  RK(exo::launch_dt_finalize(c->v, 0., false, c->stream));
+  RK(STEP(launch_dt_finalize, c->v, 0., false, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->has_state = true;
   return EXO_OK;
@@ -496,8 +511,8 @@ int exo_launch_count(exo_ctx* c, int64_t* launches) {
 int exo_calculate_fluxes(exo_ctx* c) {
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
-  RK(exo::launch_flux_x1(c->v, c->stream));
-  RK(exo::launch_flux_x23(c->v, c->stream));
+  RK(STEP(launch_flux_x1, c->v, c->stream));
+  RK(STEP(launch_flux_x23, c->v, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return EXO_OK;
 }

@@ -96,6 +96,8 @@ struct DevView {
   double* u1;
   double* du;
   double* flux[3];                 // face fluxes, same layout as u
+  float* w32;                      // mixed precision: FP32 copy of w for the flux kernels
+  float* flux32[3];                // mixed precision: FP32 face fluxes
   double* scratch;                 // implicit solver: per column L*(25+5) doubles
   // tables
   const double* x1f;
@@ -108,29 +110,37 @@ struct DevView {
   DevScalars* sc;
 };
 
-// kernels.cu
-int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream);
-int launch_flux_x1(const DevView& v, void* stream);
-int launch_flux_x23(const DevView& v, void* stream);
-int launch_update(const DevView& v, int stage, void* stream);
-int launch_implicit(const DevView& v, int stage, void* stream);
-int launch_dt_reset(const DevView& v, void* stream);
-int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
-                            const double* x1f, const double* x1v, const double* dx1f, double dt,
-                            double gamma, double grav, double* scratch, void* stream);
-int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream);
-int launch_set_dt(const DevView& v, double dt, void* stream);
-int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);
+// Launchers of one arithmetic build (exo_kernels.cuh): fp64 (kernels.cu) and
+// mixed (kernels_mixed.cu) provide the same set.
+#define EXO_DECLARE_STEP_LAUNCHERS                                                   \
+  int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream);            \
+  int launch_flux_x1(const DevView& v, void* stream);                                \
+  int launch_flux_x23(const DevView& v, void* stream);                               \
+  int launch_update(const DevView& v, int stage, void* stream);                      \
+  int launch_implicit(const DevView& v, int stage, void* stream);                    \
+  int launch_dt_reset(const DevView& v, void* stream);                               \
+  int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream); \
+  int launch_set_dt(const DevView& v, double dt, void* stream);                      \
+  int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);
+namespace fp64 { EXO_DECLARE_STEP_LAUNCHERS }
+namespace mixed { EXO_DECLARE_STEP_LAUNCHERS }
+#undef EXO_DECLARE_STEP_LAUNCHERS
+
+// kernels.cu: FP64 row-level hooks
 int launch_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
                         const double* wl, const double* wr, double* flx,
                         const double* cosf, const double* sinf, const double* cthp,
                         const double* cthc, void* stream);
+int launch_weno5(int n, const double* a, const double* b, const double* c,
+                 const double* d, const double* e, double* out, void* stream);
+int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
+                            const double* x1f, const double* x1v, const double* dx1f, double dt,
+                            double gamma, double grav, double* scratch, void* stream);
 int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
                                     const double* colgeo, const double* x1f, const double* x1v,
                                     const double* dx1f, double dt, double gamma, double grav,
                                     void* stream, std::string* err);
-int launch_weno5(int n, const double* a, const double* b, const double* c,
-                 const double* d, const double* e, double* out, void* stream);
+
 
 // cell (U,V) <-> panel vector transforms of cubed_sphere_transform.cpp:11-61
 // written as coefficient quadruples: out0 = c0*in0 + c1*in1, out1 = c2*in0 + c3*in1

@@ -1,0 +1,1320 @@
+// exo_kernels.cuh -- the device code of one arithmetic build of the step.
+//
+// Included by kernels.cu (EXO_MIXED 0: everything in FP64, compiled without
+// fused multiply-add so it reproduces the CPU restatement bit for bit) and by
+// kernels_mixed.cu (EXO_MIXED 1: WENO5, the Riemann solvers and the flux
+// divergence in FP32 -- EXO_FLUX_T -- while the hydrostatic decomposition, the
+// implicit solve, the equation of state and the conserved state stay FP64;
+// compiled with FMA).  EXO_KNS names the namespace of the build.
+//
+// One stage of SSPRK(3,3) is five launches:
+//   k_flux_x1     per radial column: hydrostatic decomposition, WENO5 in x1,
+//                 restore, Riemann solve -> x1 face fluxes         (exo3 only)
+//   k_flux_x23    per horizontal face: WENO5 on both sides; at panel edges the
+//                 outer state is the neighbour panel's own reconstruction,
+//                 rotated into this panel's basis; Riemann solve -> x2/x3 fluxes
+//   k_update      per cell: RK register average, flux divergence, geometric
+//                 source, gravity / Coriolis -> u (exo2) or du (exo3)
+//   k_implicit    per radial column: 5x5 block-tridiagonal vertical correction,
+//                 u += du, AirParcel round trip on the last stage (exo3)
+//   k_prim_ghost  per cell incl. ghosts: ConservedToPrimitive of the interior,
+//                 of the ghost bands interpolated from the neighbour panels and
+//                 of the reflected x1 ghosts; CFL time-step candidate
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+
+#include <cuda_runtime.h>
+
+#include "exo_internal.h"
+
+namespace exo {
+namespace EXO_KNS {
+namespace {
+
+constexpr double TINY_NUMBER = 1.0e-20;
+constexpr double WENO_EPS = 1.0e-7;
+
+__device__ __forceinline__ double sqr(double x) { return x * x; }
+__device__ __forceinline__ float sqr(float x) { return x * x; }
+
+__device__ __forceinline__ size_t idx(const DevView& v, int p, int n, int k, int j, int i) {
+  return ((((size_t)p * v.nv + n) * v.nc3 + k) * v.nc2 + j) * v.nc1 + i;
+}
+__device__ __forceinline__ double geo(const DevView& v, int f, int p, int k, int j) {
+  return v.geo[(((size_t)f * 6 + p) * v.nc3 + k) * v.nc2 + j];
+}
+
+// face-flux and primitive arrays in the type the flux kernels work in
+template <class T> __device__ __forceinline__ T* flux_array(const DevView& v, int d);
+template <> __device__ __forceinline__ double* flux_array<double>(const DevView& v, int d) {
+  return v.flux[d];
+}
+template <> __device__ __forceinline__ float* flux_array<float>(const DevView& v, int d) {
+  return v.flux32[d];
+}
+template <class T> __device__ __forceinline__ const T* prim_array(const DevView& v);
+template <> __device__ __forceinline__ const double* prim_array<double>(const DevView& v) {
+  return v.w;
+}
+template <> __device__ __forceinline__ const float* prim_array<float>(const DevView& v) {
+  return v.w32;
+}
+
+// interp_weno5(phip2, phip1, phi, phim1, phim2): the face value between the
+// 2nd and 3rd argument (Jiang & Shu 1996; orientation of tests/test_weno.cpp)
+template <class T>
+__device__ __forceinline__ T weno5(T phip2, T phip1, T phi, T phim1, T phim2) {
+  const T eps = T(WENO_EPS);
+  T p0 = T(1.0 / 3.0) * phim2 - T(7.0 / 6.0) * phim1 + T(11.0 / 6.0) * phi;
+  T p1 = T(-1.0 / 6.0) * phim1 + T(5.0 / 6.0) * phi + T(1.0 / 3.0) * phip1;
+  T p2 = T(1.0 / 3.0) * phi + T(5.0 / 6.0) * phip1 - T(1.0 / 6.0) * phip2;
+  T b0 = T(13. / 12.) * sqr(phim2 - T(2.) * phim1 + phi) +
+         T(.25) * sqr(phim2 - T(4.) * phim1 + T(3.) * phi);
+  T b1 = T(13. / 12.) * sqr(phim1 - T(2.) * phi + phip1) + T(.25) * sqr(phim1 - phip1);
+  T b2 = T(13. / 12.) * sqr(phi - T(2.) * phip1 + phip2) +
+         T(.25) * sqr(T(3.) * phi - T(4.) * phip1 + phip2);
+  T a0 = T(0.1) / ((b0 + eps) * (b0 + eps));
+  T a1 = T(0.6) / ((b1 + eps) * (b1 + eps));
+  T a2 = T(0.3) / ((b2 + eps) * (b2 + eps));
+  return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+}
+
+// right-face value (face c+1) and left-face value (face c) of cell c on a
+// strided line q[c*s]
+// (the stencil values are converted to the reconstruction type T first)
+template <class T, class S>
+__device__ __forceinline__ T weno_r(const S* q, long s, int c) {
+  return weno5<T>(T(q[(c + 2) * s]), T(q[(c + 1) * s]), T(q[c * s]), T(q[(c - 1) * s]),
+                  T(q[(c - 2) * s]));
+}
+template <class T, class S>
+__device__ __forceinline__ T weno_l(const S* q, long s, int c) {
+  return weno5<T>(T(q[(c - 2) * s]), T(q[(c - 1) * s]), T(q[c * s]), T(q[(c + 1) * s]),
+                  T(q[(c + 2) * s]));
+}
+
+// ------------------------------------------------------------------ EOS ----
+// CubedSphereUtility::CovariantToContravariant (cubed_sphere_utility.hpp:22-31)
+__device__ __forceinline__ void cov_to_contra(double* a, double cth) {
+  double v = a[IVY], w = a[IVZ];
+  double sth2 = 1. - cth * cth;
+  a[IVY] = v / sth2 - w * cth / sth2;
+  a[IVZ] = -v * cth / sth2 + w / sth2;
+}
+__device__ __forceinline__ void contra_to_cov(double* a, double cth) {
+  double v = a[IVY], w = a[IVZ];
+  a[IVY] = v + w * cth;
+  a[IVZ] = w + v * cth;
+}
+
+// ConservedToPrimitive of one cell (shallow_yz_hydro.cpp:42-67,
+// ideal_moist_hydro.cpp:77-159); returns 1 if the state is invalid
+__device__ __forceinline__ int cons_to_prim(const DevView& v, const double* c, double* w,
+                                            double cth) {
+  int bad = 0;
+  if (v.eqn == EXO_EQN_SHALLOW_YZ) {
+    double dfloor = (double)sqrtf(1024 * FLT_MIN);
+    double ud = c[IDN];
+    ud = (ud > dfloor) ? ud : dfloor;
+    w[IDN] = ud;
+    w[IVX] = 0.;
+    w[IVY] = c[IVY];
+    w[IVZ] = c[IVZ];
+    double di = 1. / ud;
+    cov_to_contra(w, cth);
+    w[IVY] *= di;
+    w[IVZ] *= di;
+  } else {
+    double gm1 = v.gamma - 1.0;
+    double density = 0.;
+    density += c[IDN];
+    w[IDN] = density;
+    double di = 1. / density;
+    if ((w[IDN] < 0.) || isnan(w[IDN])) bad = 1;
+    double fsig = 1., feps = 1.;
+    w[IVX] = c[IVX] * di;
+    w[IVY] = c[IVY] * di;
+    w[IVZ] = c[IVZ] * di;
+    cov_to_contra(w, cth);
+    double KE = 0.5 * (c[IVX] * w[IVX] + c[IVY] * w[IVY] + c[IVZ] * w[IVZ]);
+    w[IPR] = gm1 * (c[IEN] - KE) * feps / fsig;
+    if ((w[IPR] < 0.) || isnan(w[IPR])) bad = 1;
+  }
+  return bad;
+}
+
+__device__ __forceinline__ void prim_to_cons(const DevView& v, const double* w, double* c,
+                                             double cth) {
+  if (v.eqn == EXO_EQN_SHALLOW_YZ) {
+    double wd = w[IDN];
+    c[IDN] = wd;
+    c[IVX] = 0.;
+    c[IVY] = w[IVY];
+    c[IVZ] = w[IVZ];
+    contra_to_cov(c, cth);
+    c[IVY] *= wd;
+    c[IVZ] *= wd;
+  } else {
+    double igm1 = 1.0 / (v.gamma - 1.0);
+    double wd = w[IDN];
+    c[IDN] = wd;
+    c[IVX] = w[IVX] * wd;
+    c[IVY] = w[IVY] * wd;
+    c[IVZ] = w[IVZ] * wd;
+    contra_to_cov(c, cth);
+    double KE = 0.5 * (c[IVX] * w[IVX] + c[IVY] * w[IVY] + c[IVZ] * w[IVZ]);
+    double fsig = 1., feps = 1.;
+    c[IEN] = igm1 * w[IPR] * fsig / feps + KE;
+  }
+}
+
+// ------------------------------------------------------ Riemann solvers ----
+template <class T>
+struct FaceGeo {
+  T cosf, sinf, cthp, cthc;
+};
+
+template <class T>
+__device__ __forceinline__ void prim_to_local(int ivx, const FaceGeo<T>& fg, T* w) {
+  if (ivx == IVY) {  // PrimToLocal2, gnomonic_equiangle.cpp:604-660
+    T g23 = fg.cosf, g33 = T(1.0), gi22 = T(1.0) / (fg.sinf * fg.sinf);
+    T T11 = T(1.0), T22 = T(1.0) / sqrt(gi22), T32 = g23 / sqrt(g33), T33 = sqrt(g33);
+    T uu1 = w[IVX], uu2 = w[IVY], uu3 = w[IVZ];
+    w[IVX] = T11 * uu1;
+    w[IVY] = T22 * uu2;
+    w[IVZ] = T32 * uu2 + T33 * uu3;
+  } else if (ivx == IVZ) {  // PrimToLocal3, :662-718
+    T g23 = fg.cosf, g22 = T(1.0), gi33 = T(1.0) / (fg.sinf * fg.sinf);
+    T T11 = T(1.0), T22 = sqrt(g22), T23 = g23 / sqrt(g22), T33 = T(1.0) / sqrt(gi33);
+    T uu1 = w[IVX], uu2 = w[IVY], uu3 = w[IVZ];
+    w[IVX] = T11 * uu1;
+    w[IVY] = T22 * uu2 + T23 * uu3;
+    w[IVZ] = T33 * uu3;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void flux_to_global(int ivx, const FaceGeo<T>& fg, T* f) {
+  if (ivx == IVY) {  // FluxToGlobal2, :752-791
+    T g23 = fg.cosf, g33 = T(1.0), gi22 = T(1.0) / (fg.sinf * fg.sinf);
+    T T11 = T(1.0), T22 = sqrt(gi22), T32 = -sqrt(gi22) * g23 / g33, T33 = T(1.0) / sqrt(g33);
+    T txx = f[IVX], txy = f[IVY], txz = f[IVZ];
+    f[IVX] = T11 * txx;
+    f[IVY] = T22 * txy;
+    f[IVZ] = T32 * txy + T33 * txz;
+  } else if (ivx == IVZ) {  // FluxToGlobal3, :793-832
+    T g23 = fg.cosf, g22 = T(1.0), gi33 = T(1.0) / (fg.sinf * fg.sinf);
+    T T11 = T(1.0), T22 = T(1.0) / sqrt(g22), T23 = -g23 / g22 * sqrt(gi33), T33 = sqrt(gi33);
+    T txx = f[IVX], txy = f[IVY], txz = f[IVZ];
+    f[IVX] = T11 * txx;
+    f[IVY] = T22 * txy + T23 * txz;
+    f[IVZ] = T33 * txz;
+  }
+}
+
+// roe_shallow_yz.cpp:18-122
+template <class T>
+__device__ void riemann_roe_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wri, T* flx) {
+  const T h = T(0.5);
+  int ivy = ivx == IVY ? IVZ : IVY;
+  prim_to_local(ivx, fg, wli);
+  prim_to_local(ivx, fg, wri);
+  T ubar = (wli[ivx] * sqrt(wli[IDN]) + wri[ivx] * sqrt(wri[IDN])) /
+           (sqrt(wli[IDN]) + sqrt(wri[IDN]));
+  T vbar = (wli[ivy] * sqrt(wli[IDN]) + wri[ivy] * sqrt(wri[IDN])) /
+           (sqrt(wli[IDN]) + sqrt(wri[IDN]));
+  T cbar = sqrt(h * (wli[IDN] + wri[IDN]));
+  T delh = wri[IDN] - wli[IDN];
+  T delu = wri[ivx] - wli[ivx];
+  T delv = wri[ivy] - wli[ivy];
+  T hbar = sqrt(wli[IDN] * wri[IDN]);
+  T a1 = h * (cbar * delh - hbar * delu) / cbar;
+  T a2 = hbar * delv;
+  T a3 = h * (cbar * delh + hbar * delu) / cbar;
+  T w00 = a1, w01 = a1 * (ubar - cbar), w02 = a1 * vbar;
+  T w10 = T(0.), w11 = T(0.), w12 = a2;
+  T w20 = a3, w21 = a3 * (ubar + cbar), w22 = a3 * vbar;
+  T s0 = fabs(ubar - cbar), s1 = fabs(ubar), s2 = fabs(ubar + cbar);
+  flx[IVZ] = T(0.);
+  flx[IDN] = h * (wli[IDN] * wli[ivx] + wri[IDN] * wri[ivx]);
+  flx[ivx] = h * (wli[IDN] * wli[ivx] * wli[ivx] + h * wli[IDN] * wli[IDN] +
+                  wri[IDN] * wri[ivx] * wri[ivx] + h * wri[IDN] * wri[IDN]);
+  flx[ivy] = h * (wli[IDN] * wli[ivx] * wli[ivy] + wri[IDN] * wri[ivx] * wri[ivy]);
+  flx[IVX] = T(0.);
+  flx[IDN] -= h * s0 * w00;
+  flx[ivx] -= h * s0 * w01;
+  flx[ivy] -= h * s0 * w02;
+  flx[IDN] -= h * s1 * w10;
+  flx[ivx] -= h * s1 * w11;
+  flx[ivy] -= h * s1 * w12;
+  flx[IDN] -= h * s2 * w20;
+  flx[ivx] -= h * s2 * w21;
+  flx[ivy] -= h * s2 * w22;
+  if (ivx == IVX) {
+    flx[IVX] = T(0.);
+    return;
+  }
+  flux_to_global(ivx, fg, flx);
+  T ty = flx[ivx], tz = flx[ivy];
+  flx[ivx] = ty + tz * fg.cthp;
+  flx[ivy] = tz + ty * fg.cthp;
+}
+
+// lmars.cpp:24-110 (NVAPOR = NCLOUD = 0), no projection
+template <class T>
+__device__ void riemann_lmars(double gamma_d, int ivx, const T* wli, const T* wri, T* flx) {
+  const T h = T(0.5), one = T(1.);
+  T gamma = T(gamma_d);
+  int ivy = IVX + ((ivx - IVX) + 1) % 3;
+  int ivz = IVX + ((ivx - IVX) + 2) % 3;
+  T fsig = one, feps = one;
+  T kappal = one / (gamma - one) * fsig / feps;
+  T kappar = one / (gamma - one) * fsig / feps;
+  T hl = wli[IPR] / wli[IDN] * (kappal + one) +
+         h * (sqr(wli[ivx]) + sqr(wli[ivy]) + sqr(wli[ivz]));
+  T hr = wri[IPR] / wri[IDN] * (kappar + one) +
+         h * (sqr(wri[ivx]) + sqr(wri[ivy]) + sqr(wri[ivz]));
+  T rhobar = h * (wli[IDN] + wri[IDN]);
+  T cbar = sqrt(h * (one + (one / kappar + one / kappal) / T(2.)) *
+                (wli[IPR] + wri[IPR]) / rhobar);
+  T pbar = h * (wli[IPR] + wri[IPR]) + h * (rhobar * cbar) * (wli[ivx] - wri[ivx]);
+  T ubar = h * (wli[ivx] + wri[ivx]) + h / (rhobar * cbar) * (wli[IPR] - wri[IPR]);
+  T rdl = one, rdr = one;
+  if (ubar > T(0.)) {
+    flx[IDN] = ubar * wli[IDN] * rdl;
+    flx[ivx] = ubar * wli[IDN] * wli[ivx] + pbar;
+    flx[ivy] = ubar * wli[IDN] * wli[ivy];
+    flx[ivz] = ubar * wli[IDN] * wli[ivz];
+    flx[IEN] = ubar * wli[IDN] * hl;
+  } else {
+    flx[IDN] = ubar * wri[IDN] * rdr;
+    flx[ivx] = ubar * wri[IDN] * wri[ivx] + pbar;
+    flx[ivy] = ubar * wri[IDN] * wri[ivy];
+    flx[ivz] = ubar * wri[IDN] * wri[ivz];
+    flx[IEN] = ubar * wri[IDN] * hr;
+  }
+}
+
+// hllc_transform.cpp:24-263
+template <class T>
+__device__ void riemann_hllc(double gamma_d, int ivx, const FaceGeo<T>& fg, T* wl, T* wr, T* flx) {
+  const T h = T(.5), one = T(1.0), zero = T(0.0);
+  T gamma = T(gamma_d);
+  int ivy = IVX + ((ivx - IVX) + 1) % 3;
+  int ivz = IVX + ((ivx - IVX) + 2) % 3;
+  T gm1 = gamma - one, igm1 = one / gm1;
+  prim_to_local(ivx, fg, wl);
+  prim_to_local(ivx, fg, wr);
+  T wli[5], wri[5], fl[5], fr[5];
+  wli[IDN] = wl[IDN]; wli[IVX] = wl[ivx]; wli[IVY] = wl[ivy]; wli[IVZ] = wl[ivz]; wli[IPR] = wl[IPR];
+  wri[IDN] = wr[IDN]; wri[IVX] = wr[ivx]; wri[IVY] = wr[ivy]; wri[IVZ] = wr[ivz]; wri[IPR] = wr[IPR];
+  T fsig = one, feps = one;
+  T cl = sqrt((one + (gamma - one) * feps / fsig) * wli[IPR] / wli[IDN]);
+  T cr = sqrt((one + (gamma - one) * feps / fsig) * wri[IPR] / wri[IDN]);
+  T KE_l, KE_r;
+  if (ivx == IVX) {
+    T cth = fg.cthc, vy, vz;
+    vy = wli[IVY] + wli[IVZ] * cth;
+    vz = wli[IVZ] + wli[IVY] * cth;
+    KE_l = h * wli[IDN] * (sqr(wli[IVX]) + wli[IVY] * vy + wli[IVZ] * vz);
+    vy = wri[IVY] + wri[IVZ] * cth;
+    vz = wri[IVZ] + wri[IVY] * cth;
+    KE_r = h * wri[IDN] * (sqr(wri[IVX]) + wri[IVY] * vy + wri[IVZ] * vz);
+  } else {
+    KE_l = h * wli[IDN] * (sqr(wli[IVX]) + sqr(wli[IVY]) + sqr(wli[IVZ]));
+    KE_r = h * wri[IDN] * (sqr(wri[IVX]) + sqr(wri[IVY]) + sqr(wri[IVZ]));
+  }
+  T el = wli[IPR] * igm1 + KE_l;
+  T er = wri[IPR] * igm1 + KE_r;
+  T rhoa = h * (wli[IDN] + wri[IDN]);
+  T ca = h * (cl + cr);
+  T pmid = h * (wli[IPR] + wri[IPR] + (wli[IVX] - wri[IVX]) * rhoa * ca);
+  T ql = (pmid <= wli[IPR]) ? one
+         : sqrt(one + (gamma + one) / (T(2) * gamma) * (pmid / wli[IPR] - one));
+  T qr = (pmid <= wri[IPR]) ? one
+         : sqrt(one + (gamma + one) / (T(2) * gamma) * (pmid / wri[IPR] - one));
+  T al = wli[IVX] - cl * ql;
+  T ar = wri[IVX] + cr * qr;
+  T bp = ar > zero ? ar : T(TINY_NUMBER);
+  T bm = al < zero ? al : -T(TINY_NUMBER);
+  T vxl = wli[IVX] - al;
+  T vxr = wri[IVX] - ar;
+  T tl = wli[IPR] + vxl * wli[IDN] * wli[IVX];
+  T tr = wri[IPR] + vxr * wri[IDN] * wri[IVX];
+  T ml = wli[IDN] * vxl;
+  T mr = -(wri[IDN] * vxr);
+  T am = (tl - tr) / (ml + mr);
+  T cp = (ml * tr + mr * tl) / (ml + mr);
+  cp = cp > zero ? cp : zero;
+  vxl = wli[IVX] - bm;
+  vxr = wri[IVX] - bp;
+  fl[IDN] = wli[IDN] * vxl;
+  fr[IDN] = wri[IDN] * vxr;
+  fl[IVX] = wli[IDN] * wli[IVX] * vxl + wli[IPR];
+  fr[IVX] = wri[IDN] * wri[IVX] * vxr + wri[IPR];
+  fl[IVY] = wli[IDN] * wli[IVY] * vxl;
+  fr[IVY] = wri[IDN] * wri[IVY] * vxr;
+  fl[IVZ] = wli[IDN] * wli[IVZ] * vxl;
+  fr[IVZ] = wri[IDN] * wri[IVZ] * vxr;
+  fl[IEN] = el * vxl + wli[IPR] * wli[IVX];
+  fr[IEN] = er * vxr + wri[IPR] * wri[IVX];
+  T sl, sr, sm;
+  if (am >= zero) {
+    sl = am / (am - bm);
+    sr = zero;
+    sm = -bm / (am - bm);
+  } else {
+    sl = zero;
+    sr = -am / (bp - am);
+    sm = bp / (bp - am);
+  }
+  flx[IDN] = sl * fl[IDN] + sr * fr[IDN];
+  flx[ivx] = sl * fl[IVX] + sr * fr[IVX] + sm * cp;
+  flx[ivy] = sl * fl[IVY] + sr * fr[IVY];
+  flx[ivz] = sl * fl[IVZ] + sr * fr[IVZ];
+  flx[IEN] = sl * fl[IEN] + sr * fr[IEN] + sm * cp * am;
+  flux_to_global(ivx, fg, flx);
+  T ty = flx[IVY], tz = flx[IVZ];
+  flx[IVY] = ty + tz * fg.cthp;
+  flx[IVZ] = tz + ty * fg.cthp;
+}
+
+// lmars_shallow_yz.cpp:18-93
+template <class T>
+__device__ void riemann_lmars_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wri, T* flx) {
+  const T h = T(0.5);
+  int ivy = ivx == IVY ? IVZ : IVY;
+  prim_to_local(ivx, fg, wli);
+  prim_to_local(ivx, fg, wri);
+  T cbar = sqrt(h * (wli[IDN] + wri[IDN]));
+  T hbar = h * (wli[IDN] + wri[IDN]) + h * cbar * (wli[ivx] - wri[ivx]);
+  T ubar = h * (wli[ivx] + wri[ivx]) + h / cbar * (wli[IDN] - wri[IDN]);
+  flx[IVZ] = T(0.);
+  if (ubar > T(0.)) {
+    flx[IDN] = ubar * wli[IDN];
+    flx[ivx] = ubar * wli[IDN] * wli[ivx] + h * hbar * hbar;
+    flx[ivy] = ubar * wli[IDN] * wli[ivy];
+  } else {
+    flx[IDN] = ubar * wri[IDN];
+    flx[ivx] = ubar * wri[IDN] * wri[ivx] + h * hbar * hbar;
+    flx[ivy] = ubar * wri[IDN] * wri[ivy];
+  }
+  flx[IVX] = T(0.);
+  if (ivx == IVX) return;
+  flux_to_global(ivx, fg, flx);
+  T ty = flx[ivx], tz = flx[ivy];
+  flx[ivx] = ty + tz * fg.cthp;
+  flx[ivy] = tz + ty * fg.cthp;
+}
+
+template <class T>
+__device__ __forceinline__ void riemann(int rsolver, double gamma, int ivx, const FaceGeo<T>& fg,
+                                        T* wl, T* wr, T* flx) {
+  switch (rsolver) {
+    case EXO_RS_ROE_SHALLOW: riemann_roe_shallow(ivx, fg, wl, wr, flx); break;
+    case EXO_RS_LMARS: riemann_lmars(gamma, ivx, wl, wr, flx); break;
+    case EXO_RS_HLLC: riemann_hllc(gamma, ivx, fg, wl, wr, flx); break;
+    default: riemann_lmars_shallow(ivx, fg, wl, wr, flx); break;
+  }
+}
+
+// ----------------------------------------------------- k_prim_ghost ------
+// Conserved value of variable n at cell (p,k,j,i) where (k,j) is interior or
+// in a ghost band; vectors (IVY, IVZ) come back together.
+__device__ __forceinline__ void load_cons(const DevView& v, int p, int k, int j, int i,
+                                          bool interior, double* c) {
+  if (interior) {
+    for (int n = 0; n < v.nv; ++n) c[n] = v.u[idx(v, p, n, k, j, i)];
+    return;
+  }
+  const GhostEntry& e = v.ghost[v.ghost_map[((size_t)p * v.nc3 + k) * v.nc2 + j]];
+  int sp = e.src_panel;
+  for (int n = 0; n < v.nv; ++n) {
+    if (n == IVY || n == IVZ) continue;
+    double v1 = v.u[idx(v, sp, n, e.k0, e.j0, i)];
+    double v2 = v.u[idx(v, sp, n, e.k1, e.j1, i)];
+    c[n] = (e.A * v1 + e.B * v2) / e.C;
+  }
+  double v1y = v.u[idx(v, sp, IVY, e.k0, e.j0, i)], v1z = v.u[idx(v, sp, IVZ, e.k0, e.j0, i)];
+  double v2y = v.u[idx(v, sp, IVY, e.k1, e.j1, i)], v2z = v.u[idx(v, sp, IVZ, e.k1, e.j1, i)];
+  double vy = (e.A * v1y + e.B * v2y) / e.C;
+  double vz = (e.A * v1z + e.B * v2z) / e.C;
+  double sth = e.ss, cth = e.cs;
+  double vyt = vy, vzt = vz;
+  vy = vyt / sth / sth - vzt * cth / sth / sth;
+  vz = vzt / sth / sth - vyt * cth / sth / sth;
+  double U = e.r[0] * vy + e.r[1] * vz;
+  double V = e.r[2] * vy + e.r[3] * vz;
+  vy = e.q[0] * U + e.q[1] * V;
+  vz = e.q[2] * U + e.q[3] * V;
+  vyt = vy;
+  vzt = vz;
+  c[IVY] = vyt + vzt * e.ct;
+  c[IVZ] = vzt + vyt * e.ct;
+}
+
+__global__ void k_prim_ghost(DevView v, int compute_dt) {
+  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned total = 6u * (unsigned)v.cells;
+  if (tid >= total) return;
+  unsigned i = tid % (unsigned)v.nc1;
+  unsigned r = tid / (unsigned)v.nc1;
+  int j = (int)(r % (unsigned)v.nc2);
+  r /= (unsigned)v.nc2;
+  int k = (int)(r % (unsigned)v.nc3);
+  int p = (int)(r / (unsigned)v.nc3);
+  bool kin = (k >= v.ks && k <= v.ke), jin = (j >= v.js && j <= v.je);
+  if (!kin && !jin) return;  // corner: never read on the path
+  int ii = i;
+  bool mirror = false;
+  if (i < v.is) { ii = 2 * v.is - 1 - i; mirror = true; }
+  else if (i > v.ie) { ii = 2 * v.ie + 1 - i; mirror = true; }
+  double c[5], w[5];
+  load_cons(v, p, k, j, ii, kin && jin, c);
+  double cth = geo(v, GCOSC, p, k, j);
+  int bad = cons_to_prim(v, c, w, cth);
+  if (mirror) w[IVX] = -w[IVX];
+  for (int n = 0; n < v.nv; ++n) v.w[idx(v, p, n, k, j, i)] = w[n];
+#if EXO_MIXED
+  for (int n = 0; n < v.nv; ++n) v.w32[idx(v, p, n, k, j, i)] = (float)w[n];
+#endif
+  if (!(kin && jin) || mirror) return;
+  if (bad) atomicOr(&v.sc->invalid, 1);
+  if (compute_dt) {
+    // Hydro::NewBlockTimeStep with patches/21.new_blockdt.patch:23-35
+    bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
+    double cs;
+    if (shallow) cs = sqrt(w[IDN]);
+    else {
+      double fsig = 1., feps = 1.;
+      cs = sqrt((1. + (v.gamma - 1) * feps / fsig) * w[IPR] / w[IDN]);
+    }
+    double dt1 = v.dx1f[i], dt2 = v.x1v[i] * geo(v, GDX2A, p, k, j);
+    double dt3 = v.x1v[i] * geo(v, GDX3A, p, k, j);
+    double speed1 = fmax(0., (fabs(w[IVX]) + cs));
+    double speed2 = fmax(0., (fabs(w[IVY]) + cs));
+    double speed3 = fmax(0., (fabs(w[IVZ]) + cs));
+    if ((v.implicit_flag & 1) && (v.N > 1)) dt1 /= v.cfl * fabs(w[IVX]);
+    else dt1 /= speed1;
+    if (v.implicit_flag & 2) dt2 /= v.cfl * fabs(w[IVY]);
+    else dt2 /= speed2;
+    if (v.implicit_flag & 4) dt3 /= v.cfl * fabs(w[IVZ]);
+    else dt3 /= speed3;
+    double m = fmin(dt2, dt3);
+    if (!shallow) m = fmin(dt1, m);
+    if (m >= 0.) atomicMin(&v.sc->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// ------------------------------------------------------------ k_flux_x1 ---
+// One CTA per interior radial column.
+template <class T>
+__global__ void k_flux_x1(DevView v) {
+  extern __shared__ double sm[];
+  int col = blockIdx.x;
+  int j = v.js + col % v.N;
+  int k = v.ks + (col / v.N) % v.N;
+  int p = col / (v.N * v.N);
+  int nc1 = v.nc1, nv = v.nv;
+  double* wc = sm;              // [nv][nc1]
+  double* psf = sm + nv * nc1;  // [nc1+1]
+  __shared__ double s_gam, s_expf;
+  for (int t = threadIdx.x; t < nv * nc1; t += blockDim.x)
+    wc[t] = v.w[idx(v, p, t / nc1, k, j, t % nc1)];
+  __syncthreads();
+  bool decomp = (v.grav != 0.);
+  if (decomp) {
+    // Decomposition::ChangeToPerturbation (change_to_perturbation.cpp:39-157)
+    if (threadIdx.x == 0) {
+      double grav = -v.grav;
+      int is = v.is, ie = v.ie;
+      double* wd = wc + IDN * nc1;
+      double* wp = wc + IPR * nc1;
+      double RdTv = wp[ie] / wd[ie];
+      psf[ie + 1] = wp[ie] * exp(-grav * v.dx1f[ie] / (2 * RdTv));
+      for (int i = ie; i >= is; --i) psf[i] = psf[i + 1] + grav * wd[i] * v.dx1f[i];
+      for (int i = 1; i <= G; ++i) psf[is - i] = psf[is + i];
+      for (int i = 1; i <= G; ++i) psf[ie + i + 1] = psf[ie + 1 - i];
+      double gammad = v.gamma, fsig = 1., feps = 1.;
+      double gam = 1. + (gammad - 1.) * feps / fsig;
+      double ent = log(wp[is]) - gam * log(wd[is]);
+      s_gam = gam;
+      s_expf = exp(-ent / gam);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nc1; i += blockDim.x) {
+      double psv, dsv;
+      if (fabs(psf[i] - psf[i + 1]) < 1.E-6)
+        psv = (psf[i] + psf[i + 1]) / 2.;
+      else
+        psv = (psf[i] - psf[i + 1]) / log(psf[i] / psf[i + 1]);
+      dsv = pow(psv, 1. / s_gam) * s_expf;
+      wc[IPR * nc1 + i] -= psv;
+      wc[IDN * nc1 + i] -= dsv;
+    }
+    __syncthreads();
+  }
+  FaceGeo<T> fg{T(0.), T(1.), T(geo(v, GCTHP1, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+  T* F = flux_array<T>(v, 0);
+  for (int f = threadIdx.x; f <= v.L; f += blockDim.x) {
+    int i = v.is + f;
+    // perturbations are formed in FP64 above; WENO5 and the Riemann solve run in T
+    T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
+    for (int n = 0; n < nv; ++n) {
+      const double* q = wc + n * nc1;
+      wl[n] = weno_r<T>(q, 1, i - 1);
+      wr[n] = weno_l<T>(q, 1, i);
+    }
+    if (decomp) {
+      // RestoreFromPerturbation (change_to_perturbation.cpp:159-222), in FP64
+      double ps = psf[i];
+      double xr = wr[IPR], xl = wl[IPR];
+      xr += ps;
+      if (xr < 0.) xr = ps;
+      xl += ps;
+      if (xl < 0.) xl = ps;
+      double dsf = pow(ps, 1. / s_gam) * s_expf;
+      double dr = wr[IDN], dl = wl[IDN];
+      dr += dsf;
+      if (dr < 0.) dr = dsf;
+      dl += dsf;
+      if (dl < 0.) dl = dsf;
+      wr[IPR] = T(xr);
+      wl[IPR] = T(xl);
+      wr[IDN] = T(dr);
+      wl[IDN] = T(dl);
+    }
+    riemann<T>(v.rsolver, v.gamma, IVX, fg, wl, wr, fx);
+    for (int n = 0; n < nv; ++n) F[idx(v, p, n, k, j, i)] = fx[n];
+  }
+}
+
+// ----------------------------------------------------------- k_flux_x23 --
+// Interior-side reconstruction of panel p at its own edge face (side s,
+// along index a) for radial index i: the state CubedSphere::sendNeighborBlocks
+// sends (L at Down/Right edges, R at Up/Left edges).
+template <class T>
+__device__ __forceinline__ void edge_interior_state(const DevView& v, int p, int s, int a,
+                                                    int i, T* st) {
+  long s2 = v.nc1, s3 = (long)v.nc1 * v.nc2;
+  const T* W = prim_array<T>(v);
+  for (int n = 0; n < v.nv; ++n) {
+    if (s == UP || s == DOWN) {
+      const T* q = W + idx(v, p, n, v.ks + a, 0, i);
+      st[n] = (s == DOWN) ? weno_r<T>(q, s2, v.je) : weno_l<T>(q, s2, v.js);
+    } else {
+      const T* q = W + idx(v, p, n, 0, v.js + a, i);
+      st[n] = (s == RIGHT) ? weno_r<T>(q, s3, v.ke) : weno_l<T>(q, s3, v.ks);
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void edge_outer_state(const DevView& v, int p, int side, int a,
+                                                 int i, T* st) {
+  const EdgeEntry& e = v.edge[((size_t)p * 4 + side) * v.N + a];
+  edge_interior_state<T>(v, e.src_panel, e.src_side, e.src_along, i, st);
+  T V2 = st[IVY], V3 = st[IVZ];
+  T U = T(e.r[0]) * V2 + T(e.r[1]) * V3;
+  T V = T(e.r[2]) * V2 + T(e.r[3]) * V3;
+  st[IVY] = T(e.q[0]) * U + T(e.q[1]) * V;
+  st[IVZ] = T(e.q[2]) * U + T(e.q[3]) * V;
+}
+
+template <class T>
+__global__ void k_flux_x23(DevView v) {
+  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned nface = 6u * v.N * (v.N + 1) * v.L;  // per direction
+  if (tid >= 2 * nface) return;
+  int dir = tid < nface ? 1 : 2;
+  unsigned r = dir == 1 ? tid : tid - nface;
+  unsigned L = v.L, N = v.N;
+  int i = v.is + (int)(r % L);
+  r /= L;
+  int k, j;
+  int p;
+  if (dir == 1) {  // x2 faces: j in [js, je+1], k in [ks, ke]
+    j = v.js + (int)(r % (N + 1));
+    r /= (N + 1);
+    k = v.ks + (int)(r % N);
+    p = (int)(r / N);
+  } else {  // x3 faces: j in [js, je], k in [ks, ke+1]
+    j = v.js + (int)(r % N);
+    r /= N;
+    k = v.ks + (int)(r % (N + 1));
+    p = (int)(r / (N + 1));
+  }
+  T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
+  long s2 = v.nc1, s3 = (long)v.nc1 * v.nc2;
+  const T* W = prim_array<T>(v);
+  FaceGeo<T> fg;
+  int ivx;
+  if (dir == 1) {
+    for (int n = 0; n < v.nv; ++n) {
+      const T* q = W + idx(v, p, n, k, 0, i);
+      wl[n] = weno_r<T>(q, s2, j - 1);
+      wr[n] = weno_l<T>(q, s2, j);
+    }
+    if (j == v.js) edge_outer_state<T>(v, p, UP, k - v.ks, i, wl);
+    else if (j == v.je + 1) edge_outer_state<T>(v, p, DOWN, k - v.ks, i, wr);
+    fg = FaceGeo<T>{T(geo(v, GCOSF2, p, k, j)), T(geo(v, GSINF2, p, k, j)),
+                    T(geo(v, GCTHP2, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+    ivx = IVY;
+  } else {
+    for (int n = 0; n < v.nv; ++n) {
+      const T* q = W + idx(v, p, n, 0, j, i);
+      wl[n] = weno_r<T>(q, s3, k - 1);
+      wr[n] = weno_l<T>(q, s3, k);
+    }
+    if (k == v.ks) edge_outer_state<T>(v, p, LEFT, j - v.js, i, wl);
+    else if (k == v.ke + 1) edge_outer_state<T>(v, p, RIGHT, j - v.js, i, wr);
+    fg = FaceGeo<T>{T(geo(v, GCOSF3, p, k, j)), T(geo(v, GSINF3, p, k, j)),
+                    T(geo(v, GCTHP3, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+    ivx = IVZ;
+  }
+  riemann<T>(v.rsolver, v.gamma, ivx, fg, wl, wr, fx);
+  T* F = flux_array<T>(v, dir);
+  for (int n = 0; n < v.nv; ++n) F[idx(v, p, n, k, j, i)] = fx[n];
+}
+
+// --------------------------------------------------------------- k_update -
+template <class T>
+__global__ void k_update(DevView v, int stage) {
+  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned L = v.L, N = v.N;
+  if (tid >= 6u * N * N * L) return;
+  int i = v.is + (int)(tid % L);
+  unsigned r = tid / L;
+  int j = v.js + (int)(r % N);
+  r /= N;
+  int k = v.ks + (int)(r % N);
+  int p = (int)(r / N);
+  const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
+  double wght = kBeta[stage] * v.sc->dt;
+  bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
+  int nv = v.nv;
+  double un[5];
+  // WeightedAve(u1, u, ...) then WeightedAve(u, u1, ...) (SSPRK(3,3) registers)
+  for (int n = 0; n < nv; ++n) {
+    size_t q = idx(v, p, n, k, j, i);
+    double uu = v.u[q];
+    if (stage == 0) {
+      v.u1[q] = uu;
+      un[n] = 0. + 1.0 * uu;
+    } else if (stage == 1) {
+      un[n] = 0.25 * uu + 0.75 * v.u1[q];
+    } else {
+      un[n] = (2.0 / 3.0) * uu + (1.0 / 3.0) * v.u1[q];
+    }
+  }
+  // AddFluxDivergence
+  double s = geo(v, GSINC, p, k, j);
+  double d2 = geo(v, GDX2A, p, k, j), d3 = geo(v, GDX3A, p, k, j);
+  double a1 = d2 * d3 * v.x1f[i] * v.x1f[i] * s;
+  double a1p = d2 * d3 * v.x1f[i + 1] * v.x1f[i + 1] * s;
+  double a2 = v.x1v[i] * geo(v, GDX3A_F2, p, k, j) * v.dx1f[i];
+  double a2p = v.x1v[i] * geo(v, GDX3A_F2, p, k, j + 1) * v.dx1f[i];
+  double a3 = v.x1v[i] * geo(v, GDX2A_F3, p, k, j) * v.dx1f[i];
+  double a3p = v.x1v[i] * geo(v, GDX2A_F3, p, k + 1, j) * v.dx1f[i];
+  double vol = v.dx1f[i] * d2 * d3 * v.x1v[i] * v.x1v[i] * s;
+  double du[5];
+  const T* F0 = flux_array<T>(v, 0);
+  const T* F1 = flux_array<T>(v, 1);
+  const T* F2 = flux_array<T>(v, 2);
+  // flux divergence in T; the conserved state accumulates in FP64
+  T A1 = T(a1), A1p = T(a1p), A2 = T(a2), A2p = T(a2p), A3 = T(a3), A3p = T(a3p);
+  for (int n = 0; n < nv; ++n) {
+    T dflx;
+    if (shallow) {
+      dflx = (A1p * T(0.) - A1 * T(0.));
+    } else {
+      dflx = (A1p * F0[idx(v, p, n, k, j, i + 1)] - A1 * F0[idx(v, p, n, k, j, i)]);
+    }
+    dflx += (A2p * F1[idx(v, p, n, k, j + 1, i)] - A2 * F1[idx(v, p, n, k, j, i)]);
+    dflx += (A3p * F2[idx(v, p, n, k + 1, j, i)] - A3 * F2[idx(v, p, n, k, j, i)]);
+    double change;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      change = wght * dflx / vol;
+    } else {
+      change = wght * (double)(dflx / T(vol));
+    }
+    if (shallow) {
+      un[n] -= change;
+    } else {
+      du[n] = 0.;
+      du[n] -= change;
+    }
+  }
+  double* out = shallow ? un : du;
+  // AddCoordTermsDivergence (gnomonic_equiangle.cpp:834-879)
+  {
+    double cosine = geo(v, GCOSC, p, k, j);
+    double sine2 = s * s;
+    double x_ov_rD = (v.x1v[i] * geo(v, GDX3A_F2, p, k, j) * v.dx1f[i] * geo(v, GSINF2, p, k, j) -
+                      v.x1v[i] * geo(v, GDX3A_F2, p, k, j + 1) * v.dx1f[i] *
+                          geo(v, GSINF2, p, k, j + 1)) / vol;
+    double y_ov_rC = (v.x1v[i] * geo(v, GDX2A_F3, p, k, j) * v.dx1f[i] * geo(v, GSINF3, p, k, j) -
+                      v.x1v[i] * geo(v, GDX2A_F3, p, k + 1, j) * v.dx1f[i] *
+                          geo(v, GSINF3, p, k + 1, j)) / vol;
+    double rho = v.w[idx(v, p, IDN, k, j, i)];
+    double v1 = v.w[idx(v, p, IVX, k, j, i)], v2 = v.w[idx(v, p, IVY, k, j, i)];
+    double v3 = v.w[idx(v, p, IVZ, k, j, i)];
+    double radius = v.x1v[i];
+    double pr;
+    double v_2 = v2 + v3 * cosine;
+    double v_3 = v3 + v2 * cosine;
+    if (shallow) {
+      pr = 0.5 * rho * rho;
+    } else {
+      pr = v.w[idx(v, p, IPR, k, j, i)];
+      double src1 = (2.0 * pr + rho * (v2 * v_2 + v3 * v_3)) / radius;
+      out[IVX] += wght * src1;
+    }
+    double src2 = -x_ov_rD * (pr + rho * v3 * v3 * sine2) - rho * v1 * v_2 / radius;
+    out[IVY] += wght * src2;
+    double src3 = -y_ov_rC * (pr + rho * v2 * v2 * sine2) - rho * v1 * v_3 / radius;
+    out[IVZ] += wght * src3;
+    // constant gravity (patches/25.constant_acc.patch:35-53)
+    if (v.grav != 0.) {
+      double src = wght * rho * v.grav;
+      out[IVX] += src;
+      if (!shallow) out[IEN] += src * v1;
+    }
+    // W92 Coriolis (examples/2023-Chen-exo3/W92.cpp:48-70)
+    if (v.coriolis == EXO_CORIOLIS_W92) {
+      double f = geo(v, GFCOR, p, k, j);
+      double U = geo(v, GCR0, p, k, j) * v2 + geo(v, GCR1, p, k, j) * v3;
+      double V = geo(v, GCR2, p, k, j) * v2 + geo(v, GCR3, p, k, j) * v3;
+      U = -U;
+      double llU = f * V, llV = -f * U;
+      double mU = -llU;
+      double acc2 = geo(v, GCQ0, p, k, j) * mU + geo(v, GCQ1, p, k, j) * llV;
+      double acc3 = geo(v, GCQ2, p, k, j) * mU + geo(v, GCQ3, p, k, j) * llV;
+      double a2c = acc2 + acc3 * cosine, a3c = acc3 + acc2 * cosine;
+      out[IVY] += wght * rho * a2c;
+      out[IVZ] += wght * rho * a3c;
+    }
+  }
+  if (shallow) {
+    for (int n = 0; n < nv; ++n) v.u[idx(v, p, n, k, j, i)] = un[n];
+  } else if (v.implicit_flag & 1) {
+    for (int n = 0; n < nv; ++n) {
+      v.u[idx(v, p, n, k, j, i)] = un[n];
+      v.du[idx(v, p, n, k, j, i)] = du[n];
+    }
+  } else {
+    for (int n = 0; n < nv; ++n) v.u[idx(v, p, n, k, j, i)] = un[n] + 1. * du[n];
+  }
+}
+
+// ------------------------------------------------------------- k_implicit -
+// flux_decomposition.hpp:34-120, X1 direction
+__device__ __forceinline__ void roe_average(double* prim, double gm1, const double* wl,
+                                            const double* wr) {
+  double sqrtdl = sqrt(wl[IDN]), sqrtdr = sqrt(wr[IDN]);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  prim[IDN] = sqrtdl * sqrtdr;
+  prim[IVX] = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
+  prim[IVY] = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
+  prim[IVZ] = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
+  double el = wl[IPR] / gm1 + 0.5 * wl[IDN] * (sqr(wl[IVX]) + sqr(wl[IVY]) + sqr(wl[IVZ]));
+  double er = wr[IPR] / gm1 + 0.5 * wr[IDN] * (sqr(wr[IVX]) + sqr(wr[IVY]) + sqr(wr[IVZ]));
+  double hbar = ((el + wl[IPR]) / sqrtdl + (er + wr[IPR]) / sqrtdr) * isdlpdr;
+  prim[IPR] = (hbar - 0.5 * (sqr(prim[IVX]) + sqr(prim[IVY]) + sqr(prim[IVZ]))) * gm1 /
+              (gm1 + 1.) * prim[IDN];
+}
+
+// The vertical 5x5 block-tridiagonal correction of one radial column
+// (ImplicitSolver::SolveImplicit3D X1 branch, solve_implicit_3d.cpp:102-179,
+// with FullCorrection, full_correction.cpp:32-165, and ForwardSweep /
+// BackwardSubstitution, forward_backward.hpp:15-126), spread over the five
+// lanes base..base+4 of a warp: lane base+r holds row r of every 5x5 block
+// and component r of every vector.  Each lane evaluates exactly the sums of
+// the single-thread formulation (same terms, same order), so the result is
+// the same to the bit; the lanes exchange rows through warp shuffles.
+//   W(i, w5)     primitive state of level i (i in [is-1, ie+1])
+//   DU(i, n)     explicit update of level i, variable n
+//   SCR(lev, e)  6 scratch doubles of this lane per level: row r of A_i*c_i
+//                (5) and delta_i(r), written by the forward sweep and read
+//                back by the back substitution
+//   OUT(i, dl)   corrected update of level i (all 5 components), ie down to is
+// geo: cos/sin of the cell metric and the angular widths dx2f_ang, dx3f_ang.
+// All 32 lanes of the warp must call this together (full-mask shuffles).
+__device__ __forceinline__ double shfl(double x, int lane) {
+  return __shfl_sync(0xffffffffu, x, lane);
+}
+
+template <class WF, class DUF, class SCRF, class OUTF>
+__device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF DU, SCRF SCR,
+                                                     OUTF OUT, double cos_theta, double sin_theta,
+                                                     double d2, double d3, const double* x1f,
+                                                     const double* x1v, const double* dx1f,
+                                                     int is, int ie, double dt, double gamma,
+                                                     double grav) {
+  double s = sin_theta;
+  auto load = [&](int i, double* out) {
+    W(i, out);
+    out[IVY] += out[IVZ] * cos_theta;
+    out[IVZ] *= sin_theta;
+  };
+  double fsig = 1., feps = 1.;
+  double gmm1 = (gamma - 1.) * feps / fsig;
+  double gm1 = 0.5 * (gmm1 + gmm1);
+  // row r of the flux Jacobian dF/dq at a cell (flux_decomposition.hpp:100-120)
+  auto fj_row = [&](const double* w, double* out) {
+    double v1 = w[IVX], v2 = w[IVY], v3 = w[IVZ], rho = w[IDN], pres = w[IPR];
+    double s2 = v1 * v1 + v2 * v2 + v3 * v3;
+    if (r == 0) {
+      out[0] = 0; out[1] = 1.; out[2] = 0.; out[3] = 0.; out[4] = 0.;
+    } else if (r == 1) {
+      out[0] = gmm1 * s2 / 2 - v1 * v1; out[1] = (2. - gmm1) * v1; out[2] = -gmm1 * v2;
+      out[3] = -gmm1 * v3; out[4] = gmm1;
+    } else if (r == 2) {
+      out[0] = -v1 * v2; out[1] = v2; out[2] = v1; out[3] = 0.; out[4] = 0.;
+    } else if (r == 3) {
+      out[0] = -v1 * v3; out[1] = v3; out[2] = 0.; out[3] = v1; out[4] = 0.;
+    } else {
+      double c1 = ((gmm1 - 1) * s2 / 2 - (gmm1 + 1) / gmm1 * pres / rho) * v1;
+      double c2 = (gmm1 + 1) / gmm1 * pres / rho + s2 / 2 - gmm1 * v1 * v1;
+      out[0] = c1; out[1] = c2; out[2] = -gmm1 * v2 * v1; out[3] = -gmm1 * v3 * v1;
+      out[4] = (gmm1 + 1) * v1;
+    }
+  };
+  // row r of R |Lambda| R^-1 at the Roe average of a face
+  auto absj_row = [&](const double* wl, const double* wr, double* out) {
+    double prim[5];
+    roe_average(prim, gm1, wl, wr);
+    double cs = sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
+    double rr = prim[IDN], u = prim[IVX], v = prim[IVY], w = prim[IVZ], p = prim[IPR];
+    double ke = 0.5 * (u * u + v * v + w * w);
+    double hp = (gm1 + 1.) / gm1 * p / rr;
+    double h = hp + ke;
+    double R[5];
+    if (r == 0) { R[0] = 1.; R[1] = 1.; R[2] = 1.; R[3] = 0.; R[4] = 0.; }
+    else if (r == 1) { R[0] = u - cs; R[1] = u; R[2] = u + cs; R[3] = 0.; R[4] = 0.; }
+    else if (r == 2) { R[0] = v; R[1] = v; R[2] = v; R[3] = 1.; R[4] = 0.; }
+    else if (r == 3) { R[0] = w; R[1] = w; R[2] = w; R[3] = 0.; R[4] = 1.; }
+    else { R[0] = h - u * cs; R[1] = ke; R[2] = h + u * cs; R[3] = v; R[4] = w; }
+    double Ri[5];  // row r of R^-1
+    if (r == 0) {
+      Ri[0] = (cs * ke + u * hp) / (2. * cs * hp); Ri[1] = (-hp - cs * u) / (2. * cs * hp);
+      Ri[2] = -v / (2. * hp); Ri[3] = -w / (2. * hp); Ri[4] = 1. / (2. * hp);
+    } else if (r == 1) {
+      Ri[0] = (hp - ke) / hp; Ri[1] = u / hp; Ri[2] = v / hp; Ri[3] = w / hp; Ri[4] = -1. / hp;
+    } else if (r == 2) {
+      Ri[0] = (cs * ke - u * hp) / (2. * cs * hp); Ri[1] = (hp - cs * u) / (2. * cs * hp);
+      Ri[2] = -v / (2. * hp); Ri[3] = -w / (2. * hp); Ri[4] = 1. / (2. * hp);
+    } else if (r == 3) {
+      Ri[0] = -v; Ri[1] = 0.; Ri[2] = 1.; Ri[3] = 0.; Ri[4] = 0.;
+    } else {
+      Ri[0] = -w; Ri[1] = 0.; Ri[2] = 0.; Ri[3] = 1.; Ri[4] = 0.;
+    }
+    double lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
+    double T[5];  // row r of R * Lambda, summed as a full product
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double acc = R[0] * (c == 0 ? lam[0] : 0.);
+#pragma unroll
+      for (int k = 1; k < 5; ++k) acc += R[k] * (c == k ? lam[k] : 0.);
+      T[c] = acc;
+    }
+    double acc[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        double rik = shfl(Ri[c], base + k);  // (R^-1)(k, c)
+        if (k == 0) acc[c] = T[0] * rik;
+        else acc[c] += T[k] * rik;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) out[c] = acc[c];
+  };
+
+  double wl[5], wr[5];
+  double Am[5], Ap[5], dfm[5], df0[5], dfp[5];
+  load(is - 1, wl);
+  load(is, wr);
+  fj_row(wl, dfm);
+  fj_row(wr, df0);
+  absj_row(wl, wr, Am);
+  double Aprev[5], dprev = 0.;
+  for (int i = is; i <= ie; ++i) {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) wl[n] = wr[n];
+    load(i + 1, wr);
+    fj_row(wr, dfp);
+    absj_row(wl, wr, Ap);
+    double aleft = d2 * d3 * x1f[i] * x1f[i] * s;
+    double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
+    double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
+    double a[5], b[5], c[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double Dt = (r == q) ? 1. / dt : 0.;
+      double Phi = ((r == IVX && q == IDN) || (r == IEN && q == IVX)) ? grav : 0.;
+      a[q] = (Am[q] * aleft + Ap[q] * aright + (aright - aleft) * df0[q]) / (2. * vol) + Dt - Phi;
+      b[q] = -(Am[q] + dfm[q]) * aleft / (2. * vol);
+      c[q] = -(Ap[q] - dfp[q]) * aright / (2. * vol);
+    }
+    // reflecting boundaries: a += b * diag(1,-1,1,1,1) at is, c * ... at ie
+    if (i == is || i == ie) {
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        if ((side == 0 && i != is) || (side == 1 && i != ie)) continue;
+        const double* m = side == 0 ? b : c;
+        double t[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          double acc = m[0] * (q == 0 ? 1. : 0.);
+#pragma unroll
+          for (int k = 1; k < 5; ++k) acc += m[k] * (q == k ? (k == IVX ? -1. : 1.) : 0.);
+          t[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) a[q] += t[q];
+      }
+    }
+    double rhs = DU(i, r);
+    rhs /= dt;
+    // t = a - b * Aprev (at i = is: t = a)
+    double t[5];
+    if (i == is) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) t[q] = a[q];
+    } else {
+      double ba[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          double ak = shfl(Aprev[q], base + k);  // Aprev(k, q)
+          if (k == 0) ba[q] = b[0] * ak;
+          else ba[q] += b[k] * ak;
+        }
+#pragma unroll
+      for (int q = 0; q < 5; ++q) t[q] = a[q] - ba[q];
+    }
+    // Gauss-Jordan with partial pivoting on [t | I], one row per lane
+    double inv[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) inv[q] = (q == r) ? 1. : 0.;
+#pragma unroll
+    for (int cc = 0; cc < 5; ++cc) {
+      double col[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) col[k] = shfl(t[cc], base + k);
+      int piv = cc;
+      double best = fabs(col[cc]);
+#pragma unroll
+      for (int k = cc + 1; k < 5; ++k)
+        if (fabs(col[k]) > best) { best = fabs(col[k]); piv = k; }
+      int src = (r == cc) ? piv : (r == piv ? cc : r);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        t[q] = shfl(t[q], base + src);
+        inv[q] = shfl(inv[q], base + src);
+      }
+      if (r == cc) {
+        double d = 1.0 / t[cc];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { t[q] *= d; inv[q] *= d; }
+      }
+      double pt[5], pi[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        pt[q] = shfl(t[q], base + cc);
+        pi[q] = shfl(inv[q], base + cc);
+      }
+      if (r != cc) {
+        double f = t[cc];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { t[q] -= f * pt[q]; inv[q] -= f * pi[q]; }
+      }
+    }
+    // delta_i = A (rhs - b delta_{i-1})
+    double x = rhs;
+    if (i != is) {
+      double bd = 0.;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double dk = shfl(dprev, base + k);
+        if (k == 0) bd = b[0] * dk;
+        else bd += b[k] * dk;
+      }
+      x = rhs - bd;
+    }
+    double dl = 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      double xk = shfl(x, base + k);
+      if (k == 0) dl = inv[0] * xk;
+      else dl += inv[k] * xk;
+    }
+    // A_i c_i for the back substitution
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double ck = shfl(c[q], base + k);  // c(k, q)
+        if (k == 0) Aprev[q] = inv[0] * ck;
+        else Aprev[q] += inv[k] * ck;
+      }
+    dprev = dl;
+    int lev = i - is;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) SCR(lev, q) = Aprev[q];
+    SCR(lev, 5) = dl;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) { Am[q] = Ap[q]; dfm[q] = df0[q]; df0[q] = dfp[q]; }
+  }
+  double dnext = 0.;
+  for (int i = ie; i >= is; --i) {
+    int lev = i - is;
+    double dl = SCR(lev, 5);
+    if (i < ie) {
+      double ad = 0.;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double dk = shfl(dnext, base + k);
+        if (k == 0) ad = SCR(lev, 0) * dk;
+        else ad += SCR(lev, k) * dk;
+      }
+      dl -= ad;
+    }
+    dnext = dl;
+    double all[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) all[k] = shfl(dl, base + k);
+    OUT(i, all);
+  }
+}
+
+// UpdateAllConserved on the last stage with NVAPOR = NCLOUD = 0: the
+// AirParcel round trip MassConc -> MoleFrac -> MassConc of one cell
+// (impl.cpp:138-304, air_parcel.cpp:190-278)
+__device__ __forceinline__ void airparcel_round_trip(double* uu, double Rd, double gammad) {
+  const double Rgas = 8.314462;  // src/constants.hpp:5
+  double mu0 = Rgas / Rd;
+  double inv_mu0 = 1. / (mu0 * 1.);
+  double cv0 = 1. * (Rd / (gammad - 1.));
+  double w[5];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) w[n] = uu[n];
+  double rho = 0., cvt = 0.;
+  rho += w[0];
+  cvt += w[0] * cv0;
+  double KE = 0.5 / rho * (sqr(w[IVX]) + sqr(w[IVY]) + sqr(w[IVZ]));
+  double tem = (w[IEN] - KE) / cvt;
+  w[IEN] = cvt * tem;
+  {
+    double r2 = 0., cv = 0., rhoR = 0.;
+    r2 += w[0];
+    cv += w[0] * cv0;
+    rhoR += w[0] * Rgas * inv_mu0;
+    double di = 1. / r2;
+    w[IDN] = w[IEN] / cv;
+    w[IPR] = rhoR * w[IDN];
+    w[IVX] *= di; w[IVY] *= di; w[IVZ] *= di;
+  }
+  {
+    double tt = w[IDN], sum = 1., gg = 1.;
+    double r2 = w[IPR] * sum / (Rd * tt * gg);
+    w[IDN] = r2;
+    w[IEN] = 0.;
+    w[IEN] += w[IDN] * cv0 * tt;
+    w[IVX] *= r2; w[IVY] *= r2; w[IVZ] *= r2;
+  }
+  double r2 = 0.;
+  r2 += w[0];
+  double vx = w[IVX] / r2, vy = w[IVY] / r2, vz = w[IVZ] / r2;
+  double e = w[IEN] + 0.5 * w[0] * (sqr(vx) + sqr(vy) + sqr(vz));
+#pragma unroll
+  for (int n = 0; n < 4; ++n) uu[n] = w[n];
+  uu[IEN] = e;
+}
+
+// Lane layout of the implicit kernels: 6 columns per warp, 5 lanes each
+// (lanes 30 and 31 idle).  Lanes of columns beyond ncol compute on the last
+// column and store nothing.
+struct ColumnLanes {
+  int col, r, base;
+  bool active;
+};
+__device__ __forceinline__ ColumnLanes column_lanes(int ncol) {
+  int lane = threadIdx.x & 31;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int g = lane / 5;
+  ColumnLanes c;
+  c.r = lane - 5 * g;
+  c.base = 5 * g;
+  int col = warp * 6 + g;
+  c.active = (g < 6) && (col < ncol);
+  c.col = col < ncol ? col : ncol - 1;
+  if (g == 6) { c.r = 0; c.base = 30; }
+  return c;
+}
+
+// One radial column of the stepping context: solve, then u += du and, on
+// the last stage, the AirParcel round trip.
+__global__ void __launch_bounds__(128) k_implicit(DevView v, int stage, double* scratch) {
+  int ncol = 6 * v.N * v.N;
+  ColumnLanes cl = column_lanes(ncol);
+  int col = cl.col, r = cl.r;
+  int j = v.js + col % v.N;
+  int k = v.ks + (col / v.N) % v.N;
+  int p = col / (v.N * v.N);
+  const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
+  double dt = kBeta[stage] * v.sc->dt;
+  size_t nslot = (size_t)ncol * 5;
+  size_t slot = (size_t)col * 5 + r;
+  double dummy = 0.;
+  auto W = [&](int i, double* out) {
+    for (int n = 0; n < 5; ++n) out[n] = v.w[idx(v, p, n, k, j, i)];
+  };
+  auto DU = [&](int i, int n) { return n < 5 ? v.du[idx(v, p, n, k, j, i)] : 0.; };
+  auto SCR = [&](int lev, int e) -> double& {
+    return cl.active ? scratch[((size_t)lev * 6 + e) * nslot + slot] : dummy;
+  };
+  auto OUT = [&](int i, const double* dl) {
+    if (!cl.active) return;
+    double uu[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uu[n] = v.u[idx(v, p, n, k, j, i)] + 1. * dl[n];
+    if (stage == 2) airparcel_round_trip(uu, v.Rd, v.gamma);
+    v.u[idx(v, p, r, k, j, i)] = uu[r];
+  };
+  implicit_column_rows(cl.base, r, W, DU, SCR, OUT, geo(v, GCOSC, p, k, j),
+                       geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j),
+                       v.x1f, v.x1v, v.dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+}
+
+// last-stage round trip when the implicit solver is off
+__global__ void k_roundtrip(DevView v) {
+  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned L = v.L, N = v.N;
+  if (tid >= 6u * N * N * L) return;
+  int i = v.is + (int)(tid % L);
+  unsigned r = tid / L;
+  int j = v.js + (int)(r % N);
+  r /= N;
+  int k = v.ks + (int)(r % N);
+  int p = (int)(r / N);
+  double uu[5];
+  for (int n = 0; n < 5; ++n) uu[n] = v.u[idx(v, p, n, k, j, i)];
+  airparcel_round_trip(uu, v.Rd, v.gamma);
+  for (int n = 0; n < 5; ++n) v.u[idx(v, p, n, k, j, i)] = uu[n];
+}
+
+__global__ void k_p2c(DevView v, const double* wsrc) {
+  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned L = v.L, N = v.N;
+  if (tid >= 6u * N * N * L) return;
+  int i = v.is + (int)(tid % L);
+  unsigned r = tid / L;
+  int j = v.js + (int)(r % N);
+  r /= N;
+  int k = v.ks + (int)(r % N);
+  int p = (int)(r / N);
+  double w[5], c[5];
+  for (int n = 0; n < v.nv; ++n) w[n] = wsrc[idx(v, p, n, k, j, i)];
+  prim_to_cons(v, w, c, geo(v, GCOSC, p, k, j));
+  for (int n = 0; n < v.nv; ++n) v.u[idx(v, p, n, k, j, i)] = c[n];
+}
+
+__global__ void k_set_dt(DevScalars* sc, double dt) { sc->dt = dt; }
+
+__global__ void k_dt_reset(DevScalars* sc) {
+  sc->dtmin_bits = 0x7FEFFFFFFFFFFFFFull;  // DBL_MAX
+}
+
+// Mesh::NewTimeStep: dt = min(2 dt, cfl * min over cells); advance time
+__global__ void k_dt_finalize(DevScalars* sc, double cfl, double dt_fixed, int advance,
+                              int first) {
+  if (advance) {
+    sc->time += sc->dt;
+    sc->ncycle += 1;
+  }
+  if (dt_fixed > 0.) {
+    sc->dt = dt_fixed;
+    return;
+  }
+  double nd = cfl * __longlong_as_double((long long)sc->dtmin_bits);
+  sc->dt = first ? nd : fmin(2.0 * sc->dt, nd);
+}
+inline int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : EXO_ERR_CUDA;
+}
+
+inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream) {
+  size_t total = (size_t)6 * v.cells;
+  k_prim_ghost<<<nblk(total, 256), 256, 0, (cudaStream_t)stream>>>(v, compute_dt ? 1 : 0);
+  return check_launch();
+}
+
+int launch_flux_x1(const DevView& v, void* stream) {
+  if (v.eqn == EXO_EQN_SHALLOW_YZ) return 0;
+  int threads = ((v.L + 1 + 31) / 32) * 32;
+  if (threads > 256) threads = 256;
+  size_t smem = ((size_t)v.nv * v.nc1 + v.nc1 + 1) * sizeof(double);
+  k_flux_x1<EXO_FLUX_T><<<6 * v.N * v.N, threads, smem, (cudaStream_t)stream>>>(v);
+  return check_launch();
+}
+
+int launch_flux_x23(const DevView& v, void* stream) {
+  size_t total = (size_t)2 * 6 * v.N * (v.N + 1) * v.L;
+  k_flux_x23<EXO_FLUX_T><<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v);
+  return check_launch();
+}
+
+int launch_update(const DevView& v, int stage, void* stream) {
+  size_t total = (size_t)6 * v.N * v.N * v.L;
+  k_update<EXO_FLUX_T><<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v, stage);
+  int rc = check_launch();
+  if (rc) return rc;
+  if (v.eqn != EXO_EQN_SHALLOW_YZ && !(v.implicit_flag & 1) && stage == 2) {
+    k_roundtrip<<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v);
+    rc = check_launch();
+  }
+  return rc;
+}
+
+int launch_implicit(const DevView& v, int stage, void* stream) {
+  if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
+  int ncol = 6 * v.N * v.N;
+  size_t threads = (size_t)((ncol + 5) / 6) * 32;
+  k_implicit<<<nblk(threads, 128), 128, 0, (cudaStream_t)stream>>>(v, stage, v.scratch);
+  return check_launch();
+}
+
+int launch_dt_reset(const DevView& v, void* stream) {
+  k_dt_reset<<<1, 1, 0, (cudaStream_t)stream>>>(v.sc);
+  return check_launch();
+}
+
+int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream) {
+  k_dt_finalize<<<1, 1, 0, (cudaStream_t)stream>>>(v.sc, v.cfl, dt_fixed, advance_time ? 1 : 0,
+                                                   advance_time ? 0 : 1);
+  return check_launch();
+}
+
+int launch_set_dt(const DevView& v, double dt, void* stream) {
+  k_set_dt<<<1, 1, 0, (cudaStream_t)stream>>>(v.sc, dt);
+  return check_launch();
+}
+
+int launch_p2c_interior(const DevView& v, const double* w_src, void* stream) {
+  size_t total = (size_t)6 * v.N * v.N * v.L;
+  k_p2c<<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v, w_src);
+  return check_launch();
+}
+
+}  // namespace EXO_KNS
+}  // namespace exo
