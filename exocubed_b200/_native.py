@@ -27,6 +27,10 @@ EXPORTED = [
     "exo_get_time", "exo_check_state", "exo_synchronize",
     "exo_calculate_fluxes", "exo_get_flux", "exo_riemann", "exo_weno5",
     "exo_get_stream", "exo_profile", "exo_profile_read", "exo_launch_count",
+    "exo_ensemble_create", "exo_ensemble_destroy", "exo_ensemble_footprint",
+    "exo_ensemble_add", "exo_ensemble_remove", "exo_ensemble_step",
+    "exo_ensemble_synchronize", "exo_ensemble_get_conserved", "exo_ensemble_get_primitive",
+    "exo_ensemble_member_time", "exo_ensemble_stats", "exo_ensemble_get_stream",
     "exo_implicit_columns", "exo_implicit_columns_noalloc",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
@@ -98,6 +102,21 @@ def lib():
     L.exo_weno5.argtypes = [i, p, p, p, p, p, p, p]
     L.exo_implicit_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
     L.exo_implicit_columns_noalloc.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p]
+    sz = ctypes.c_size_t
+    L.exo_ensemble_create.argtypes = [i, i, sz, ctypes.POINTER(p)]
+    L.exo_ensemble_destroy.argtypes = [p]
+    L.exo_ensemble_destroy.restype = None
+    L.exo_ensemble_footprint.argtypes = [cfgp, ctypes.POINTER(sz)]
+    L.exo_ensemble_add.argtypes = [p, cfgp, dp, ctypes.POINTER(i)]
+    L.exo_ensemble_remove.argtypes = [p, i]
+    L.exo_ensemble_step.argtypes = [p, i]
+    L.exo_ensemble_synchronize.argtypes = [p]
+    L.exo_ensemble_get_conserved.argtypes = [p, i, dp]
+    L.exo_ensemble_get_primitive.argtypes = [p, i, dp]
+    L.exo_ensemble_member_time.argtypes = [p, i, dp, dp, ctypes.POINTER(ctypes.c_int64)]
+    L.exo_ensemble_stats.argtypes = [p, ctypes.POINTER(i), ctypes.POINTER(sz),
+                                     ctypes.POINTER(ctypes.c_int64)]
+    L.exo_ensemble_get_stream.argtypes = [p, ctypes.POINTER(p)]
     L.exo_get_stream.argtypes = [p, ctypes.POINTER(p)]
     L.exo_profile.argtypes = [p, i]
     L.exo_profile_read.argtypes = [p, i, ctypes.POINTER(ctypes.c_int64), dp]

@@ -150,6 +150,175 @@ static int one_step(exo_ctx* c, double dt_fixed) {
                [&] { return STEP(launch_dt_finalize, v, dt_fixed, true, c->stream); });
 }
 
+namespace exo {
+
+bool validate_config(const exo_config& c, std::string* err) {
+  auto bad = [&](const char* m) { *err = m; return false; };
+  if (c.eqn != EXO_EQN_SHALLOW_YZ && c.eqn != EXO_EQN_IDEAL) return bad("unknown equation set");
+  bool shallow = c.eqn == EXO_EQN_SHALLOW_YZ;
+  if (shallow && c.rsolver != EXO_RS_ROE_SHALLOW && c.rsolver != EXO_RS_LMARS_SHALLOW)
+    return bad("shallow water needs the Roe or LMARS shallow-water solver");
+  if (!shallow && c.rsolver != EXO_RS_LMARS && c.rsolver != EXO_RS_HLLC)
+    return bad("the ideal gas needs the LMARS or HLLC solver");
+  if (c.precision != EXO_PREC_FP64 && c.precision != EXO_PREC_MIXED)
+    return bad("precision must be EXO_PREC_FP64 or EXO_PREC_MIXED");
+  if (!shallow && (c.implicit_flag & ~9))
+    return bad("implicit_flag: only bits 1 (x1) and 8 (full 5x5) are supported");
+  if (!shallow && (c.implicit_flag & 1) && !(c.implicit_flag & 8))
+    return bad("implicit_flag 1 (partial 3x3 correction) is not available; use 9");
+  if (!(c.cfl > 0.) || !(c.gamma > 1.) || !(c.x1max > c.x1min))
+    return bad("cfl, gamma or x1 range out of range");
+  if (c.N < 6 || (c.N % 2) != 0) return bad("N must be even and >= 6");
+  if (c.L < 1 || c.L > 250) return bad("L must be in [1, 250]");
+  return true;
+}
+
+size_t view_footprint(const exo_config& c) {
+  bool shallow = c.eqn == EXO_EQN_SHALLOW_YZ;
+  size_t nv = shallow ? 4 : 5;
+  size_t nc1 = c.L + 2 * G, nc2 = c.N + 2 * G;
+  size_t elems = 6 * nv * nc1 * nc2 * nc2;
+  size_t nd = shallow ? 5 : 7;  // u, w, u1, flux x2, x3 (+ du, flux x1)
+  size_t bytes = nd * elems * sizeof(double);
+  if (!shallow && (c.implicit_flag & 1)) bytes += (size_t)6 * c.N * c.N * c.L * 30 * sizeof(double);
+  if (c.precision == EXO_PREC_MIXED) bytes += (shallow ? 3 : 4) * elems * sizeof(float);
+  bytes += (size_t)NGEO2D * 6 * nc2 * nc2 * sizeof(double);       // metric
+  bytes += (size_t)6 * nc2 * nc2 * sizeof(int);                   // ghost map
+  bytes += (size_t)6 * 12 * c.N * sizeof(GhostEntry) + (size_t)24 * c.N * sizeof(EdgeEntry);
+  bytes += 3 * (nc1 + 1) * sizeof(double) + sizeof(DevScalars);
+  return bytes;
+}
+
+// Allocates and fills the device side of one atmosphere.  stream == nullptr:
+// cudaMalloc; otherwise stream-ordered allocation on that stream, from `pool`
+// when given (the ensemble's pool).
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
+                  std::vector<void*>& owned, void* stream_v, void* pool_v, std::string* err) {
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  cudaMemPool_t pool = (cudaMemPool_t)pool_v;
+  bool shallow = cfg.eqn == EXO_EQN_SHALLOW_YZ;
+  std::memset(&v, 0, sizeof(v));
+  v.N = cfg.N;
+  v.L = cfg.L;
+  v.nv = shallow ? 4 : 5;
+  v.nc1 = t.nc1;
+  v.nc2 = t.nc2;
+  v.nc3 = t.nc3;
+  v.is = v.js = v.ks = G;
+  v.ie = G + cfg.L - 1;
+  v.je = v.ke = G + cfg.N - 1;
+  v.eqn = cfg.eqn;
+  v.rsolver = cfg.rsolver;
+  v.implicit_flag = shallow ? 0 : cfg.implicit_flag;
+  v.coriolis = cfg.coriolis;
+  v.precision = cfg.precision;
+  v.gamma = cfg.gamma;
+  v.Rd = cfg.Rd;
+  v.grav = shallow ? 0. : cfg.grav;
+  v.cfl = cfg.cfl;
+  v.cells = (size_t)t.nc3 * t.nc2 * t.nc1;
+  size_t elems = (size_t)6 * v.nv * v.cells;
+  auto alloc = [&](void** p, size_t bytes, bool zero) -> bool {
+    cudaError_t e = stream ? (pool ? cudaMallocFromPoolAsync(p, bytes, pool, stream)
+                                   : cudaMallocAsync(p, bytes, stream))
+                           : cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+      *err = std::string("device allocation: ") + cudaGetErrorString(e);
+      return false;
+    }
+    owned.push_back(*p);
+    if (zero) {
+      e = stream ? cudaMemsetAsync(*p, 0, bytes, stream) : cudaMemset(*p, 0, bytes);
+      if (e != cudaSuccess) {
+        *err = std::string("cudaMemset: ") + cudaGetErrorString(e);
+        return false;
+      }
+    }
+    return true;
+  };
+  auto put = [&](void** p, const void* src, size_t bytes) -> bool {
+    if (!alloc(p, bytes ? bytes : 8, false)) return false;
+    if (!bytes) return true;
+    cudaError_t e = stream ? cudaMemcpyAsync(*p, src, bytes, cudaMemcpyHostToDevice, stream)
+                           : cudaMemcpy(*p, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      *err = std::string("table upload: ") + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  };
+  size_t db = elems * sizeof(double), fb = elems * sizeof(float);
+  if (!alloc((void**)&v.u, db, true) || !alloc((void**)&v.w, db, true) ||
+      !alloc((void**)&v.u1, db, true) || !alloc((void**)&v.flux[1], db, true) ||
+      !alloc((void**)&v.flux[2], db, true))
+    return EXO_ERR_CAPACITY;
+  if (!shallow) {
+    if (!alloc((void**)&v.du, db, true) || !alloc((void**)&v.flux[0], db, true))
+      return EXO_ERR_CAPACITY;
+    if ((v.implicit_flag & 1) &&
+        !alloc((void**)&v.scratch, (size_t)6 * cfg.N * cfg.N * cfg.L * 30 * sizeof(double), false))
+      return EXO_ERR_CAPACITY;
+  }
+  if (cfg.precision == EXO_PREC_MIXED) {
+    if (!alloc((void**)&v.w32, fb, true) || !alloc((void**)&v.flux32[1], fb, true) ||
+        !alloc((void**)&v.flux32[2], fb, true))
+      return EXO_ERR_CAPACITY;
+    if (!shallow && !alloc((void**)&v.flux32[0], fb, true)) return EXO_ERR_CAPACITY;
+  }
+  void *x1f, *x1v, *dx1f, *geo, *gmap, *gh, *ed;
+  if (!put(&x1f, t.x1f.data(), t.x1f.size() * sizeof(double)) ||
+      !put(&x1v, t.x1v.data(), t.x1v.size() * sizeof(double)) ||
+      !put(&dx1f, t.dx1f.data(), t.dx1f.size() * sizeof(double)) ||
+      !put(&geo, t.geo.data(), t.geo.size() * sizeof(double)) ||
+      !put(&gmap, t.ghost_map.data(), t.ghost_map.size() * sizeof(int)) ||
+      !put(&gh, t.ghost.data(), t.ghost.size() * sizeof(GhostEntry)) ||
+      !put(&ed, t.edge.data(), t.edge.size() * sizeof(EdgeEntry)))
+    return EXO_ERR_CAPACITY;
+  v.x1f = (const double*)x1f;
+  v.x1v = (const double*)x1v;
+  v.dx1f = (const double*)dx1f;
+  v.geo = (const double*)geo;
+  v.ghost_map = (const int*)gmap;
+  v.ghost = (const GhostEntry*)gh;
+  v.edge = (const EdgeEntry*)ed;
+  if (!alloc((void**)&v.sc, sizeof(DevScalars), true)) return EXO_ERR_CAPACITY;
+  // tables must stay alive until the (possibly asynchronous) uploads finish
+  cudaError_t e = stream ? cudaStreamSynchronize(stream) : cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    *err = std::string("upload: ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
+  return 0;
+}
+
+void view_free(std::vector<void*>& owned, void* stream_v) {
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  for (void* p : owned) {
+    if (stream) cudaFreeAsync(p, stream);
+    else cudaFree(p);
+  }
+  owned.clear();
+}
+
+void member_blocks(const DevView& v, unsigned b[BK_COUNT]) {
+  bool shallow = v.eqn == EXO_EQN_SHALLOW_YZ;
+  bool implicit = !shallow && (v.implicit_flag & 1);
+  auto nb = [](size_t n, int t) { return (unsigned)((n + t - 1) / t); };
+  b[BK_X1] = shallow ? 0u : (unsigned)(6 * v.N * v.N);
+  b[BK_X23] = nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, 128);
+  b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, 128);
+  b[BK_IMPLICIT] = implicit ? nb((size_t)((6 * v.N * v.N + 5) / 6) * 32, 128) : 0u;
+  b[BK_PRIM] = nb((size_t)6 * v.cells, 256);
+  b[BK_ROUNDTRIP] = (!shallow && !implicit) ? nb((size_t)6 * v.N * v.N * v.L, 128) : 0u;
+}
+
+}  // namespace exo
+
 extern "C" {
 
 const char* exo_last_error(void) { return g_err.c_str(); }
@@ -196,21 +365,10 @@ int exo_config_default(exo_config* cfg, int eqn) {
 int exo_create(const exo_config* cfg, exo_ctx** out) {
   if (!cfg || !out) return fail(EXO_ERR_ARG, "NULL argument");
   *out = nullptr;
-  if (cfg->eqn != EXO_EQN_SHALLOW_YZ && cfg->eqn != EXO_EQN_IDEAL)
-    return fail(EXO_ERR_ARG, "unknown equation set");
-  bool shallow = cfg->eqn == EXO_EQN_SHALLOW_YZ;
-  if (shallow && cfg->rsolver != EXO_RS_ROE_SHALLOW && cfg->rsolver != EXO_RS_LMARS_SHALLOW)
-    return fail(EXO_ERR_ARG, "shallow water needs the Roe or LMARS shallow-water solver");
-  if (!shallow && cfg->rsolver != EXO_RS_LMARS && cfg->rsolver != EXO_RS_HLLC)
-    return fail(EXO_ERR_ARG, "the ideal gas needs the LMARS or HLLC solver");
-  if (cfg->precision != EXO_PREC_FP64 && cfg->precision != EXO_PREC_MIXED)
-    return fail(EXO_ERR_ARG, "precision must be EXO_PREC_FP64 or EXO_PREC_MIXED");
-  if (!shallow && (cfg->implicit_flag & ~9))
-    return fail(EXO_ERR_ARG, "implicit_flag: only bits 1 (x1) and 8 (full 5x5) are supported");
-  if (!shallow && (cfg->implicit_flag & 1) && !(cfg->implicit_flag & 8))
-    return fail(EXO_ERR_ARG, "implicit_flag 1 (partial 3x3 correction) is not available; use 9");
-  if (!(cfg->cfl > 0.) || !(cfg->gamma > 1.) || !(cfg->x1max > cfg->x1min))
-    return fail(EXO_ERR_ARG, "cfl, gamma or x1 range out of range");
+  {
+    std::string verr;
+    if (!exo::validate_config(*cfg, &verr)) return fail(EXO_ERR_ARG, verr);
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(EXO_ERR_NOGPU, "no CUDA device");
@@ -232,84 +390,11 @@ int exo_create(const exo_config* cfg, exo_ctx** out) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup(fail(EXO_ERR_CUDA, "cudaStreamCreate failed"));
 
-  DevView& v = c->v;
-  std::memset(&v, 0, sizeof(v));
-  const exo::HostTables& t = c->tab;
-  v.N = cfg->N;
-  v.L = cfg->L;
-  v.nv = shallow ? 4 : 5;
-  v.nc1 = t.nc1;
-  v.nc2 = t.nc2;
-  v.nc3 = t.nc3;
-  v.is = v.js = v.ks = exo::G;
-  v.ie = exo::G + cfg->L - 1;
-  v.je = v.ke = exo::G + cfg->N - 1;
-  v.eqn = cfg->eqn;
-  v.rsolver = cfg->rsolver;
-  v.implicit_flag = shallow ? 0 : cfg->implicit_flag;
-  v.coriolis = cfg->coriolis;
-  v.precision = cfg->precision;
-  v.gamma = cfg->gamma;
-  v.Rd = cfg->Rd;
-  v.grav = shallow ? 0. : cfg->grav;
-  v.cfl = cfg->cfl;
-  v.cells = (size_t)t.nc3 * t.nc2 * t.nc1;
-  c->state_elems = (size_t)6 * v.nv * v.cells;
-  size_t bytes = c->state_elems * sizeof(double);
-
-  double** arrays[] = {&v.u, &v.w, &v.u1, &v.flux[1], &v.flux[2]};
-  for (double** a : arrays) {
-    cudaError_t e = cudaMalloc((void**)a, bytes);
-    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(state)"));
-    c->owned.push_back(*a);
-    cudaMemset(*a, 0, bytes);
-  }
-  if (!shallow) {
-    double** more[] = {&v.du, &v.flux[0]};
-    for (double** a : more) {
-      cudaError_t e = cudaMalloc((void**)a, bytes);
-      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(state)"));
-      c->owned.push_back(*a);
-      cudaMemset(*a, 0, bytes);
-    }
-    if (v.implicit_flag & 1) {
-      size_t sbytes = (size_t)6 * cfg->N * cfg->N * cfg->L * 30 * sizeof(double);
-      cudaError_t e = cudaMalloc((void**)&v.scratch, sbytes);
-      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(implicit scratch)"));
-      c->owned.push_back(v.scratch);
-    }
-  }
-  if (cfg->precision == EXO_PREC_MIXED) {
-    size_t fbytes = c->state_elems * sizeof(float);
-    float** f32[] = {&v.w32, &v.flux32[0], &v.flux32[1], &v.flux32[2]};
-    for (float** a : f32) {
-      if (a == &v.flux32[0] && shallow) continue;
-      cudaError_t e = cudaMalloc((void**)a, fbytes);
-      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(fp32 arrays)"));
-      c->owned.push_back(*a);
-      cudaMemset(*a, 0, fbytes);
-    }
-  }
-  double *x1f, *x1v, *dx1f, *geo;
-  int* gmap;
-  exo::GhostEntry* gh;
-  exo::EdgeEntry* ed;
-  if (upload(&x1f, t.x1f, c->owned) || upload(&x1v, t.x1v, c->owned) ||
-      upload(&dx1f, t.dx1f, c->owned) || upload(&geo, t.geo, c->owned) ||
-      upload(&gmap, t.ghost_map, c->owned) || upload(&gh, t.ghost, c->owned) ||
-      upload(&ed, t.edge, c->owned))
-    return cleanup(EXO_ERR_CUDA);
-  v.x1f = x1f;
-  v.x1v = x1v;
-  v.dx1f = dx1f;
-  v.geo = geo;
-  v.ghost_map = gmap;
-  v.ghost = gh;
-  v.edge = ed;
-  cudaError_t e = cudaMalloc((void**)&v.sc, sizeof(DevScalars));
-  if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(scalars)"));
-  c->owned.push_back(v.sc);
-  cudaMemset(v.sc, 0, sizeof(DevScalars));
+  std::string aerr;
+  int rc = exo::view_allocate(*cfg, c->tab, c->v, c->owned, nullptr, nullptr, &aerr);
+  if (rc) return cleanup(fail(rc, aerr));
+  c->state_elems = (size_t)6 * c->v.nv * c->v.cells;
+  cudaError_t e;
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "exo_create"));
   *out = c;

@@ -110,6 +110,20 @@ struct DevView {
   DevScalars* sc;
 };
 
+// A batched step: every member's DevView in device memory and, per kernel
+// kind, the first block of every member (start[k][n] = total blocks).
+enum BatchKind { BK_X1 = 0, BK_X23, BK_UPDATE, BK_IMPLICIT, BK_PRIM, BK_ROUNDTRIP, BK_COUNT };
+struct BatchPlan {
+  const DevView* views;          // device, n entries
+  int n;
+  const unsigned* start[BK_COUNT];  // device, n+1 entries each
+  unsigned total[BK_COUNT];
+  int x1_threads;                // block size of the x1 flux kernel
+  size_t x1_smem;                // its dynamic shared memory
+};
+// block counts of one member, as the single-atmosphere launchers use them
+void member_blocks(const DevView& v, unsigned blocks[BK_COUNT]);
+
 // Launchers of one arithmetic build (exo_kernels.cuh): fp64 (kernels.cu) and
 // mixed (kernels_mixed.cu) provide the same set.
 #define EXO_DECLARE_STEP_LAUNCHERS                                                   \
@@ -121,7 +135,8 @@ struct DevView {
   int launch_dt_reset(const DevView& v, void* stream);                               \
   int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream); \
   int launch_set_dt(const DevView& v, double dt, void* stream);                      \
-  int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);
+  int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);          \
+  int launch_batched_step(const BatchPlan& plan, void* stream);
 namespace fp64 { EXO_DECLARE_STEP_LAUNCHERS }
 namespace mixed { EXO_DECLARE_STEP_LAUNCHERS }
 #undef EXO_DECLARE_STEP_LAUNCHERS
@@ -141,6 +156,14 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
                                     const double* dx1f, double dt, double gamma, double grav,
                                     void* stream, std::string* err);
 
+
+// capi.cpp: shared by the single-atmosphere context and the ensemble
+bool validate_config(const exo_config& cfg, std::string* err);
+size_t view_footprint(const exo_config& cfg);
+int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
+                  std::vector<void*>& owned, void* stream, void* pool, std::string* err);
+int set_error(int code, const std::string& msg);
+void view_free(std::vector<void*>& owned, void* stream);
 
 // cell (U,V) <-> panel vector transforms of cubed_sphere_transform.cpp:11-61
 // written as coefficient quadruples: out0 = c0*in0 + c1*in1, out1 = c2*in0 + c3*in1

@@ -454,10 +454,35 @@ __device__ __forceinline__ void load_cons(const DevView& v, int p, int k, int j,
   c[IVZ] = vzt + vyt * e.ct;
 }
 
-__global__ void k_prim_ghost(DevView v, int compute_dt) {
-  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+// the CFL candidate of the block's cells is reduced in shared memory first,
+// so one atomic per block reaches the global minimum
+__device__ __forceinline__ void block_min_atomic(unsigned long long* target, unsigned long long x) {
+  __shared__ unsigned long long warp_min[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long y = __shfl_down_sync(0xffffffffu, x, o);
+    x = y < x ? y : x;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_min[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    x = lane < nw ? warp_min[lane] : ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long y = __shfl_down_sync(0xffffffffu, x, o);
+      x = y < x ? y : x;
+    }
+    if (lane == 0 && x != ~0ull) atomicMin(target, x);
+  }
+}
+
+__device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, unsigned tid,
+                                                              int compute_dt) {
+  const unsigned long long none = ~0ull;
   unsigned total = 6u * (unsigned)v.cells;
-  if (tid >= total) return;
+  if (tid >= total) return none;
   unsigned i = tid % (unsigned)v.nc1;
   unsigned r = tid / (unsigned)v.nc1;
   int j = (int)(r % (unsigned)v.nc2);
@@ -465,7 +490,7 @@ __global__ void k_prim_ghost(DevView v, int compute_dt) {
   int k = (int)(r % (unsigned)v.nc3);
   int p = (int)(r / (unsigned)v.nc3);
   bool kin = (k >= v.ks && k <= v.ke), jin = (j >= v.js && j <= v.je);
-  if (!kin && !jin) return;  // corner: never read on the path
+  if (!kin && !jin) return none;  // corner: never read on the path
   int ii = i;
   bool mirror = false;
   if (i < v.is) { ii = 2 * v.is - 1 - i; mirror = true; }
@@ -479,7 +504,7 @@ __global__ void k_prim_ghost(DevView v, int compute_dt) {
 #if EXO_MIXED
   for (int n = 0; n < v.nv; ++n) v.w32[idx(v, p, n, k, j, i)] = (float)w[n];
 #endif
-  if (!(kin && jin) || mirror) return;
+  if (!(kin && jin) || mirror) return none;
   if (bad) atomicOr(&v.sc->invalid, 1);
   if (compute_dt) {
     // Hydro::NewBlockTimeStep with patches/21.new_blockdt.patch:23-35
@@ -503,16 +528,23 @@ __global__ void k_prim_ghost(DevView v, int compute_dt) {
     else dt3 /= speed3;
     double m = fmin(dt2, dt3);
     if (!shallow) m = fmin(dt1, m);
-    if (m >= 0.) atomicMin(&v.sc->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+    if (m >= 0.) return (unsigned long long)__double_as_longlong(m);
   }
+  return none;
+}
+
+__device__ __forceinline__ void prim_ghost_block(const DevView& v, unsigned blk, int compute_dt) {
+  unsigned tid = blk * blockDim.x + threadIdx.x;
+  unsigned long long m = prim_ghost_cell(v, tid, compute_dt);
+  if (compute_dt) block_min_atomic(&v.sc->dtmin_bits, m);
 }
 
 // ------------------------------------------------------------ k_flux_x1 ---
 // One CTA per interior radial column.
 template <class T>
-__global__ void k_flux_x1(DevView v) {
+__device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
   extern __shared__ double sm[];
-  int col = blockIdx.x;
+  int col = blk;
   int j = v.js + col % v.N;
   int k = v.ks + (col / v.N) % v.N;
   int p = col / (v.N * v.N);
@@ -623,8 +655,8 @@ __device__ __forceinline__ void edge_outer_state(const DevView& v, int p, int si
 }
 
 template <class T>
-__global__ void k_flux_x23(DevView v) {
-  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
+  unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned nface = 6u * v.N * (v.N + 1) * v.L;  // per direction
   if (tid >= 2 * nface) return;
   int dir = tid < nface ? 1 : 2;
@@ -680,8 +712,8 @@ __global__ void k_flux_x23(DevView v) {
 
 // --------------------------------------------------------------- k_update -
 template <class T>
-__global__ void k_update(DevView v, int stage) {
-  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int stage) {
+  unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
   int i = v.is + (int)(tid % L);
@@ -861,10 +893,29 @@ __device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF 
   double fsig = 1., feps = 1.;
   double gmm1 = (gamma - 1.) * feps / fsig;
   double gm1 = 0.5 * (gmm1 + gmm1);
+#if EXO_MIXED
+  const double inv_gm1 = 1. / gm1, gp1_over_gm1 = (gm1 + 1.) / gm1, gm1_over_gp1 = gm1 / (gm1 + 1.);
+  const double gamma_eff = 1. + (gamma - 1) * feps / fsig;
+  const double inv_dt = 1. / dt;
+#endif
   // row r of the flux Jacobian dF/dq at a cell (flux_decomposition.hpp:100-120)
   auto fj_row = [&](const double* w, double* out) {
     double v1 = w[IVX], v2 = w[IVY], v3 = w[IVZ], rho = w[IDN], pres = w[IPR];
     double s2 = v1 * v1 + v2 * v2 + v3 * v3;
+#if EXO_MIXED
+    {  // same entries, divisions folded into one reciprocal, no divergent branches
+      double hr = gp1_over_gm1 * pres * (1. / rho);
+      double c1 = ((gmm1 - 1) * s2 * 0.5 - hr) * v1;
+      double c2 = hr + s2 * 0.5 - gmm1 * v1 * v1;
+      double e0 = r == 0 ? 0. : r == 1 ? gmm1 * s2 * 0.5 - v1 * v1 : r == 2 ? -v1 * v2 : r == 3 ? -v1 * v3 : c1;
+      double e1 = r == 0 ? 1. : r == 1 ? (2. - gmm1) * v1 : r == 2 ? v2 : r == 3 ? v3 : c2;
+      double e2 = r == 0 ? 0. : r == 1 ? -gmm1 * v2 : r == 2 ? v1 : r == 3 ? 0. : -gmm1 * v2 * v1;
+      double e3 = r == 0 ? 0. : r == 1 ? -gmm1 * v3 : r == 2 ? 0. : r == 3 ? v1 : -gmm1 * v3 * v1;
+      double e4 = r == 0 ? 0. : r == 1 ? gmm1 : r == 4 ? (gmm1 + 1) * v1 : 0.;
+      out[0] = e0; out[1] = e1; out[2] = e2; out[3] = e3; out[4] = e4;
+      return;
+    }
+#endif
     if (r == 0) {
       out[0] = 0; out[1] = 1.; out[2] = 0.; out[3] = 0.; out[4] = 0.;
     } else if (r == 1) {
@@ -884,6 +935,57 @@ __device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF 
   // row r of R |Lambda| R^-1 at the Roe average of a face
   auto absj_row = [&](const double* wl, const double* wr, double* out) {
     double prim[5];
+#if EXO_MIXED
+    {
+      // Roe average with shared reciprocals
+      double sqrtdl = sqrt(wl[IDN]), sqrtdr = sqrt(wr[IDN]);
+      double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+      double isl = isdlpdr / sqrtdl, isr = isdlpdr / sqrtdr;
+      prim[IDN] = sqrtdl * sqrtdr;
+      prim[IVX] = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
+      prim[IVY] = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
+      prim[IVZ] = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
+      double el = wl[IPR] * inv_gm1 + 0.5 * wl[IDN] * (sqr(wl[IVX]) + sqr(wl[IVY]) + sqr(wl[IVZ]));
+      double er = wr[IPR] * inv_gm1 + 0.5 * wr[IDN] * (sqr(wr[IVX]) + sqr(wr[IVY]) + sqr(wr[IVZ]));
+      double hbar = (el + wl[IPR]) * isl + (er + wr[IPR]) * isr;
+      prim[IPR] = (hbar - 0.5 * (sqr(prim[IVX]) + sqr(prim[IVY]) + sqr(prim[IVZ]))) * gm1_over_gp1 *
+                  prim[IDN];
+      double irr = 1. / prim[IDN];
+      double cs = sqrt(gamma_eff * prim[IPR] * irr);
+      double u = prim[IVX], v = prim[IVY], w = prim[IVZ], p = prim[IPR];
+      double ke = 0.5 * (u * u + v * v + w * w);
+      double hp = gp1_over_gm1 * p * irr;
+      double h = hp + ke;
+      double ihp = 1. / hp, i2hp = 0.5 * ihp, i2cshp = i2hp / cs;
+      double R0 = r == 0 ? 1. : r == 1 ? u - cs : r == 2 ? v : r == 3 ? w : h - u * cs;
+      double R1 = r == 0 ? 1. : r == 1 ? u : r == 2 ? v : r == 3 ? w : ke;
+      double R2 = r == 0 ? 1. : r == 1 ? u + cs : r == 2 ? v : r == 3 ? w : h + u * cs;
+      double R3 = r == 2 ? 1. : r == 4 ? v : 0.;
+      double R4 = r == 3 ? 1. : r == 4 ? w : 0.;
+      double Ri[5];
+      Ri[0] = r == 0 ? (cs * ke + u * hp) * i2cshp : r == 1 ? (hp - ke) * ihp
+            : r == 2 ? (cs * ke - u * hp) * i2cshp : r == 3 ? -v : -w;
+      Ri[1] = r == 0 ? (-hp - cs * u) * i2cshp : r == 1 ? u * ihp
+            : r == 2 ? (hp - cs * u) * i2cshp : 0.;
+      Ri[2] = r == 0 || r == 2 ? -v * i2hp : r == 1 ? v * ihp : r == 3 ? 1. : 0.;
+      Ri[3] = r == 0 || r == 2 ? -w * i2hp : r == 1 ? w * ihp : r == 4 ? 1. : 0.;
+      Ri[4] = r == 0 || r == 2 ? i2hp : r == 1 ? -ihp : 0.;
+      double lam0 = fabs(u - cs), lam1 = fabs(u), lam2 = fabs(u + cs);
+      double T[5] = {R0 * lam0, R1 * lam1, R2 * lam2, R3 * lam1, R4 * lam1};
+      double acc[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          double rik = shfl(Ri[c], base + k);
+          acc[c] = k == 0 ? T[0] * rik : acc[c] + T[k] * rik;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 5; ++c) out[c] = acc[c];
+      return;
+    }
+#endif
     roe_average(prim, gm1, wl, wr);
     double cs = sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
     double rr = prim[IDN], u = prim[IVX], v = prim[IVY], w = prim[IVZ], p = prim[IPR];
@@ -951,6 +1053,17 @@ __device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF 
     double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
     double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
     double a[5], b[5], c[5];
+#if EXO_MIXED
+    double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double Dt = (r == q) ? inv_dt : 0.;
+      double Phi = ((r == IVX && q == IDN) || (r == IEN && q == IVX)) ? grav : 0.;
+      a[q] = Am[q] * bl + Ap[q] * cr + dd * df0[q] + Dt - Phi;
+      b[q] = -(Am[q] + dfm[q]) * bl;
+      c[q] = -(Ap[q] - dfp[q]) * cr;
+    }
+#else
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       double Dt = (r == q) ? 1. / dt : 0.;
@@ -959,6 +1072,7 @@ __device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF 
       b[q] = -(Am[q] + dfm[q]) * aleft / (2. * vol);
       c[q] = -(Ap[q] - dfp[q]) * aright / (2. * vol);
     }
+#endif
     // reflecting boundaries: a += b * diag(1,-1,1,1,1) at is, c * ... at ie
     if (i == is || i == ie) {
 #pragma unroll
@@ -978,7 +1092,11 @@ __device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF 
       }
     }
     double rhs = DU(i, r);
+#if EXO_MIXED
+    rhs *= inv_dt;
+#else
     rhs /= dt;
+#endif
     // t = a - b * Aprev (at i = is: t = a)
     double t[5];
     if (i == is) {
@@ -1143,9 +1261,9 @@ struct ColumnLanes {
   int col, r, base;
   bool active;
 };
-__device__ __forceinline__ ColumnLanes column_lanes(int ncol) {
+__device__ __forceinline__ ColumnLanes column_lanes(int ncol, unsigned blk) {
   int lane = threadIdx.x & 31;
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int warp = (blk * blockDim.x + threadIdx.x) >> 5;
   int g = lane / 5;
   ColumnLanes c;
   c.r = lane - 5 * g;
@@ -1159,9 +1277,10 @@ __device__ __forceinline__ ColumnLanes column_lanes(int ncol) {
 
 // One radial column of the stepping context: solve, then u += du and, on
 // the last stage, the AirParcel round trip.
-__global__ void __launch_bounds__(128) k_implicit(DevView v, int stage, double* scratch) {
+__device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, int stage) {
+  double* scratch = v.scratch;
   int ncol = 6 * v.N * v.N;
-  ColumnLanes cl = column_lanes(ncol);
+  ColumnLanes cl = column_lanes(ncol, blk);
   int col = cl.col, r = cl.r;
   int j = v.js + col % v.N;
   int k = v.ks + (col / v.N) % v.N;
@@ -1192,8 +1311,8 @@ __global__ void __launch_bounds__(128) k_implicit(DevView v, int stage, double* 
 }
 
 // last-stage round trip when the implicit solver is off
-__global__ void k_roundtrip(DevView v) {
-  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void roundtrip_block(const DevView& v, unsigned blk) {
+  unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
   int i = v.is + (int)(tid % L);
@@ -1208,8 +1327,8 @@ __global__ void k_roundtrip(DevView v) {
   for (int n = 0; n < 5; ++n) v.u[idx(v, p, n, k, j, i)] = uu[n];
 }
 
-__global__ void k_p2c(DevView v, const double* wsrc) {
-  unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void p2c_block(const DevView& v, unsigned blk, const double* wsrc) {
+  unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
   int i = v.is + (int)(tid % L);
@@ -1244,6 +1363,114 @@ __global__ void k_dt_finalize(DevScalars* sc, double cfl, double dt_fixed, int a
   double nd = cfl * __longlong_as_double((long long)sc->dtmin_bits);
   sc->dt = first ? nd : fmin(2.0 * sc->dt, nd);
 }
+
+// ------------------------------------------------------------ wrappers ----
+// Each kernel body above works on one atmosphere and one block index of it.
+// The single-atmosphere kernels take the DevView by value; the batched ones
+// take a table of DevViews and, per launch, the first block of every member
+// (start[m], start[n] = total): block b belongs to the member m with
+// start[m] <= b < start[m+1] and works on its block b - start[m].  One
+// batched launch per kernel advances every member of an ensemble.
+struct Batch {
+  const DevView* views;
+  const unsigned* start;
+  int n;
+};
+
+__device__ __forceinline__ int batch_member(const Batch& bt, unsigned b) {
+  int lo = 0, hi = bt.n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (bt.start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// copies the member's view into shared memory; returns its local block
+__device__ __forceinline__ unsigned batch_enter(const Batch& bt, DevView& sv) {
+  __shared__ unsigned local;
+  if (threadIdx.x == 0) {
+    int m = batch_member(bt, blockIdx.x);
+    sv = bt.views[m];
+    local = blockIdx.x - bt.start[m];
+  }
+  __syncthreads();
+  return local;
+}
+
+__global__ void k_prim_ghost(DevView v, int compute_dt) { prim_ghost_block(v, blockIdx.x, compute_dt); }
+__global__ void kb_prim_ghost(Batch bt, int compute_dt) {
+  __shared__ DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  prim_ghost_block(sv, b, compute_dt);
+}
+
+template <class T>
+__global__ void k_flux_x1(DevView v) { flux_x1_block<T>(v, blockIdx.x); }
+template <class T>
+__global__ void kb_flux_x1(Batch bt) {
+  __shared__ DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  if (sv.eqn == EXO_EQN_SHALLOW_YZ) return;
+  flux_x1_block<T>(sv, b);
+}
+
+template <class T>
+__global__ void k_flux_x23(DevView v) { flux_x23_block<T>(v, blockIdx.x); }
+template <class T>
+__global__ void kb_flux_x23(Batch bt) {
+  __shared__ DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  flux_x23_block<T>(sv, b);
+}
+
+template <class T>
+__global__ void k_update(DevView v, int stage) { update_block<T>(v, blockIdx.x, stage); }
+template <class T>
+__global__ void kb_update(Batch bt, int stage) {
+  __shared__ DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  update_block<T>(sv, b, stage);
+}
+
+__global__ void __launch_bounds__(128) k_implicit(DevView v, int stage) {
+  implicit_block(v, blockIdx.x, stage);
+}
+__global__ void __launch_bounds__(128) kb_implicit(Batch bt, int stage) {
+  __shared__ DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
+  implicit_block(sv, b, stage);
+}
+
+__global__ void k_roundtrip(DevView v) { roundtrip_block(v, blockIdx.x); }
+__global__ void kb_roundtrip(Batch bt) {
+  __shared__ DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  if (sv.eqn == EXO_EQN_SHALLOW_YZ || (sv.implicit_flag & 1)) return;
+  roundtrip_block(sv, b);
+}
+
+__global__ void k_p2c(DevView v, const double* wsrc) { p2c_block(v, blockIdx.x, wsrc); }
+
+// time-step bookkeeping of every member (one thread per member)
+__global__ void kb_dt_reset(const DevView* views, int n) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n) views[m].sc->dtmin_bits = 0x7FEFFFFFFFFFFFFFull;
+}
+__global__ void kb_dt_finalize(const DevView* views, int n, int advance) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  DevScalars* sc = views[m].sc;
+  if (advance) {
+    sc->time += sc->dt;
+    sc->ncycle += 1;
+  }
+  double nd = views[m].cfl * __longlong_as_double((long long)sc->dtmin_bits);
+  sc->dt = advance ? fmin(2.0 * sc->dt, nd) : nd;
+}
+
 inline int check_launch() {
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? 0 : EXO_ERR_CUDA;
@@ -1290,7 +1517,7 @@ int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   int ncol = 6 * v.N * v.N;
   size_t threads = (size_t)((ncol + 5) / 6) * 32;
-  k_implicit<<<nblk(threads, 128), 128, 0, (cudaStream_t)stream>>>(v, stage, v.scratch);
+  k_implicit<<<nblk(threads, 128), 128, 0, (cudaStream_t)stream>>>(v, stage);
   return check_launch();
 }
 
@@ -1313,6 +1540,41 @@ int launch_set_dt(const DevView& v, double dt, void* stream) {
 int launch_p2c_interior(const DevView& v, const double* w_src, void* stream) {
   size_t total = (size_t)6 * v.N * v.N * v.L;
   k_p2c<<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v, w_src);
+  return check_launch();
+}
+
+// One SSPRK(3,3) step of every member of a batch: the stage sequence of
+// one_step() (capi.cpp) with each kernel launched once for all members.
+int launch_batched_step(const BatchPlan& pl, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (pl.n <= 0) return 0;
+  auto B = [&](int kind) { return Batch{pl.views, pl.start[kind], pl.n}; };
+  int rc;
+  for (int s = 0; s < 3; ++s) {
+    if (pl.total[BK_X1]) {
+      kb_flux_x1<EXO_FLUX_T><<<pl.total[BK_X1], pl.x1_threads, pl.x1_smem, st>>>(B(BK_X1));
+      if ((rc = check_launch())) return rc;
+    }
+    kb_flux_x23<EXO_FLUX_T><<<pl.total[BK_X23], 128, 0, st>>>(B(BK_X23));
+    if ((rc = check_launch())) return rc;
+    kb_update<EXO_FLUX_T><<<pl.total[BK_UPDATE], 128, 0, st>>>(B(BK_UPDATE), s);
+    if ((rc = check_launch())) return rc;
+    if (s == 2 && pl.total[BK_ROUNDTRIP]) {
+      kb_roundtrip<<<pl.total[BK_ROUNDTRIP], 128, 0, st>>>(B(BK_ROUNDTRIP));
+      if ((rc = check_launch())) return rc;
+    }
+    if (pl.total[BK_IMPLICIT]) {
+      kb_implicit<<<pl.total[BK_IMPLICIT], 128, 0, st>>>(B(BK_IMPLICIT), s);
+      if ((rc = check_launch())) return rc;
+    }
+    if (s == 2) {
+      kb_dt_reset<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n);
+      if ((rc = check_launch())) return rc;
+    }
+    kb_prim_ghost<<<pl.total[BK_PRIM], 256, 0, st>>>(B(BK_PRIM), s == 2 ? 1 : 0);
+    if ((rc = check_launch())) return rc;
+  }
+  kb_dt_finalize<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n, 1);
   return check_launch();
 }
 

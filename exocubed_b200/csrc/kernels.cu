@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(128) k_implicit_columns(int ncol, int L, const
                                                           const double* dx1f, double dt,
                                                           double gamma, double grav,
                                                           double* scratch) {
-  ColumnLanes cl = column_lanes(ncol);
+  ColumnLanes cl = column_lanes(ncol, blockIdx.x);
   int col = cl.col, r = cl.r;
   int nc1 = L + 2 * G;
   const double* wc = w + (size_t)col * 5 * nc1;

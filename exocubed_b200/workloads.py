@@ -121,3 +121,72 @@ def dry_atmosphere_state(cfg, seed=0, T0=250., ps=1e5, temp_sigma=1.0, wind_sigm
 def interior(a):
     """View of the interior cells of a (6, nvar, nc3, nc2, nc1) array."""
     return a[:, :, G:-G, G:-G, G:-G]
+
+
+ENSEMBLE_N = (24, 32, 48, 64, 96)
+ENSEMBLE_L = (32, 48, 64, 96)
+
+
+def _adiabat_isothermal(z, Ts, Ttop, g, Rd, gamma, ps):
+    """Dry adiabat from (Ts, ps) up to T = Ttop, isothermal above: the
+    analytic form of the column examples/2023-Chen-exo3/hs94.cpp:263-289
+    integrates level by level.  Returns (T, p) at heights z."""
+    cp = gamma / (gamma - 1.) * Rd
+    lapse = g / cp
+    zt = (Ts - Ttop) / lapse
+    T = np.where(z < zt, Ts - lapse * z, Ttop)
+    pt = ps * (Ttop / Ts) ** (cp / Rd)
+    p = np.where(z < zt, ps * (np.maximum(T, Ttop) / Ts) ** (cp / Rd),
+                 pt * np.exp(-g * (z - zt) / (Rd * Ttop)))
+    return T, p
+
+
+def ensemble_member_config(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
+                           ps=1e5, ptop=1e3, Rd=287.):
+    """Configuration of one forward-model run of the batched ensemble.
+    N ~ U{24,32,48,64,96}, L ~ U{32,48,64,96}, surface temperature
+    U[150,400] K, top temperature U[100,250] K (at most the surface's),
+    gravity U[3,25] m/s^2, gamma U[1.3,1.67]; the model top sits where the
+    profile reaches ptop.  Returns (config dict, profile parameters)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    N = int(rng.choice(ENSEMBLE_N))
+    L = int(rng.choice(ENSEMBLE_L))
+    Ts = rng.uniform(150., 400.)
+    Ttop = min(rng.uniform(100., 250.), Ts)
+    g = rng.uniform(3., 25.)
+    gamma = rng.uniform(1.3, 1.67)
+    cp = gamma / (gamma - 1.) * Rd
+    zt = (Ts - Ttop) / (g / cp)
+    pt = ps * (Ttop / Ts) ** (cp / Rd)
+    if pt <= ptop:
+        ztop = (Ts - Ts * (ptop / ps) ** (Rd / cp)) / (g / cp)
+    else:
+        ztop = zt + Rd * Ttop / g * math.log(pt / ptop)
+    cfg = dict(N=N, L=L, eqn=nat.EXO_EQN_IDEAL, rsolver=rsolver, implicit_flag=9,
+               precision=precision, coriolis=nat.EXO_CORIOLIS_NONE, x1min=6.371e6,
+               x1max=6.371e6 + ztop, gamma=gamma, Rd=Rd, grav=-g, cfl=0.4, omega=0.)
+    return cfg, dict(Ts=Ts, Ttop=Ttop, ps=ps)
+
+
+def ensemble_member(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
+                    temp_sigma=1.0, wind_sigma=5.0, **kw):
+    """One forward-model run of the batched ensemble: (config dict, primitive
+    array) for ensemble_member_config(seed); temperature and wind noise as in
+    dry_atmosphere_state, drawn from a generator seeded by (seed, 1)."""
+    cfg, prof = ensemble_member_config(seed, precision, rsolver, **kw)
+    c = make_config(**cfg)
+    N, L, Rd, g = c.N, c.L, c.Rd, -c.grav
+    rng = np.random.Generator(np.random.PCG64([seed, 1]))
+    lat, lon, m, x1v = cell_geometry(c)
+    T0, p = _adiabat_isothermal(x1v - c.x1min, prof["Ts"], prof["Ttop"], g, Rd, c.gamma,
+                                prof["ps"])
+    T = T0[None, None, None, :] + temp_sigma * rng.standard_normal((6, N, N, L))
+    U = wind_sigma * rng.standard_normal((6, N, N, L))
+    V = wind_sigma * rng.standard_normal((6, N, N, L))
+    w = np.zeros((6, 5, N + 2 * G, N + 2 * G, L + 2 * G))
+    sl = (slice(None), slice(G, G + N), slice(G, G + N), slice(G, G + L))
+    w[:, 4][sl] = p[None, None, None, :]
+    w[:, 0][sl] = p[None, None, None, :] / (Rd * T)
+    w[:, 2][sl] = m[..., 0, None] * U + m[..., 1, None] * V
+    w[:, 3][sl] = m[..., 2, None] * U + m[..., 3, None] * V
+    return cfg, w

@@ -251,6 +251,47 @@ int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
 int exo_weno5(int n, const double* a, const double* b, const double* c,
               const double* d, const double* e, double* out, void* stream);
 
+/* ------------------------------------------------------------- ensembles */
+
+/* A batch of independent atmospheres of uneven size (different N, L, gas,
+   gravity, solver) advanced together: every kernel of a step is launched
+   once for all members and the step is one CUDA graph.  This is the
+   forward-model workload of the reference's MCMC inversion
+   (src/inversion/profile_inversion.cpp:112-120), which the reference runs as
+   one atmosphere per process.  Members are admitted against a device-memory
+   budget (bytes) and a slot capacity; their memory comes from the
+   ensemble's own stream-ordered pool.  All members share one precision. */
+typedef struct exo_ensemble exo_ensemble;
+
+int exo_ensemble_create(int precision, int capacity, size_t budget_bytes,
+                        exo_ensemble** out);
+void exo_ensemble_destroy(exo_ensemble* ens);
+
+/* Device bytes one member of this configuration holds (state, scratch,
+   tables); host only. */
+int exo_ensemble_footprint(const exo_config* cfg, size_t* bytes);
+
+/* Admit a member with the primitive initial state w_host (layout as for
+   exo_set_primitive).  EXO_ERR_CAPACITY if no slot is free or its footprint
+   does not fit the remaining budget.  *slot receives its slot index. */
+int exo_ensemble_add(exo_ensemble* ens, const exo_config* cfg, const double* w_host,
+                     int* slot);
+int exo_ensemble_remove(exo_ensemble* ens, int slot);
+
+/* Advance every member nsteps SSPRK(3,3) steps, each with its own CFL time
+   step (asynchronous; exo_ensemble_synchronize waits). */
+int exo_ensemble_step(exo_ensemble* ens, int nsteps);
+int exo_ensemble_synchronize(exo_ensemble* ens);
+
+int exo_ensemble_get_conserved(exo_ensemble* ens, int slot, double* u_host);
+int exo_ensemble_get_primitive(exo_ensemble* ens, int slot, double* w_host);
+int exo_ensemble_member_time(exo_ensemble* ens, int slot, double* time, double* dt,
+                             int64_t* ncycle);
+/* Members admitted, device bytes held by them, kernel launches issued. */
+int exo_ensemble_stats(exo_ensemble* ens, int* members, size_t* bytes_in_use,
+                       int64_t* launches);
+int exo_ensemble_get_stream(exo_ensemble* ens, void** stream);
+
 #ifdef __cplusplus
 }
 #endif
