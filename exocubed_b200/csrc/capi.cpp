@@ -312,7 +312,7 @@ void member_blocks(const DevView& v, unsigned b[BK_COUNT]) {
   b[BK_X1] = shallow ? 0u : (unsigned)(6 * v.N * v.N);
   b[BK_X23] = nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, 128);
   b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, 128);
-  b[BK_IMPLICIT] = implicit ? nb((size_t)((6 * v.N * v.N + 5) / 6) * 32, 128) : 0u;
+  b[BK_IMPLICIT] = implicit ? nb((size_t)6 * v.N * v.N, 64) : 0u;  // one thread per column
   b[BK_PRIM] = nb((size_t)6 * v.cells, 256);
   b[BK_ROUNDTRIP] = (!shallow && !implicit) ? nb((size_t)6 * v.N * v.N * v.L, 128) : 0u;
 }

@@ -23,6 +23,8 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
+#include <utility>
 
 #include <cuda_runtime.h>
 
@@ -857,356 +859,480 @@ __device__ __forceinline__ void roe_average(double* prim, double gm1, const doub
               (gm1 + 1.) * prim[IDN];
 }
 
+// Structural non-zeros of the X1 flux Jacobian dF/dq (flux_decomposition.hpp:
+// 100-120): row 0 = e_1; rows 2 and 3 carry three entries each.
+__host__ __device__ constexpr bool fj_nz(int r, int q) {
+  return r == 1 || r == 4 || (r == 0 && q == 1) || (r == 2 && q <= 2) ||
+         (r == 3 && (q <= 1 || q == 3));
+}
+// structural non-zeros of R (right eigenvectors, columns) and R^-1 (rows)
+__host__ __device__ constexpr bool r_nz(int r, int c) {
+  return c < 3 || (r == 2 && c == 3) || (r == 3 && c == 4) || r == 4;
+}
+__host__ __device__ constexpr bool ri_nz(int r, int c) {
+  return r < 3 || c == 0 || (r == 3 && c == 2) || (r == 4 && c == 3);
+}
+
+// One cell of a column, velocities projected (v2 += v3 cos, v3 *= sin): the
+// primitives and the two derived quantities of its flux Jacobian.
+struct ColCell {
+  double rho, v1, v2, v3, p, s2, hr;  // s2 = |v|^2, hr = (g+1)/g * p/rho (g = gamma-1)
+};
+
+// entry (r, q) of dF/dq at a cell, in the reference's expression order
+template <int r, int q>
+__device__ __forceinline__ double fj_entry(const ColCell& c, double gm1) {
+  if constexpr (r == 0) return 1.;
+  else if constexpr (r == 1) {
+    if constexpr (q == 0) return gm1 * c.s2 / 2 - c.v1 * c.v1;
+    else if constexpr (q == 1) return (2. - gm1) * c.v1;
+    else if constexpr (q == 2) return -gm1 * c.v2;
+    else if constexpr (q == 3) return -gm1 * c.v3;
+    else return gm1;
+  } else if constexpr (r == 2) {
+    if constexpr (q == 0) return -c.v1 * c.v2;
+    else if constexpr (q == 1) return c.v2;
+    else return c.v1;
+  } else if constexpr (r == 3) {
+    if constexpr (q == 0) return -c.v1 * c.v3;
+    else if constexpr (q == 1) return c.v3;
+    else return c.v1;
+  } else {
+    if constexpr (q == 0) return ((gm1 - 1) * c.s2 / 2 - c.hr) * c.v1;
+    else if constexpr (q == 1) return c.hr + c.s2 / 2 - gm1 * c.v1 * c.v1;
+    else if constexpr (q == 2) return -gm1 * c.v2 * c.v1;
+    else if constexpr (q == 3) return -gm1 * c.v3 * c.v1;
+    else return (gm1 + 1) * c.v1;
+  }
+}
+
+// compile-time loops (the matrix entries live in registers, so every index
+// has to be a constant)
+template <int N, class F, int... I>
+__device__ __forceinline__ void unroll_impl(F&& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void unroll(F&& f) {
+  unroll_impl<N>(f, std::make_integer_sequence<int, N>{});
+}
+
+// |A| = R |Lambda| R^-1 at the Roe average of a face (flux_decomposition.hpp:
+// 34-98).  Exact build: the reference's products R*Lambda and (R*Lambda)*R^-1
+// summed in its order, skipping only terms that are structurally zero (the
+// value is the same; at most the sign of an exact zero differs).  Mixed
+// build: the same matrix as |u| I + (|u-c|-|u|) r0 l0^T + (|u+c|-|u|) r2 l2^T
+// (the three |u| eigenvalues coincide), with shared reciprocals.
+__device__ __forceinline__ void abs_jacobian(const ColCell& L, const ColCell& R_, double gm1,
+                                             double gamma, double A[5][5]) {
+  double wl[5] = {L.rho, L.v1, L.v2, L.v3, L.p};
+  double wr[5] = {R_.rho, R_.v1, R_.v2, R_.v3, R_.p};
+#if EXO_MIXED
+  double sqrtdl = sqrt(wl[IDN]), sqrtdr = sqrt(wr[IDN]);
+  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
+  double isl = isdlpdr / sqrtdl, isr = isdlpdr / sqrtdr;
+  double rr = sqrtdl * sqrtdr;
+  double u = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
+  double v = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
+  double w = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
+  double inv_gm1 = 1. / gm1;
+  double el = wl[IPR] * inv_gm1 + 0.5 * wl[IDN] * L.s2;
+  double er = wr[IPR] * inv_gm1 + 0.5 * wr[IDN] * R_.s2;
+  double hbar = (el + wl[IPR]) * isl + (er + wr[IPR]) * isr;
+  double ke = 0.5 * (u * u + v * v + w * w);
+  double p = (hbar - ke) * (gm1 / (gm1 + 1.)) * rr;
+  double irr = 1. / rr;
+  double cs = sqrt(gamma * p * irr);
+  double hp = (gm1 + 1.) * inv_gm1 * p * irr;
+  double h = hp + ke;
+  double ihp = 1. / hp, i2hp = 0.5 * ihp, i2cshp = i2hp / cs;
+  double au = fabs(u), al = fabs(u - cs) - au, ar = fabs(u + cs) - au;
+  double l0[5] = {al * (cs * ke + u * hp) * i2cshp, al * (-hp - cs * u) * i2cshp, -al * v * i2hp,
+                  -al * w * i2hp, al * i2hp};
+  double l2[5] = {ar * (cs * ke - u * hp) * i2cshp, ar * (hp - cs * u) * i2cshp, -ar * v * i2hp,
+                  -ar * w * i2hp, ar * i2hp};
+  double r0[5] = {1., u - cs, v, w, h - u * cs};
+  double r2[5] = {1., u + cs, v, w, h + u * cs};
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) A[r][c] = (r == c ? au : 0.) + r0[r] * l0[c] + r2[r] * l2[c];
+#else
+  double prim[5];
+  roe_average(prim, gm1, wl, wr);
+  double fsig = 1., feps = 1.;
+  double cs = sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
+  double rr = prim[IDN], u = prim[IVX], v = prim[IVY], w = prim[IVZ], p = prim[IPR];
+  double ke = 0.5 * (u * u + v * v + w * w);
+  double hp = (gm1 + 1.) / gm1 * p / rr;
+  double h = hp + ke;
+  const double Rm[5][5] = {{1., 1., 1., 0., 0.},
+                           {u - cs, u, u + cs, 0., 0.},
+                           {v, v, v, 1., 0.},
+                           {w, w, w, 0., 1.},
+                           {h - u * cs, ke, h + u * cs, v, w}};
+  double mv2 = -v / (2. * hp), mw2 = -w / (2. * hp), i2 = 1. / (2. * hp);
+  const double Ri[5][5] = {
+      {(cs * ke + u * hp) / (2. * cs * hp), (-hp - cs * u) / (2. * cs * hp), mv2, mw2, i2},
+      {(hp - ke) / hp, u / hp, v / hp, w / hp, -1. / hp},
+      {(cs * ke - u * hp) / (2. * cs * hp), (hp - cs * u) / (2. * cs * hp), mv2, mw2, i2},
+      {-v, 0., 1., 0., 0.},
+      {-w, 0., 0., 1., 0.}};
+  const double lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double s = 0.;
+      bool first = true;
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if (r_nz(r, k) && ri_nz(k, c)) {
+          double term = (Rm[r][k] * lam[k]) * Ri[k][c];
+          s = first ? term : s + term;
+          first = false;
+        }
+      A[r][c] = s;
+    }
+#endif
+}
+
 // The vertical 5x5 block-tridiagonal correction of one radial column
 // (ImplicitSolver::SolveImplicit3D X1 branch, solve_implicit_3d.cpp:102-179,
 // with FullCorrection, full_correction.cpp:32-165, and ForwardSweep /
-// BackwardSubstitution, forward_backward.hpp:15-126), spread over the five
-// lanes base..base+4 of a warp: lane base+r holds row r of every 5x5 block
-// and component r of every vector.  Each lane evaluates exactly the sums of
-// the single-thread formulation (same terms, same order), so the result is
-// the same to the bit; the lanes exchange rows through warp shuffles.
-//   W(i, w5)     primitive state of level i (i in [is-1, ie+1])
-//   DU(i, n)     explicit update of level i, variable n
-//   SCR(lev, e)  6 scratch doubles of this lane per level: row r of A_i*c_i
-//                (5) and delta_i(r), written by the forward sweep and read
-//                back by the back substitution
-//   OUT(i, dl)   corrected update of level i (all 5 components), ie down to is
-// geo: cos/sin of the cell metric and the angular widths dx2f_ang, dx3f_ang.
-// All 32 lanes of the warp must call this together (full-mask shuffles).
-__device__ __forceinline__ double shfl(double x, int lane) {
-  return __shfl_sync(0xffffffffu, x, lane);
-}
-
-template <class WF, class DUF, class SCRF, class OUTF>
-__device__ __forceinline__ void implicit_column_rows(int base, int r, WF W, DUF DU, SCRF SCR,
-                                                     OUTF OUT, double cos_theta, double sin_theta,
-                                                     double d2, double d3, const double* x1f,
-                                                     const double* x1v, const double* dx1f,
-                                                     int is, int ie, double dt, double gamma,
-                                                     double grav) {
-  double s = sin_theta;
-  auto load = [&](int i, double* out) {
-    W(i, out);
-    out[IVY] += out[IVZ] * cos_theta;
-    out[IVZ] *= sin_theta;
-  };
-  double fsig = 1., feps = 1.;
-  double gmm1 = (gamma - 1.) * feps / fsig;
-  double gm1 = 0.5 * (gmm1 + gmm1);
+// BackwardSubstitution, forward_backward.hpp:15-126), one thread per column.
+//
+// Per level the forward sweep builds the rows of a_i, b_i, c_i from the two
+// face Jacobians |A|(i-1/2), |A|(i+1/2) and the three cell Jacobians, forms
+// t = a_i - b_i (A c)_{i-1} and x = du_i/dt - b_i delta_{i-1} row by row,
+// then
+//   exact build: inverts t by Gauss-Jordan with partial pivoting (the
+//                reference's inverse) and multiplies, every sum in the
+//                reference's order: the result is the CPU restatement's to
+//                the bit;
+//   mixed build: solves t [X | y] = [c_i | x] by LU with partial pivoting.
+// (A c)_i (25) and delta_i (5) go to scratch for the back substitution.  The
+// face Jacobian |A|(i+1/2) waits in this thread's slice of shared memory
+// until it becomes |A|(i-1/2) of the next level.
+//   io.w(i, out[5])  primitives of level i (is-1 .. ie+2), unprojected
+//   io.du(i, n)      explicit update of level i
+//   io.scr(lev, e)   scratch double e (0..29) of level lev = i - is
+//   io.out(i, d[5])  corrected update of level i, from ie down to is
+//   sm               this thread's 50 doubles of shared memory, stride sms
+template <class IO>
+__device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, double cos_theta,
+                                                double sin_theta, double d2, double d3,
+                                                const double* x1f, const double* x1v,
+                                                const double* dx1f, int is, int ie, double dt,
+                                                double gamma, double grav) {
+  const double s = sin_theta;
+  const double gm1 = (gamma - 1.) * 1. / 1.;  // gmm1 of every cell; the face average equals it
+  const double gp = (gm1 + 1.) / gm1;
 #if EXO_MIXED
-  const double inv_gm1 = 1. / gm1, gp1_over_gm1 = (gm1 + 1.) / gm1, gm1_over_gp1 = gm1 / (gm1 + 1.);
-  const double gamma_eff = 1. + (gamma - 1) * feps / fsig;
-  const double inv_dt = 1. / dt;
-#endif
-  // row r of the flux Jacobian dF/dq at a cell (flux_decomposition.hpp:100-120)
-  auto fj_row = [&](const double* w, double* out) {
-    double v1 = w[IVX], v2 = w[IVY], v3 = w[IVZ], rho = w[IDN], pres = w[IPR];
-    double s2 = v1 * v1 + v2 * v2 + v3 * v3;
-#if EXO_MIXED
-    {  // same entries, divisions folded into one reciprocal, no divergent branches
-      double hr = gp1_over_gm1 * pres * (1. / rho);
-      double c1 = ((gmm1 - 1) * s2 * 0.5 - hr) * v1;
-      double c2 = hr + s2 * 0.5 - gmm1 * v1 * v1;
-      double e0 = r == 0 ? 0. : r == 1 ? gmm1 * s2 * 0.5 - v1 * v1 : r == 2 ? -v1 * v2 : r == 3 ? -v1 * v3 : c1;
-      double e1 = r == 0 ? 1. : r == 1 ? (2. - gmm1) * v1 : r == 2 ? v2 : r == 3 ? v3 : c2;
-      double e2 = r == 0 ? 0. : r == 1 ? -gmm1 * v2 : r == 2 ? v1 : r == 3 ? 0. : -gmm1 * v2 * v1;
-      double e3 = r == 0 ? 0. : r == 1 ? -gmm1 * v3 : r == 2 ? 0. : r == 3 ? v1 : -gmm1 * v3 * v1;
-      double e4 = r == 0 ? 0. : r == 1 ? gmm1 : r == 4 ? (gmm1 + 1) * v1 : 0.;
-      out[0] = e0; out[1] = e1; out[2] = e2; out[3] = e3; out[4] = e4;
-      return;
-    }
-#endif
-    if (r == 0) {
-      out[0] = 0; out[1] = 1.; out[2] = 0.; out[3] = 0.; out[4] = 0.;
-    } else if (r == 1) {
-      out[0] = gmm1 * s2 / 2 - v1 * v1; out[1] = (2. - gmm1) * v1; out[2] = -gmm1 * v2;
-      out[3] = -gmm1 * v3; out[4] = gmm1;
-    } else if (r == 2) {
-      out[0] = -v1 * v2; out[1] = v2; out[2] = v1; out[3] = 0.; out[4] = 0.;
-    } else if (r == 3) {
-      out[0] = -v1 * v3; out[1] = v3; out[2] = 0.; out[3] = v1; out[4] = 0.;
-    } else {
-      double c1 = ((gmm1 - 1) * s2 / 2 - (gmm1 + 1) / gmm1 * pres / rho) * v1;
-      double c2 = (gmm1 + 1) / gmm1 * pres / rho + s2 / 2 - gmm1 * v1 * v1;
-      out[0] = c1; out[1] = c2; out[2] = -gmm1 * v2 * v1; out[3] = -gmm1 * v3 * v1;
-      out[4] = (gmm1 + 1) * v1;
-    }
-  };
-  // row r of R |Lambda| R^-1 at the Roe average of a face
-  auto absj_row = [&](const double* wl, const double* wr, double* out) {
-    double prim[5];
-#if EXO_MIXED
-    {
-      // Roe average with shared reciprocals
-      double sqrtdl = sqrt(wl[IDN]), sqrtdr = sqrt(wr[IDN]);
-      double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
-      double isl = isdlpdr / sqrtdl, isr = isdlpdr / sqrtdr;
-      prim[IDN] = sqrtdl * sqrtdr;
-      prim[IVX] = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
-      prim[IVY] = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
-      prim[IVZ] = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
-      double el = wl[IPR] * inv_gm1 + 0.5 * wl[IDN] * (sqr(wl[IVX]) + sqr(wl[IVY]) + sqr(wl[IVZ]));
-      double er = wr[IPR] * inv_gm1 + 0.5 * wr[IDN] * (sqr(wr[IVX]) + sqr(wr[IVY]) + sqr(wr[IVZ]));
-      double hbar = (el + wl[IPR]) * isl + (er + wr[IPR]) * isr;
-      prim[IPR] = (hbar - 0.5 * (sqr(prim[IVX]) + sqr(prim[IVY]) + sqr(prim[IVZ]))) * gm1_over_gp1 *
-                  prim[IDN];
-      double irr = 1. / prim[IDN];
-      double cs = sqrt(gamma_eff * prim[IPR] * irr);
-      double u = prim[IVX], v = prim[IVY], w = prim[IVZ], p = prim[IPR];
-      double ke = 0.5 * (u * u + v * v + w * w);
-      double hp = gp1_over_gm1 * p * irr;
-      double h = hp + ke;
-      double ihp = 1. / hp, i2hp = 0.5 * ihp, i2cshp = i2hp / cs;
-      double R0 = r == 0 ? 1. : r == 1 ? u - cs : r == 2 ? v : r == 3 ? w : h - u * cs;
-      double R1 = r == 0 ? 1. : r == 1 ? u : r == 2 ? v : r == 3 ? w : ke;
-      double R2 = r == 0 ? 1. : r == 1 ? u + cs : r == 2 ? v : r == 3 ? w : h + u * cs;
-      double R3 = r == 2 ? 1. : r == 4 ? v : 0.;
-      double R4 = r == 3 ? 1. : r == 4 ? w : 0.;
-      double Ri[5];
-      Ri[0] = r == 0 ? (cs * ke + u * hp) * i2cshp : r == 1 ? (hp - ke) * ihp
-            : r == 2 ? (cs * ke - u * hp) * i2cshp : r == 3 ? -v : -w;
-      Ri[1] = r == 0 ? (-hp - cs * u) * i2cshp : r == 1 ? u * ihp
-            : r == 2 ? (hp - cs * u) * i2cshp : 0.;
-      Ri[2] = r == 0 || r == 2 ? -v * i2hp : r == 1 ? v * ihp : r == 3 ? 1. : 0.;
-      Ri[3] = r == 0 || r == 2 ? -w * i2hp : r == 1 ? w * ihp : r == 4 ? 1. : 0.;
-      Ri[4] = r == 0 || r == 2 ? i2hp : r == 1 ? -ihp : 0.;
-      double lam0 = fabs(u - cs), lam1 = fabs(u), lam2 = fabs(u + cs);
-      double T[5] = {R0 * lam0, R1 * lam1, R2 * lam2, R3 * lam1, R4 * lam1};
-      double acc[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-          double rik = shfl(Ri[c], base + k);
-          acc[c] = k == 0 ? T[0] * rik : acc[c] + T[k] * rik;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 5; ++c) out[c] = acc[c];
-      return;
-    }
-#endif
-    roe_average(prim, gm1, wl, wr);
-    double cs = sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
-    double rr = prim[IDN], u = prim[IVX], v = prim[IVY], w = prim[IVZ], p = prim[IPR];
-    double ke = 0.5 * (u * u + v * v + w * w);
-    double hp = (gm1 + 1.) / gm1 * p / rr;
-    double h = hp + ke;
-    double R[5];
-    if (r == 0) { R[0] = 1.; R[1] = 1.; R[2] = 1.; R[3] = 0.; R[4] = 0.; }
-    else if (r == 1) { R[0] = u - cs; R[1] = u; R[2] = u + cs; R[3] = 0.; R[4] = 0.; }
-    else if (r == 2) { R[0] = v; R[1] = v; R[2] = v; R[3] = 1.; R[4] = 0.; }
-    else if (r == 3) { R[0] = w; R[1] = w; R[2] = w; R[3] = 0.; R[4] = 1.; }
-    else { R[0] = h - u * cs; R[1] = ke; R[2] = h + u * cs; R[3] = v; R[4] = w; }
-    double Ri[5];  // row r of R^-1
-    if (r == 0) {
-      Ri[0] = (cs * ke + u * hp) / (2. * cs * hp); Ri[1] = (-hp - cs * u) / (2. * cs * hp);
-      Ri[2] = -v / (2. * hp); Ri[3] = -w / (2. * hp); Ri[4] = 1. / (2. * hp);
-    } else if (r == 1) {
-      Ri[0] = (hp - ke) / hp; Ri[1] = u / hp; Ri[2] = v / hp; Ri[3] = w / hp; Ri[4] = -1. / hp;
-    } else if (r == 2) {
-      Ri[0] = (cs * ke - u * hp) / (2. * cs * hp); Ri[1] = (hp - cs * u) / (2. * cs * hp);
-      Ri[2] = -v / (2. * hp); Ri[3] = -w / (2. * hp); Ri[4] = 1. / (2. * hp);
-    } else if (r == 3) {
-      Ri[0] = -v; Ri[1] = 0.; Ri[2] = 1.; Ri[3] = 0.; Ri[4] = 0.;
-    } else {
-      Ri[0] = -w; Ri[1] = 0.; Ri[2] = 0.; Ri[3] = 1.; Ri[4] = 0.;
-    }
-    double lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
-    double T[5];  // row r of R * Lambda, summed as a full product
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      double acc = R[0] * (c == 0 ? lam[0] : 0.);
-#pragma unroll
-      for (int k = 1; k < 5; ++k) acc += R[k] * (c == k ? lam[k] : 0.);
-      T[c] = acc;
-    }
-    double acc[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) {
-        double rik = shfl(Ri[c], base + k);  // (R^-1)(k, c)
-        if (k == 0) acc[c] = T[0] * rik;
-        else acc[c] += T[k] * rik;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 5; ++c) out[c] = acc[c];
-  };
-
-  double wl[5], wr[5];
-  double Am[5], Ap[5], dfm[5], df0[5], dfp[5];
-  load(is - 1, wl);
-  load(is, wr);
-  fj_row(wl, dfm);
-  fj_row(wr, df0);
-  absj_row(wl, wr, Am);
-  double Aprev[5], dprev = 0.;
-  for (int i = is; i <= ie; ++i) {
-#pragma unroll
-    for (int n = 0; n < 5; ++n) wl[n] = wr[n];
-    load(i + 1, wr);
-    fj_row(wr, dfp);
-    absj_row(wl, wr, Ap);
-    double aleft = d2 * d3 * x1f[i] * x1f[i] * s;
-    double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
-    double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
-    double a[5], b[5], c[5];
-#if EXO_MIXED
-    double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      double Dt = (r == q) ? inv_dt : 0.;
-      double Phi = ((r == IVX && q == IDN) || (r == IEN && q == IVX)) ? grav : 0.;
-      a[q] = Am[q] * bl + Ap[q] * cr + dd * df0[q] + Dt - Phi;
-      b[q] = -(Am[q] + dfm[q]) * bl;
-      c[q] = -(Ap[q] - dfp[q]) * cr;
-    }
+  const double rdt = 1. / dt;
 #else
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      double Dt = (r == q) ? 1. / dt : 0.;
-      double Phi = ((r == IVX && q == IDN) || (r == IEN && q == IVX)) ? grav : 0.;
-      a[q] = (Am[q] * aleft + Ap[q] * aright + (aright - aleft) * df0[q]) / (2. * vol) + Dt - Phi;
-      b[q] = -(Am[q] + dfm[q]) * aleft / (2. * vol);
-      c[q] = -(Ap[q] - dfp[q]) * aright / (2. * vol);
-    }
+  const double rdt = 1. / dt;  // the reference's Dt = 1/dt, the same value every time
 #endif
-    // reflecting boundaries: a += b * diag(1,-1,1,1,1) at is, c * ... at ie
-    if (i == is || i == ie) {
-#pragma unroll
-      for (int side = 0; side < 2; ++side) {
-        if ((side == 0 && i != is) || (side == 1 && i != ie)) continue;
-        const double* m = side == 0 ? b : c;
-        double t[5];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          double acc = m[0] * (q == 0 ? 1. : 0.);
-#pragma unroll
-          for (int k = 1; k < 5; ++k) acc += m[k] * (q == k ? (k == IVX ? -1. : 1.) : 0.);
-          t[q] = acc;
-        }
-#pragma unroll
-        for (int q = 0; q < 5; ++q) a[q] += t[q];
-      }
-    }
-    double rhs = DU(i, r);
+  auto cell = [&](const double* w) {
+    ColCell c;
+    c.rho = w[IDN];
+    c.v1 = w[IVX];
+    c.v2 = w[IVY] + w[IVZ] * cos_theta;
+    c.v3 = w[IVZ] * sin_theta;
+    c.p = w[IPR];
+    c.s2 = c.v1 * c.v1 + c.v2 * c.v2 + c.v3 * c.v3;
 #if EXO_MIXED
-    rhs *= inv_dt;
+    c.hr = gp * c.p * (1. / c.rho);
 #else
-    rhs /= dt;
+    c.hr = gp * c.p / c.rho;
 #endif
-    // t = a - b * Aprev (at i = is: t = a)
-    double t[5];
-    if (i == is) {
+    return c;
+  };
+  auto AMs = [&](int slot, int r, int q) -> double& { return sm[(slot * 25 + r * 5 + q) * sms]; };
+
+  double raw[5];
+  io.w(is - 1, raw);
+  ColCell cm = cell(raw);
+  io.w(is, raw);
+  ColCell c0 = cell(raw);
+  io.w(is + 1, raw);  // prefetched level: raw holds w(i+1) at the top of level i
+  {
+    double A[5][5];
+    abs_jacobian(cm, c0, gm1, gamma, A);
 #pragma unroll
-      for (int q = 0; q < 5; ++q) t[q] = a[q];
-    } else {
-      double ba[5];
+    for (int r = 0; r < 5; ++r)
 #pragma unroll
-      for (int k = 0; k < 5; ++k)
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          double ak = shfl(Aprev[q], base + k);  // Aprev(k, q)
-          if (k == 0) ba[q] = b[0] * ak;
-          else ba[q] += b[k] * ak;
-        }
-#pragma unroll
-      for (int q = 0; q < 5; ++q) t[q] = a[q] - ba[q];
-    }
-    // Gauss-Jordan with partial pivoting on [t | I], one row per lane
-    double inv[5];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) inv[q] = (q == r) ? 1. : 0.;
-#pragma unroll
-    for (int cc = 0; cc < 5; ++cc) {
-      double col[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) col[k] = shfl(t[cc], base + k);
-      int piv = cc;
-      double best = fabs(col[cc]);
-#pragma unroll
-      for (int k = cc + 1; k < 5; ++k)
-        if (fabs(col[k]) > best) { best = fabs(col[k]); piv = k; }
-      int src = (r == cc) ? piv : (r == piv ? cc : r);
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        t[q] = shfl(t[q], base + src);
-        inv[q] = shfl(inv[q], base + src);
-      }
-      if (r == cc) {
-        double d = 1.0 / t[cc];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) { t[q] *= d; inv[q] *= d; }
-      }
-      double pt[5], pi[5];
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        pt[q] = shfl(t[q], base + cc);
-        pi[q] = shfl(inv[q], base + cc);
-      }
-      if (r != cc) {
-        double f = t[cc];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) { t[q] -= f * pt[q]; inv[q] -= f * pi[q]; }
-      }
-    }
-    // delta_i = A (rhs - b delta_{i-1})
-    double x = rhs;
-    if (i != is) {
-      double bd = 0.;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        double dk = shfl(dprev, base + k);
-        if (k == 0) bd = b[0] * dk;
-        else bd += b[k] * dk;
-      }
-      x = rhs - bd;
-    }
-    double dl = 0.;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      double xk = shfl(x, base + k);
-      if (k == 0) dl = inv[0] * xk;
-      else dl += inv[k] * xk;
-    }
-    // A_i c_i for the back substitution
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        double ck = shfl(c[q], base + k);  // c(k, q)
-        if (k == 0) Aprev[q] = inv[0] * ck;
-        else Aprev[q] += inv[k] * ck;
-      }
-    dprev = dl;
-    int lev = i - is;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) SCR(lev, q) = Aprev[q];
-    SCR(lev, 5) = dl;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) { Am[q] = Ap[q]; dfm[q] = df0[q]; df0[q] = dfp[q]; }
+      for (int q = 0; q < 5; ++q) AMs(0, r, q) = A[r][q];
   }
-  double dnext = 0.;
-  for (int i = ie; i >= is; --i) {
-    int lev = i - is;
-    double dl = SCR(lev, 5);
+  double Ap[5][5], dp[5];  // (A c)_{i-1}, delta_{i-1}
+  double dun[5];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) dun[n] = io.du(is, n);
+  int cur = 0;
+  for (int i = is; i <= ie; ++i) {
+    ColCell cp = cell(raw);
+    double rhs[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) rhs[n] = dun[n];
+    io.w(i + 2, raw);  // prefetch for the next level
     if (i < ie) {
-      double ad = 0.;
 #pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        double dk = shfl(dnext, base + k);
-        if (k == 0) ad = SCR(lev, 0) * dk;
-        else ad += SCR(lev, k) * dk;
-      }
-      dl -= ad;
+      for (int n = 0; n < 5; ++n) dun[n] = io.du(i + 1, n);
     }
-    dnext = dl;
-    double all[5];
+    const int nxt = cur ^ 1;
+    {
+      double A[5][5];
+      abs_jacobian(c0, cp, gm1, gamma, A);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) all[k] = shfl(dl, base + k);
-    OUT(i, all);
+      for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) AMs(nxt, r, q) = A[r][q];
+    }
+    const double aleft = d2 * d3 * x1f[i] * x1f[i] * s;
+    const double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
+    const double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
+#if EXO_MIXED
+    const double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
+#endif
+    const bool first = (i == is), last = (i == ie);
+    double t[5][5], x[5];
+    // rows of a, b (and c at the top boundary), then t and x
+    unroll<5>([&](auto R) {
+      constexpr int r = decltype(R)::value;
+      double brow[5];
+      unroll<5>([&](auto Q) {
+        constexpr int q = decltype(Q)::value;
+        const double am = AMs(cur, r, q), ap = AMs(nxt, r, q);
+#if EXO_MIXED
+        double a = am * bl + ap * cr;
+        if constexpr (fj_nz(r, q)) a += dd * fj_entry<r, q>(c0, gm1);
+        if constexpr (r == q) a += rdt;
+        if constexpr ((r == IVX && q == IDN) || (r == IEN && q == IVX)) a -= grav;
+        double bm = am;
+        if constexpr (fj_nz(r, q)) bm += fj_entry<r, q>(cm, gm1);
+        double b = -bm * bl;
+        if (first) a += (q == IVX) ? -b : b;
+        if (last) {
+          double cmv = ap;
+          if constexpr (fj_nz(r, q)) cmv -= fj_entry<r, q>(cp, gm1);
+          double c = -cmv * cr;
+          a += (q == IVX) ? -c : c;
+        }
+#else
+        double num = am * aleft + ap * aright;
+        if constexpr (fj_nz(r, q)) num = num + (aright - aleft) * fj_entry<r, q>(c0, gm1);
+        double a = num / (2. * vol);
+        if constexpr (r == q) a = a + rdt;
+        if constexpr ((r == IVX && q == IDN) || (r == IEN && q == IVX)) a = a - grav;
+        double bm = am;
+        if constexpr (fj_nz(r, q)) bm = am + fj_entry<r, q>(cm, gm1);
+        double b = -bm * aleft / (2. * vol);
+        if (first) a = a + ((q == IVX) ? -b : b);
+        if (last) {
+          double cmv = ap;
+          if constexpr (fj_nz(r, q)) cmv = ap - fj_entry<r, q>(cp, gm1);
+          double c = -cmv * aright / (2. * vol);
+          a = a + ((q == IVX) ? -c : c);
+        }
+#endif
+        brow[q] = b;
+        t[r][q] = a;
+      });
+#if EXO_MIXED
+      x[r] = rhs[r] * rdt;
+#else
+      x[r] = rhs[r] / dt;
+#endif
+      if (!first) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          double ba = brow[0] * Ap[0][q];
+#pragma unroll
+          for (int k = 1; k < 5; ++k) ba += brow[k] * Ap[k][q];
+          t[r][q] = t[r][q] - ba;
+        }
+        double bd = brow[0] * dp[0];
+#pragma unroll
+        for (int k = 1; k < 5; ++k) bd += brow[k] * dp[k];
+        x[r] = x[r] - bd;
+      }
+    });
+    // c_i column by column, from |A|(i+1/2) in shared memory and the upper cell
+    auto ccol = [&](auto Q, double* c) {
+      constexpr int q = decltype(Q)::value;
+      unroll<5>([&](auto R) {
+        constexpr int r = decltype(R)::value;
+        double cmv = AMs(nxt, r, q);
+#if EXO_MIXED
+        if constexpr (fj_nz(r, q)) cmv -= fj_entry<r, q>(cp, gm1);
+        c[r] = -cmv * cr;
+#else
+        if constexpr (fj_nz(r, q)) cmv = cmv - fj_entry<r, q>(cp, gm1);
+        c[r] = -cmv * aright / (2. * vol);
+#endif
+      });
+    };
+#if EXO_MIXED
+    // LU with partial pivoting, multipliers below the diagonal
+    int perm[4];
+    double idg[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      if (k < 4) {
+        int piv = k;
+        double best = fabs(t[k][k]);
+#pragma unroll
+        for (int r = k + 1; r < 5; ++r)
+          if (fabs(t[r][k]) > best) { best = fabs(t[r][k]); piv = r; }
+        perm[k] = piv;
+#pragma unroll
+        for (int r = k + 1; r < 5; ++r) {
+          bool sw = (piv == r);
+#pragma unroll
+          for (int q = 0; q < 5; ++q) {
+            double a = t[k][q], b = t[r][q];
+            t[k][q] = sw ? b : a;
+            t[r][q] = sw ? a : b;
+          }
+        }
+      }
+      idg[k] = 1. / t[k][k];
+#pragma unroll
+      for (int r = k + 1; r < 5; ++r) {
+        double l = t[r][k] * idg[k];
+        t[r][k] = l;
+#pragma unroll
+        for (int q = k + 1; q < 5; ++q) t[r][q] -= l * t[k][q];
+      }
+    }
+    auto solve = [&](double* y) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int r = k + 1; r < 5; ++r) {
+          bool sw = (perm[k] == r);
+          double a = y[k], b = y[r];
+          y[k] = sw ? b : a;
+          y[r] = sw ? a : b;
+        }
+#pragma unroll
+      for (int r = 1; r < 5; ++r)
+#pragma unroll
+        for (int k = 0; k < r; ++k) y[r] -= t[r][k] * y[k];
+#pragma unroll
+      for (int r = 4; r >= 0; --r) {
+#pragma unroll
+        for (int q = r + 1; q < 5; ++q) y[r] -= t[r][q] * y[q];
+        y[r] *= idg[r];
+      }
+    };
+    solve(x);
+    unroll<5>([&](auto Q) {
+      constexpr int q = decltype(Q)::value;
+      double c[5];
+      ccol(Q, c);
+      solve(c);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Ap[r][q] = c[r];
+    });
+#pragma unroll
+    for (int r = 0; r < 5; ++r) dp[r] = x[r];
+#else
+    // Gauss-Jordan with partial pivoting on [t | I]; columns of t left of the
+    // pivot are never read again and are not updated
+    double B[5][5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) B[r][q] = (r == q) ? 1. : 0.;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      int piv = k;
+      double best = fabs(t[k][k]);
+#pragma unroll
+      for (int r = k + 1; r < 5; ++r)
+        if (fabs(t[r][k]) > best) { best = fabs(t[r][k]); piv = r; }
+#pragma unroll
+      for (int r = k + 1; r < 5; ++r) {
+        bool sw = (piv == r);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          if (q >= k) {
+            double a = t[k][q], b = t[r][q];
+            t[k][q] = sw ? b : a;
+            t[r][q] = sw ? a : b;
+          }
+          double a = B[k][q], b = B[r][q];
+          B[k][q] = sw ? b : a;
+          B[r][q] = sw ? a : b;
+        }
+      }
+      double d = 1.0 / t[k][k];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        if (q > k) t[k][q] *= d;
+        B[k][q] *= d;
+      }
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        if (r == k) continue;
+        double f = t[r][k];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          if (q > k) t[r][q] -= f * t[k][q];
+          B[r][q] -= f * B[k][q];
+        }
+      }
+    }
+    // delta_i = B x, (A c)_i = B c_i
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double acc = B[r][0] * x[0];
+#pragma unroll
+      for (int k = 1; k < 5; ++k) acc += B[r][k] * x[k];
+      dp[r] = acc;
+    }
+    unroll<5>([&](auto Q) {
+      constexpr int q = decltype(Q)::value;
+      double c[5];
+      ccol(Q, c);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        double acc = B[r][0] * c[0];
+#pragma unroll
+        for (int k = 1; k < 5; ++k) acc += B[r][k] * c[k];
+        Ap[r][q] = acc;
+      }
+    });
+#endif
+    const int lev = i - is;
+    if (!last) {
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) io.scr(lev, r * 5 + q) = Ap[r][q];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) io.scr(lev, 25 + r) = dp[r];
+    }
+    cm = c0;
+    c0 = cp;
+    cur = nxt;
+  }
+  // back substitution: delta_i -= (A c)_i delta_{i+1}
+  io.out(ie, dp);
+  for (int i = ie - 1; i >= is; --i) {
+    const int lev = i - is;
+    double dl[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double ad = io.scr(lev, r * 5) * dp[0];
+#pragma unroll
+      for (int k = 1; k < 5; ++k) ad += io.scr(lev, r * 5 + k) * dp[k];
+      dl[r] = io.scr(lev, 25 + r) - ad;
+    }
+#pragma unroll
+    for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+    io.out(i, dp);
   }
 }
 
@@ -1254,60 +1380,60 @@ __device__ __forceinline__ void airparcel_round_trip(double* uu, double Rd, doub
   uu[IEN] = e;
 }
 
-// Lane layout of the implicit kernels: 6 columns per warp, 5 lanes each
-// (lanes 30 and 31 idle).  Lanes of columns beyond ncol compute on the last
-// column and store nothing.
-struct ColumnLanes {
-  int col, r, base;
-  bool active;
+// Launch shape of the implicit kernels: one thread per radial column, 64
+// columns per block, 50 doubles of shared memory per thread (the face
+// Jacobians |A|(i-1/2) and |A|(i+1/2)).
+constexpr int IMPL_THREADS = 64;
+constexpr size_t IMPL_SMEM = (size_t)50 * IMPL_THREADS * sizeof(double);
+
+// A column of the stepping context: primitives and update from the state
+// arrays, the corrected update added to u (with the AirParcel round trip on
+// the last stage).
+struct StepColumnIO {
+  const double* wc;
+  const double* duc;
+  double* uc;
+  size_t vs;       // stride between variables
+  double* scr0;    // scratch of this column, stride nslot between entries
+  size_t nslot;
+  int stage;
+  double Rd, gamma;
+  __device__ __forceinline__ void w(int i, double* out) const {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) out[n] = wc[n * vs + i];
+  }
+  __device__ __forceinline__ double du(int i, int n) const { return duc[n * vs + i]; }
+  __device__ __forceinline__ double& scr(int lev, int e) const {
+    return scr0[((size_t)lev * 30 + e) * nslot];
+  }
+  __device__ __forceinline__ void out(int i, const double* dl) const {
+    double uu[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uu[n] = uc[n * vs + i] + 1. * dl[n];
+    if (stage == 2) airparcel_round_trip(uu, Rd, gamma);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uc[n * vs + i] = uu[n];
+  }
 };
-__device__ __forceinline__ ColumnLanes column_lanes(int ncol, unsigned blk) {
-  int lane = threadIdx.x & 31;
-  int warp = (blk * blockDim.x + threadIdx.x) >> 5;
-  int g = lane / 5;
-  ColumnLanes c;
-  c.r = lane - 5 * g;
-  c.base = 5 * g;
-  int col = warp * 6 + g;
-  c.active = (g < 6) && (col < ncol);
-  c.col = col < ncol ? col : ncol - 1;
-  if (g == 6) { c.r = 0; c.base = 30; }
-  return c;
-}
 
 // One radial column of the stepping context: solve, then u += du and, on
 // the last stage, the AirParcel round trip.
 __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, int stage) {
-  double* scratch = v.scratch;
-  int ncol = 6 * v.N * v.N;
-  ColumnLanes cl = column_lanes(ncol, blk);
-  int col = cl.col, r = cl.r;
-  int j = v.js + col % v.N;
-  int k = v.ks + (col / v.N) % v.N;
-  int p = col / (v.N * v.N);
+  extern __shared__ double ism[];
+  const int ncol = 6 * v.N * v.N;
+  const int col = (int)(blk * blockDim.x + threadIdx.x);
+  if (col >= ncol) return;
+  const int j = v.js + col % v.N;
+  const int k = v.ks + (col / v.N) % v.N;
+  const int p = col / (v.N * v.N);
   const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
-  double dt = kBeta[stage] * v.sc->dt;
-  size_t nslot = (size_t)ncol * 5;
-  size_t slot = (size_t)col * 5 + r;
-  double dummy = 0.;
-  auto W = [&](int i, double* out) {
-    for (int n = 0; n < 5; ++n) out[n] = v.w[idx(v, p, n, k, j, i)];
-  };
-  auto DU = [&](int i, int n) { return n < 5 ? v.du[idx(v, p, n, k, j, i)] : 0.; };
-  auto SCR = [&](int lev, int e) -> double& {
-    return cl.active ? scratch[((size_t)lev * 6 + e) * nslot + slot] : dummy;
-  };
-  auto OUT = [&](int i, const double* dl) {
-    if (!cl.active) return;
-    double uu[5];
-#pragma unroll
-    for (int n = 0; n < 5; ++n) uu[n] = v.u[idx(v, p, n, k, j, i)] + 1. * dl[n];
-    if (stage == 2) airparcel_round_trip(uu, v.Rd, v.gamma);
-    v.u[idx(v, p, r, k, j, i)] = uu[r];
-  };
-  implicit_column_rows(cl.base, r, W, DU, SCR, OUT, geo(v, GCOSC, p, k, j),
-                       geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j),
-                       v.x1f, v.x1v, v.dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+  const double dt = kBeta[stage] * v.sc->dt;
+  const size_t base = idx(v, p, 0, k, j, 0);
+  StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, v.scratch + col, (size_t)ncol,
+                  stage, v.Rd, v.gamma};
+  implicit_column(io, ism + threadIdx.x, blockDim.x, geo(v, GCOSC, p, k, j),
+                  geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), v.x1f,
+                  v.x1v, v.dx1f, v.is, v.ie, dt, v.gamma, v.grav);
 }
 
 // last-stage round trip when the implicit solver is off
@@ -1434,10 +1560,10 @@ __global__ void kb_update(Batch bt, int stage) {
   update_block<T>(sv, b, stage);
 }
 
-__global__ void __launch_bounds__(128) k_implicit(DevView v, int stage) {
+__global__ void __launch_bounds__(IMPL_THREADS) k_implicit(DevView v, int stage) {
   implicit_block(v, blockIdx.x, stage);
 }
-__global__ void __launch_bounds__(128) kb_implicit(Batch bt, int stage) {
+__global__ void __launch_bounds__(IMPL_THREADS) kb_implicit(Batch bt, int stage) {
   __shared__ DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
@@ -1516,8 +1642,7 @@ int launch_update(const DevView& v, int stage, void* stream) {
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   int ncol = 6 * v.N * v.N;
-  size_t threads = (size_t)((ncol + 5) / 6) * 32;
-  k_implicit<<<nblk(threads, 128), 128, 0, (cudaStream_t)stream>>>(v, stage);
+  k_implicit<<<nblk(ncol, IMPL_THREADS), IMPL_THREADS, IMPL_SMEM, (cudaStream_t)stream>>>(v, stage);
   return check_launch();
 }
 
@@ -1564,7 +1689,7 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
       if ((rc = check_launch())) return rc;
     }
     if (pl.total[BK_IMPLICIT]) {
-      kb_implicit<<<pl.total[BK_IMPLICIT], 128, 0, st>>>(B(BK_IMPLICIT), s);
+      kb_implicit<<<pl.total[BK_IMPLICIT], IMPL_THREADS, IMPL_SMEM, st>>>(B(BK_IMPLICIT), s);
       if ((rc = check_launch())) return rc;
     }
     if (s == 2) {

@@ -18,33 +18,41 @@ namespace {
 // as plain arrays: w [ncol][5][L+6] primitives with ghosts, du [ncol][5][L]
 // explicit update (overwritten by the corrected one), colgeo [ncol][4] =
 // (cos, sin, dx2f_ang, dx3f_ang), scratch ncol*L*30 doubles.
-__global__ void __launch_bounds__(128) k_implicit_columns(int ncol, int L, const double* w,
-                                                          double* du, const double* colgeo,
-                                                          const double* x1f, const double* x1v,
-                                                          const double* dx1f, double dt,
-                                                          double gamma, double grav,
-                                                          double* scratch) {
-  ColumnLanes cl = column_lanes(ncol, blockIdx.x);
-  int col = cl.col, r = cl.r;
-  int nc1 = L + 2 * G;
-  const double* wc = w + (size_t)col * 5 * nc1;
-  double* duc = du + (size_t)col * 5 * L;
-  size_t nslot = (size_t)ncol * 5;
-  size_t slot = (size_t)col * 5 + r;
-  double dummy = 0.;
-  auto W = [&](int i, double* out) {
+// A column of exo_implicit_columns: w [5][L+6] and du [5][L] of this column,
+// the corrected update written back into du.
+struct HookColumnIO {
+  const double* wc;
+  double* duc;
+  int nc1, L;
+  double* scr0;
+  size_t nslot;
+  __device__ __forceinline__ void w(int i, double* out) const {
+#pragma unroll
     for (int n = 0; n < 5; ++n) out[n] = wc[n * nc1 + i];
-  };
-  auto DU = [&](int i, int n) { return n < 5 ? duc[n * L + (i - G)] : 0.; };
-  auto SCR = [&](int lev, int e) -> double& {
-    return cl.active ? scratch[((size_t)lev * 6 + e) * nslot + slot] : dummy;
-  };
-  auto OUT = [&](int i, const double* dl) {
-    if (cl.active) duc[r * L + (i - G)] = dl[r];
-  };
+  }
+  __device__ __forceinline__ double du(int i, int n) const { return duc[n * L + (i - G)]; }
+  __device__ __forceinline__ double& scr(int lev, int e) const {
+    return scr0[((size_t)lev * 30 + e) * nslot];
+  }
+  __device__ __forceinline__ void out(int i, const double* dl) const {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) duc[n * L + (i - G)] = dl[n];
+  }
+};
+
+__global__ void __launch_bounds__(IMPL_THREADS) k_implicit_columns(
+    int ncol, int L, const double* w, double* du, const double* colgeo, const double* x1f,
+    const double* x1v, const double* dx1f, double dt, double gamma, double grav,
+    double* scratch) {
+  extern __shared__ double ism[];
+  const int col = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (col >= ncol) return;
+  const int nc1 = L + 2 * G;
+  HookColumnIO io{w + (size_t)col * 5 * nc1, du + (size_t)col * 5 * L, nc1, L, scratch + col,
+                  (size_t)ncol};
   const double* g4 = colgeo + (size_t)col * 4;
-  implicit_column_rows(cl.base, r, W, DU, SCR, OUT, g4[0], g4[1], g4[2], g4[3], x1f, x1v, dx1f,
-                       G, G + L - 1, dt, gamma, grav);
+  implicit_column(io, ism + threadIdx.x, blockDim.x, g4[0], g4[1], g4[2], g4[3], x1f, x1v, dx1f,
+                  G, G + L - 1, dt, gamma, grav);
 }
 
 __global__ void k_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
@@ -74,8 +82,8 @@ int launch_implicit_columns(int ncol, int L, const double* w, double* du, const 
                             const double* x1f, const double* x1v, const double* dx1f, double dt,
                             double gamma, double grav, double* scratch, void* stream) {
   if (ncol <= 0) return 0;
-  size_t threads = (size_t)((ncol + 5) / 6) * 32;
-  fp64::k_implicit_columns<<<fp64::nblk(threads, 128), 128, 0, (cudaStream_t)stream>>>(
+  fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
+                              fp64::IMPL_SMEM, (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
   return fp64::check_launch();
 }
@@ -125,8 +133,8 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
     scratch = g_noalloc_addr[dev];
   }
   if (ncol <= 0) return 0;
-  size_t threads = (size_t)((ncol + 5) / 6) * 32;
-  fp64::k_implicit_columns<<<fp64::nblk(threads, 128), 128, 0, (cudaStream_t)stream>>>(
+  fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
+                              fp64::IMPL_SMEM, (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
