@@ -20,6 +20,7 @@ and Eigen are not available), so the C++ restatement in oracle/ stands in
 for it ("kind": "port").
 """
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -349,7 +350,7 @@ def run_ensemble(args):
     ms_max = max_over_ranks(pg, e0.elapsed_time(e1))
     launches = ens.stats()["launches"] - l0
     clk = clocks.stop() if rank == 0 else None
-    valid = all(np.isfinite(ens.conserved(s)).all() for s in slots[:4])
+    valid = all(ens.invalid(s) == 0 for s in slots)
     nbytes_state = sum(w.nbytes for _, w in members)
     ens.close()
 
@@ -402,6 +403,37 @@ def run_ensemble(args):
             "gpu_launches": launches, "clocks": clk, "state_valid": bool(valid)}))
     if pg is not None:
         pg.destroy_process_group()
+
+
+def run_serving(args):
+    """Serving sweep: for each arrival rate, a Poisson stream of args.requests
+    forward-model requests (ensemble members, 200 steps each) served by the
+    continuous-batching server in mixed precision, and the same requests on
+    the plain FP64 path one at a time; one JSON line per rate."""
+    import torch
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.serving import (Request, Server, poisson_arrivals,
+                                       served_one_at_a_time, summarize)
+    torch.cuda.init()
+    for rate in [float(x) for x in args.serve.split(",")]:
+        t_arr = poisson_arrivals(rate, args.requests, seed=int(rate))
+        reqs = []
+        for n, a in enumerate(t_arr):
+            cfg, w = W.ensemble_member(50_000 + n, precision=1)
+            reqs.append(Request(n, cfg, w, float(a), args.serve_steps))
+        srv = Server(precision=1, capacity=64, budget_bytes=150 * 10 ** 9, max_chunk=8)
+        srv.run(reqs[:2], clock="steps")  # warm-up: graph capture, pools
+        mixed = summarize(srv.run(reqs))
+        srv.close()
+        base = None
+        if not args.no_fp64_baseline:
+            base = summarize(served_one_at_a_time(
+                [dataclasses.replace(r, cfg=dict(r.cfg, precision=0)) for r in reqs]))
+        print(json.dumps({"serving": {
+            "rate_per_s": rate, "requests": args.requests, "steps_per_request": args.serve_steps,
+            "members": "ensemble distribution (N in 24..96, L in 32..96, varied gas and gravity)",
+            "continuous_batching_mixed": mixed, "one_at_a_time_fp64": base}}), flush=True)
 
 
 def run_accuracy(args):
@@ -476,6 +508,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3", "c4"])
     ap.add_argument("--members", type=int, default=64, help="ensemble members (c4)")
+    ap.add_argument("--serve", default="", help="comma-separated arrival rates (req/s): serving sweep")
+    ap.add_argument("--requests", type=int, default=24, help="requests per rate (serving)")
+    ap.add_argument("--serve-steps", type=int, default=200)
+    ap.add_argument("--no-fp64-baseline", action="store_true")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
                     help="0: FP64; 1: FP32 reconstruction/Riemann/divergence, FP64 rest")
     ap.add_argument("--cpu-steps", type=int, default=2)
@@ -489,6 +525,8 @@ def main():
         cpu_worker(args)
     elif args.accuracy > 0:
         run_accuracy(args)
+    elif args.serve:
+        run_serving(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "c4":

@@ -30,7 +30,8 @@ EXPORTED = [
     "exo_ensemble_create", "exo_ensemble_destroy", "exo_ensemble_footprint",
     "exo_ensemble_add", "exo_ensemble_remove", "exo_ensemble_step",
     "exo_ensemble_synchronize", "exo_ensemble_get_conserved", "exo_ensemble_get_primitive",
-    "exo_ensemble_member_time", "exo_ensemble_stats", "exo_ensemble_get_stream",
+    "exo_ensemble_member_time", "exo_ensemble_check_state", "exo_ensemble_stats",
+    "exo_ensemble_get_stream",
     "exo_implicit_columns", "exo_implicit_columns_noalloc",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
@@ -114,6 +115,7 @@ def lib():
     L.exo_ensemble_get_conserved.argtypes = [p, i, dp]
     L.exo_ensemble_get_primitive.argtypes = [p, i, dp]
     L.exo_ensemble_member_time.argtypes = [p, i, dp, dp, ctypes.POINTER(ctypes.c_int64)]
+    L.exo_ensemble_check_state.argtypes = [p, i, ctypes.POINTER(i)]
     L.exo_ensemble_stats.argtypes = [p, ctypes.POINTER(i), ctypes.POINTER(sz),
                                      ctypes.POINTER(ctypes.c_int64)]
     L.exo_ensemble_get_stream.argtypes = [p, ctypes.POINTER(p)]

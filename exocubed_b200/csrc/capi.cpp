@@ -252,6 +252,15 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
     }
     return true;
   };
+  auto put_to = [&](void* dst, const void* src, size_t bytes) -> bool {
+    cudaError_t e = stream ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream)
+                           : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      *err = std::string("view upload: ") + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  };
   size_t db = elems * sizeof(double), fb = elems * sizeof(float);
   if (!alloc((void**)&v.u, db, true) || !alloc((void**)&v.w, db, true) ||
       !alloc((void**)&v.u1, db, true) || !alloc((void**)&v.flux[1], db, true) ||
@@ -287,6 +296,24 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
   v.ghost = (const GhostEntry*)gh;
   v.edge = (const EdgeEntry*)ed;
   if (!alloc((void**)&v.sc, sizeof(DevScalars), true)) return EXO_ERR_CAPACITY;
+  // the view's own device copy and its one-member block table: the stepping
+  // kernels are the batched ones, launched on a batch of one, so an
+  // atmosphere runs the same machine code alone as in an ensemble
+  struct SelfBlock {
+    DevView view;
+    unsigned start[BK_COUNT][2];
+  };
+  SelfBlock* dself = nullptr;
+  if (!alloc((void**)&dself, sizeof(SelfBlock), false)) return EXO_ERR_CAPACITY;
+  v.self = &dself->view;
+  v.starts = &dself->start[0][0];
+  SelfBlock hself;
+  std::memset(&hself, 0, sizeof(hself));
+  hself.view = v;
+  unsigned b[BK_COUNT];
+  member_blocks(v, b);
+  for (int k = 0; k < BK_COUNT; ++k) hself.start[k][1] = b[k];
+  if (!put_to(dself, &hself, sizeof(hself))) return EXO_ERR_CUDA;
   // tables must stay alive until the (possibly asynchronous) uploads finish
   cudaError_t e = stream ? cudaStreamSynchronize(stream) : cudaDeviceSynchronize();
   if (e != cudaSuccess) {

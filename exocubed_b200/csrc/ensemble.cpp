@@ -333,6 +333,19 @@ int exo_ensemble_member_time(exo_ensemble* e, int slot, double* time, double* dt
   return EXO_OK;
 }
 
+int exo_ensemble_check_state(exo_ensemble* e, int slot, int* invalid) {
+  Member* m = member_at(e, slot);
+  if (!m || !invalid) return efail(EXO_ERR_ARG, "bad slot or NULL argument");
+  DevScalars s;
+  ECK(cudaMemcpyAsync(&s, m->v.sc, sizeof(s), cudaMemcpyDeviceToHost, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  *invalid = s.invalid;
+  int zero = 0;
+  ECK(cudaMemcpyAsync(&m->v.sc->invalid, &zero, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  return EXO_OK;
+}
+
 int exo_ensemble_stats(exo_ensemble* e, int* members, size_t* bytes_in_use, int64_t* launches) {
   if (!e) return efail(EXO_ERR_ARG, "NULL ensemble");
   int n = 0;

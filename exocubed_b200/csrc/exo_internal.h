@@ -108,6 +108,10 @@ struct DevView {
   const GhostEntry* ghost;
   const EdgeEntry* edge;           // [6][4][N]
   DevScalars* sc;
+  // device copy of this view and its block table [BK_COUNT][2] = {0, blocks}:
+  // the single-atmosphere launches are batches of one
+  const DevView* self;
+  const unsigned* starts;
 };
 
 // A batched step: every member's DevView in device memory and, per kernel

@@ -7,17 +7,18 @@
 // implicit solve, the equation of state and the conserved state stay FP64;
 // compiled with FMA).  EXO_KNS names the namespace of the build.
 //
-// One stage of SSPRK(3,3) is five launches:
-//   k_flux_x1     per radial column: hydrostatic decomposition, WENO5 in x1,
+// One stage of SSPRK(3,3) is five launches, each one kernel over every
+// member of a batch (a single atmosphere is a batch of one):
+//   kb_flux_x1    per radial column: hydrostatic decomposition, WENO5 in x1,
 //                 restore, Riemann solve -> x1 face fluxes         (exo3 only)
-//   k_flux_x23    per horizontal face: WENO5 on both sides; at panel edges the
+//   kb_flux_x23   per horizontal face: WENO5 on both sides; at panel edges the
 //                 outer state is the neighbour panel's own reconstruction,
 //                 rotated into this panel's basis; Riemann solve -> x2/x3 fluxes
-//   k_update      per cell: RK register average, flux divergence, geometric
+//   kb_update     per cell: RK register average, flux divergence, geometric
 //                 source, gravity / Coriolis -> u (exo2) or du (exo3)
-//   k_implicit    per radial column: 5x5 block-tridiagonal vertical correction,
+//   kb_implicit   per radial column: 5x5 block-tridiagonal vertical correction,
 //                 u += du, AirParcel round trip on the last stage (exo3)
-//   k_prim_ghost  per cell incl. ghosts: ConservedToPrimitive of the interior,
+//   kb_prim_ghost per cell incl. ghosts: ConservedToPrimitive of the interior,
 //                 of the ghost bands interpolated from the neighbour panels and
 //                 of the reflected x1 ghosts; CFL time-step candidate
 #include <cfloat>
@@ -906,6 +907,18 @@ __device__ __forceinline__ double fj_entry(const ColCell& c, double gm1) {
   }
 }
 
+// asynchronous 8-byte global -> shared copies (the next level's inputs)
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // compile-time loops (the matrix entries live in registers, so every index
 // has to be a constant)
 template <int N, class F, int... I>
@@ -997,6 +1010,42 @@ __device__ __forceinline__ void abs_jacobian(const ColCell& L, const ColCell& R_
 #endif
 }
 
+// Solve with the LU factors of implicit_column's mixed build (rows taken in
+// the order 1, 4, 2, 3, 0, threshold row swaps packed 3 bits per step): y
+// holds the right-hand side with its rows in natural order on entry and the
+// solution, unknowns in order, on exit.
+__device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const double (&idg)[5],
+                                              unsigned perm, bool swapped, double* y) {
+  constexpr int O[5] = {1, 4, 2, 3, 0};
+  if (swapped) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const unsigned pk = (perm >> (3 * k)) & 7u;
+#pragma unroll
+      for (int r = k + 1; r < 5; ++r) {
+        const bool sw = (pk == (unsigned)r);
+        const double a = y[O[k]], b = y[O[r]];
+        y[O[k]] = sw ? b : a;
+        y[O[r]] = sw ? a : b;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 1; r < 5; ++r)
+#pragma unroll
+    for (int k = 0; k < r; ++k) y[O[r]] -= t[O[r]][k] * y[O[k]];
+  double z[5];
+#pragma unroll
+  for (int r = 4; r >= 0; --r) {
+    double acc = y[O[r]];
+#pragma unroll
+    for (int q = r + 1; q < 5; ++q) acc -= t[O[r]][q] * z[q];
+    z[r] = acc * idg[r];
+  }
+#pragma unroll
+  for (int r = 0; r < 5; ++r) y[r] = z[r];
+}
+
 // The vertical 5x5 block-tridiagonal correction of one radial column
 // (ImplicitSolver::SolveImplicit3D X1 branch, solve_implicit_3d.cpp:102-179,
 // with FullCorrection, full_correction.cpp:32-165, and ForwardSweep /
@@ -1015,10 +1064,11 @@ __device__ __forceinline__ void abs_jacobian(const ColCell& L, const ColCell& R_
 // face Jacobian |A|(i+1/2) waits in this thread's slice of shared memory
 // until it becomes |A|(i-1/2) of the next level.
 //   io.w(i, out[5])  primitives of level i (is-1 .. ie+2), unprojected
-//   io.du(i, n)      explicit update of level i
 //   io.scr(lev, e)   scratch double e (0..29) of level lev = i - is
 //   io.out(i, d[5])  corrected update of level i, from ie down to is
-//   sm               this thread's 50 doubles of shared memory, stride sms
+//   io.wptr(i, n), io.duptr(i, n)  addresses of w and of the explicit update
+//                    du of level i (the inputs are prefetched through shared memory)
+//   sm               this thread's 60 doubles of shared memory, stride sms
 template <class IO>
 __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, double cos_theta,
                                                 double sin_theta, double d2, double d3,
@@ -1050,12 +1100,24 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
   };
   auto AMs = [&](int slot, int r, int q) -> double& { return sm[(slot * 25 + r * 5 + q) * sms]; };
 
+  // prefetch slots: w(i+1) and du(i) of the next level, copied asynchronously
+  double* pw = sm + 50 * sms;
+  double* pdu = sm + 55 * sms;
+  auto prefetch = [&](int iw, int idu) {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) cp_async8(pw + n * sms, io.wptr(iw, n));
+    if (idu >= 0) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) cp_async8(pdu + n * sms, io.duptr(idu, n));
+    }
+    cp_async_commit();
+  };
   double raw[5];
   io.w(is - 1, raw);
   ColCell cm = cell(raw);
   io.w(is, raw);
   ColCell c0 = cell(raw);
-  io.w(is + 1, raw);  // prefetched level: raw holds w(i+1) at the top of level i
+  prefetch(is + 1, is);
   {
     double A[5][5];
     abs_jacobian(cm, c0, gm1, gamma, A);
@@ -1065,20 +1127,17 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
       for (int q = 0; q < 5; ++q) AMs(0, r, q) = A[r][q];
   }
   double Ap[5][5], dp[5];  // (A c)_{i-1}, delta_{i-1}
-  double dun[5];
-#pragma unroll
-  for (int n = 0; n < 5; ++n) dun[n] = io.du(is, n);
   int cur = 0;
   for (int i = is; i <= ie; ++i) {
-    ColCell cp = cell(raw);
+    cp_async_wait_all();
     double rhs[5];
 #pragma unroll
-    for (int n = 0; n < 5; ++n) rhs[n] = dun[n];
-    io.w(i + 2, raw);  // prefetch for the next level
-    if (i < ie) {
-#pragma unroll
-      for (int n = 0; n < 5; ++n) dun[n] = io.du(i + 1, n);
+    for (int n = 0; n < 5; ++n) {
+      raw[n] = pw[n * sms];
+      rhs[n] = pdu[n * sms];
     }
+    ColCell cp = cell(raw);
+    prefetch(i + 2, i < ie ? i + 1 : -1);
     const int nxt = cur ^ 1;
     {
       double A[5][5];
@@ -1095,11 +1154,12 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
     const double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
 #endif
     const bool first = (i == is), last = (i == ie);
-    double t[5][5], x[5];
-    // rows of a, b (and c at the top boundary), then t and x
+    double x[5];
+    // rows of a, b (and c at the top boundary), then of t = a - b (A c)_{i-1},
+    // written over row r of |A|(i-1/2) once that row has been read; and x
     unroll<5>([&](auto R) {
       constexpr int r = decltype(R)::value;
-      double brow[5];
+      double brow[5], trow[5];
       unroll<5>([&](auto Q) {
         constexpr int q = decltype(Q)::value;
         const double am = AMs(cur, r, q), ap = AMs(nxt, r, q);
@@ -1136,7 +1196,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
         }
 #endif
         brow[q] = b;
-        t[r][q] = a;
+        trow[q] = a;
       });
 #if EXO_MIXED
       x[r] = rhs[r] * rdt;
@@ -1149,14 +1209,21 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
           double ba = brow[0] * Ap[0][q];
 #pragma unroll
           for (int k = 1; k < 5; ++k) ba += brow[k] * Ap[k][q];
-          t[r][q] = t[r][q] - ba;
+          trow[q] = trow[q] - ba;
         }
         double bd = brow[0] * dp[0];
 #pragma unroll
         for (int k = 1; k < 5; ++k) bd += brow[k] * dp[k];
         x[r] = x[r] - bd;
       }
+#pragma unroll
+      for (int q = 0; q < 5; ++q) AMs(cur, r, q) = trow[q];
     });
+    double t[5][5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) t[r][q] = AMs(cur, r, q);
     // c_i column by column, from |A|(i+1/2) in shared memory and the upper cell
     auto ccol = [&](auto Q, double* c) {
       constexpr int q = decltype(Q)::value;
@@ -1173,59 +1240,53 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
       });
     };
 #if EXO_MIXED
-    // LU with partial pivoting, multipliers below the diagonal
-    int perm[4];
+    // LU with the rows taken in the order 1, 4, 2, 3, 0 -- the order partial
+    // pivoting ends with for nearly every block of this solve (density last,
+    // energy and x1 momentum first) -- and threshold partial pivoting on top:
+    // a row swap only where the diagonal falls below a tenth of the largest
+    // entry of its column, so the swap code is skipped almost always.
+    constexpr int O[5] = {1, 4, 2, 3, 0};
+    unsigned perm = 0;  // 3 bits per step: the position swapped in
+    bool swapped = false;
     double idg[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       if (k < 4) {
+        const double dk = fabs(t[O[k]][k]);
+        double best = dk;
         int piv = k;
-        double best = fabs(t[k][k]);
-#pragma unroll
-        for (int r = k + 1; r < 5; ++r)
-          if (fabs(t[r][k]) > best) { best = fabs(t[r][k]); piv = r; }
-        perm[k] = piv;
 #pragma unroll
         for (int r = k + 1; r < 5; ++r) {
-          bool sw = (piv == r);
+          const double m = fabs(t[O[r]][k]);
+          if (m > best) { best = m; piv = r; }
+        }
+        if (dk < 0.1 * best) {
+          swapped = true;
+          perm |= (unsigned)piv << (3 * k);
 #pragma unroll
-          for (int q = 0; q < 5; ++q) {
-            double a = t[k][q], b = t[r][q];
-            t[k][q] = sw ? b : a;
-            t[r][q] = sw ? a : b;
+          for (int r = k + 1; r < 5; ++r) {
+            const bool sw = (piv == r);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+              const double a = t[O[k]][q], b = t[O[r]][q];
+              t[O[k]][q] = sw ? b : a;
+              t[O[r]][q] = sw ? a : b;
+            }
           }
+        } else {
+          perm |= (unsigned)k << (3 * k);
         }
       }
-      idg[k] = 1. / t[k][k];
+      idg[k] = 1. / t[O[k]][k];
 #pragma unroll
       for (int r = k + 1; r < 5; ++r) {
-        double l = t[r][k] * idg[k];
-        t[r][k] = l;
+        const double l = t[O[r]][k] * idg[k];
+        t[O[r]][k] = l;
 #pragma unroll
-        for (int q = k + 1; q < 5; ++q) t[r][q] -= l * t[k][q];
+        for (int q = k + 1; q < 5; ++q) t[O[r]][q] -= l * t[O[k]][q];
       }
     }
-    auto solve = [&](double* y) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int r = k + 1; r < 5; ++r) {
-          bool sw = (perm[k] == r);
-          double a = y[k], b = y[r];
-          y[k] = sw ? b : a;
-          y[r] = sw ? a : b;
-        }
-#pragma unroll
-      for (int r = 1; r < 5; ++r)
-#pragma unroll
-        for (int k = 0; k < r; ++k) y[r] -= t[r][k] * y[k];
-#pragma unroll
-      for (int r = 4; r >= 0; --r) {
-#pragma unroll
-        for (int q = r + 1; q < 5; ++q) y[r] -= t[r][q] * y[q];
-        y[r] *= idg[r];
-      }
-    };
+    auto solve = [&](double* y) { lu_solve_rows(t, idg, perm, swapped, y); };
     solve(x);
     unroll<5>([&](auto Q) {
       constexpr int q = decltype(Q)::value;
@@ -1381,10 +1442,14 @@ __device__ __forceinline__ void airparcel_round_trip(double* uu, double Rd, doub
 }
 
 // Launch shape of the implicit kernels: one thread per radial column, 64
-// columns per block, 50 doubles of shared memory per thread (the face
-// Jacobians |A|(i-1/2) and |A|(i+1/2)).
+// columns per block, 60 doubles of shared memory per thread (the face
+// Jacobians |A|(i-1/2) and |A|(i+1/2), the next level's w and du).
 constexpr int IMPL_THREADS = 64;
-constexpr size_t IMPL_SMEM = (size_t)50 * IMPL_THREADS * sizeof(double);
+#ifndef EXO_IMPL_MINB
+#define EXO_IMPL_MINB 4  // resident blocks per SM the register budget is sized for
+#endif
+#define EXO_IMPL_BOUNDS __launch_bounds__(IMPL_THREADS, EXO_IMPL_MINB)
+constexpr size_t IMPL_SMEM = (size_t)60 * IMPL_THREADS * sizeof(double);
 
 // A column of the stepping context: primitives and update from the state
 // arrays, the corrected update added to u (with the AirParcel round trip on
@@ -1402,7 +1467,8 @@ struct StepColumnIO {
 #pragma unroll
     for (int n = 0; n < 5; ++n) out[n] = wc[n * vs + i];
   }
-  __device__ __forceinline__ double du(int i, int n) const { return duc[n * vs + i]; }
+  __device__ __forceinline__ const double* wptr(int i, int n) const { return wc + n * vs + i; }
+  __device__ __forceinline__ const double* duptr(int i, int n) const { return duc + n * vs + i; }
   __device__ __forceinline__ double& scr(int lev, int e) const {
     return scr0[((size_t)lev * 30 + e) * nslot];
   }
@@ -1525,15 +1591,12 @@ __device__ __forceinline__ unsigned batch_enter(const Batch& bt, DevView& sv) {
   return local;
 }
 
-__global__ void k_prim_ghost(DevView v, int compute_dt) { prim_ghost_block(v, blockIdx.x, compute_dt); }
 __global__ void kb_prim_ghost(Batch bt, int compute_dt) {
   __shared__ DevView sv;
   unsigned b = batch_enter(bt, sv);
   prim_ghost_block(sv, b, compute_dt);
 }
 
-template <class T>
-__global__ void k_flux_x1(DevView v) { flux_x1_block<T>(v, blockIdx.x); }
 template <class T>
 __global__ void kb_flux_x1(Batch bt) {
   __shared__ DevView sv;
@@ -1543,8 +1606,6 @@ __global__ void kb_flux_x1(Batch bt) {
 }
 
 template <class T>
-__global__ void k_flux_x23(DevView v) { flux_x23_block<T>(v, blockIdx.x); }
-template <class T>
 __global__ void kb_flux_x23(Batch bt) {
   __shared__ DevView sv;
   unsigned b = batch_enter(bt, sv);
@@ -1552,25 +1613,19 @@ __global__ void kb_flux_x23(Batch bt) {
 }
 
 template <class T>
-__global__ void k_update(DevView v, int stage) { update_block<T>(v, blockIdx.x, stage); }
-template <class T>
 __global__ void kb_update(Batch bt, int stage) {
   __shared__ DevView sv;
   unsigned b = batch_enter(bt, sv);
   update_block<T>(sv, b, stage);
 }
 
-__global__ void __launch_bounds__(IMPL_THREADS) k_implicit(DevView v, int stage) {
-  implicit_block(v, blockIdx.x, stage);
-}
-__global__ void __launch_bounds__(IMPL_THREADS) kb_implicit(Batch bt, int stage) {
+__global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage) {
   __shared__ DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
   implicit_block(sv, b, stage);
 }
 
-__global__ void k_roundtrip(DevView v) { roundtrip_block(v, blockIdx.x); }
 __global__ void kb_roundtrip(Batch bt) {
   __shared__ DevView sv;
   unsigned b = batch_enter(bt, sv);
@@ -1606,9 +1661,20 @@ inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
 
+// The single-atmosphere launches run the batched kernels on a batch of one
+// (the view's own device copy and block table), so an atmosphere advanced
+// alone executes exactly the code it executes inside an ensemble.
+inline Batch one(const DevView& v, int kind) { return Batch{v.self, v.starts + 2 * kind, 1}; }
+
+inline unsigned member_block_count(const DevView& v, int kind) {
+  unsigned b[BK_COUNT];
+  member_blocks(v, b);
+  return b[kind];
+}
+
 int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream) {
-  size_t total = (size_t)6 * v.cells;
-  k_prim_ghost<<<nblk(total, 256), 256, 0, (cudaStream_t)stream>>>(v, compute_dt ? 1 : 0);
+  kb_prim_ghost<<<member_block_count(v, BK_PRIM), 256, 0, (cudaStream_t)stream>>>(
+      one(v, BK_PRIM), compute_dt ? 1 : 0);
   return check_launch();
 }
 
@@ -1617,23 +1683,25 @@ int launch_flux_x1(const DevView& v, void* stream) {
   int threads = ((v.L + 1 + 31) / 32) * 32;
   if (threads > 256) threads = 256;
   size_t smem = ((size_t)v.nv * v.nc1 + v.nc1 + 1) * sizeof(double);
-  k_flux_x1<EXO_FLUX_T><<<6 * v.N * v.N, threads, smem, (cudaStream_t)stream>>>(v);
+  kb_flux_x1<EXO_FLUX_T><<<member_block_count(v, BK_X1), threads, smem, (cudaStream_t)stream>>>(
+      one(v, BK_X1));
   return check_launch();
 }
 
 int launch_flux_x23(const DevView& v, void* stream) {
-  size_t total = (size_t)2 * 6 * v.N * (v.N + 1) * v.L;
-  k_flux_x23<EXO_FLUX_T><<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v);
+  kb_flux_x23<EXO_FLUX_T><<<member_block_count(v, BK_X23), 128, 0, (cudaStream_t)stream>>>(
+      one(v, BK_X23));
   return check_launch();
 }
 
 int launch_update(const DevView& v, int stage, void* stream) {
-  size_t total = (size_t)6 * v.N * v.N * v.L;
-  k_update<EXO_FLUX_T><<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v, stage);
+  kb_update<EXO_FLUX_T><<<member_block_count(v, BK_UPDATE), 128, 0, (cudaStream_t)stream>>>(
+      one(v, BK_UPDATE), stage);
   int rc = check_launch();
   if (rc) return rc;
   if (v.eqn != EXO_EQN_SHALLOW_YZ && !(v.implicit_flag & 1) && stage == 2) {
-    k_roundtrip<<<nblk(total, 128), 128, 0, (cudaStream_t)stream>>>(v);
+    kb_roundtrip<<<member_block_count(v, BK_ROUNDTRIP), 128, 0, (cudaStream_t)stream>>>(
+        one(v, BK_ROUNDTRIP));
     rc = check_launch();
   }
   return rc;
@@ -1641,8 +1709,8 @@ int launch_update(const DevView& v, int stage, void* stream) {
 
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
-  int ncol = 6 * v.N * v.N;
-  k_implicit<<<nblk(ncol, IMPL_THREADS), IMPL_THREADS, IMPL_SMEM, (cudaStream_t)stream>>>(v, stage);
+  kb_implicit<<<member_block_count(v, BK_IMPLICIT), IMPL_THREADS, IMPL_SMEM,
+                (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), stage);
   return check_launch();
 }
 

@@ -30,7 +30,10 @@ struct HookColumnIO {
 #pragma unroll
     for (int n = 0; n < 5; ++n) out[n] = wc[n * nc1 + i];
   }
-  __device__ __forceinline__ double du(int i, int n) const { return duc[n * L + (i - G)]; }
+  __device__ __forceinline__ const double* wptr(int i, int n) const { return wc + n * nc1 + i; }
+  __device__ __forceinline__ const double* duptr(int i, int n) const {
+    return duc + n * L + (i - G);
+  }
   __device__ __forceinline__ double& scr(int lev, int e) const {
     return scr0[((size_t)lev * 30 + e) * nslot];
   }
@@ -40,7 +43,7 @@ struct HookColumnIO {
   }
 };
 
-__global__ void __launch_bounds__(IMPL_THREADS) k_implicit_columns(
+__global__ void EXO_IMPL_BOUNDS k_implicit_columns(
     int ncol, int L, const double* w, double* du, const double* colgeo, const double* x1f,
     const double* x1v, const double* dx1f, double dt, double gamma, double grav,
     double* scratch) {

@@ -91,6 +91,12 @@ class Ensemble:
                                                      ctypes.byref(dt), ctypes.byref(n)))
         return t.value, dt.value, n.value
 
+    def invalid(self, slot):
+        """Non-zero if the member's state turned invalid since the last call."""
+        f = ctypes.c_int()
+        nat.check(nat.lib().exo_ensemble_check_state(self._h, int(slot), ctypes.byref(f)))
+        return f.value
+
     def stats(self):
         m, b, l = ctypes.c_int(), ctypes.c_size_t(), ctypes.c_int64()
         nat.check(nat.lib().exo_ensemble_stats(self._h, ctypes.byref(m), ctypes.byref(b),

@@ -287,6 +287,10 @@ int exo_ensemble_get_conserved(exo_ensemble* ens, int slot, double* u_host);
 int exo_ensemble_get_primitive(exo_ensemble* ens, int slot, double* w_host);
 int exo_ensemble_member_time(exo_ensemble* ens, int slot, double* time, double* dt,
                              int64_t* ncycle);
+/* MeshBlock::Impl::IsStateValid for one member: the sticky device flag set
+   when a cell's density or pressure turned non-positive or NaN, cleared on
+   read (as exo_check_state). */
+int exo_ensemble_check_state(exo_ensemble* ens, int slot, int* invalid);
 /* Members admitted, device bytes held by them, kernel launches issued. */
 int exo_ensemble_stats(exo_ensemble* ens, int* members, size_t* bytes_in_use,
                        int64_t* launches);
