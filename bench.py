@@ -330,6 +330,9 @@ def run_ensemble(args):
     cells = sum(cells_of(c) for c, _ in members)
     ens = Ensemble(precision=prec, capacity=args.members)
     slots = [ens.add(c, w) for c, w in members]
+    t_tune = time.perf_counter()
+    tiles = ens.autotune() if not args.no_autotune else ens.tiles
+    t_tune = time.perf_counter() - t_tune
     stream = torch.cuda.ExternalStream(ens.stream)
     ens.step(args.warmup)
     ens.synchronize()
@@ -359,6 +362,7 @@ def run_ensemble(args):
     pinned = [(c, torch.from_numpy(w).pin_memory().numpy()) for c, w in members]
     outs = [np.empty_like(w) for _, w in pinned]
     ens = Ensemble(precision=prec, capacity=args.members)
+    ens.set_tiles(tiles)
     s2 = torch.cuda.ExternalStream(ens.stream)
     barrier(pg)
     torch.cuda.synchronize()
@@ -391,6 +395,9 @@ def run_ensemble(args):
                                    f"{'FP64' if prec == 0 else 'mixed FP32/FP64'}, "
                                    "one graph-captured batched SSPRK3 step per step",
                        "members": args.members, "cells_per_step": cells,
+                       "tiles": dict(zip(["x1", "x23", "update", "implicit", "prim_ghost",
+                                          "roundtrip"], tiles)),
+                       "autotune_s": round(t_tune, 2),
                        "l2": f"{nbytes_state / 1e9:.1f} GB of member state exceeds the 126 MB L2"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -422,7 +429,13 @@ def run_serving(args):
         for n, a in enumerate(t_arr):
             cfg, w = W.ensemble_member(50_000 + n, precision=1)
             reqs.append(Request(n, cfg, w, float(a), args.serve_steps))
-        srv = Server(precision=1, capacity=64, budget_bytes=150 * 10 ** 9, max_chunk=8)
+        cache = None
+        if not args.no_autotune:
+            from exocubed_b200 import autotune
+            cache = autotune.TileCache()
+            autotune.batch_tiles([r.cfg for r in reqs], cache)  # measured before the clock starts
+        srv = Server(precision=1, capacity=64, budget_bytes=150 * 10 ** 9, max_chunk=8,
+                     tile_cache=cache)
         srv.run(reqs[:2], clock="steps")  # warm-up: graph capture, pools
         mixed = summarize(srv.run(reqs))
         srv.close()
@@ -512,6 +525,7 @@ def main():
     ap.add_argument("--requests", type=int, default=24, help="requests per rate (serving)")
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--no-fp64-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tiles")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
                     help="0: FP64; 1: FP32 reconstruction/Riemann/divergence, FP64 rest")
     ap.add_argument("--cpu-steps", type=int, default=2)

@@ -17,6 +17,8 @@ EXO_RS_ROE_SHALLOW, EXO_RS_LMARS, EXO_RS_HLLC, EXO_RS_LMARS_SHALLOW = 0, 1, 2, 3
 EXO_PREC_FP64, EXO_PREC_MIXED = 0, 1
 EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92 = 0, 1
 NGHOST = 3
+EXO_TILE_COUNT = 6
+EXO_K_FLUX_X1, EXO_K_FLUX_X23, EXO_K_UPDATE, EXO_K_IMPLICIT, EXO_K_PRIM_GHOST, EXO_K_OTHER = range(6)
 NOALLOC_SCRATCH_DOUBLES = 1048576  # EXO_NOALLOC_SCRATCH_DOUBLES
 
 # every symbol include/exo_b200.h declares
@@ -31,6 +33,7 @@ EXPORTED = [
     "exo_ensemble_add", "exo_ensemble_remove", "exo_ensemble_step",
     "exo_ensemble_synchronize", "exo_ensemble_get_conserved", "exo_ensemble_get_primitive",
     "exo_ensemble_member_time", "exo_ensemble_check_state", "exo_ensemble_stats",
+    "exo_set_tiles", "exo_get_tiles", "exo_ensemble_set_tiles", "exo_ensemble_get_tiles",
     "exo_ensemble_get_stream",
     "exo_implicit_columns", "exo_implicit_columns_noalloc",
 ]
@@ -115,6 +118,11 @@ def lib():
     L.exo_ensemble_get_conserved.argtypes = [p, i, dp]
     L.exo_ensemble_get_primitive.argtypes = [p, i, dp]
     L.exo_ensemble_member_time.argtypes = [p, i, dp, dp, ctypes.POINTER(ctypes.c_int64)]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.exo_set_tiles.argtypes = [p, ip]
+    L.exo_get_tiles.argtypes = [p, ip]
+    L.exo_ensemble_set_tiles.argtypes = [p, ip]
+    L.exo_ensemble_get_tiles.argtypes = [p, ip]
     L.exo_ensemble_check_state.argtypes = [p, i, ctypes.POINTER(i)]
     L.exo_ensemble_stats.argtypes = [p, ctypes.POINTER(i), ctypes.POINTER(sz),
                                      ctypes.POINTER(ctypes.c_int64)]

@@ -118,6 +118,18 @@ class CubedSphereAtmosphere:
         nat.check(nat.lib().exo_get_time(self._ctx, ctypes.byref(t), ctypes.byref(n)))
         return t.value
 
+    @property
+    def tiles(self):
+        """Threads per block of each kernel, indexed by EXO_K_* (exo_get_tiles)."""
+        t = (ctypes.c_int * nat.EXO_TILE_COUNT)()
+        nat.check(nat.lib().exo_get_tiles(self._ctx, t))
+        return list(t)
+
+    def set_tiles(self, threads):
+        """Set launch tiles (entries 0 keep the current value); see exo_set_tiles."""
+        t = (ctypes.c_int * nat.EXO_TILE_COUNT)(*[int(x) for x in threads])
+        nat.check(nat.lib().exo_set_tiles(self._ctx, t))
+
     def invalid(self):
         f = ctypes.c_int()
         nat.check(nat.lib().exo_check_state(self._ctx, ctypes.byref(f)))

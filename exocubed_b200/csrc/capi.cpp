@@ -150,7 +150,21 @@ static int one_step(exo_ctx* c, double dt_fixed) {
                [&] { return STEP(launch_dt_finalize, v, dt_fixed, true, c->stream); });
 }
 
+static_assert((int)exo::BK_X1 == (int)EXO_K_FLUX_X1 && (int)exo::BK_X23 == (int)EXO_K_FLUX_X23 &&
+                  (int)exo::BK_UPDATE == (int)EXO_K_UPDATE &&
+                  (int)exo::BK_IMPLICIT == (int)EXO_K_IMPLICIT &&
+                  (int)exo::BK_PRIM == (int)EXO_K_PRIM_GHOST &&
+                  (int)exo::BK_ROUNDTRIP == (int)EXO_K_OTHER && (int)exo::BK_COUNT == EXO_TILE_COUNT,
+              "tile slots follow the EXO_K_* kernel ids");
+
 namespace exo {
+
+// the view's device copy and its one-member block table
+struct SelfBlock {
+  DevView view;
+  unsigned start[BK_COUNT][2];
+};
+
 
 bool validate_config(const exo_config& c, std::string* err) {
   auto bad = [&](const char* m) { *err = m; return false; };
@@ -252,15 +266,6 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
     }
     return true;
   };
-  auto put_to = [&](void* dst, const void* src, size_t bytes) -> bool {
-    cudaError_t e = stream ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream)
-                           : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-      *err = std::string("view upload: ") + cudaGetErrorString(e);
-      return false;
-    }
-    return true;
-  };
   size_t db = elems * sizeof(double), fb = elems * sizeof(float);
   if (!alloc((void**)&v.u, db, true) || !alloc((void**)&v.w, db, true) ||
       !alloc((void**)&v.u1, db, true) || !alloc((void**)&v.flux[1], db, true) ||
@@ -299,28 +304,19 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
   // the view's own device copy and its one-member block table: the stepping
   // kernels are the batched ones, launched on a batch of one, so an
   // atmosphere runs the same machine code alone as in an ensemble
-  struct SelfBlock {
-    DevView view;
-    unsigned start[BK_COUNT][2];
-  };
   SelfBlock* dself = nullptr;
   if (!alloc((void**)&dself, sizeof(SelfBlock), false)) return EXO_ERR_CAPACITY;
   v.self = &dself->view;
   v.starts = &dself->start[0][0];
-  SelfBlock hself;
-  std::memset(&hself, 0, sizeof(hself));
-  hself.view = v;
-  unsigned b[BK_COUNT];
-  member_blocks(v, b);
-  for (int k = 0; k < BK_COUNT; ++k) hself.start[k][1] = b[k];
-  if (!put_to(dself, &hself, sizeof(hself))) return EXO_ERR_CUDA;
+  Tiles dt = default_tiles();
+  for (int k = 0; k < BK_COUNT; ++k) v.tiles[k] = dt.t[k];
   // tables must stay alive until the (possibly asynchronous) uploads finish
   cudaError_t e = stream ? cudaStreamSynchronize(stream) : cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     *err = std::string("upload: ") + cudaGetErrorString(e);
     return EXO_ERR_CUDA;
   }
-  return 0;
+  return view_refresh_self(v, stream, err);
 }
 
 void view_free(std::vector<void*>& owned, void* stream_v) {
@@ -332,16 +328,60 @@ void view_free(std::vector<void*>& owned, void* stream_v) {
   owned.clear();
 }
 
-void member_blocks(const DevView& v, unsigned b[BK_COUNT]) {
+Tiles default_tiles() {
+  Tiles t;
+  t.t[BK_X1] = 0;
+  t.t[BK_X23] = 128;
+  t.t[BK_UPDATE] = 128;
+  t.t[BK_IMPLICIT] = 64;
+  t.t[BK_PRIM] = 256;
+  t.t[BK_ROUNDTRIP] = 128;
+  return t;
+}
+
+bool valid_tiles(const int* t, std::string* err) {
+  for (int k = 0; k < BK_COUNT; ++k) {
+    if (k == BK_X1) continue;
+    bool ok = t[k] >= 32 && t[k] <= 512 && t[k] % 32 == 0;
+    if (k == BK_IMPLICIT) ok = t[k] == 32 || t[k] == 64 || t[k] == 128;
+    if (!ok) {
+      *err = "tile " + std::to_string(k) + " = " + std::to_string(t[k]) +
+             ": threads per block must be a multiple of 32 in [32, 512] (implicit: 32, 64, 128)";
+      return false;
+    }
+  }
+  return true;
+}
+
+void member_blocks(const DevView& v, const int* t, unsigned b[BK_COUNT]) {
   bool shallow = v.eqn == EXO_EQN_SHALLOW_YZ;
   bool implicit = !shallow && (v.implicit_flag & 1);
-  auto nb = [](size_t n, int t) { return (unsigned)((n + t - 1) / t); };
+  auto nb = [](size_t n, int th) { return (unsigned)((n + th - 1) / th); };
   b[BK_X1] = shallow ? 0u : (unsigned)(6 * v.N * v.N);
-  b[BK_X23] = nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, 128);
-  b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, 128);
-  b[BK_IMPLICIT] = implicit ? nb((size_t)6 * v.N * v.N, 64) : 0u;  // one thread per column
-  b[BK_PRIM] = nb((size_t)6 * v.cells, 256);
-  b[BK_ROUNDTRIP] = (!shallow && !implicit) ? nb((size_t)6 * v.N * v.N * v.L, 128) : 0u;
+  b[BK_X23] = nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, t[BK_X23]);
+  b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, t[BK_UPDATE]);
+  b[BK_IMPLICIT] = implicit ? nb((size_t)6 * v.N * v.N, t[BK_IMPLICIT]) : 0u;  // thread per column
+  b[BK_PRIM] = nb((size_t)6 * v.cells, t[BK_PRIM]);
+  b[BK_ROUNDTRIP] = (!shallow && !implicit) ? nb((size_t)6 * v.N * v.N * v.L, t[BK_ROUNDTRIP]) : 0u;
+}
+
+int view_refresh_self(DevView& v, void* stream_v, std::string* err) {
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  SelfBlock h;
+  std::memset(&h, 0, sizeof(h));
+  h.view = v;
+  unsigned b[BK_COUNT];
+  member_blocks(v, v.tiles, b);
+  for (int k = 0; k < BK_COUNT; ++k) h.start[k][1] = b[k];
+  SelfBlock* d = (SelfBlock*)const_cast<DevView*>(v.self);
+  cudaError_t e = stream ? cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, stream)
+                         : cudaMemcpy(d, &h, sizeof(h), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && stream) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    *err = std::string("view upload: ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
+  return 0;
 }
 
 }  // namespace exo
@@ -408,6 +448,10 @@ int exo_create(const exo_config* cfg, exo_ctx** out) {
     return fail(EXO_ERR_ARG, err);
   }
   cudaGetDevice(&c->device);
+  if (exo::fp64::prepare_kernels() || exo::mixed::prepare_kernels()) {
+    delete c;
+    return fail(EXO_ERR_CUDA, "kernel attributes could not be set");
+  }
   auto cleanup = [&](int rc) {
     for (void* p : c->owned) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -560,6 +604,24 @@ int exo_get_time(exo_ctx* c, double* time, int64_t* ncycle) {
   CK(cudaStreamSynchronize(c->stream));
   if (time) *time = s.time;
   if (ncycle) *ncycle = s.ncycle;
+  return EXO_OK;
+}
+
+int exo_set_tiles(exo_ctx* c, const int* threads) {
+  if (!c || !threads) return fail(EXO_ERR_ARG, "NULL argument");
+  int t[exo::BK_COUNT];
+  for (int k = 0; k < exo::BK_COUNT; ++k) t[k] = threads[k] > 0 ? threads[k] : c->v.tiles[k];
+  std::string err;
+  if (!exo::valid_tiles(t, &err)) return fail(EXO_ERR_ARG, err);
+  CK(cudaStreamSynchronize(c->stream));  // launches already queued keep their tables
+  for (int k = 0; k < exo::BK_COUNT; ++k) c->v.tiles[k] = t[k];
+  int rc = exo::view_refresh_self(c->v, c->stream, &err);
+  return rc ? fail(rc, err) : EXO_OK;
+}
+
+int exo_get_tiles(exo_ctx* c, int* threads) {
+  if (!c || !threads) return fail(EXO_ERR_ARG, "NULL argument");
+  for (int k = 0; k < exo::BK_COUNT; ++k) threads[k] = c->v.tiles[k];
   return EXO_OK;
 }
 

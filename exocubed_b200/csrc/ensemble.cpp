@@ -51,6 +51,7 @@ struct exo_ensemble {
   int64_t launches_per_step = 0;
   int64_t launches = 0;
   int device = 0;
+  exo::Tiles tiles = exo::default_tiles();
 };
 
 namespace {
@@ -97,7 +98,7 @@ int rebuild(exo_ensemble* e) {
     int idx = (int)views.size();
     views.push_back(m->v);
     unsigned b[exo::BK_COUNT];
-    exo::member_blocks(m->v, b);
+    exo::member_blocks(m->v, e->tiles.t, b);
     for (int k = 0; k < exo::BK_COUNT; ++k) {
       start[(size_t)k * (e->capacity + 1) + idx] = tot[k];
       tot[k] += b[k];
@@ -127,6 +128,7 @@ int rebuild(exo_ensemble* e) {
   }
   pl.x1_threads = x1_threads;
   pl.x1_smem = x1_smem;
+  for (int k = 0; k < exo::BK_COUNT; ++k) pl.threads[k] = e->tiles.t[k];
   // count the kernel nodes of one step
   int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 + (tot[exo::BK_IMPLICIT] ? 1 : 0) + 1;
   e->launches_per_step = 3 * per_stage + (tot[exo::BK_ROUNDTRIP] ? 1 : 0) + 1 + 1;
@@ -175,6 +177,10 @@ int exo_ensemble_create(int precision, int capacity, size_t budget_bytes, exo_en
   e->budget = budget_bytes;
   e->slots.assign(capacity, nullptr);
   cudaGetDevice(&e->device);
+  if (exo::fp64::prepare_kernels() || exo::mixed::prepare_kernels()) {
+    delete e;
+    return efail(EXO_ERR_CUDA, "kernel attributes could not be set");
+  }
   auto undo = [&](int rc) {
     if (e->d_views) cudaFree(e->d_views);
     if (e->d_start) cudaFree(e->d_start);
@@ -330,6 +336,24 @@ int exo_ensemble_member_time(exo_ensemble* e, int slot, double* time, double* dt
   if (time) *time = s.time;
   if (dt) *dt = s.dt;
   if (ncycle) *ncycle = s.ncycle;
+  return EXO_OK;
+}
+
+int exo_ensemble_set_tiles(exo_ensemble* e, const int* threads) {
+  if (!e || !threads) return efail(EXO_ERR_ARG, "NULL argument");
+  exo::Tiles t = e->tiles;
+  for (int k = 0; k < exo::BK_COUNT; ++k)
+    if (threads[k] > 0) t.t[k] = threads[k];
+  std::string err;
+  if (!exo::valid_tiles(t.t, &err)) return efail(EXO_ERR_ARG, err);
+  e->tiles = t;
+  e->dirty = true;
+  return EXO_OK;
+}
+
+int exo_ensemble_get_tiles(exo_ensemble* e, int* threads) {
+  if (!e || !threads) return efail(EXO_ERR_ARG, "NULL argument");
+  for (int k = 0; k < exo::BK_COUNT; ++k) threads[k] = e->tiles.t[k];
   return EXO_OK;
 }
 

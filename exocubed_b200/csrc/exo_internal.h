@@ -112,6 +112,7 @@ struct DevView {
   // the single-atmosphere launches are batches of one
   const DevView* self;
   const unsigned* starts;
+  int tiles[6];                    // threads per block by BatchKind (see Tiles)
 };
 
 // A batched step: every member's DevView in device memory and, per kernel
@@ -124,9 +125,21 @@ struct BatchPlan {
   unsigned total[BK_COUNT];
   int x1_threads;                // block size of the x1 flux kernel
   size_t x1_smem;                // its dynamic shared memory
+  int threads[BK_COUNT];         // tiles of the other kernels
 };
-// block counts of one member, as the single-atmosphere launchers use them
-void member_blocks(const DevView& v, unsigned blocks[BK_COUNT]);
+// Threads per block ("tile") of each batched kernel by BatchKind.  BK_X1
+// takes one radial column per block (its size follows L) and ignores its
+// entry; the others may be any multiple of 32 in [32, 512], BK_IMPLICIT one of
+// 32, 64, 128.  The per-cell arithmetic does not depend on them.
+struct Tiles {
+  int t[BK_COUNT];
+};
+Tiles default_tiles();
+bool valid_tiles(const int* t, std::string* err);
+// block counts of one member for the given tiles
+void member_blocks(const DevView& v, const int* tiles, unsigned blocks[BK_COUNT]);
+// re-uploads the view's own device copy (tiles and block table)
+int view_refresh_self(DevView& v, void* stream, std::string* err);
 
 // Launchers of one arithmetic build (exo_kernels.cuh): fp64 (kernels.cu) and
 // mixed (kernels_mixed.cu) provide the same set.
@@ -140,7 +153,8 @@ void member_blocks(const DevView& v, unsigned blocks[BK_COUNT]);
   int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream); \
   int launch_set_dt(const DevView& v, double dt, void* stream);                      \
   int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);          \
-  int launch_batched_step(const BatchPlan& plan, void* stream);
+  int launch_batched_step(const BatchPlan& plan, void* stream);                     \
+  int prepare_kernels();
 namespace fp64 { EXO_DECLARE_STEP_LAUNCHERS }
 namespace mixed { EXO_DECLARE_STEP_LAUNCHERS }
 #undef EXO_DECLARE_STEP_LAUNCHERS

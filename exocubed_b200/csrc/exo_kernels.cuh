@@ -1444,12 +1444,14 @@ __device__ __forceinline__ void airparcel_round_trip(double* uu, double Rd, doub
 // Launch shape of the implicit kernels: one thread per radial column, 64
 // columns per block, 60 doubles of shared memory per thread (the face
 // Jacobians |A|(i-1/2) and |A|(i+1/2), the next level's w and du).
-constexpr int IMPL_THREADS = 64;
+constexpr int IMPL_THREADS = 64;      // default; 32 and 128 are the other tiles
+constexpr int IMPL_MAX_THREADS = 128;
 #ifndef EXO_IMPL_MINB
-#define EXO_IMPL_MINB 4  // resident blocks per SM the register budget is sized for
+#define EXO_IMPL_MINB 2  // resident 128-thread blocks per SM the register budget is sized for
 #endif
-#define EXO_IMPL_BOUNDS __launch_bounds__(IMPL_THREADS, EXO_IMPL_MINB)
-constexpr size_t IMPL_SMEM = (size_t)60 * IMPL_THREADS * sizeof(double);
+#define EXO_IMPL_BOUNDS __launch_bounds__(IMPL_MAX_THREADS, EXO_IMPL_MINB)
+constexpr size_t impl_smem(int threads) { return (size_t)60 * threads * sizeof(double); }
+constexpr size_t IMPL_SMEM = impl_smem(IMPL_THREADS);
 
 // A column of the stepping context: primitives and update from the state
 // arrays, the corrected update added to u (with the AirParcel round trip on
@@ -1668,12 +1670,18 @@ inline Batch one(const DevView& v, int kind) { return Batch{v.self, v.starts + 2
 
 inline unsigned member_block_count(const DevView& v, int kind) {
   unsigned b[BK_COUNT];
-  member_blocks(v, b);
+  member_blocks(v, v.tiles, b);
   return b[kind];
 }
 
+int prepare_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(kb_implicit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)impl_smem(IMPL_MAX_THREADS));
+  return e == cudaSuccess ? 0 : EXO_ERR_CUDA;
+}
+
 int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream) {
-  kb_prim_ghost<<<member_block_count(v, BK_PRIM), 256, 0, (cudaStream_t)stream>>>(
+  kb_prim_ghost<<<member_block_count(v, BK_PRIM), v.tiles[BK_PRIM], 0, (cudaStream_t)stream>>>(
       one(v, BK_PRIM), compute_dt ? 1 : 0);
   return check_launch();
 }
@@ -1689,18 +1697,21 @@ int launch_flux_x1(const DevView& v, void* stream) {
 }
 
 int launch_flux_x23(const DevView& v, void* stream) {
-  kb_flux_x23<EXO_FLUX_T><<<member_block_count(v, BK_X23), 128, 0, (cudaStream_t)stream>>>(
+  kb_flux_x23<EXO_FLUX_T><<<member_block_count(v, BK_X23), v.tiles[BK_X23], 0,
+                            (cudaStream_t)stream>>>(
       one(v, BK_X23));
   return check_launch();
 }
 
 int launch_update(const DevView& v, int stage, void* stream) {
-  kb_update<EXO_FLUX_T><<<member_block_count(v, BK_UPDATE), 128, 0, (cudaStream_t)stream>>>(
+  kb_update<EXO_FLUX_T><<<member_block_count(v, BK_UPDATE), v.tiles[BK_UPDATE], 0,
+                          (cudaStream_t)stream>>>(
       one(v, BK_UPDATE), stage);
   int rc = check_launch();
   if (rc) return rc;
   if (v.eqn != EXO_EQN_SHALLOW_YZ && !(v.implicit_flag & 1) && stage == 2) {
-    kb_roundtrip<<<member_block_count(v, BK_ROUNDTRIP), 128, 0, (cudaStream_t)stream>>>(
+    kb_roundtrip<<<member_block_count(v, BK_ROUNDTRIP), v.tiles[BK_ROUNDTRIP], 0,
+                   (cudaStream_t)stream>>>(
         one(v, BK_ROUNDTRIP));
     rc = check_launch();
   }
@@ -1709,8 +1720,8 @@ int launch_update(const DevView& v, int stage, void* stream) {
 
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
-  kb_implicit<<<member_block_count(v, BK_IMPLICIT), IMPL_THREADS, IMPL_SMEM,
-                (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), stage);
+  kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
+                impl_smem(v.tiles[BK_IMPLICIT]), (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), stage);
   return check_launch();
 }
 
@@ -1748,23 +1759,24 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
       kb_flux_x1<EXO_FLUX_T><<<pl.total[BK_X1], pl.x1_threads, pl.x1_smem, st>>>(B(BK_X1));
       if ((rc = check_launch())) return rc;
     }
-    kb_flux_x23<EXO_FLUX_T><<<pl.total[BK_X23], 128, 0, st>>>(B(BK_X23));
+    kb_flux_x23<EXO_FLUX_T><<<pl.total[BK_X23], pl.threads[BK_X23], 0, st>>>(B(BK_X23));
     if ((rc = check_launch())) return rc;
-    kb_update<EXO_FLUX_T><<<pl.total[BK_UPDATE], 128, 0, st>>>(B(BK_UPDATE), s);
+    kb_update<EXO_FLUX_T><<<pl.total[BK_UPDATE], pl.threads[BK_UPDATE], 0, st>>>(B(BK_UPDATE), s);
     if ((rc = check_launch())) return rc;
     if (s == 2 && pl.total[BK_ROUNDTRIP]) {
-      kb_roundtrip<<<pl.total[BK_ROUNDTRIP], 128, 0, st>>>(B(BK_ROUNDTRIP));
+      kb_roundtrip<<<pl.total[BK_ROUNDTRIP], pl.threads[BK_ROUNDTRIP], 0, st>>>(B(BK_ROUNDTRIP));
       if ((rc = check_launch())) return rc;
     }
     if (pl.total[BK_IMPLICIT]) {
-      kb_implicit<<<pl.total[BK_IMPLICIT], IMPL_THREADS, IMPL_SMEM, st>>>(B(BK_IMPLICIT), s);
+      kb_implicit<<<pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT], impl_smem(pl.threads[BK_IMPLICIT]),
+                    st>>>(B(BK_IMPLICIT), s);
       if ((rc = check_launch())) return rc;
     }
     if (s == 2) {
       kb_dt_reset<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n);
       if ((rc = check_launch())) return rc;
     }
-    kb_prim_ghost<<<pl.total[BK_PRIM], 256, 0, st>>>(B(BK_PRIM), s == 2 ? 1 : 0);
+    kb_prim_ghost<<<pl.total[BK_PRIM], pl.threads[BK_PRIM], 0, st>>>(B(BK_PRIM), s == 2 ? 1 : 0);
     if ((rc = check_launch())) return rc;
   }
   kb_dt_finalize<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n, 1);

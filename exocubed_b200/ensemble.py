@@ -32,6 +32,7 @@ class Ensemble:
         nat.check(nat.lib().exo_ensemble_create(int(precision), int(capacity),
                                                 int(budget_bytes), ctypes.byref(self._h)))
         self.shapes = {}
+        self.cfgs = {}
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -55,6 +56,7 @@ class Ensemble:
         nat.check(nat.lib().exo_ensemble_add(self._h, ctypes.byref(c), nat.dptr(w),
                                              ctypes.byref(slot)))
         self.shapes[slot.value] = w.shape
+        self.cfgs[slot.value] = {f: getattr(c, f) for f, _ in nat.ExoConfig._fields_}
         return slot.value
 
     def try_add(self, cfg, w):
@@ -68,6 +70,7 @@ class Ensemble:
     def remove(self, slot):
         nat.check(nat.lib().exo_ensemble_remove(self._h, int(slot)))
         self.shapes.pop(slot, None)
+        self.cfgs.pop(slot, None)
 
     def step(self, nsteps=1):
         nat.check(nat.lib().exo_ensemble_step(self._h, int(nsteps)))
@@ -90,6 +93,24 @@ class Ensemble:
         nat.check(nat.lib().exo_ensemble_member_time(self._h, int(slot), ctypes.byref(t),
                                                      ctypes.byref(dt), ctypes.byref(n)))
         return t.value, dt.value, n.value
+
+    @property
+    def tiles(self):
+        t = (ctypes.c_int * nat.EXO_TILE_COUNT)()
+        nat.check(nat.lib().exo_ensemble_get_tiles(self._h, t))
+        return list(t)
+
+    def set_tiles(self, threads):
+        """Launch tiles of the batched step (exo_ensemble_set_tiles)."""
+        t = (ctypes.c_int * nat.EXO_TILE_COUNT)(*[int(x) for x in threads])
+        nat.check(nat.lib().exo_ensemble_set_tiles(self._h, t))
+
+    def autotune(self, cache=None):
+        """Tiles minimising the summed per-member kernel times (autotune.py)."""
+        from . import autotune
+        tiles = autotune.batch_tiles(list(self.cfgs.values()), cache)
+        self.set_tiles(tiles)
+        return tiles
 
     def invalid(self, slot):
         """Non-zero if the member's state turned invalid since the last call."""

@@ -66,10 +66,14 @@ class Server:
     max_chunk      steps launched between two admission checks (a chunk never
                    runs a member past its last step)
     keep_results   keep each request's final conserved state in its record
+    tile_cache     an autotune.TileCache: when given, the batch's launch tiles
+                   follow its members (autotune.batch_tiles) after every
+                   membership change
     """
 
     def __init__(self, precision=nat.EXO_PREC_MIXED, capacity=64, budget_bytes=150 * 10 ** 9,
-                 max_chunk=8, keep_results=False):
+                 max_chunk=8, keep_results=False, tile_cache=None):
+        self.tile_cache = tile_cache
         self.precision = precision
         self.capacity = capacity
         self.budget = budget_bytes
@@ -101,6 +105,7 @@ class Server:
         def now():
             return time.perf_counter() - t0 if clock == "wall" else float(nstep)
 
+        changed = False
         while pending or queue or active:
             t = now()
             while pending and pending[0].arrival <= t:
@@ -115,6 +120,7 @@ class Server:
                 queue.popleft()
                 active[slot] = [r, r.steps]
                 recs[r.rid].admitted = now()
+                changed = True
             if not active:
                 if pending:
                     if clock == "wall":
@@ -122,6 +128,9 @@ class Server:
                     else:
                         nstep = int(np.ceil(pending[0].arrival))
                 continue
+            if changed and self.tile_cache is not None:
+                self.ens.autotune(self.tile_cache)
+            changed = False
             chunk = min(self.max_chunk, min(left for _, left in active.values()))
             if clock == "steps" and pending:
                 chunk = max(1, min(chunk, int(np.ceil(pending[0].arrival)) - nstep))
@@ -138,6 +147,7 @@ class Server:
                 rec = recs[r.rid]
                 rec.valid = self.ens.invalid(slot) == 0
                 self.ens.remove(slot)
+                changed = True
                 rec.done = now()
                 if self.keep:
                     rec.result = u

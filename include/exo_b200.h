@@ -179,6 +179,17 @@ enum {
    synchronizes and returns the launches and the summed device time (ms) of
    one kernel since profiling was enabled. */
 int exo_profile(exo_ctx* ctx, int enable);
+
+/* Launch tiles: threads per block of each kernel, indexed by EXO_K_* (the
+   EXO_K_OTHER slot is the last-stage AirParcel round trip of atmospheres
+   without the implicit solver).  The x1 kernel takes one radial column per
+   block and ignores its slot; the others take a multiple of 32 in [32, 512],
+   EXO_K_IMPLICIT one of 32, 64, 128 (radial columns per block); 0 keeps the
+   current value.  The results do not depend on the tiles, only the speed
+   does.  No counterpart in the reference (its CPU loops have no launch shape). */
+#define EXO_TILE_COUNT 6
+int exo_set_tiles(exo_ctx* ctx, const int* threads);
+int exo_get_tiles(exo_ctx* ctx, int* threads);
 int exo_profile_read(exo_ctx* ctx, int kernel, int64_t* launches, double* total_ms);
 
 /* Kernel launches issued by this context since it was created. */
@@ -287,6 +298,10 @@ int exo_ensemble_get_conserved(exo_ensemble* ens, int slot, double* u_host);
 int exo_ensemble_get_primitive(exo_ensemble* ens, int slot, double* w_host);
 int exo_ensemble_member_time(exo_ensemble* ens, int slot, double* time, double* dt,
                              int64_t* ncycle);
+/* Launch tiles of the batched step (as exo_set_tiles); the next
+   exo_ensemble_step re-captures its graph with them. */
+int exo_ensemble_set_tiles(exo_ensemble* ens, const int* threads);
+int exo_ensemble_get_tiles(exo_ensemble* ens, int* threads);
 /* MeshBlock::Impl::IsStateValid for one member: the sticky device flag set
    when a cell's density or pressure turned non-positive or NaN, cleared on
    read (as exo_check_state). */
