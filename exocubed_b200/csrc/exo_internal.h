@@ -83,7 +83,7 @@ struct DevScalars {
 
 // Sizes, parameters and device pointers of one atmosphere; passed by value
 // to every kernel.
-struct DevView {
+struct alignas(16) DevView {
   int N, L, nv, nc1, nc2, nc3;
   int is, ie, js, je, ks, ke;
   int eqn, rsolver, implicit_flag, coriolis;

@@ -41,6 +41,11 @@ constexpr double WENO_EPS = 1.0e-7;
 __device__ __forceinline__ double sqr(double x) { return x * x; }
 __device__ __forceinline__ float sqr(float x) { return x * x; }
 
+// SSPRK(3,3) stage weights beta = 1, 1/4, 2/3
+__device__ __forceinline__ double rk_beta(int stage) {
+  return stage == 0 ? 1.0 : (stage == 1 ? 0.25 : 2.0 / 3.0);
+}
+
 __device__ __forceinline__ size_t idx(const DevView& v, int p, int n, int k, int j, int i) {
   return ((((size_t)p * v.nv + n) * v.nc3 + k) * v.nc2 + j) * v.nc1 + i;
 }
@@ -218,7 +223,7 @@ __device__ __forceinline__ void flux_to_global(int ivx, const FaceGeo<T>& fg, T*
 
 // roe_shallow_yz.cpp:18-122
 template <class T>
-__device__ void riemann_roe_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wri, T* flx) {
+__device__ __forceinline__ void riemann_roe_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wri, T* flx) {
   const T h = T(0.5);
   int ivy = ivx == IVY ? IVZ : IVY;
   prim_to_local(ivx, fg, wli);
@@ -266,7 +271,7 @@ __device__ void riemann_roe_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wr
 
 // lmars.cpp:24-110 (NVAPOR = NCLOUD = 0), no projection
 template <class T>
-__device__ void riemann_lmars(double gamma_d, int ivx, const T* wli, const T* wri, T* flx) {
+__device__ __forceinline__ void riemann_lmars(double gamma_d, int ivx, const T* wli, const T* wri, T* flx) {
   const T h = T(0.5), one = T(1.);
   T gamma = T(gamma_d);
   int ivy = IVX + ((ivx - IVX) + 1) % 3;
@@ -301,7 +306,7 @@ __device__ void riemann_lmars(double gamma_d, int ivx, const T* wli, const T* wr
 
 // hllc_transform.cpp:24-263
 template <class T>
-__device__ void riemann_hllc(double gamma_d, int ivx, const FaceGeo<T>& fg, T* wl, T* wr, T* flx) {
+__device__ __forceinline__ void riemann_hllc(double gamma_d, int ivx, const FaceGeo<T>& fg, T* wl, T* wr, T* flx) {
   const T h = T(.5), one = T(1.0), zero = T(0.0);
   T gamma = T(gamma_d);
   int ivy = IVX + ((ivx - IVX) + 1) % 3;
@@ -385,7 +390,7 @@ __device__ void riemann_hllc(double gamma_d, int ivx, const FaceGeo<T>& fg, T* w
 
 // lmars_shallow_yz.cpp:18-93
 template <class T>
-__device__ void riemann_lmars_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wri, T* flx) {
+__device__ __forceinline__ void riemann_lmars_shallow(int ivx, const FaceGeo<T>& fg, T* wli, T* wri, T* flx) {
   const T h = T(0.5);
   int ivy = ivx == IVY ? IVZ : IVY;
   prim_to_local(ivx, fg, wli);
@@ -428,12 +433,18 @@ __device__ __forceinline__ void riemann(int rsolver, double gamma, int ivx, cons
 __device__ __forceinline__ void load_cons(const DevView& v, int p, int k, int j, int i,
                                           bool interior, double* c) {
   if (interior) {
-    for (int n = 0; n < v.nv; ++n) c[n] = v.u[idx(v, p, n, k, j, i)];
+    #pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= v.nv) break;
+      c[n] = v.u[idx(v, p, n, k, j, i)];
+    }
     return;
   }
   const GhostEntry& e = v.ghost[v.ghost_map[((size_t)p * v.nc3 + k) * v.nc2 + j]];
   int sp = e.src_panel;
-  for (int n = 0; n < v.nv; ++n) {
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
     if (n == IVY || n == IVZ) continue;
     double v1 = v.u[idx(v, sp, n, e.k0, e.j0, i)];
     double v2 = v.u[idx(v, sp, n, e.k1, e.j1, i)];
@@ -503,9 +514,17 @@ __device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, 
   double cth = geo(v, GCOSC, p, k, j);
   int bad = cons_to_prim(v, c, w, cth);
   if (mirror) w[IVX] = -w[IVX];
-  for (int n = 0; n < v.nv; ++n) v.w[idx(v, p, n, k, j, i)] = w[n];
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
+    v.w[idx(v, p, n, k, j, i)] = w[n];
+  }
 #if EXO_MIXED
-  for (int n = 0; n < v.nv; ++n) v.w32[idx(v, p, n, k, j, i)] = (float)w[n];
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
+    v.w32[idx(v, p, n, k, j, i)] = (float)w[n];
+  }
 #endif
   if (!(kin && jin) || mirror) return none;
   if (bad) atomicOr(&v.sc->invalid, 1);
@@ -596,7 +615,9 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
     int i = v.is + f;
     // perturbations are formed in FP64 above; WENO5 and the Riemann solve run in T
     T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
-    for (int n = 0; n < nv; ++n) {
+    #pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
       const double* q = wc + n * nc1;
       wl[n] = weno_r<T>(q, 1, i - 1);
       wr[n] = weno_l<T>(q, 1, i);
@@ -620,8 +641,14 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       wr[IDN] = T(dr);
       wl[IDN] = T(dl);
     }
-    riemann<T>(v.rsolver, v.gamma, IVX, fg, wl, wr, fx);
-    for (int n = 0; n < nv; ++n) F[idx(v, p, n, k, j, i)] = fx[n];
+    // x1 runs for the ideal gas only: LMARS or HLLC
+    if (v.rsolver == EXO_RS_HLLC) riemann_hllc<T>(v.gamma, IVX, fg, wl, wr, fx);
+    else riemann_lmars<T>(v.gamma, IVX, wl, wr, fx);
+    #pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
+      F[idx(v, p, n, k, j, i)] = fx[n];
+    }
   }
 }
 
@@ -634,7 +661,9 @@ __device__ __forceinline__ void edge_interior_state(const DevView& v, int p, int
                                                     int i, T* st) {
   long s2 = v.nc1, s3 = (long)v.nc1 * v.nc2;
   const T* W = prim_array<T>(v);
-  for (int n = 0; n < v.nv; ++n) {
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
     if (s == UP || s == DOWN) {
       const T* q = W + idx(v, p, n, v.ks + a, 0, i);
       st[n] = (s == DOWN) ? weno_r<T>(q, s2, v.je) : weno_l<T>(q, s2, v.js);
@@ -686,7 +715,9 @@ __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
   FaceGeo<T> fg;
   int ivx;
   if (dir == 1) {
-    for (int n = 0; n < v.nv; ++n) {
+    #pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= v.nv) break;
       const T* q = W + idx(v, p, n, k, 0, i);
       wl[n] = weno_r<T>(q, s2, j - 1);
       wr[n] = weno_l<T>(q, s2, j);
@@ -697,7 +728,9 @@ __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
                     T(geo(v, GCTHP2, p, k, j)), T(geo(v, GCOSC, p, k, j))};
     ivx = IVY;
   } else {
-    for (int n = 0; n < v.nv; ++n) {
+    #pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= v.nv) break;
       const T* q = W + idx(v, p, n, 0, j, i);
       wl[n] = weno_r<T>(q, s3, k - 1);
       wr[n] = weno_l<T>(q, s3, k);
@@ -708,66 +741,97 @@ __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
                     T(geo(v, GCTHP3, p, k, j)), T(geo(v, GCOSC, p, k, j))};
     ivx = IVZ;
   }
-  riemann<T>(v.rsolver, v.gamma, ivx, fg, wl, wr, fx);
+  // the velocity index as a literal, so the solvers index registers only
+  if (ivx == IVY) riemann<T>(v.rsolver, v.gamma, IVY, fg, wl, wr, fx);
+  else riemann<T>(v.rsolver, v.gamma, IVZ, fg, wl, wr, fx);
   T* F = flux_array<T>(v, dir);
-  for (int n = 0; n < v.nv; ++n) F[idx(v, p, n, k, j, i)] = fx[n];
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
+    F[idx(v, p, n, k, j, i)] = fx[n];
+  }
 }
 
 // --------------------------------------------------------------- k_update -
 template <class T>
 __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int stage) {
-  unsigned tid = blk * blockDim.x + threadIdx.x;
-  unsigned L = v.L, N = v.N;
+  const unsigned tid = blk * blockDim.x + threadIdx.x;
+  const unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
-  int i = v.is + (int)(tid % L);
+  const int i = v.is + (int)(tid % L);
   unsigned r = tid / L;
-  int j = v.js + (int)(r % N);
+  const int j = v.js + (int)(r % N);
   r /= N;
-  int k = v.ks + (int)(r % N);
-  int p = (int)(r / N);
-  const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
-  double wght = kBeta[stage] * v.sc->dt;
-  bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
-  int nv = v.nv;
+  const int k = v.ks + (int)(r % N);
+  const int p = (int)(r / N);
+  const double wght = rk_beta(stage) * v.sc->dt;
+  const bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
+  const int nv = v.nv;
+  // offsets: this cell (variable 0), variable stride, +1 in j and in k
+  const size_t c0 = idx(v, p, 0, k, j, i), vs = v.cells;
+  const size_t sj = (size_t)v.nc1, sk = (size_t)v.nc2 * v.nc1;
+  // geometry of the column (k,j) and of its upper x2/x3 neighbours
+  const size_t g0 = ((size_t)p * v.nc3 + k) * v.nc2 + j, gs = (size_t)6 * v.nc3 * v.nc2;
+  auto G2 = [&](int f, size_t off) { return __ldg(v.geo + f * gs + g0 + off); };
+  const double* uin = v.u + c0;  // read here, written below
+  const double* u1in = v.u1 + c0;
+  const double* __restrict__ win = v.w + c0;
+  const T* __restrict__ F0 = flux_array<T>(v, 0) + c0;
+  const T* __restrict__ F1 = flux_array<T>(v, 1) + c0;
+  const T* __restrict__ F2 = flux_array<T>(v, 2) + c0;
+  // every input of the cell is requested before any is used
+  double uu[5], u1v[5], wv[5];
+  T f0l[5], f0r[5], f1l[5], f1r[5], f2l[5], f2r[5];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= nv) break;
+    uu[n] = uin[n * vs];
+    u1v[n] = stage ? u1in[n * vs] : 0.;
+    wv[n] = __ldg(win + n * vs);
+    f0l[n] = shallow ? T(0.) : __ldg(F0 + n * vs);
+    f0r[n] = shallow ? T(0.) : __ldg(F0 + n * vs + 1);
+    f1l[n] = __ldg(F1 + n * vs);
+    f1r[n] = __ldg(F1 + n * vs + sj);
+    f2l[n] = __ldg(F2 + n * vs);
+    f2r[n] = __ldg(F2 + n * vs + sk);
+  }
+  const double x1fi = __ldg(v.x1f + i), x1fp = __ldg(v.x1f + i + 1);
+  const double x1vi = __ldg(v.x1v + i), dx1fi = __ldg(v.dx1f + i);
   double un[5];
   // WeightedAve(u1, u, ...) then WeightedAve(u, u1, ...) (SSPRK(3,3) registers)
-  for (int n = 0; n < nv; ++n) {
-    size_t q = idx(v, p, n, k, j, i);
-    double uu = v.u[q];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= nv) break;
     if (stage == 0) {
-      v.u1[q] = uu;
-      un[n] = 0. + 1.0 * uu;
+      v.u1[c0 + n * vs] = uu[n];
+      un[n] = 0. + 1.0 * uu[n];
     } else if (stage == 1) {
-      un[n] = 0.25 * uu + 0.75 * v.u1[q];
+      un[n] = 0.25 * uu[n] + 0.75 * u1v[n];
     } else {
-      un[n] = (2.0 / 3.0) * uu + (1.0 / 3.0) * v.u1[q];
+      un[n] = (2.0 / 3.0) * uu[n] + (1.0 / 3.0) * u1v[n];
     }
   }
   // AddFluxDivergence
-  double s = geo(v, GSINC, p, k, j);
-  double d2 = geo(v, GDX2A, p, k, j), d3 = geo(v, GDX3A, p, k, j);
-  double a1 = d2 * d3 * v.x1f[i] * v.x1f[i] * s;
-  double a1p = d2 * d3 * v.x1f[i + 1] * v.x1f[i + 1] * s;
-  double a2 = v.x1v[i] * geo(v, GDX3A_F2, p, k, j) * v.dx1f[i];
-  double a2p = v.x1v[i] * geo(v, GDX3A_F2, p, k, j + 1) * v.dx1f[i];
-  double a3 = v.x1v[i] * geo(v, GDX2A_F3, p, k, j) * v.dx1f[i];
-  double a3p = v.x1v[i] * geo(v, GDX2A_F3, p, k + 1, j) * v.dx1f[i];
-  double vol = v.dx1f[i] * d2 * d3 * v.x1v[i] * v.x1v[i] * s;
+  const double s = G2(GSINC, 0);
+  const double d2 = G2(GDX2A, 0), d3 = G2(GDX3A, 0);
+  const double dx3f2 = G2(GDX3A_F2, 0), dx3f2p = G2(GDX3A_F2, 1);
+  const double dx2f3 = G2(GDX2A_F3, 0), dx2f3p = G2(GDX2A_F3, v.nc2);
+  const double a1 = d2 * d3 * x1fi * x1fi * s;
+  const double a1p = d2 * d3 * x1fp * x1fp * s;
+  const double a2 = x1vi * dx3f2 * dx1fi;
+  const double a2p = x1vi * dx3f2p * dx1fi;
+  const double a3 = x1vi * dx2f3 * dx1fi;
+  const double a3p = x1vi * dx2f3p * dx1fi;
+  const double vol = dx1fi * d2 * d3 * x1vi * x1vi * s;
   double du[5];
-  const T* F0 = flux_array<T>(v, 0);
-  const T* F1 = flux_array<T>(v, 1);
-  const T* F2 = flux_array<T>(v, 2);
   // flux divergence in T; the conserved state accumulates in FP64
-  T A1 = T(a1), A1p = T(a1p), A2 = T(a2), A2p = T(a2p), A3 = T(a3), A3p = T(a3p);
-  for (int n = 0; n < nv; ++n) {
-    T dflx;
-    if (shallow) {
-      dflx = (A1p * T(0.) - A1 * T(0.));
-    } else {
-      dflx = (A1p * F0[idx(v, p, n, k, j, i + 1)] - A1 * F0[idx(v, p, n, k, j, i)]);
-    }
-    dflx += (A2p * F1[idx(v, p, n, k, j + 1, i)] - A2 * F1[idx(v, p, n, k, j, i)]);
-    dflx += (A3p * F2[idx(v, p, n, k + 1, j, i)] - A3 * F2[idx(v, p, n, k, j, i)]);
+  const T A1 = T(a1), A1p = T(a1p), A2 = T(a2), A2p = T(a2p), A3 = T(a3), A3p = T(a3p);
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= nv) break;
+    T dflx = (A1p * f0r[n] - A1 * f0l[n]);
+    dflx += (A2p * f1r[n] - A2 * f1l[n]);
+    dflx += (A3p * f2r[n] - A3 * f2l[n]);
     double change;
     if constexpr (sizeof(T) == sizeof(double)) {
       change = wght * dflx / vol;
@@ -784,25 +848,21 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   double* out = shallow ? un : du;
   // AddCoordTermsDivergence (gnomonic_equiangle.cpp:834-879)
   {
-    double cosine = geo(v, GCOSC, p, k, j);
-    double sine2 = s * s;
-    double x_ov_rD = (v.x1v[i] * geo(v, GDX3A_F2, p, k, j) * v.dx1f[i] * geo(v, GSINF2, p, k, j) -
-                      v.x1v[i] * geo(v, GDX3A_F2, p, k, j + 1) * v.dx1f[i] *
-                          geo(v, GSINF2, p, k, j + 1)) / vol;
-    double y_ov_rC = (v.x1v[i] * geo(v, GDX2A_F3, p, k, j) * v.dx1f[i] * geo(v, GSINF3, p, k, j) -
-                      v.x1v[i] * geo(v, GDX2A_F3, p, k + 1, j) * v.dx1f[i] *
-                          geo(v, GSINF3, p, k + 1, j)) / vol;
-    double rho = v.w[idx(v, p, IDN, k, j, i)];
-    double v1 = v.w[idx(v, p, IVX, k, j, i)], v2 = v.w[idx(v, p, IVY, k, j, i)];
-    double v3 = v.w[idx(v, p, IVZ, k, j, i)];
-    double radius = v.x1v[i];
+    const double cosine = G2(GCOSC, 0);
+    const double sine2 = s * s;
+    const double x_ov_rD = (x1vi * dx3f2 * dx1fi * G2(GSINF2, 0) -
+                            x1vi * dx3f2p * dx1fi * G2(GSINF2, 1)) / vol;
+    const double y_ov_rC = (x1vi * dx2f3 * dx1fi * G2(GSINF3, 0) -
+                            x1vi * dx2f3p * dx1fi * G2(GSINF3, v.nc2)) / vol;
+    const double rho = wv[IDN], v1 = wv[IVX], v2 = wv[IVY], v3 = wv[IVZ];
+    const double radius = x1vi;
     double pr;
-    double v_2 = v2 + v3 * cosine;
-    double v_3 = v3 + v2 * cosine;
+    const double v_2 = v2 + v3 * cosine;
+    const double v_3 = v3 + v2 * cosine;
     if (shallow) {
       pr = 0.5 * rho * rho;
     } else {
-      pr = v.w[idx(v, p, IPR, k, j, i)];
+      pr = wv[IPR];
       double src1 = (2.0 * pr + rho * (v2 * v_2 + v3 * v_3)) / radius;
       out[IVX] += wght * src1;
     }
@@ -818,28 +878,33 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
     }
     // W92 Coriolis (examples/2023-Chen-exo3/W92.cpp:48-70)
     if (v.coriolis == EXO_CORIOLIS_W92) {
-      double f = geo(v, GFCOR, p, k, j);
-      double U = geo(v, GCR0, p, k, j) * v2 + geo(v, GCR1, p, k, j) * v3;
-      double V = geo(v, GCR2, p, k, j) * v2 + geo(v, GCR3, p, k, j) * v3;
+      double f = G2(GFCOR, 0);
+      double U = G2(GCR0, 0) * v2 + G2(GCR1, 0) * v3;
+      double V = G2(GCR2, 0) * v2 + G2(GCR3, 0) * v3;
       U = -U;
       double llU = f * V, llV = -f * U;
       double mU = -llU;
-      double acc2 = geo(v, GCQ0, p, k, j) * mU + geo(v, GCQ1, p, k, j) * llV;
-      double acc3 = geo(v, GCQ2, p, k, j) * mU + geo(v, GCQ3, p, k, j) * llV;
+      double acc2 = G2(GCQ0, 0) * mU + G2(GCQ1, 0) * llV;
+      double acc3 = G2(GCQ2, 0) * mU + G2(GCQ3, 0) * llV;
       double a2c = acc2 + acc3 * cosine, a3c = acc3 + acc2 * cosine;
       out[IVY] += wght * rho * a2c;
       out[IVZ] += wght * rho * a3c;
     }
   }
+  double* uout = v.u + c0;
   if (shallow) {
-    for (int n = 0; n < nv; ++n) v.u[idx(v, p, n, k, j, i)] = un[n];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) uout[n * vs] = un[n];
   } else if (v.implicit_flag & 1) {
-    for (int n = 0; n < nv; ++n) {
-      v.u[idx(v, p, n, k, j, i)] = un[n];
-      v.du[idx(v, p, n, k, j, i)] = du[n];
+    double* duout = v.du + c0;
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      uout[n * vs] = un[n];
+      duout[n * vs] = du[n];
     }
   } else {
-    for (int n = 0; n < nv; ++n) v.u[idx(v, p, n, k, j, i)] = un[n] + 1. * du[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uout[n * vs] = un[n] + 1. * du[n];
   }
 }
 
@@ -1065,7 +1130,9 @@ __device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const dou
 // until it becomes |A|(i-1/2) of the next level.
 //   io.w(i, out[5])  primitives of level i (is-1 .. ie+2), unprojected
 //   io.scr(lev, e)   scratch double e (0..29) of level lev = i - is
-//   io.out(i, d[5])  corrected update of level i, from ie down to is
+//   io.uload(i, u[5]), io.ustore(i, u[5], d[5])  the corrected update d of
+//                    level i, from ie down to is, with the state u loaded
+//                    for it beforehand (callers that only need d load nothing)
 //   io.wptr(i, n), io.duptr(i, n)  addresses of w and of the explicit update
 //                    du of level i (the inputs are prefetched through shared memory)
 //   sm               this thread's 60 doubles of shared memory, stride sms
@@ -1379,21 +1446,41 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
     c0 = cp;
     cur = nxt;
   }
-  // back substitution: delta_i -= (A c)_i delta_{i+1}
-  io.out(ie, dp);
+  // back substitution: delta_i -= (A c)_i delta_{i+1}, software-pipelined:
+  // the next level's scratch and state are in flight while this level ends
+  double cur_s[30], cur_u[5];
+  io.uload(ie, cur_u);
+  io.ustore(ie, cur_u, dp);
+  if (ie > is) {
+#pragma unroll
+    for (int e = 0; e < 30; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
+    io.uload(ie - 1, cur_u);
+  }
+#pragma unroll 1
   for (int i = ie - 1; i >= is; --i) {
-    const int lev = i - is;
+    double nxt_s[30], nxt_u[5];
+    if (i > is) {
+#pragma unroll
+      for (int e = 0; e < 30; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
+      io.uload(i - 1, nxt_u);
+    }
     double dl[5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      double ad = io.scr(lev, r * 5) * dp[0];
+      double ad = cur_s[r * 5] * dp[0];
 #pragma unroll
-      for (int k = 1; k < 5; ++k) ad += io.scr(lev, r * 5 + k) * dp[k];
-      dl[r] = io.scr(lev, 25 + r) - ad;
+      for (int k = 1; k < 5; ++k) ad += cur_s[r * 5 + k] * dp[k];
+      dl[r] = cur_s[25 + r] - ad;
     }
 #pragma unroll
     for (int r = 0; r < 5; ++r) dp[r] = dl[r];
-    io.out(i, dp);
+    io.ustore(i, cur_u, dp);
+    if (i > is) {
+#pragma unroll
+      for (int e = 0; e < 30; ++e) cur_s[e] = nxt_s[e];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) cur_u[n] = nxt_u[n];
+    }
   }
 }
 
@@ -1474,10 +1561,14 @@ struct StepColumnIO {
   __device__ __forceinline__ double& scr(int lev, int e) const {
     return scr0[((size_t)lev * 30 + e) * nslot];
   }
-  __device__ __forceinline__ void out(int i, const double* dl) const {
+  __device__ __forceinline__ void uload(int i, double* u) const {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) u[n] = uc[n * vs + i];
+  }
+  __device__ __forceinline__ void ustore(int i, const double* u, const double* dl) const {
     double uu[5];
 #pragma unroll
-    for (int n = 0; n < 5; ++n) uu[n] = uc[n * vs + i] + 1. * dl[n];
+    for (int n = 0; n < 5; ++n) uu[n] = u[n] + 1. * dl[n];
     if (stage == 2) airparcel_round_trip(uu, Rd, gamma);
 #pragma unroll
     for (int n = 0; n < 5; ++n) uc[n * vs + i] = uu[n];
@@ -1494,8 +1585,7 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const int j = v.js + col % v.N;
   const int k = v.ks + (col / v.N) % v.N;
   const int p = col / (v.N * v.N);
-  const double kBeta[3] = {1.0, 0.25, 2.0 / 3.0};
-  const double dt = kBeta[stage] * v.sc->dt;
+  const double dt = rk_beta(stage) * v.sc->dt;
   const size_t base = idx(v, p, 0, k, j, 0);
   StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, v.scratch + col, (size_t)ncol,
                   stage, v.Rd, v.gamma};
@@ -1532,9 +1622,17 @@ __device__ __forceinline__ void p2c_block(const DevView& v, unsigned blk, const 
   int k = v.ks + (int)(r % N);
   int p = (int)(r / N);
   double w[5], c[5];
-  for (int n = 0; n < v.nv; ++n) w[n] = wsrc[idx(v, p, n, k, j, i)];
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
+    w[n] = wsrc[idx(v, p, n, k, j, i)];
+  }
   prim_to_cons(v, w, c, geo(v, GCOSC, p, k, j));
-  for (int n = 0; n < v.nv; ++n) v.u[idx(v, p, n, k, j, i)] = c[n];
+  #pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= v.nv) break;
+    v.u[idx(v, p, n, k, j, i)] = c[n];
+  }
 }
 
 __global__ void k_set_dt(DevScalars* sc, double dt) { sc->dt = dt; }
@@ -1581,27 +1679,34 @@ __device__ __forceinline__ int batch_member(const Batch& bt, unsigned b) {
   return lo;
 }
 
-// copies the member's view into shared memory; returns its local block
+// copies the member's view into shared memory, 16 bytes per thread; returns
+// the block's index within the member
 __device__ __forceinline__ unsigned batch_enter(const Batch& bt, DevView& sv) {
-  __shared__ unsigned local;
-  if (threadIdx.x == 0) {
-    int m = batch_member(bt, blockIdx.x);
-    sv = bt.views[m];
-    local = blockIdx.x - bt.start[m];
-  }
+  static_assert(sizeof(DevView) % 16 == 0, "DevView is copied in 16-byte words");
+  const int m = batch_member(bt, blockIdx.x);  // the same for every thread
+  const int4* src = reinterpret_cast<const int4*>(bt.views + m);
+  int4* dst = reinterpret_cast<int4*>(&sv);
+  for (int t = threadIdx.x; t < (int)(sizeof(DevView) / 16); t += blockDim.x) dst[t] = src[t];
+  const unsigned local = blockIdx.x - bt.start[m];
   __syncthreads();
   return local;
 }
 
 __global__ void kb_prim_ghost(Batch bt, int compute_dt) {
-  __shared__ DevView sv;
+  __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   prim_ghost_block(sv, b, compute_dt);
 }
 
+// The x1 kernel is latency bound (one thread walks the hydrostatic scan of
+// the column while the others wait): occupancy beats registers, measured
+#ifndef EXO_X1_MINB
+#define EXO_X1_MINB 5
+#endif
+#define EXO_X1_BOUNDS __launch_bounds__(256, EXO_X1_MINB)
 template <class T>
-__global__ void kb_flux_x1(Batch bt) {
-  __shared__ DevView sv;
+__global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
+  __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ) return;
   flux_x1_block<T>(sv, b);
@@ -1609,27 +1714,27 @@ __global__ void kb_flux_x1(Batch bt) {
 
 template <class T>
 __global__ void kb_flux_x23(Batch bt) {
-  __shared__ DevView sv;
+  __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   flux_x23_block<T>(sv, b);
 }
 
 template <class T>
 __global__ void kb_update(Batch bt, int stage) {
-  __shared__ DevView sv;
+  __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   update_block<T>(sv, b, stage);
 }
 
 __global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage) {
-  __shared__ DevView sv;
+  __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
   implicit_block(sv, b, stage);
 }
 
 __global__ void kb_roundtrip(Batch bt) {
-  __shared__ DevView sv;
+  __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || (sv.implicit_flag & 1)) return;
   roundtrip_block(sv, b);

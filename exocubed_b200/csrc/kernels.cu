@@ -37,7 +37,8 @@ struct HookColumnIO {
   __device__ __forceinline__ double& scr(int lev, int e) const {
     return scr0[((size_t)lev * 30 + e) * nslot];
   }
-  __device__ __forceinline__ void out(int i, const double* dl) const {
+  __device__ __forceinline__ void uload(int, double*) const {}
+  __device__ __forceinline__ void ustore(int i, const double*, const double* dl) const {
 #pragma unroll
     for (int n = 0; n < 5; ++n) duc[n * L + (i - G)] = dl[n];
   }
