@@ -1,13 +1,23 @@
 """Benchmark: cell-updates/s of the cubed-sphere finite-volume step on B200.
 
-Workload (default): the exo3 dry ideal-gas atmosphere, 6 panels x 96 x 96 x
-64 levels, FP64, WENO5 + LMARS + the 5x5 implicit vertical solver
-(implicit_flag 9), SSPRK(3,3), CFL time step -- a seeded synthetic state
+Default workload (c3): the exo3 dry ideal-gas atmosphere, 6 panels x 192 x
+192 x 96 levels, WENO5 + LMARS + the 5x5 implicit vertical solver
+(implicit_flag 9), SSPRK(3,3), CFL time step, on a seeded synthetic state
 (isothermal 250 K hydrostatic column, 1 K temperature noise, 5 m/s winds).
 A "step" is one SSPRK(3,3) step of the whole atmosphere; one cell-update is
 one interior cell advanced one step (6*N*N*L per step).
 
+The line's value is the mixed-precision path (FP32 reconstruction, Riemann
+fluxes and flux divergence; FP64 decomposition, implicit solve and state);
+"fp64" is the plain FP64 path on the same workload in the same run;
+"accuracy" compares the two after --accuracy-steps steps; "serving" is a
+short continuous-batching sample (ensemble-member requests, p50/p99 latency)
+with the FP64 one-at-a-time path beside it.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1|c2|c2s|c3|c4] [--precision 0|1]
+  python bench.py --accuracy 1000            (mixed vs FP64 after 1000 steps)
+  python bench.py --serve 10,100,2000        (serving sweep, one line per rate)
 
 Multi-GPU: one process per GPU; every rank advances its own atmosphere (an
 independent ensemble member), so there is no data-path collective and the
@@ -17,7 +27,8 @@ synchronize on both sides, max over ranks.
 --impl reference times the reference's CPU algorithm on this host's cores.
 The reference itself cannot be built here (its Athena++ fork, MPI, NetCDF
 and Eigen are not available), so the C++ restatement in oracle/ stands in
-for it ("kind": "port").
+for it ("kind": "port"); it computes in FP64 and runs a bounded sample of
+full steps of the same workload (--ref-steps).
 """
 import argparse
 import dataclasses
@@ -188,27 +199,28 @@ def run_cpu(workload, steps, warmup):
 
 
 # -------------------------------------------------------------- our arm --
-def run_ours(args):
-    import numpy as np
+# algorithmic DRAM bytes per interior cell and launch, by kernel and flux type
+# (each array element read or written once; the implicit solve's factors
+# (A c)_i and delta_i, 30 doubles per level, are written and read back)
+def alg_bytes_per_cell(kernel, precision):
+    t = 4 if precision == 1 else 8
+    return {"flux_x1": 40 + 5 * t, "flux_x23": 5 * t + 10 * t, "update": 120 + 15 * t + 80,
+            "implicit": 160 + 480, "prim_ghost": 80 + (20 if precision == 1 else 0),
+            "other": 0}[kernel]
+
+
+def measure_path(cfg, state, steps, warmup, pg, local, sample_clocks):
+    """Device-timed steps of one atmosphere with the state resident."""
     import torch
 
-    from exocubed_b200 import _native as nat
     from exocubed_b200.atmosphere import CubedSphereAtmosphere
-
-    world, rank, local, pg = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
-    cfg, desc = workload_config(args.workload, args.precision)
-    state = make_state(cfg, seed=rank)
     g = CubedSphereAtmosphere(cfg)
     g.set_primitive(state)
     stream = torch.cuda.ExternalStream(g.stream)
-    cells = cells_of(cfg)
-
-    g.step(args.warmup)
+    g.step(warmup)
     g.synchronize()
-
     clocks = ClockSampler(local)
-    if rank == 0:
+    if sample_clocks:
         clocks.start()
     launches0 = g.launch_count()
     g.profile(True)
@@ -217,7 +229,7 @@ def run_ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    g.step(args.steps)
+    g.step(steps)
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
@@ -225,89 +237,189 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     prof = g.profile_read()
     g.profile(False)
-    launches = g.launch_count() - launches0
-    clk = clocks.stop() if rank == 0 else None
-    ms_max = max_over_ranks(pg, ms)
-    invalid = g.invalid()
+    out = {"ms": max_over_ranks(pg, ms), "prof": prof, "launches": g.launch_count() - launches0,
+           "clocks": clocks.stop() if sample_clocks else None, "invalid": g.invalid()}
+    g.close()
+    return out
 
-    # end to end through the public API: pinned host state in, K steps,
-    # pinned host state out
-    nbytes = state.nbytes
+
+def measure_e2e(cfg, state, steps, pg):
+    """The same steps through the public API with the state in pinned host
+    memory: upload, steps, download inside the timed region."""
+    import torch
+
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
     h_in = torch.from_numpy(state).pin_memory()
     h_out = torch.empty(state.shape, dtype=torch.float64).pin_memory()
-    g2 = CubedSphereAtmosphere(cfg)
-    s2 = torch.cuda.ExternalStream(g2.stream)
-    g2.set_primitive_ptr(h_in.data_ptr())
-    g2.step(1)
-    g2.synchronize()
+    g = CubedSphereAtmosphere(cfg)
+    s2 = torch.cuda.ExternalStream(g.stream)
+    g.set_primitive_ptr(h_in.data_ptr())
+    g.step(1)
+    g.synchronize()
     barrier(pg)
     torch.cuda.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(s2)
-    g2.set_primitive_ptr(h_in.data_ptr())
-    g2.step(args.steps)
-    g2.conserved_ptr(h_out.data_ptr())
+    g.set_primitive_ptr(h_in.data_ptr())
+    g.step(steps)
+    g.conserved_ptr(h_out.data_ptr())
     f1.record(s2)
     f1.synchronize()
     barrier(pg)
-    ms_e2e = max_over_ranks(pg, f0.elapsed_time(f1))
-    g2.close()
+    ms = max_over_ranks(pg, f0.elapsed_time(f1))
+    g.close()
+    return ms, state.nbytes
 
-    value = world * cells * args.steps / (ms_max / 1e3)
+
+def accuracy(cfg, state, steps):
+    """Mixed precision against the FP64 path on the same state, the FP64
+    path's first CFL step held fixed: relative L2 / Linf per field."""
+    import numpy as np
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
+    ref = CubedSphereAtmosphere(dict(cfg, precision=0))
+    ref.set_primitive(state)
+    dt = ref.dt
+    ref.step(steps, dt)
+    wr = W.interior(ref.primitive())
+    ref.close()
+    mix = CubedSphereAtmosphere(dict(cfg, precision=1))
+    mix.set_primitive(state)
+    mix.step(steps, dt)
+    wm = W.interior(mix.primitive())
+    invalid = mix.invalid()
+    mix.close()
+    names = ["rho", "v1", "v2", "v3", "p"] if cfg["eqn"] == 1 else ["phi", "v1", "v2", "v3"]
+    err = {}
+    for n, name in enumerate(names):
+        if name == "v1" and cfg["eqn"] == 0:
+            continue
+        d = wm[:, n] - wr[:, n]
+        scale = np.linalg.norm(wr[:, n])
+        err[name] = {"rel_l2": float(np.linalg.norm(d) / scale) if scale > 0
+                     else float(np.linalg.norm(d)),
+                     "linf": float(np.abs(d).max()),
+                     "rel_linf": float(np.abs(d).max() / max(np.abs(wr[:, n]).max(), 1e-300))}
+    return {"steps": steps, "dt": dt, "simulated_seconds": dt * steps, "fields": err,
+            "state_valid": invalid == 0}
+
+
+def serving_sample(rate, nreq, steps, fp64_baseline=True):
+    """A short continuous-batching run (mixed) and, for the same requests,
+    the plain FP64 path one request at a time."""
+    from exocubed_b200 import autotune
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.serving import (Request, Server, poisson_arrivals,
+                                       served_one_at_a_time, summarize)
+    t_arr = poisson_arrivals(rate, nreq, seed=int(rate))
+    reqs = []
+    for n, a in enumerate(t_arr):
+        cfg, w = W.ensemble_member(50_000 + n, precision=1)
+        reqs.append(Request(n, cfg, w, float(a), steps))
+    cache = autotune.TileCache()
+    autotune.batch_tiles([r.cfg for r in reqs], cache)  # measured before the clock starts
+    srv = Server(precision=1, capacity=64, budget_bytes=150 * 10 ** 9, max_chunk=8,
+                 tile_cache=cache)
+    srv.run(reqs[:2], clock="steps")  # warm-up: graph capture, pools
+    mixed = summarize(srv.run(reqs))
+    srv.close()
+    base = None
+    if fp64_baseline:
+        base = summarize(served_one_at_a_time(
+            [dataclasses.replace(r, cfg=dict(r.cfg, precision=0)) for r in reqs]))
+    return {"rate_per_s": rate, "requests": nreq, "steps_per_request": steps,
+            "members": "ensemble distribution (N in 24..96, L in 32..96, varied gas and gravity)",
+            "continuous_batching_mixed": mixed, "one_at_a_time_fp64": base}
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    prec = args.precision
+    cfg, desc = workload_config(args.workload, prec)
+    state = make_state(cfg, seed=rank)
+    cells = cells_of(cfg)
+
+    main = measure_path(cfg, state, args.steps, args.warmup, pg, local, rank == 0)
+    ms_e2e, nbytes = measure_e2e(cfg, state, args.steps, pg)
+    plain = None
+    if prec == 1 and not args.no_fp64:
+        plain = measure_path(dict(cfg, precision=0), state, args.steps, args.warmup, pg, local,
+                             False)
+    value = world * cells * args.steps / (main["ms"] / 1e3)
     e2e_value = world * cells * args.steps / (ms_e2e / 1e3)
 
     # dominant kernel and its roofline (algorithmic bytes per launch)
-    per_cell_alg = {"flux_x1": 10, "flux_x23": 15, "update": 35, "implicit": 20,
-                    "prim_ghost": 10, "other": 0}  # doubles moved once per cell
+    prof = main["prof"]
     dom = max((k for k in prof if k != "other"), key=lambda k: prof[k][1])
     n_l, t_l = prof[dom]
     avg_ms = t_l / max(n_l, 1)
-    alg_bytes = per_cell_alg[dom] * 8 * cells
+    alg_bytes = alg_bytes_per_cell(dom, prec) * cells
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic_c2.json")
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dom)
+        tr = json.load(open(tp)).get(f"{dom}:{'mixed' if prec == 1 else 'fp64'}")
+        if tr:  # DRAM bytes per cell measured by ncu, scaled to this launch
+            traffic = tr["bytes_per_cell"] * cells
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
 
+    extra = {}
+    if rank == 0 and world == 1:
+        if args.accuracy_steps > 0 and prec == 1:
+            extra["accuracy"] = accuracy(workload_config(args.workload, 0)[0], state,
+                                         args.accuracy_steps)
+        if args.serve_requests > 0:
+            extra["serving"] = serving_sample(args.serve_rate, args.serve_requests,
+                                              args.serve_steps, not args.no_fp64_baseline)
+        if not args.no_cpu_baseline:
+            r = run_cpu(args.workload, args.cpu_steps, args.cpu_warmup)
+            extra["cpu_baseline"] = {
+                "value": r["cells"] * r["steps"] / r["seconds"], "unit": "cell-updates/s",
+                "cores": r["threads"], "kind": "port",
+                "sample": f"oracle/ C++ restatement, OpenMP on {r['threads']} threads, "
+                          f"{r['steps']} full step(s) of the same workload after "
+                          f"{args.cpu_warmup} warm-up step(s)"}
     if rank != 0:
-        g.close()
         if pg is not None:
             pg.destroy_process_group()
         return
-    cpu = None
-    if world == 1 and not args.no_cpu_baseline:
-        r = run_cpu(args.workload, args.cpu_steps, 1)
-        cpu = {"value": r["cells"] * r["steps"] / r["seconds"], "unit": "cell-updates/s",
-               "cores": r["threads"], "kind": "port",
-               "sample": f"oracle/ C++ restatement, OpenMP on {r['threads']} threads, "
-                         f"{r['steps']} steps of the same workload after 1 warm-up step"}
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f32+f64",
+        "ms_per_step": main["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32+f64",
         "data": "synthetic",
         "config": {"workload": desc, "cells_per_step": cells, "replicas": world,
-                   "l2": "state arrays of 175 MB each exceed the 126 MB L2",
+                   "l2": "every state array is larger than the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
+        "fp64": None if plain is None else {
+            "value": world * cells * args.steps / (plain["ms"] / 1e3),
+            "ms_per_step": plain["ms"] / args.steps,
+            "note": "the plain FP64 path on the same workload, same run"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": dom,
                      "peak_kind": peak_kind,
                      "step_frac": value / world * BYTES_PER_CELL_UPDATE / 1e9 / peak},
         "kernel_share": shares,
-        "cpu_baseline": cpu,
+        "cpu_baseline": extra.get("cpu_baseline"),
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
                 "steps_per_request": args.steps},
-        "gpu_launches": launches,
-        "clocks": clk,
-        "state_valid": invalid == 0,
+        "gpu_launches": main["launches"],
+        "clocks": main["clocks"],
+        "state_valid": main["invalid"] == 0,
     }
+    if "accuracy" in extra:
+        line["accuracy"] = extra["accuracy"]
+    if "serving" in extra:
+        line["serving"] = extra["serving"]
     print(json.dumps(line))
-    g.close()
     if pg is not None:
         pg.destroy_process_group()
 
@@ -450,42 +562,12 @@ def run_serving(args):
 
 
 def run_accuracy(args):
-    """Mixed precision against the FP64 path on the same seeded state: both
-    advance args.accuracy steps with the FP64 path's first CFL step held
-    fixed, then relative L2 and Linf errors per field are reported."""
-    import numpy as np
+    """Mixed precision against the FP64 path after args.accuracy steps."""
     import torch  # noqa: F401  (CUDA context)
-
-    from exocubed_b200 import workloads as W
-    from exocubed_b200.atmosphere import CubedSphereAtmosphere
     cfg, desc = workload_config(args.workload, 0)
-    state = make_state(cfg, seed=0)
-    ref = CubedSphereAtmosphere(cfg)
-    ref.set_primitive(state)
-    dt = ref.dt
-    ref.step(args.accuracy, dt)
-    wr = W.interior(ref.primitive())
-    ref.close()
-    mix = CubedSphereAtmosphere(dict(cfg, precision=1))
-    mix.set_primitive(state)
-    mix.step(args.accuracy, dt)
-    wm = W.interior(mix.primitive())
-    invalid = mix.invalid()
-    mix.close()
-    names = ["rho", "v1", "v2", "v3", "p"] if cfg["eqn"] == 1 else ["phi", "v1", "v2", "v3"]
-    err = {}
-    for n, name in enumerate(names):
-        if name == "v1" and cfg["eqn"] == 0:
-            continue
-        d = wm[:, n] - wr[:, n]
-        scale = np.linalg.norm(wr[:, n])
-        err[name] = {"rel_l2": float(np.linalg.norm(d) / scale) if scale > 0 else float(np.linalg.norm(d)),
-                     "linf": float(np.abs(d).max()),
-                     "rel_linf": float(np.abs(d).max() / max(np.abs(wr[:, n]).max(), 1e-300))}
-    print(json.dumps({"accuracy": {"workload": desc.replace("FP64", "mixed vs FP64"),
-                                   "steps": args.accuracy, "dt": dt,
-                                   "simulated_seconds": dt * args.accuracy,
-                                   "fields": err, "state_valid": invalid == 0}}))
+    res = accuracy(cfg, make_state(cfg, seed=0), args.accuracy)
+    res["workload"] = desc.replace("FP64", "mixed vs FP64")
+    print(json.dumps({"accuracy": res}))
 
 
 def run_reference(args):
@@ -493,8 +575,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cfg, desc = workload_config(args.workload)
-    r = run_cpu(args.workload, args.steps, args.warmup)
+    cfg, desc = workload_config(args.workload, args.precision)
+    steps, warm = min(args.steps, args.ref_steps), min(args.warmup, 1)
+    r = run_cpu(args.workload, steps, warm)
     v = r["cells"] * r["steps"] / r["seconds"]
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s",
@@ -504,9 +587,11 @@ def run_reference(args):
         "config": {"workload": desc, "cells_per_step": r["cells"]},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": r["threads"],
                          "kind": "port",
-                         "sample": f"{r['steps']} full steps after {args.warmup} warm-up steps; "
-                                   "the reference cannot be built here, its C++ restatement "
-                                   "(oracle/) runs with OpenMP on all host threads"},
+                         "sample": f"{r['steps']} full FP64 step(s) of the workload after "
+                                   f"{warm} warm-up step(s) (of the {args.steps} + {args.warmup} "
+                                   "requested: a bounded sample of the same rate); the reference "
+                                   "cannot be built here, its C++ restatement (oracle/) runs "
+                                   "with OpenMP on all host threads"},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -519,16 +604,24 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c2s", "c3", "c4"])
     ap.add_argument("--members", type=int, default=64, help="ensemble members (c4)")
     ap.add_argument("--serve", default="", help="comma-separated arrival rates (req/s): serving sweep")
     ap.add_argument("--requests", type=int, default=24, help="requests per rate (serving)")
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--no-fp64-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tiles")
-    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--precision", type=int, default=1, choices=[0, 1],
                     help="0: FP64; 1: FP32 reconstruction/Riemann/divergence, FP64 rest")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="steps of the mixed-vs-FP64 error check in the bench line (0: none)")
+    ap.add_argument("--serve-requests", type=int, default=8,
+                    help="requests of the serving sample in the bench line (0: none)")
+    ap.add_argument("--serve-rate", type=float, default=100.0)
+    ap.add_argument("--ref-steps", type=int, default=2,
+                    help="full steps the reference arm times at most (its bounded sample)")
+    ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--cpu-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-worker", action="store_true")
