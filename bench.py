@@ -152,8 +152,10 @@ def dist_setup(gpus):
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -167,9 +169,16 @@ def max_over_ranks(pg, x):
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def member_seeds(rank, n):
+    """Seeds of the ensemble members rank `rank` advances: disjoint across
+    ranks, so N ranks hold N different ensembles (weak scaling)."""
+    return [10_000 * rank + i for i in range(n)]
 
 
 # ---------------------------------------------------------- CPU baseline --
@@ -438,7 +447,7 @@ def run_ensemble(args):
     world, rank, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     prec = args.precision
-    members = [W.ensemble_member(10_000 * rank + i, precision=prec) for i in range(args.members)]
+    members = [W.ensemble_member(sd, precision=prec) for sd in member_seeds(rank, args.members)]
     cells = sum(cells_of(c) for c, _ in members)
     ens = Ensemble(precision=prec, capacity=args.members)
     slots = [ens.add(c, w) for c, w in members]
