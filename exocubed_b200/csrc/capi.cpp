@@ -83,7 +83,11 @@ struct exo_ctx {
   size_t state_elems = 0;  // 6*nv*cells
   bool has_state = false;
   int device = 0;
+  // one CFL step captured as a graph (profiling off): exo_step replays it
+  cudaGraphExec_t step_graph = nullptr;
+  int64_t graph_launches = 0;
 };
+
 
 // Run one launch, bracketed by events when profiling.  `nlaunch` is the
 // number of kernels the launcher issues.
@@ -156,6 +160,36 @@ static_assert((int)exo::BK_X1 == (int)EXO_K_FLUX_X1 && (int)exo::BK_X23 == (int)
                   (int)exo::BK_PRIM == (int)EXO_K_PRIM_GHOST &&
                   (int)exo::BK_ROUNDTRIP == (int)EXO_K_OTHER && (int)exo::BK_COUNT == EXO_TILE_COUNT,
               "tile slots follow the EXO_K_* kernel ids");
+
+// Captures one CFL step (the launches of one_step) into a graph, once.
+static int capture_step(exo_ctx* c) {
+  if (c->step_graph) return 0;
+  const int64_t l0 = c->launches;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = one_step(c, 0.);
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    c->launches = l0;
+    return rc;
+  }
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+  ce = cudaGraphInstantiate(&c->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    c->step_graph = nullptr;
+    return cuda_fail(ce, "cudaGraphInstantiate");
+  }
+  c->graph_launches = c->launches - l0;
+  c->launches = l0;
+  return 0;
+}
+
+static void drop_step_graph(exo_ctx* c) {
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  c->step_graph = nullptr;
+}
 
 namespace exo {
 
@@ -358,7 +392,9 @@ void member_blocks(const DevView& v, const int* t, unsigned b[BK_COUNT]) {
   bool implicit = !shallow && (v.implicit_flag & 1);
   auto nb = [](size_t n, int th) { return (unsigned)((n + th - 1) / th); };
   b[BK_X1] = shallow ? 0u : (unsigned)(6 * v.N * v.N);
-  b[BK_X23] = nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, t[BK_X23]);
+  // mixed build: one thread per line of faces; FP64 build: one per face
+  b[BK_X23] = v.precision == EXO_PREC_MIXED ? nb((size_t)2 * 6 * v.N * v.L, t[BK_X23])
+                                            : nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, t[BK_X23]);
   b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, t[BK_UPDATE]);
   b[BK_IMPLICIT] = implicit ? nb((size_t)6 * v.N * v.N, t[BK_IMPLICIT]) : 0u;  // thread per column
   b[BK_PRIM] = nb((size_t)6 * v.cells, t[BK_PRIM]);
@@ -478,6 +514,7 @@ void exo_destroy(exo_ctx* c) {
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  drop_step_graph(c);
   for (auto& e : c->prof_used) c->prof_pool.push_back(e);
   for (auto& e : c->prof_pool) {
     cudaEventDestroy(e.a);
@@ -581,6 +618,14 @@ int exo_step(exo_ctx* c, int nsteps, double dt_fixed) {
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
   if (nsteps < 0) return fail(EXO_ERR_ARG, "nsteps < 0");
+  if (!c->profiling && dt_fixed <= 0. && nsteps > 0) {
+    // the CFL step is replayed from its graph: one launch per step on the host
+    int rc = capture_step(c);
+    if (rc) return rc;
+    for (int n = 0; n < nsteps; ++n) CK(cudaGraphLaunch(c->step_graph, c->stream));
+    c->launches += (int64_t)nsteps * c->graph_launches;
+    return EXO_OK;
+  }
   for (int n = 0; n < nsteps; ++n) {
     int rc = one_step(c, dt_fixed);
     if (rc) return rc;
@@ -614,6 +659,7 @@ int exo_set_tiles(exo_ctx* c, const int* threads) {
   std::string err;
   if (!exo::valid_tiles(t, &err)) return fail(EXO_ERR_ARG, err);
   CK(cudaStreamSynchronize(c->stream));  // launches already queued keep their tables
+  drop_step_graph(c);                     // it holds the old launch shapes
   for (int k = 0; k < exo::BK_COUNT; ++k) c->v.tiles[k] = t[k];
   int rc = exo::view_refresh_self(c->v, c->stream, &err);
   return rc ? fail(rc, err) : EXO_OK;

@@ -686,8 +686,10 @@ __device__ __forceinline__ void edge_outer_state(const DevView& v, int p, int si
   st[IVZ] = T(e.q[2]) * U + T(e.q[3]) * V;
 }
 
+// One thread per face (the FP64 build: its solvers need too many registers
+// to also hold a sliding stencil window).
 template <class T>
-__device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
+__device__ __forceinline__ void flux_x23_faces(const DevView& v, unsigned blk) {
   unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned nface = 6u * v.N * (v.N + 1) * v.L;  // per direction
   if (tid >= 2 * nface) return;
@@ -750,6 +752,87 @@ __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
     if (n >= v.nv) break;
     F[idx(v, p, n, k, j, i)] = fx[n];
   }
+}
+
+
+// One thread per line of faces (the mixed build): for x2 faces the line (p, k, i) runs over
+// j = js .. je+1, for x3 faces the line (p, j, i) over k = ks .. ke+1.  The
+// six cells of the face's WENO5 stencils slide along the line in
+// registers, so every cell is read once per line instead of six times; each
+// face's reconstruction, edge replacement and Riemann solve are those of a
+// face on its own (same values, same operations).
+template <class T>
+__device__ __forceinline__ void flux_x23_lines(const DevView& v, unsigned blk) {
+  const unsigned tid = blk * blockDim.x + threadIdx.x;
+  const unsigned L = v.L, N = v.N;
+  const unsigned nline = 6u * N * L;  // per direction
+  if (tid >= 2 * nline) return;
+  const int dir = tid < nline ? 1 : 2;
+  unsigned r = dir == 1 ? tid : tid - nline;
+  const int i = v.is + (int)(r % L);
+  r /= L;
+  const int a = (int)(r % N);  // position across the line: k - ks (x2) or j - js (x3)
+  const int p = (int)(r / N);
+  const int nv = v.nv;
+  const size_t vs = v.cells;
+  const long s = dir == 1 ? (long)v.nc1 : (long)v.nc1 * v.nc2;  // stride along the line
+  const size_t base = dir == 1 ? idx(v, p, 0, v.ks + a, 0, i) : idx(v, p, 0, 0, v.js + a, i);
+  const T* __restrict__ W = prim_array<T>(v) + base;
+  const int c0 = dir == 1 ? v.js : v.ks, c1 = dir == 1 ? v.je : v.ke;
+  T* F = flux_array<T>(v, dir);
+  // window q[n][m] = cell (c - 3 + m) of the line for face c (cells c-1 | c)
+  T q[5][6];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= nv) break;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) q[n][m] = T(__ldg(W + n * vs + (long)(c0 - 3 + m) * s));
+  }
+  for (int c = c0; c <= c1 + 1; ++c) {
+    T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
+      wl[n] = weno5<T>(q[n][4], q[n][3], q[n][2], q[n][1], q[n][0]);  // weno_r of cell c-1
+      wr[n] = weno5<T>(q[n][1], q[n][2], q[n][3], q[n][4], q[n][5]);  // weno_l of cell c
+    }
+    const int k = dir == 1 ? v.ks + a : c;
+    const int j = dir == 1 ? c : v.js + a;
+    if (dir == 1) {
+      if (c == c0) edge_outer_state<T>(v, p, UP, a, i, wl);
+      else if (c == c1 + 1) edge_outer_state<T>(v, p, DOWN, a, i, wr);
+      FaceGeo<T> fg{T(geo(v, GCOSF2, p, k, j)), T(geo(v, GSINF2, p, k, j)),
+                    T(geo(v, GCTHP2, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+      riemann<T>(v.rsolver, v.gamma, IVY, fg, wl, wr, fx);
+    } else {
+      if (c == c0) edge_outer_state<T>(v, p, LEFT, a, i, wl);
+      else if (c == c1 + 1) edge_outer_state<T>(v, p, RIGHT, a, i, wr);
+      FaceGeo<T> fg{T(geo(v, GCOSF3, p, k, j)), T(geo(v, GSINF3, p, k, j)),
+                    T(geo(v, GCTHP3, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+      riemann<T>(v.rsolver, v.gamma, IVZ, fg, wl, wr, fx);
+    }
+    const size_t f0 = idx(v, p, 0, k, j, i);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
+      F[f0 + n * vs] = fx[n];
+    }
+    if (c <= c1) {  // slide: the next face needs cell c + 3
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        if (n >= nv) break;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) q[n][m] = q[n][m + 1];
+        q[n][5] = T(__ldg(W + n * vs + (long)(c + 3) * s));
+      }
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
+  if constexpr (sizeof(T) == sizeof(double)) flux_x23_faces<T>(v, blk);
+  else flux_x23_lines<T>(v, blk);
 }
 
 // --------------------------------------------------------------- k_update -
@@ -1712,8 +1795,13 @@ __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
   flux_x1_block<T>(sv, b);
 }
 
+#ifdef EXO_X23_MINB
+#define EXO_X23_BOUNDS __launch_bounds__(256, EXO_X23_MINB)
+#else
+#define EXO_X23_BOUNDS
+#endif
 template <class T>
-__global__ void kb_flux_x23(Batch bt) {
+__global__ void EXO_X23_BOUNDS kb_flux_x23(Batch bt) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   flux_x23_block<T>(sv, b);
