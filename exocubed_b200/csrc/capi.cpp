@@ -221,6 +221,13 @@ bool validate_config(const exo_config& c, std::string* err) {
   return true;
 }
 
+// the implicit solve's factors: 30 doubles per column level, columns in
+// blocks of 32 (the last block padded)
+size_t implicit_scratch_doubles(int N, int L) {
+  size_t ncol = (size_t)6 * N * N;
+  return (ncol + 31) / 32 * 32 * (size_t)L * 30;
+}
+
 size_t view_footprint(const exo_config& c) {
   bool shallow = c.eqn == EXO_EQN_SHALLOW_YZ;
   size_t nv = shallow ? 4 : 5;
@@ -228,7 +235,7 @@ size_t view_footprint(const exo_config& c) {
   size_t elems = 6 * nv * nc1 * nc2 * nc2;
   size_t nd = shallow ? 5 : 7;  // u, w, u1, flux x2, x3 (+ du, flux x1)
   size_t bytes = nd * elems * sizeof(double);
-  if (!shallow && (c.implicit_flag & 1)) bytes += (size_t)6 * c.N * c.N * c.L * 30 * sizeof(double);
+  if (!shallow && (c.implicit_flag & 1)) bytes += implicit_scratch_doubles(c.N, c.L) * sizeof(double);
   if (c.precision == EXO_PREC_MIXED) bytes += (shallow ? 3 : 4) * elems * sizeof(float);
   bytes += (size_t)NGEO2D * 6 * nc2 * nc2 * sizeof(double);       // metric
   bytes += (size_t)6 * nc2 * nc2 * sizeof(int);                   // ghost map
@@ -309,7 +316,7 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
     if (!alloc((void**)&v.du, db, true) || !alloc((void**)&v.flux[0], db, true))
       return EXO_ERR_CAPACITY;
     if ((v.implicit_flag & 1) &&
-        !alloc((void**)&v.scratch, (size_t)6 * cfg.N * cfg.N * cfg.L * 30 * sizeof(double), false))
+        !alloc((void**)&v.scratch, implicit_scratch_doubles(cfg.N, cfg.L) * sizeof(double), false))
       return EXO_ERR_CAPACITY;
   }
   if (cfg.precision == EXO_PREC_MIXED) {

@@ -106,7 +106,7 @@ int rebuild(exo_ensemble* e) {
     if (m->v.eqn != EXO_EQN_SHALLOW_YZ) {
       int t = std::min(256, ((m->v.L + 1 + 31) / 32) * 32);
       x1_threads = std::max(x1_threads, t);
-      x1_smem = std::max(x1_smem, ((size_t)m->v.nv * m->v.nc1 + m->v.nc1 + 1) * sizeof(double));
+      x1_smem = std::max(x1_smem, exo::x1_smem_bytes(m->v));
     }
   }
   int n = (int)views.size();

@@ -136,6 +136,12 @@ struct Tiles {
 };
 Tiles default_tiles();
 bool valid_tiles(const int* t, std::string* err);
+// dynamic shared memory of the x1 kernel for one column: the primitives and
+// the face pressures, and in the mixed build ln psf and the face densities
+inline size_t x1_smem_bytes(const DevView& v) {
+  size_t faces = (size_t)v.nc1 + 1;
+  return ((size_t)v.nv * v.nc1 + (v.precision == EXO_PREC_MIXED ? 3 : 1) * faces) * sizeof(double);
+}
 // block counts of one member for the given tiles
 void member_blocks(const DevView& v, const int* tiles, unsigned blocks[BK_COUNT]);
 // re-uploads the view's own device copy (tiles and block table)

@@ -31,6 +31,11 @@
 
 #include "exo_internal.h"
 
+// 1: the implicit solve keeps (A c)_{i-1} in shared memory instead of registers
+#ifndef EXO_IMPL_AP_SMEM
+#define EXO_IMPL_AP_SMEM 0
+#endif
+
 namespace exo {
 namespace EXO_KNS {
 namespace {
@@ -597,6 +602,30 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       s_expf = exp(-ent / gam);
     }
     __syncthreads();
+#if EXO_MIXED
+    // FP64 still, with the powers as exp(log(x) / gamma) and one log per face
+    // shared by its two cells: ln psf and the face density of the isentropic
+    // reference go to shared memory for the cells and for the restore
+    double* lpsf = psf + nc1 + 1;  // [nc1+1]
+    double* dsf = lpsf + nc1 + 1;  // [nc1+1]
+    const double igam = 1. / s_gam;
+    for (int i = threadIdx.x; i <= nc1; i += blockDim.x) {
+      const double l = log(psf[i]);
+      lpsf[i] = l;
+      dsf[i] = exp(l * igam) * s_expf;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nc1; i += blockDim.x) {
+      double psv;
+      if (fabs(psf[i] - psf[i + 1]) < 1.E-6)
+        psv = (psf[i] + psf[i + 1]) * 0.5;
+      else
+        psv = (psf[i] - psf[i + 1]) / (lpsf[i] - lpsf[i + 1]);
+      const double dsv = exp(log(psv) * igam) * s_expf;
+      wc[IPR * nc1 + i] -= psv;
+      wc[IDN * nc1 + i] -= dsv;
+    }
+#else
     for (int i = threadIdx.x; i < nc1; i += blockDim.x) {
       double psv, dsv;
       if (fabs(psf[i] - psf[i + 1]) < 1.E-6)
@@ -607,6 +636,7 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       wc[IPR * nc1 + i] -= psv;
       wc[IDN * nc1 + i] -= dsv;
     }
+#endif
     __syncthreads();
   }
   FaceGeo<T> fg{T(0.), T(1.), T(geo(v, GCTHP1, p, k, j)), T(geo(v, GCOSC, p, k, j))};
@@ -630,7 +660,11 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       if (xr < 0.) xr = ps;
       xl += ps;
       if (xl < 0.) xl = ps;
+#if EXO_MIXED
+      const double dsf = psf[2 * (nc1 + 1) + i];
+#else
       double dsf = pow(ps, 1. / s_gam) * s_expf;
+#endif
       double dr = wr[IDN], dl = wl[IDN];
       dr += dsf;
       if (dr < 0.) dr = dsf;
@@ -1218,9 +1252,9 @@ __device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const dou
 //                    for it beforehand (callers that only need d load nothing)
 //   io.wptr(i, n), io.duptr(i, n)  addresses of w and of the explicit update
 //                    du of level i (the inputs are prefetched through shared memory)
-//   sm               this thread's 60 doubles of shared memory, stride sms
+//   sm               this thread's 60 contiguous doubles of shared memory
 template <class IO>
-__device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, double cos_theta,
+__device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_theta,
                                                 double sin_theta, double d2, double d3,
                                                 const double* x1f, const double* x1v,
                                                 const double* dx1f, int is, int ie, double dt,
@@ -1248,17 +1282,17 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
 #endif
     return c;
   };
-  auto AMs = [&](int slot, int r, int q) -> double& { return sm[(slot * 25 + r * 5 + q) * sms]; };
+  auto AMs = [&](int slot, int r, int q) -> double& { return sm[slot * 25 + r * 5 + q]; };
 
   // prefetch slots: w(i+1) and du(i) of the next level, copied asynchronously
-  double* pw = sm + 50 * sms;
-  double* pdu = sm + 55 * sms;
+  double* pw = sm + 50;
+  double* pdu = sm + 55;
   auto prefetch = [&](int iw, int idu) {
 #pragma unroll
-    for (int n = 0; n < 5; ++n) cp_async8(pw + n * sms, io.wptr(iw, n));
+    for (int n = 0; n < 5; ++n) cp_async8(pw + n, io.wptr(iw, n));
     if (idu >= 0) {
 #pragma unroll
-      for (int n = 0; n < 5; ++n) cp_async8(pdu + n * sms, io.duptr(idu, n));
+      for (int n = 0; n < 5; ++n) cp_async8(pdu + n, io.duptr(idu, n));
     }
     cp_async_commit();
   };
@@ -1276,15 +1310,24 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
 #pragma unroll
       for (int q = 0; q < 5; ++q) AMs(0, r, q) = A[r][q];
   }
-  double Ap[5][5], dp[5];  // (A c)_{i-1}, delta_{i-1}
+  // (A c)_{i-1} lives in registers, or in this thread's shared memory when
+  // EXO_IMPL_AP_SMEM (fewer registers, more resident warps)
+#if EXO_IMPL_AP_SMEM
+  double* const aps = sm + 60;
+#define EXO_AP(r, q) aps[(r) * 5 + (q)]
+#else
+  double Ap[5][5];
+#define EXO_AP(r, q) Ap[r][q]
+#endif
+  double dp[5];  // delta_{i-1}
   int cur = 0;
   for (int i = is; i <= ie; ++i) {
     cp_async_wait_all();
     double rhs[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-      raw[n] = pw[n * sms];
-      rhs[n] = pdu[n * sms];
+      raw[n] = pw[n];
+      rhs[n] = pdu[n];
     }
     ColCell cp = cell(raw);
     prefetch(i + 2, i < ie ? i + 1 : -1);
@@ -1356,9 +1399,9 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
       if (!first) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-          double ba = brow[0] * Ap[0][q];
+          double ba = brow[0] * EXO_AP(0, q);
 #pragma unroll
-          for (int k = 1; k < 5; ++k) ba += brow[k] * Ap[k][q];
+          for (int k = 1; k < 5; ++k) ba += brow[k] * EXO_AP(k, q);
           trow[q] = trow[q] - ba;
         }
         double bd = brow[0] * dp[0];
@@ -1444,7 +1487,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
       ccol(Q, c);
       solve(c);
 #pragma unroll
-      for (int r = 0; r < 5; ++r) Ap[r][q] = c[r];
+      for (int r = 0; r < 5; ++r) EXO_AP(r, q) = c[r];
     });
 #pragma unroll
     for (int r = 0; r < 5; ++r) dp[r] = x[r];
@@ -1512,7 +1555,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
         double acc = B[r][0] * c[0];
 #pragma unroll
         for (int k = 1; k < 5; ++k) acc += B[r][k] * c[k];
-        Ap[r][q] = acc;
+        EXO_AP(r, q) = acc;
       }
     });
 #endif
@@ -1521,7 +1564,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
 #pragma unroll
       for (int r = 0; r < 5; ++r)
 #pragma unroll
-        for (int q = 0; q < 5; ++q) io.scr(lev, r * 5 + q) = Ap[r][q];
+        for (int q = 0; q < 5; ++q) io.scr(lev, r * 5 + q) = EXO_AP(r, q);
 #pragma unroll
       for (int r = 0; r < 5; ++r) io.scr(lev, 25 + r) = dp[r];
     }
@@ -1566,6 +1609,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, int sms, dou
     }
   }
 }
+#undef EXO_AP
 
 // UpdateAllConserved on the last stage with NVAPOR = NCLOUD = 0: the
 // AirParcel round trip MassConc -> MoleFrac -> MassConc of one cell
@@ -1619,8 +1663,24 @@ constexpr int IMPL_MAX_THREADS = 128;
 #ifndef EXO_IMPL_MINB
 #define EXO_IMPL_MINB 2  // resident 128-thread blocks per SM the register budget is sized for
 #endif
+// the mixed build's solve fits 204 registers without spilling: 5 blocks of
+// 64 columns per SM instead of 4 (measured 18 % faster at 6x192^2x96); the
+// FP64 build spills there and keeps the full register file
+#if !defined(EXO_IMPL_MAXNREG) && EXO_MIXED
+#define EXO_IMPL_MAXNREG 204
+#endif
+#ifdef EXO_IMPL_MAXNREG
+#define EXO_IMPL_BOUNDS __maxnreg__(EXO_IMPL_MAXNREG)
+#else
 #define EXO_IMPL_BOUNDS __launch_bounds__(IMPL_MAX_THREADS, EXO_IMPL_MINB)
-constexpr size_t impl_smem(int threads) { return (size_t)60 * threads * sizeof(double); }
+#endif
+// each thread's doubles are contiguous (60, or 85 with (A c)_{i-1} kept
+// there), threads IMPL_SM_STRIDE doubles apart: an odd stride keeps a
+// half-warp's 8-byte accesses on distinct banks
+constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : 61;
+constexpr size_t impl_smem(int threads) {
+  return (size_t)IMPL_SM_STRIDE * threads * sizeof(double);
+}
 constexpr size_t IMPL_SMEM = impl_smem(IMPL_THREADS);
 
 // A column of the stepping context: primitives and update from the state
@@ -1631,8 +1691,7 @@ struct StepColumnIO {
   const double* duc;
   double* uc;
   size_t vs;       // stride between variables
-  double* scr0;    // scratch of this column, stride nslot between entries
-  size_t nslot;
+  double* scr0;    // scratch of this column: [level][entry][32 lanes] per warp of columns
   int stage;
   double Rd, gamma;
   __device__ __forceinline__ void w(int i, double* out) const {
@@ -1642,7 +1701,7 @@ struct StepColumnIO {
   __device__ __forceinline__ const double* wptr(int i, int n) const { return wc + n * vs + i; }
   __device__ __forceinline__ const double* duptr(int i, int n) const { return duc + n * vs + i; }
   __device__ __forceinline__ double& scr(int lev, int e) const {
-    return scr0[((size_t)lev * 30 + e) * nslot];
+    return scr0[(lev * 30 + e) * 32];
   }
   __device__ __forceinline__ void uload(int i, double* u) const {
 #pragma unroll
@@ -1670,9 +1729,10 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const int p = col / (v.N * v.N);
   const double dt = rk_beta(stage) * v.sc->dt;
   const size_t base = idx(v, p, 0, k, j, 0);
-  StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, v.scratch + col, (size_t)ncol,
-                  stage, v.Rd, v.gamma};
-  implicit_column(io, ism + threadIdx.x, blockDim.x, geo(v, GCOSC, p, k, j),
+  // scratch in blocks of 32 columns: a warp's 32 entries are 256 contiguous bytes
+  double* scr0 = v.scratch + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
+  StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma};
+  implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
                   geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), v.x1f,
                   v.x1v, v.dx1f, v.is, v.ie, dt, v.gamma, v.grav);
 }
@@ -1883,7 +1943,7 @@ int launch_flux_x1(const DevView& v, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ) return 0;
   int threads = ((v.L + 1 + 31) / 32) * 32;
   if (threads > 256) threads = 256;
-  size_t smem = ((size_t)v.nv * v.nc1 + v.nc1 + 1) * sizeof(double);
+  size_t smem = x1_smem_bytes(v);
   kb_flux_x1<EXO_FLUX_T><<<member_block_count(v, BK_X1), threads, smem, (cudaStream_t)stream>>>(
       one(v, BK_X1));
   return check_launch();

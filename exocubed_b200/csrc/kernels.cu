@@ -55,7 +55,7 @@ __global__ void EXO_IMPL_BOUNDS k_implicit_columns(
   HookColumnIO io{w + (size_t)col * 5 * nc1, du + (size_t)col * 5 * L, nc1, L, scratch + col,
                   (size_t)ncol};
   const double* g4 = colgeo + (size_t)col * 4;
-  implicit_column(io, ism + threadIdx.x, blockDim.x, g4[0], g4[1], g4[2], g4[3], x1f, x1v, dx1f,
+  implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3], x1f, x1v, dx1f,
                   G, G + L - 1, dt, gamma, grav);
 }
 
