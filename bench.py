@@ -47,8 +47,15 @@ sys.path.insert(0, ROOT)
 BYTES_PER_CELL_UPDATE = 320  # 8 registers x 5 vars x 8 B per SSPRK(3,3) step
 
 
+RSOLVER = {1: "LMARS", 2: "HLLC"}
+_RS = [None]  # the --rsolver choice for exo3 workloads (None: LMARS)
+
+
 def workload_config(name, precision=0):
     cfg, desc = _workload(name)
+    if _RS[0] is not None and cfg["eqn"] == 1:
+        cfg = dict(cfg, rsolver=_RS[0])
+        desc = desc.replace("LMARS", RSOLVER[_RS[0]])
     if precision == 1:
         cfg = dict(cfg, precision=1)
         desc = desc.replace("FP64", "mixed FP32/FP64")
@@ -203,6 +210,8 @@ def run_cpu(workload, steps, warmup):
     env.pop("CUDA_VISIBLE_DEVICES", None)
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--workload", workload,
            "--cpu-steps", str(steps), "--cpu-warmup", str(warmup)]
+    if _RS[0] is not None:
+        cmd += ["--rsolver", str(_RS[0])]
     r = subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
     return json.loads(r.stdout.strip().splitlines()[-1])
 
@@ -641,7 +650,10 @@ def main():
     ap.add_argument("--cpu-worker", action="store_true")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="run N steps mixed vs FP64 and report the field errors")
+    ap.add_argument("--rsolver", type=int, default=None, choices=[1, 2],
+                    help="Riemann solver of exo3 workloads: 1 LMARS (default), 2 HLLC")
     args = ap.parse_args()
+    _RS[0] = args.rsolver
     if args.cpu_worker:
         cpu_worker(args)
     elif args.accuracy > 0:

@@ -34,6 +34,7 @@ EXPORTED = [
     "exo_ensemble_synchronize", "exo_ensemble_get_conserved", "exo_ensemble_get_primitive",
     "exo_ensemble_member_time", "exo_ensemble_check_state", "exo_ensemble_stats",
     "exo_set_tiles", "exo_get_tiles", "exo_ensemble_set_tiles", "exo_ensemble_get_tiles",
+    "exo_stage", "exo_boundary", "exo_solve_implicit_3d",
     "exo_ensemble_get_stream",
     "exo_implicit_columns", "exo_implicit_columns_noalloc",
 ]
@@ -118,6 +119,9 @@ def lib():
     L.exo_ensemble_get_conserved.argtypes = [p, i, dp]
     L.exo_ensemble_get_primitive.argtypes = [p, i, dp]
     L.exo_ensemble_member_time.argtypes = [p, i, dp, dp, ctypes.POINTER(ctypes.c_int64)]
+    L.exo_stage.argtypes = [p, i]
+    L.exo_boundary.argtypes = [p]
+    L.exo_solve_implicit_3d.argtypes = [p, dp, dp, d]
     ip = ctypes.POINTER(ctypes.c_int)
     L.exo_set_tiles.argtypes = [p, ip]
     L.exo_get_tiles.argtypes = [p, ip]

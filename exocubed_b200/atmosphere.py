@@ -100,6 +100,21 @@ class CubedSphereAtmosphere:
     def step(self, nsteps=1, dt_fixed=0.0):
         nat.check(nat.lib().exo_step(self._ctx, int(nsteps), float(dt_fixed)))
 
+    def stage(self, s):
+        """One SSPRK(3,3) stage (0, 1, 2) on the CFL step; see exo_stage."""
+        nat.check(nat.lib().exo_stage(self._ctx, int(s)))
+
+    def boundary(self):
+        """Ghost syncs and ConservedToPrimitive of the current state."""
+        nat.check(nat.lib().exo_boundary(self._ctx))
+
+    def solve_implicit_3d(self, du, w, dt):
+        """ImplicitSolver::SolveImplicit3D: du corrected in place from w.  It
+        uses the context's device arrays; load a state before stepping on."""
+        assert du.shape == self.shape and du.flags.c_contiguous and du.dtype == np.float64
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        nat.check(nat.lib().exo_solve_implicit_3d(self._ctx, nat.dptr(du), nat.dptr(w), float(dt)))
+
     def synchronize(self):
         nat.check(nat.lib().exo_synchronize(self._ctx))
 

@@ -128,28 +128,36 @@ static int boundary_and_prim(exo_ctx* c, bool dt) {
                [&] { return STEP(launch_prim_ghost, c->v, dt, c->stream); });
 }
 
-static int one_step(exo_ctx* c, double dt_fixed) {
+// One stage of SSPRK(3,3) (DoTaskListOneStage): fluxes, update, implicit
+// correction, boundaries and primitives (with the CFL candidate on the last
+// stage unless the step is fixed).
+static int one_stage(exo_ctx* c, int s, bool cfl) {
   const DevView& v = c->v;
   bool shallow = v.eqn == EXO_EQN_SHALLOW_YZ;
   bool implicit = !shallow && (v.implicit_flag & 1);
   int rc;
+  if (!shallow &&
+      (rc = timed(c, EXO_K_FLUX_X1, 1, [&] { return STEP(launch_flux_x1, v, c->stream); })))
+    return rc;
+  if ((rc = timed(c, EXO_K_FLUX_X23, 1, [&] { return STEP(launch_flux_x23, v, c->stream); })))
+    return rc;
+  int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
+  if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return STEP(launch_update, v, s, c->stream); })))
+    return rc;
+  if (implicit &&
+      (rc = timed(c, EXO_K_IMPLICIT, 1, [&] { return STEP(launch_implicit, v, s, c->stream); })))
+    return rc;
+  return boundary_and_prim(c, s == 2 && cfl);
+}
+
+static int one_step(exo_ctx* c, double dt_fixed) {
+  const DevView& v = c->v;
+  int rc;
   if (dt_fixed > 0. &&
       (rc = timed(c, EXO_K_OTHER, 1, [&] { return STEP(launch_set_dt, v, dt_fixed, c->stream); })))
     return rc;
-  for (int s = 0; s < 3; ++s) {
-    if (!shallow &&
-        (rc = timed(c, EXO_K_FLUX_X1, 1, [&] { return STEP(launch_flux_x1, v, c->stream); })))
-      return rc;
-    if ((rc = timed(c, EXO_K_FLUX_X23, 1, [&] { return STEP(launch_flux_x23, v, c->stream); })))
-      return rc;
-    int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
-    if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return STEP(launch_update, v, s, c->stream); })))
-      return rc;
-    if (implicit &&
-        (rc = timed(c, EXO_K_IMPLICIT, 1, [&] { return STEP(launch_implicit, v, s, c->stream); })))
-      return rc;
-    if ((rc = boundary_and_prim(c, s == 2 && dt_fixed <= 0.))) return rc;
-  }
+  for (int s = 0; s < 3; ++s)
+    if ((rc = one_stage(c, s, dt_fixed <= 0.))) return rc;
   return timed(c, EXO_K_OTHER, 1,
                [&] { return STEP(launch_dt_finalize, v, dt_fixed, true, c->stream); });
 }
@@ -637,6 +645,41 @@ int exo_step(exo_ctx* c, int nsteps, double dt_fixed) {
     int rc = one_step(c, dt_fixed);
     if (rc) return rc;
   }
+  return EXO_OK;
+}
+
+int exo_stage(exo_ctx* c, int stage) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
+  if (stage < 0 || stage > 2) return fail(EXO_ERR_ARG, "stage must be 0, 1 or 2");
+  int rc = one_stage(c, stage, true);
+  if (rc) return fail(rc, "stage launch failed");
+  if (stage == 2) {
+    rc = timed(c, EXO_K_OTHER, 1, [&] { return STEP(launch_dt_finalize, c->v, 0., true, c->stream); });
+    if (rc) return fail(rc, "time-step launch failed");
+  }
+  return EXO_OK;
+}
+
+int exo_boundary(exo_ctx* c) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = boundary_and_prim(c, false);
+  return rc ? fail(rc, "boundary launch failed") : EXO_OK;
+}
+
+int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, double dt) {
+  if (!c || !du_host || !w_host) return fail(EXO_ERR_ARG, "NULL argument");
+  if (c->v.eqn == EXO_EQN_SHALLOW_YZ || !(c->v.implicit_flag & 1))
+    return fail(EXO_ERR_ARG, "the context has no implicit x1 solve (ideal gas, implicit_flag 9)");
+  if (!(dt > 0.)) return fail(EXO_ERR_ARG, "dt must be positive");
+  size_t bytes = c->state_elems * sizeof(double);
+  CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->v.du, du_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = timed(c, EXO_K_IMPLICIT, 1,
+                 [&] { return STEP(launch_implicit_du, c->v, dt, c->stream); });
+  if (rc) return fail(rc, "implicit launch failed");
+  CK(cudaMemcpyAsync(du_host, c->v.du, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return EXO_OK;
 }
 

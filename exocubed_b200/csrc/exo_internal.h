@@ -155,6 +155,7 @@ int view_refresh_self(DevView& v, void* stream, std::string* err);
   int launch_flux_x23(const DevView& v, void* stream);                               \
   int launch_update(const DevView& v, int stage, void* stream);                      \
   int launch_implicit(const DevView& v, int stage, void* stream);                    \
+  int launch_implicit_du(const DevView& v, double dt, void* stream);                 \
   int launch_dt_reset(const DevView& v, void* stream);                               \
   int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream); \
   int launch_set_dt(const DevView& v, double dt, void* stream);                      \

@@ -1692,8 +1692,9 @@ struct StepColumnIO {
   double* uc;
   size_t vs;       // stride between variables
   double* scr0;    // scratch of this column: [level][entry][32 lanes] per warp of columns
-  int stage;
+  int stage;            // < 0: write the corrected update into du, leave u alone
   double Rd, gamma;
+  double* duw;          // du of this column, for stage < 0
   __device__ __forceinline__ void w(int i, double* out) const {
 #pragma unroll
     for (int n = 0; n < 5; ++n) out[n] = wc[n * vs + i];
@@ -1704,10 +1705,16 @@ struct StepColumnIO {
     return scr0[(lev * 30 + e) * 32];
   }
   __device__ __forceinline__ void uload(int i, double* u) const {
+    if (stage < 0) return;
 #pragma unroll
     for (int n = 0; n < 5; ++n) u[n] = uc[n * vs + i];
   }
   __device__ __forceinline__ void ustore(int i, const double* u, const double* dl) const {
+    if (stage < 0) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) duw[n * vs + i] = dl[n];
+      return;
+    }
     double uu[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) uu[n] = u[n] + 1. * dl[n];
@@ -1719,7 +1726,11 @@ struct StepColumnIO {
 
 // One radial column of the stepping context: solve, then u += du and, on
 // the last stage, the AirParcel round trip.
-__device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, int stage) {
+// stage 0..2: a stage of the step (dt = beta_stage * the CFL step, u += du);
+// stage -1: ImplicitSolver::SolveImplicit3D alone (dt given, du corrected in
+// place)
+__device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, int stage,
+                                               double dt_given = 0.) {
   extern __shared__ double ism[];
   const int ncol = 6 * v.N * v.N;
   const int col = (int)(blk * blockDim.x + threadIdx.x);
@@ -1727,11 +1738,12 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const int j = v.js + col % v.N;
   const int k = v.ks + (col / v.N) % v.N;
   const int p = col / (v.N * v.N);
-  const double dt = rk_beta(stage) * v.sc->dt;
+  const double dt = stage < 0 ? dt_given : rk_beta(stage) * v.sc->dt;
   const size_t base = idx(v, p, 0, k, j, 0);
   // scratch in blocks of 32 columns: a warp's 32 entries are 256 contiguous bytes
   double* scr0 = v.scratch + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
-  StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma};
+  StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
+                  v.du + base};
   implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
                   geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), v.x1f,
                   v.x1v, v.dx1f, v.is, v.ie, dt, v.gamma, v.grav);
@@ -1874,11 +1886,11 @@ __global__ void kb_update(Batch bt, int stage) {
   update_block<T>(sv, b, stage);
 }
 
-__global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage) {
+__global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage, double dt_given) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
-  implicit_block(sv, b, stage);
+  implicit_block(sv, b, stage, dt_given);
 }
 
 __global__ void kb_roundtrip(Batch bt) {
@@ -1974,7 +1986,15 @@ int launch_update(const DevView& v, int stage, void* stream) {
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
-                impl_smem(v.tiles[BK_IMPLICIT]), (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), stage);
+                impl_smem(v.tiles[BK_IMPLICIT]), (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), stage,
+                                                                          0.);
+  return check_launch();
+}
+
+int launch_implicit_du(const DevView& v, double dt, void* stream) {
+  if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
+  kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
+                impl_smem(v.tiles[BK_IMPLICIT]), (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), -1, dt);
   return check_launch();
 }
 
@@ -2022,7 +2042,7 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
     }
     if (pl.total[BK_IMPLICIT]) {
       kb_implicit<<<pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT], impl_smem(pl.threads[BK_IMPLICIT]),
-                    st>>>(B(BK_IMPLICIT), s);
+                    st>>>(B(BK_IMPLICIT), s, 0.);
       if ((rc = check_launch())) return rc;
     }
     if (s == 2) {

@@ -148,6 +148,24 @@ int exo_step(exo_ctx* ctx, int nsteps, double dt_fixed);
 
 /* Current time step, simulated time and step count. */
 int exo_get_dt(exo_ctx* ctx, double* dt);
+
+/* One stage (0, 1, 2) of SSPRK(3,3) on the CFL time step: the reference's
+   DoTaskListOneStage(stage) for the whole atmosphere (fluxes, update,
+   implicit correction, boundaries, primitives); stage 2 also advances the
+   time and computes the next step.  Three calls equal one exo_step. */
+int exo_stage(exo_ctx* ctx, int stage);
+/* The two ghost syncs of a stage and ConservedToPrimitive (PackData /
+   unpack of the panel boundaries, cubed_sphere_utility.cpp:18-619, and the
+   reflecting x1 ghosts): the primitives, ghosts included, from the current
+   conserved state. */
+int exo_boundary(exo_ctx* ctx);
+/* ImplicitSolver::SolveImplicit3D(du, w, dt) (solve_implicit_3d.cpp:27-180,
+   FullCorrection): du_host (six AthenaArray(NHYDRO, nc3, nc2, nc1) blocks,
+   interior used) is corrected in place from the primitives w_host (ghosts
+   used at the x1 boundaries) with time step dt.  It works in the context's
+   own primitive and update arrays: load a state (exo_set_primitive) before
+   stepping the context again. */
+int exo_solve_implicit_3d(exo_ctx* ctx, double* du_host, const double* w_host, double dt);
 int exo_get_time(exo_ctx* ctx, double* time, int64_t* ncycle);
 
 /* Sticky device-side validity flag (MeshBlock::Impl::SetStateInvalid,

@@ -1681,6 +1681,16 @@ void ora_step(void* h, int nsteps, double dt_fixed) {
   }
 }
 
+// ImplicitSolver::SolveImplicit3D on whole arrays: du (in/out, interior) and
+// w (ghosts used) in the AthenaArray layout of six panels, time step dt
+void ora_solve_implicit_3d(void* h, double* du, const double* w, double dt) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  std::memcpy(o.w.data(), w, o.w.size() * sizeof(double));
+  std::memcpy(o.du.data(), du, o.du.size() * sizeof(double));
+  implicit_x1(o, dt);
+  std::memcpy(du, o.du.data(), o.du.size() * sizeof(double));
+}
+
 // geometry exports for the tests
 void ora_get_mesh(void* h, int panel, double* x1f, double* x2f, double* x3f) {
   Oracle& o = *static_cast<Oracle*>(h);

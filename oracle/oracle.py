@@ -71,6 +71,7 @@ def lib():
         L.ora_get_mesh.argtypes = [p, i, dp, dp, dp]
         L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
         L.ora_implicit_columns.argtypes = [i, i, dp, dp, dp, dp, dp, dp, d, d, d]
+        L.ora_solve_implicit_3d.argtypes = [p, dp, dp, d]
         _lib = L
     return _lib
 
@@ -147,6 +148,12 @@ class Oracle:
 
     def invalid(self):
         return lib().ora_get_invalid(self._h)
+
+    def solve_implicit_3d(self, du, w, dt):
+        """SolveImplicit3D: du (whole-array layout) corrected in place."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        assert du.flags.c_contiguous and du.dtype == np.float64
+        lib().ora_solve_implicit_3d(self._h, _ptr(du), _ptr(w), float(dt))
 
     def mesh(self, panel):
         c = self.cfg

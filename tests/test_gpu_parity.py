@@ -97,6 +97,22 @@ def test_shallow_water_fixed_dt_many_steps_bitwise(oracle_mod):
                           W.interior(o.conserved())[:, [0, 2, 3]])
 
 
+@pytest.mark.parametrize("seed", [0, 1])
+def test_c1_config_100_steps_bitwise(oracle_mod, seed):
+    """The exo2 configuration as specified: 6 x 48 x 48, Roe, CFL 0.4,
+    100 steps on the CFL time step, bit-compared with the oracle (conserved
+    state, primitives incl. ghosts, time step and time)."""
+    cfg = W.shallow_water_config(N=48)
+    o, g = _pair(oracle_mod, cfg, W.shallow_water_state(cfg, seed=seed))
+    o.step(100)
+    g.step(100)
+    assert g.dt == o.dt and g.time == o.time
+    ug, uo = W.interior(g.conserved()), W.interior(o.conserved())
+    assert np.isfinite(ug).all()
+    assert np.array_equal(ug[:, [0, 2, 3]], uo[:, [0, 2, 3]]), np.abs(ug - uo).max()
+    assert np.array_equal(_noncorner(g.primitive()), _noncorner(o.primitive()))
+
+
 @pytest.mark.parametrize("rsolver", [1, 2])
 def test_dry_atmosphere_fluxes(oracle_mod, rsolver):
     N, L = 8, 12
