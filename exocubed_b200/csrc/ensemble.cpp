@@ -91,12 +91,14 @@ int rebuild(exo_ensemble* e) {
   std::vector<DevView> views;
   std::vector<unsigned> start((size_t)exo::BK_COUNT * (e->capacity + 1), 0);
   unsigned tot[exo::BK_COUNT] = {0, 0, 0, 0, 0, 0};
+  int max_nc1 = 1;
   int x1_threads = 32;
   size_t x1_smem = 8;
   for (Member* m : e->slots) {
     if (!m) continue;
     int idx = (int)views.size();
     views.push_back(m->v);
+    max_nc1 = std::max(max_nc1, m->v.nc1);
     unsigned b[exo::BK_COUNT];
     exo::member_blocks(m->v, e->tiles.t, b);
     for (int k = 0; k < exo::BK_COUNT; ++k) {
@@ -129,6 +131,7 @@ int rebuild(exo_ensemble* e) {
   pl.x1_threads = x1_threads;
   pl.x1_smem = x1_smem;
   for (int k = 0; k < exo::BK_COUNT; ++k) pl.threads[k] = e->tiles.t[k];
+  pl.max_nc1 = max_nc1;
   // count the kernel nodes of one step
   int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 + (tot[exo::BK_IMPLICIT] ? 1 : 0) + 1;
   e->launches_per_step = 3 * per_stage + (tot[exo::BK_ROUNDTRIP] ? 1 : 0) + 1 + 1;

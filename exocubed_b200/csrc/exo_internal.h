@@ -126,6 +126,7 @@ struct BatchPlan {
   int x1_threads;                // block size of the x1 flux kernel
   size_t x1_smem;                // its dynamic shared memory
   int threads[BK_COUNT];         // tiles of the other kernels
+  int max_nc1;                   // largest nc1 of the members (radial tables in shared memory)
 };
 // Threads per block ("tile") of each batched kernel by BatchKind.  BK_X1
 // takes one radial column per block (its size follows L) and ignores its

@@ -1678,10 +1678,34 @@ constexpr int IMPL_MAX_THREADS = 128;
 // there), threads IMPL_SM_STRIDE doubles apart: an odd stride keeps a
 // half-warp's 8-byte accesses on distinct banks
 constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : 61;
-constexpr size_t impl_smem(int threads) {
-  return (size_t)IMPL_SM_STRIDE * threads * sizeof(double);
+// per block: the threads' slices, then x1f (nc1+1), x1v (nc1), dx1f (nc1)
+constexpr size_t impl_smem(int threads, int nc1) {
+  return ((size_t)IMPL_SM_STRIDE * threads + 3 * (size_t)(nc1 + 1)) * sizeof(double);
 }
-constexpr size_t IMPL_SMEM = impl_smem(IMPL_THREADS);
+// the largest dynamic shared memory a launch may ask for
+constexpr int IMPL_SMEM_MAX = 160 * 1024;
+
+// copies the radial geometry of the member into shared memory (all threads
+// of the block take part; returns the shared copies)
+__device__ __forceinline__ void stage_radial(double* sg, int nc1, const double* x1f,
+                                             const double* x1v, const double* dx1f,
+                                             const double*& sx1f, const double*& sx1v,
+                                             const double*& sdx1f) {
+  double* a = sg;
+  double* b = sg + nc1 + 1;
+  double* c = b + nc1 + 1;
+  for (int t = threadIdx.x; t <= nc1; t += blockDim.x) {
+    a[t] = x1f[t];
+    if (t < nc1) {
+      b[t] = x1v[t];
+      c[t] = dx1f[t];
+    }
+  }
+  __syncthreads();
+  sx1f = a;
+  sx1v = b;
+  sdx1f = c;
+}
 
 // A column of the stepping context: primitives and update from the state
 // arrays, the corrected update added to u (with the AirParcel round trip on
@@ -1734,6 +1758,12 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   extern __shared__ double ism[];
   const int ncol = 6 * v.N * v.N;
   const int col = (int)(blk * blockDim.x + threadIdx.x);
+  // the radial geometry, read every level by every column, staged once per
+  // block: kept out of L1, which the columns' strided loads churn each level
+  const double* x1f;
+  const double* x1v;
+  const double* dx1f;
+  stage_radial(ism + blockDim.x * IMPL_SM_STRIDE, v.nc1, v.x1f, v.x1v, v.dx1f, x1f, x1v, dx1f);
   if (col >= ncol) return;
   const int j = v.js + col % v.N;
   const int k = v.ks + (col / v.N) % v.N;
@@ -1745,8 +1775,8 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
                   v.du + base};
   implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
-                  geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), v.x1f,
-                  v.x1v, v.dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+                  geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), x1f,
+                  x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
 }
 
 // last-stage round trip when the implicit solver is off
@@ -1941,7 +1971,7 @@ inline unsigned member_block_count(const DevView& v, int kind) {
 
 int prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(kb_implicit, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)impl_smem(IMPL_MAX_THREADS));
+                                       IMPL_SMEM_MAX);
   return e == cudaSuccess ? 0 : EXO_ERR_CUDA;
 }
 
@@ -1986,15 +2016,16 @@ int launch_update(const DevView& v, int stage, void* stream) {
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
-                impl_smem(v.tiles[BK_IMPLICIT]), (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), stage,
-                                                                          0.);
+                impl_smem(v.tiles[BK_IMPLICIT], v.nc1), (cudaStream_t)stream>>>(
+      one(v, BK_IMPLICIT), stage, 0.);
   return check_launch();
 }
 
 int launch_implicit_du(const DevView& v, double dt, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
-                impl_smem(v.tiles[BK_IMPLICIT]), (cudaStream_t)stream>>>(one(v, BK_IMPLICIT), -1, dt);
+                impl_smem(v.tiles[BK_IMPLICIT], v.nc1), (cudaStream_t)stream>>>(
+      one(v, BK_IMPLICIT), -1, dt);
   return check_launch();
 }
 
@@ -2041,8 +2072,8 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
       if ((rc = check_launch())) return rc;
     }
     if (pl.total[BK_IMPLICIT]) {
-      kb_implicit<<<pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT], impl_smem(pl.threads[BK_IMPLICIT]),
-                    st>>>(B(BK_IMPLICIT), s, 0.);
+      kb_implicit<<<pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT],
+                    impl_smem(pl.threads[BK_IMPLICIT], pl.max_nc1), st>>>(B(BK_IMPLICIT), s, 0.);
       if ((rc = check_launch())) return rc;
     }
     if (s == 2) {

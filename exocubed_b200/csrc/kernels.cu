@@ -50,13 +50,15 @@ __global__ void EXO_IMPL_BOUNDS k_implicit_columns(
     double* scratch) {
   extern __shared__ double ism[];
   const int col = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (col >= ncol) return;
   const int nc1 = L + 2 * G;
+  const double *sx1f, *sx1v, *sdx1f;
+  stage_radial(ism + blockDim.x * IMPL_SM_STRIDE, nc1, x1f, x1v, dx1f, sx1f, sx1v, sdx1f);
+  if (col >= ncol) return;
   HookColumnIO io{w + (size_t)col * 5 * nc1, du + (size_t)col * 5 * L, nc1, L, scratch + col,
                   (size_t)ncol};
   const double* g4 = colgeo + (size_t)col * 4;
-  implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3], x1f, x1v, dx1f,
-                  G, G + L - 1, dt, gamma, grav);
+  implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3], sx1f, sx1v,
+                  sdx1f, G, G + L - 1, dt, gamma, grav);
 }
 
 __global__ void k_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
@@ -87,7 +89,8 @@ int launch_implicit_columns(int ncol, int L, const double* w, double* du, const 
                             double gamma, double grav, double* scratch, void* stream) {
   if (ncol <= 0) return 0;
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
-                              fp64::IMPL_SMEM, (cudaStream_t)stream>>>(
+                              fp64::impl_smem(fp64::IMPL_THREADS, L + 2 * G),
+                              (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
   return fp64::check_launch();
 }
@@ -138,7 +141,8 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
   }
   if (ncol <= 0) return 0;
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
-                              fp64::IMPL_SMEM, (cudaStream_t)stream>>>(
+                              fp64::impl_smem(fp64::IMPL_THREADS, L + 2 * G),
+                              (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
