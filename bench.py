@@ -222,7 +222,9 @@ def run_cpu(workload, steps, warmup):
 # (A c)_i and delta_i, 30 doubles per level, are written and read back)
 def alg_bytes_per_cell(kernel, precision):
     t = 4 if precision == 1 else 8
-    return {"flux_x1": 40 + 5 * t, "flux_x23": 5 * t + 10 * t, "update": 120 + 15 * t + 80,
+    # mixed flux_x23: one thread per line of faces reads every cell once per direction
+    x23 = 10 * t + 10 * t if precision == 1 else 5 * t + 10 * t
+    return {"flux_x1": 40 + 5 * t, "flux_x23": x23, "update": 120 + 15 * t + 80,
             "implicit": 160 + 480, "prim_ghost": 80 + (20 if precision == 1 else 0),
             "other": 0}[kernel]
 
