@@ -24,6 +24,7 @@ from . import _native as nat
 # candidate tiles per kernel id; EXO_K_OTHER (the round trip of atmospheres
 # without the implicit solver) is timed inside EXO_K_UPDATE and follows it
 CANDIDATES = {
+    nat.EXO_K_FLUX_X1: (1, 2, 4),        # radial columns per block
     nat.EXO_K_FLUX_X23: (64, 128, 256),
     nat.EXO_K_UPDATE: (64, 128, 256),
     nat.EXO_K_IMPLICIT: (32, 64, 128),

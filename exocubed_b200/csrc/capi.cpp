@@ -379,7 +379,7 @@ void view_free(std::vector<void*>& owned, void* stream_v) {
 
 Tiles default_tiles() {
   Tiles t;
-  t.t[BK_X1] = 0;
+  t.t[BK_X1] = 4;  // radial columns per block
   t.t[BK_X23] = 128;
   t.t[BK_UPDATE] = 128;
   t.t[BK_IMPLICIT] = 64;
@@ -390,12 +390,13 @@ Tiles default_tiles() {
 
 bool valid_tiles(const int* t, std::string* err) {
   for (int k = 0; k < BK_COUNT; ++k) {
-    if (k == BK_X1) continue;
     bool ok = t[k] >= 32 && t[k] <= 512 && t[k] % 32 == 0;
+    if (k == BK_X1) ok = t[k] >= 1 && t[k] <= X1_MAX_COLUMNS;
     if (k == BK_IMPLICIT) ok = t[k] == 32 || t[k] == 64 || t[k] == 128;
     if (!ok) {
       *err = "tile " + std::to_string(k) + " = " + std::to_string(t[k]) +
-             ": threads per block must be a multiple of 32 in [32, 512] (implicit: 32, 64, 128)";
+             ": threads per block must be a multiple of 32 in [32, 512] (implicit: 32, 64, "
+             "128; x1: columns per block, 1 to " + std::to_string(X1_MAX_COLUMNS) + ")";
       return false;
     }
   }
@@ -406,7 +407,7 @@ void member_blocks(const DevView& v, const int* t, unsigned b[BK_COUNT]) {
   bool shallow = v.eqn == EXO_EQN_SHALLOW_YZ;
   bool implicit = !shallow && (v.implicit_flag & 1);
   auto nb = [](size_t n, int th) { return (unsigned)((n + th - 1) / th); };
-  b[BK_X1] = shallow ? 0u : (unsigned)(6 * v.N * v.N);
+  b[BK_X1] = shallow ? 0u : nb((size_t)6 * v.N * v.N, t[BK_X1]);  // t[BK_X1] columns per block
   // mixed build: one thread per line of faces; FP64 build: one per face
   b[BK_X23] = v.precision == EXO_PREC_MIXED ? nb((size_t)2 * 6 * v.N * v.L, t[BK_X23])
                                             : nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, t[BK_X23]);

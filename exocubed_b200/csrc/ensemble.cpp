@@ -98,6 +98,7 @@ int rebuild(exo_ensemble* e) {
     if (!m) continue;
     int idx = (int)views.size();
     views.push_back(m->v);
+    for (int k = 0; k < exo::BK_COUNT; ++k) views.back().tiles[k] = e->tiles.t[k];
     max_nc1 = std::max(max_nc1, m->v.nc1);
     unsigned b[exo::BK_COUNT];
     exo::member_blocks(m->v, e->tiles.t, b);
@@ -106,9 +107,10 @@ int rebuild(exo_ensemble* e) {
       tot[k] += b[k];
     }
     if (m->v.eqn != EXO_EQN_SHALLOW_YZ) {
-      int t = std::min(256, ((m->v.L + 1 + 31) / 32) * 32);
-      x1_threads = std::max(x1_threads, t);
-      x1_smem = std::max(x1_smem, exo::x1_smem_bytes(m->v));
+      DevView tv = m->v;  // with the ensemble's tiles
+      for (int k = 0; k < exo::BK_COUNT; ++k) tv.tiles[k] = e->tiles.t[k];
+      x1_threads = std::max(x1_threads, exo::x1_threads(tv));
+      x1_smem = std::max(x1_smem, exo::x1_smem_bytes(tv));
     }
   }
   int n = (int)views.size();

@@ -137,11 +137,27 @@ struct Tiles {
 };
 Tiles default_tiles();
 bool valid_tiles(const int* t, std::string* err);
-// dynamic shared memory of the x1 kernel for one column: the primitives and
-// the face pressures, and in the mixed build ln psf and the face densities
+// The x1 kernel takes tiles[BK_X1] radial columns per block (1..X1_MAX_COLUMNS).
+// Shared memory per column: the primitives and the face pressures, and in
+// the mixed build ln psf and the face densities.
+constexpr int X1_MAX_COLUMNS = 8;
+#ifdef __CUDACC__
+#define EXO_HD __host__ __device__
+#else
+#define EXO_HD
+#endif
+EXO_HD inline int x1_column_doubles(const DevView& v) {
+  int faces = v.nc1 + 1;
+  return v.nv * v.nc1 + (v.precision == EXO_PREC_MIXED ? 3 : 1) * faces;
+}
+inline int x1_cols(const DevView& v) { return v.tiles[BK_X1] > 0 ? v.tiles[BK_X1] : 1; }
 inline size_t x1_smem_bytes(const DevView& v) {
-  size_t faces = (size_t)v.nc1 + 1;
-  return ((size_t)v.nv * v.nc1 + (v.precision == EXO_PREC_MIXED ? 3 : 1) * faces) * sizeof(double);
+  return (size_t)x1_cols(v) * x1_column_doubles(v) * sizeof(double);
+}
+// threads: the block's faces in whole warps, at most 1024
+inline int x1_threads(const DevView& v) {
+  int t = ((x1_cols(v) * (v.L + 1) + 31) / 32) * 32;
+  return t > 1024 ? 1024 : t;
 }
 // block counts of one member for the given tiles
 void member_blocks(const DevView& v, const int* tiles, unsigned blocks[BK_COUNT]);

@@ -568,24 +568,68 @@ __device__ __forceinline__ void prim_ghost_block(const DevView& v, unsigned blk,
 
 // ------------------------------------------------------------ k_flux_x1 ---
 // One CTA per interior radial column.
+// Several radial columns per block (the x1 tile): each column's faces,
+// cells and hydrostatic scan are spread over the block's threads, so the
+// block's lanes stay busy (one column of L+1 faces leaves most of a warp
+// idle) and the columns' serial scans run side by side.
+__device__ __forceinline__ int x1_columns_per_block(const DevView& v) {
+  return v.tiles[BK_X1] > 0 ? v.tiles[BK_X1] : 1;
+}
+
+// q = t / d, r = t - q d for small non-negative t (< 2^20) through a float
+// reciprocal, corrected by one step either way
+__device__ __forceinline__ void divmod_small(int t, int d, float inv_d, int& q, int& r) {
+  q = (int)((float)t * inv_d);
+  r = t - q * d;
+  if (r < 0) { --q; r += d; }
+  else if (r >= d) { ++q; r -= d; }
+}
+
 template <class T>
 __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
   extern __shared__ double sm[];
-  int col = blk;
-  int j = v.js + col % v.N;
-  int k = v.ks + (col / v.N) % v.N;
-  int p = col / (v.N * v.N);
-  int nc1 = v.nc1, nv = v.nv;
-  double* wc = sm;              // [nv][nc1]
-  double* psf = sm + nv * nc1;  // [nc1+1]
-  __shared__ double s_gam, s_expf;
-  for (int t = threadIdx.x; t < nv * nc1; t += blockDim.x)
-    wc[t] = v.w[idx(v, p, t / nc1, k, j, t % nc1)];
+  __shared__ double s_gam[X1_MAX_COLUMNS], s_expf[X1_MAX_COLUMNS];
+  __shared__ double s_cthp[X1_MAX_COLUMNS], s_cosc[X1_MAX_COLUMNS];
+  __shared__ long long s_base[X1_MAX_COLUMNS];  // idx(p, 0, k, j, 0) of each column
+  const int cpb = x1_columns_per_block(v);
+  const int ncol_total = 6 * v.N * v.N;
+  const int col0 = (int)blk * cpb;
+  const int ncb = min(cpb, ncol_total - col0);  // columns of this block
+  const int nc1 = v.nc1, nv = v.nv, L = v.L;
+  const int cstride = x1_column_doubles(v);    // shared doubles per column
+  const size_t vs = v.cells;
+  // shared memory of column c: w [nv][nc1], psf [nc1+1] (mixed: ln psf, dsf)
+  auto WC = [&](int c) { return sm + (size_t)c * cstride; };
+  auto PSF = [&](int c) { return sm + (size_t)c * cstride + nv * nc1; };
+  if ((int)threadIdx.x < ncb) {
+    const int c = threadIdx.x, col = col0 + c;
+    const int j = v.js + col % v.N;
+    const int k = v.ks + (col / v.N) % v.N;
+    const int p = col / (v.N * v.N);
+    s_base[c] = (long long)idx(v, p, 0, k, j, 0);
+    s_cthp[c] = geo(v, GCTHP1, p, k, j);
+    s_cosc[c] = geo(v, GCOSC, p, k, j);
+  }
   __syncthreads();
-  bool decomp = (v.grav != 0.);
+  {
+    const int per = nv * nc1;
+    const float inv_per = 1.f / (float)per, inv_nc1 = 1.f / (float)nc1;
+    for (int t = threadIdx.x; t < ncb * per; t += blockDim.x) {
+      int c, r, n, i;
+      divmod_small(t, per, inv_per, c, r);
+      divmod_small(r, nc1, inv_nc1, n, i);
+      WC(c)[r] = v.w[(size_t)s_base[c] + n * vs + i];
+    }
+  }
+  __syncthreads();
+  const bool decomp = (v.grav != 0.);
   if (decomp) {
-    // Decomposition::ChangeToPerturbation (change_to_perturbation.cpp:39-157)
-    if (threadIdx.x == 0) {
+    // Decomposition::ChangeToPerturbation (change_to_perturbation.cpp:39-157),
+    // one thread per column for the downward scan
+    if ((int)threadIdx.x < ncb) {
+      const int c = threadIdx.x;
+      double* wc = WC(c);
+      double* psf = PSF(c);
       double grav = -v.grav;
       int is = v.is, ie = v.ie;
       double* wd = wc + IDN * nc1;
@@ -598,51 +642,67 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       double gammad = v.gamma, fsig = 1., feps = 1.;
       double gam = 1. + (gammad - 1.) * feps / fsig;
       double ent = log(wp[is]) - gam * log(wd[is]);
-      s_gam = gam;
-      s_expf = exp(-ent / gam);
+      s_gam[c] = gam;
+      s_expf[c] = exp(-ent / gam);
     }
     __syncthreads();
+    const float inv_nc1 = 1.f / (float)nc1;
 #if EXO_MIXED
     // FP64 still, with the powers as exp(log(x) / gamma) and one log per face
     // shared by its two cells: ln psf and the face density of the isentropic
     // reference go to shared memory for the cells and for the restore
-    double* lpsf = psf + nc1 + 1;  // [nc1+1]
-    double* dsf = lpsf + nc1 + 1;  // [nc1+1]
-    const double igam = 1. / s_gam;
-    for (int i = threadIdx.x; i <= nc1; i += blockDim.x) {
+    const float inv_f = 1.f / (float)(nc1 + 1);
+    for (int t = threadIdx.x; t < ncb * (nc1 + 1); t += blockDim.x) {
+      int c, i;
+      divmod_small(t, nc1 + 1, inv_f, c, i);
+      double* psf = PSF(c);
       const double l = log(psf[i]);
-      lpsf[i] = l;
-      dsf[i] = exp(l * igam) * s_expf;
+      psf[nc1 + 1 + i] = l;
+      psf[2 * (nc1 + 1) + i] = exp(l * (1. / s_gam[c])) * s_expf[c];
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nc1; i += blockDim.x) {
+    for (int t = threadIdx.x; t < ncb * nc1; t += blockDim.x) {
+      int c, i;
+      divmod_small(t, nc1, inv_nc1, c, i);
+      double* wc = WC(c);
+      const double* psf = PSF(c);
+      const double* lpsf = psf + nc1 + 1;
       double psv;
       if (fabs(psf[i] - psf[i + 1]) < 1.E-6)
         psv = (psf[i] + psf[i + 1]) * 0.5;
       else
         psv = (psf[i] - psf[i + 1]) / (lpsf[i] - lpsf[i + 1]);
-      const double dsv = exp(log(psv) * igam) * s_expf;
+      const double dsv = exp(log(psv) * (1. / s_gam[c])) * s_expf[c];
       wc[IPR * nc1 + i] -= psv;
       wc[IDN * nc1 + i] -= dsv;
     }
 #else
-    for (int i = threadIdx.x; i < nc1; i += blockDim.x) {
+    for (int t = threadIdx.x; t < ncb * nc1; t += blockDim.x) {
+      int c, i;
+      divmod_small(t, nc1, inv_nc1, c, i);
+      double* wc = WC(c);
+      const double* psf = PSF(c);
       double psv, dsv;
       if (fabs(psf[i] - psf[i + 1]) < 1.E-6)
         psv = (psf[i] + psf[i + 1]) / 2.;
       else
         psv = (psf[i] - psf[i + 1]) / log(psf[i] / psf[i + 1]);
-      dsv = pow(psv, 1. / s_gam) * s_expf;
+      dsv = pow(psv, 1. / s_gam[c]) * s_expf[c];
       wc[IPR * nc1 + i] -= psv;
       wc[IDN * nc1 + i] -= dsv;
     }
 #endif
     __syncthreads();
   }
-  FaceGeo<T> fg{T(0.), T(1.), T(geo(v, GCTHP1, p, k, j)), T(geo(v, GCOSC, p, k, j))};
   T* F = flux_array<T>(v, 0);
-  for (int f = threadIdx.x; f <= v.L; f += blockDim.x) {
-    int i = v.is + f;
+  const float inv_faces = 1.f / (float)(L + 1);
+  for (int t = threadIdx.x; t < ncb * (L + 1); t += blockDim.x) {
+    int c, f;
+    divmod_small(t, L + 1, inv_faces, c, f);
+    const double* wc = WC(c);
+    const double* psf = PSF(c);
+    const int i = v.is + f;
+    FaceGeo<T> fg{T(0.), T(1.), T(s_cthp[c]), T(s_cosc[c])};
     // perturbations are formed in FP64 above; WENO5 and the Riemann solve run in T
     T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
     #pragma unroll
@@ -663,7 +723,7 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
 #if EXO_MIXED
       const double dsf = psf[2 * (nc1 + 1) + i];
 #else
-      double dsf = pow(ps, 1. / s_gam) * s_expf;
+      double dsf = pow(ps, 1. / s_gam[c]) * s_expf[c];
 #endif
       double dr = wr[IDN], dl = wl[IDN];
       dr += dsf;
@@ -678,10 +738,11 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
     // x1 runs for the ideal gas only: LMARS or HLLC
     if (v.rsolver == EXO_RS_HLLC) riemann_hllc<T>(v.gamma, IVX, fg, wl, wr, fx);
     else riemann_lmars<T>(v.gamma, IVX, wl, wr, fx);
+    T* Fc = F + (size_t)s_base[c] + i;
     #pragma unroll
     for (int n = 0; n < 5; ++n) {
       if (n >= nv) break;
-      F[idx(v, p, n, k, j, i)] = fx[n];
+      Fc[n * vs] = fx[n];
     }
   }
 }
@@ -1684,6 +1745,7 @@ constexpr size_t impl_smem(int threads, int nc1) {
 }
 // the largest dynamic shared memory a launch may ask for
 constexpr int IMPL_SMEM_MAX = 160 * 1024;
+constexpr int X1_SMEM_MAX = 160 * 1024;
 
 // copies the radial geometry of the member into shared memory (all threads
 // of the block take part; returns the shared copies)
@@ -1883,12 +1945,12 @@ __global__ void kb_prim_ghost(Batch bt, int compute_dt) {
   prim_ghost_block(sv, b, compute_dt);
 }
 
-// The x1 kernel is latency bound (one thread walks the hydrostatic scan of
-// the column while the others wait): occupancy beats registers, measured
-#ifndef EXO_X1_MINB
-#define EXO_X1_MINB 5
+// The x1 kernel is latency bound (a thread per column walks the hydrostatic
+// scan while the others wait): occupancy beats registers, measured
+#ifndef EXO_X1_MAXNREG
+#define EXO_X1_MAXNREG 48
 #endif
-#define EXO_X1_BOUNDS __launch_bounds__(256, EXO_X1_MINB)
+#define EXO_X1_BOUNDS __maxnreg__(EXO_X1_MAXNREG)
 template <class T>
 __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
   __shared__ __align__(16) DevView sv;
@@ -1972,6 +2034,9 @@ inline unsigned member_block_count(const DevView& v, int kind) {
 int prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(kb_implicit, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        IMPL_SMEM_MAX);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kb_flux_x1<EXO_FLUX_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             X1_SMEM_MAX);
   return e == cudaSuccess ? 0 : EXO_ERR_CUDA;
 }
 
@@ -1983,8 +2048,7 @@ int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream) {
 
 int launch_flux_x1(const DevView& v, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ) return 0;
-  int threads = ((v.L + 1 + 31) / 32) * 32;
-  if (threads > 256) threads = 256;
+  const int threads = x1_threads(v);
   size_t smem = x1_smem_bytes(v);
   kb_flux_x1<EXO_FLUX_T><<<member_block_count(v, BK_X1), threads, smem, (cudaStream_t)stream>>>(
       one(v, BK_X1));

@@ -200,10 +200,10 @@ int exo_profile(exo_ctx* ctx, int enable);
 
 /* Launch tiles: threads per block of each kernel, indexed by EXO_K_* (the
    EXO_K_OTHER slot is the last-stage AirParcel round trip of atmospheres
-   without the implicit solver).  The x1 kernel takes one radial column per
-   block and ignores its slot; the others take a multiple of 32 in [32, 512],
-   EXO_K_IMPLICIT one of 32, 64, 128 (radial columns per block); 0 keeps the
-   current value.  The results do not depend on the tiles, only the speed
+   without the implicit solver).  EXO_K_FLUX_X1 is the radial columns per
+   block of the x1 kernel (1 to 8, its threads follow from L); the others
+   take a multiple of 32 in [32, 512], EXO_K_IMPLICIT one of 32, 64, 128
+   (radial columns per block); 0 keeps the current value.  The results do not depend on the tiles, only the speed
    does.  No counterpart in the reference (its CPU loops have no launch shape). */
 #define EXO_TILE_COUNT 6
 int exo_set_tiles(exo_ctx* ctx, const int* threads);

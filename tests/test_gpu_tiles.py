@@ -29,9 +29,10 @@ def test_tiles_do_not_change_results(precision, implicit):
     w = W.dry_atmosphere_state(cfg, seed=5)
     ref, t0 = _run(cfg, w, None)
     assert t0[1:] == [128, 128, 64, 256, 128]
-    for tiles in ([0, 64, 256, 32, 512, 64], [0, 256, 64, 128, 128, 256], [0, 32, 32, 32, 32, 32]):
+    assert t0[0] == 4
+    for tiles in ([1, 64, 256, 32, 512, 64], [2, 256, 64, 128, 128, 256], [8, 32, 32, 32, 32, 32]):
         got, t = _run(cfg, w, tiles)
-        assert t[1:] == tiles[1:]
+        assert t == tiles
         assert np.array_equal(got, ref), tiles
 
 
@@ -45,10 +46,10 @@ def test_ensemble_tiles_keep_members_exact():
     ens = Ensemble(precision=prec, capacity=4)
     slots = [ens.add(c, w) for c, w in members]
     ens.step(1)
-    ens.set_tiles([0, 256, 64, 128, 512, 64])   # changes shape mid-run
+    ens.set_tiles([2, 256, 64, 128, 512, 64])   # changes shape mid-run
     ens.step(2)
     ens.synchronize()
-    assert ens.tiles[1:] == [256, 64, 128, 512, 64]
+    assert ens.tiles == [2, 256, 64, 128, 512, 64]
     for s, a in zip(slots, alone):
         assert np.array_equal(ens.conserved(s), a)
     ens.close()
@@ -57,7 +58,8 @@ def test_ensemble_tiles_keep_members_exact():
 def test_invalid_tiles_are_refused():
     cfg = W.dry_atmosphere_config(N=6, L=8)
     with CubedSphereAtmosphere(cfg) as a:
-        for bad in ([0, 100, 0, 0, 0, 0], [0, 0, 0, 96, 0, 0], [0, 0, 1024, 0, 0, 0]):
+        for bad in ([0, 100, 0, 0, 0, 0], [0, 0, 0, 96, 0, 0], [0, 0, 1024, 0, 0, 0],
+                    [9, 0, 0, 0, 0, 0]):
             with pytest.raises(nat.ExoError) as e:
                 a.set_tiles(bad)
             assert e.value.code == 1
