@@ -1939,7 +1939,16 @@ __device__ __forceinline__ unsigned batch_enter(const Batch& bt, DevView& sv) {
   return local;
 }
 
-__global__ void kb_prim_ghost(Batch bt, int compute_dt) {
+// 48 registers (5 blocks of 256 threads per SM): 5-6 % faster than 70
+#ifndef EXO_PRIM_MAXNREG
+#define EXO_PRIM_MAXNREG 48
+#endif
+#ifdef EXO_PRIM_MAXNREG
+#define EXO_PRIM_BOUNDS __maxnreg__(EXO_PRIM_MAXNREG)
+#else
+#define EXO_PRIM_BOUNDS
+#endif
+__global__ void EXO_PRIM_BOUNDS kb_prim_ghost(Batch bt, int compute_dt) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   prim_ghost_block(sv, b, compute_dt);
@@ -1962,7 +1971,7 @@ __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
 // the mixed build's sliding-window kernel: 168 registers (3 blocks of 128
 // threads per SM) measured 16 % faster than its natural 208 at 6x192^2x96;
 // the FP64 per-face kernel needs fewer
-#ifndef EXO_X23_MAXNREG
+#if !defined(EXO_X23_MAXNREG) && EXO_MIXED
 #define EXO_X23_MAXNREG 168
 #endif
 #ifdef EXO_X23_MAXNREG
@@ -1977,8 +1986,13 @@ __global__ void EXO_X23_BOUNDS kb_flux_x23(Batch bt) {
   flux_x23_block<T>(sv, b);
 }
 
+#ifdef EXO_UPD_MAXNREG
+#define EXO_UPD_BOUNDS __maxnreg__(EXO_UPD_MAXNREG)
+#else
+#define EXO_UPD_BOUNDS
+#endif
 template <class T>
-__global__ void kb_update(Batch bt, int stage) {
+__global__ void EXO_UPD_BOUNDS kb_update(Batch bt, int stage) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   update_block<T>(sv, b, stage);
