@@ -34,7 +34,8 @@ EXPORTED = [
     "exo_ensemble_synchronize", "exo_ensemble_get_conserved", "exo_ensemble_get_primitive",
     "exo_ensemble_member_time", "exo_ensemble_check_state", "exo_ensemble_stats",
     "exo_set_tiles", "exo_get_tiles", "exo_ensemble_set_tiles", "exo_ensemble_get_tiles",
-    "exo_stage", "exo_boundary", "exo_solve_implicit_3d",
+    "exo_stage", "exo_boundary", "exo_solve_implicit_3d", "exo_change_to_perturbation",
+    "exo_restore_from_perturbation",
     "exo_ensemble_get_stream",
     "exo_implicit_columns", "exo_implicit_columns_noalloc",
 ]
@@ -122,6 +123,8 @@ def lib():
     L.exo_stage.argtypes = [p, i]
     L.exo_boundary.argtypes = [p]
     L.exo_solve_implicit_3d.argtypes = [p, dp, dp, d]
+    L.exo_change_to_perturbation.argtypes = [p, dp]
+    L.exo_restore_from_perturbation.argtypes = [p, dp, dp, dp]
     ip = ctypes.POINTER(ctypes.c_int)
     L.exo_set_tiles.argtypes = [p, ip]
     L.exo_get_tiles.argtypes = [p, ip]

@@ -115,6 +115,19 @@ class CubedSphereAtmosphere:
         w = np.ascontiguousarray(w, dtype=np.float64)
         nat.check(nat.lib().exo_solve_implicit_3d(self._ctx, nat.dptr(du), nat.dptr(w), float(dt)))
 
+    def change_to_perturbation(self, w):
+        """Decomposition::ChangeToPerturbation on w (whole-array layout, in place)."""
+        assert w.shape == self.shape and w.flags.c_contiguous and w.dtype == np.float64
+        nat.check(nat.lib().exo_change_to_perturbation(self._ctx, nat.dptr(w)))
+
+    def restore_from_perturbation(self, w, wl, wr):
+        """Decomposition::RestoreFromPerturbation: w, and the x1 face states wl,
+        wr (same layout as w), restored in place."""
+        for a in (w, wl, wr):
+            assert a.shape == self.shape and a.flags.c_contiguous and a.dtype == np.float64
+        nat.check(nat.lib().exo_restore_from_perturbation(self._ctx, nat.dptr(w), nat.dptr(wl),
+                                                          nat.dptr(wr)))
+
     def synchronize(self):
         nat.check(nat.lib().exo_synchronize(self._ctx))
 

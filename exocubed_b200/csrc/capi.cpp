@@ -86,6 +86,10 @@ struct exo_ctx {
   // one CFL step captured as a graph (profiling off): exo_step replays it
   cudaGraphExec_t step_graph = nullptr;
   int64_t graph_launches = 0;
+  // Decomposition hooks: face pressures, original pressure and density and
+  // column constants between the two calls (allocated on the first call)
+  double* dec_refs = nullptr;
+  bool dec_done = false;
 };
 
 
@@ -537,6 +541,7 @@ void exo_destroy(exo_ctx* c) {
     cudaEventDestroy(e.b);
   }
   for (void* p : c->owned) cudaFree(p);
+  if (c->dec_refs) cudaFree(c->dec_refs);
   cudaStreamDestroy(c->stream);
   cudaSetDevice(prev);
   delete c;
@@ -666,6 +671,45 @@ int exo_boundary(exo_ctx* c) {
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   int rc = boundary_and_prim(c, false);
   return rc ? fail(rc, "boundary launch failed") : EXO_OK;
+}
+
+int exo_change_to_perturbation(exo_ctx* c, double* w_host) {
+  if (!c || !w_host) return fail(EXO_ERR_ARG, "NULL argument");
+  if (c->v.eqn == EXO_EQN_SHALLOW_YZ)
+    return fail(EXO_ERR_ARG, "the decomposition applies to the ideal gas (exo3)");
+  if (c->v.grav == 0.) return EXO_OK;  // no gravity: nothing is decomposed
+  if (!c->dec_refs) {
+    CK(cudaMalloc((void**)&c->dec_refs, exo::decomposition_refs_doubles(c->v) * sizeof(double)));
+  }
+  size_t bytes = c->state_elems * sizeof(double);
+  CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = exo::launch_change_to_perturbation(c->v, c->v.w, c->dec_refs, c->stream);
+  if (rc) return fail(rc, "decomposition launch failed");
+  CK(cudaMemcpyAsync(w_host, c->v.w, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->dec_done = true;
+  return EXO_OK;
+}
+
+int exo_restore_from_perturbation(exo_ctx* c, double* w_host, double* wl_host, double* wr_host) {
+  if (!c || !w_host || !wl_host || !wr_host) return fail(EXO_ERR_ARG, "NULL argument");
+  if (c->v.eqn == EXO_EQN_SHALLOW_YZ)
+    return fail(EXO_ERR_ARG, "the decomposition applies to the ideal gas (exo3)");
+  if (c->v.grav == 0.) return EXO_OK;
+  if (!c->dec_done) return fail(EXO_ERR_ARG, "no exo_change_to_perturbation before the restore");
+  size_t bytes = c->state_elems * sizeof(double);
+  double* wl = c->v.flux[1];  // staging: the context's x2/x3 flux arrays (same layout)
+  double* wr = c->v.flux[2];
+  CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(wl, wl_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(wr, wr_host, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = exo::launch_restore_from_perturbation(c->v, c->v.w, wl, wr, c->dec_refs, c->stream);
+  if (rc) return fail(rc, "restore launch failed");
+  CK(cudaMemcpyAsync(w_host, c->v.w, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(wl_host, wl, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(wr_host, wr, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
 }
 
 int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, double dt) {

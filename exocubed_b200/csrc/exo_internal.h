@@ -193,6 +193,12 @@ int launch_weno5(int n, const double* a, const double* b, const double* c,
 int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
                             const double* x1f, const double* x1v, const double* dx1f, double dt,
                             double gamma, double grav, double* scratch, void* stream);
+// Decomposition hooks on whole arrays of one atmosphere (refs: face
+// pressures, original pressure and density, column constants)
+int launch_change_to_perturbation(const DevView& v, double* w, double* refs, void* stream);
+int launch_restore_from_perturbation(const DevView& v, double* w, double* wl, double* wr,
+                                     double* refs, void* stream);
+size_t decomposition_refs_doubles(const DevView& v);
 int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
                                     const double* colgeo, const double* x1f, const double* x1v,
                                     const double* dx1f, double dt, double gamma, double grav,

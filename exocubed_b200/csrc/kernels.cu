@@ -81,8 +81,118 @@ __global__ void k_weno5(int n, const double* a, const double* b, const double* c
   if (m < n) out[m] = weno5<double>(a[m], b[m], c[m], d[m], e[m]);
 }
 
+// Decomposition::ChangeToPerturbation (change_to_perturbation.cpp:39-157) on
+// one interior radial column of w (in place), one thread per column: the
+// original pressure and density are kept in orig, the face pressures in psf,
+// the column's gamma and entropy in colc, for RestoreFromPerturbation.
+struct DecompRefs {
+  double* psf;   // [6][nc3][nc2][nc1+1]
+  double* pres;  // [6][nc3][nc2][nc1]
+  double* dens;  // [6][nc3][nc2][nc1]
+  double* colc;  // [6][nc3][nc2][2]: gamma, entropy
+};
+
+__device__ __forceinline__ bool decomp_column(const DevView& v, int col, int& p, int& k, int& j) {
+  if (col >= 6 * v.N * v.N) return false;
+  j = v.js + col % v.N;
+  k = v.ks + (col / v.N) % v.N;
+  p = col / (v.N * v.N);
+  return true;
+}
+
+__global__ void k_change_to_perturbation(DevView v, double* w, DecompRefs r) {
+  int p, k, j;
+  if (!decomp_column(v, blockIdx.x * blockDim.x + threadIdx.x, p, k, j)) return;
+  const int nc1 = v.nc1, is = v.is, ie = v.ie;
+  const size_t q = ((size_t)p * v.nc3 + k) * v.nc2 + j;
+  double* wd = w + idx(v, p, IDN, k, j, 0);
+  double* wp = w + idx(v, p, IPR, k, j, 0);
+  double* psf = r.psf + q * (nc1 + 1);
+  for (int i = 0; i < nc1; ++i) {
+    r.pres[q * nc1 + i] = wp[i];
+    r.dens[q * nc1 + i] = wd[i];
+  }
+  const double grav = -v.grav;
+  const double RdTv = wp[ie] / wd[ie];
+  psf[ie + 1] = wp[ie] * exp(-grav * v.dx1f[ie] / (2 * RdTv));
+  for (int i = ie; i >= is; --i) psf[i] = psf[i + 1] + grav * wd[i] * v.dx1f[i];
+  for (int i = 1; i <= G; ++i) psf[is - i] = psf[is + i];
+  for (int i = 1; i <= G; ++i) psf[ie + i + 1] = psf[ie + 1 - i];
+  // PopulateBotEntropy (decomposition.cpp:341-388), no bottom neighbour
+  const double gammad = v.gamma, fsig = 1., feps = 1.;
+  const double gam = 1. + (gammad - 1.) * feps / fsig;
+  const double ent = log(wp[is]) - gam * log(wd[is]);
+  r.colc[2 * q] = gam;
+  r.colc[2 * q + 1] = ent;
+  const double expf = exp(-ent / gam);
+  for (int i = 0; i < nc1; ++i) {
+    double psv;
+    if (fabs(psf[i] - psf[i + 1]) < 1.E-6)
+      psv = (psf[i] + psf[i + 1]) / 2.;
+    else
+      psv = (psf[i] - psf[i + 1]) / log(psf[i] / psf[i + 1]);
+    const double dsv = pow(psv, 1. / gam) * expf;
+    wp[i] -= psv;
+    wd[i] -= dsv;
+  }
+}
+
+// Decomposition::RestoreFromPerturbation (:159-222): the column's pressure
+// and density back in w, the face pressure and isentropic face density added
+// to the x1 face states wl, wr (same layout as w, faces is..ie+1)
+__global__ void k_restore_from_perturbation(DevView v, double* w, double* wl, double* wr,
+                                            DecompRefs r) {
+  int p, k, j;
+  if (!decomp_column(v, blockIdx.x * blockDim.x + threadIdx.x, p, k, j)) return;
+  const int nc1 = v.nc1;
+  const size_t q = ((size_t)p * v.nc3 + k) * v.nc2 + j;
+  const size_t bp = idx(v, p, IPR, k, j, 0), bd = idx(v, p, IDN, k, j, 0);
+  for (int i = 0; i < nc1; ++i) {
+    w[bp + i] = r.pres[q * nc1 + i];
+    w[bd + i] = r.dens[q * nc1 + i];
+  }
+  const double* psf = r.psf + q * (nc1 + 1);
+  const double gam = r.colc[2 * q], ent = r.colc[2 * q + 1];
+  for (int i = v.is; i <= v.ie + 1; ++i) {
+    wr[bp + i] += psf[i];
+    if (wr[bp + i] < 0.) wr[bp + i] = psf[i];
+    wl[bp + i] += psf[i];
+    if (wl[bp + i] < 0.) wl[bp + i] = psf[i];
+    const double dsf = pow(psf[i], 1. / gam) * exp(-ent / gam);
+    wr[bd + i] += dsf;
+    if (wr[bd + i] < 0.) wr[bd + i] = dsf;
+    wl[bd + i] += dsf;
+    if (wl[bd + i] < 0.) wl[bd + i] = dsf;
+  }
+}
+
 }  // namespace
 }  // namespace fp64
+
+int launch_change_to_perturbation(const DevView& v, double* w, double* refs, void* stream) {
+  const size_t nq = (size_t)6 * v.nc3 * v.nc2;
+  fp64::DecompRefs r{refs, refs + nq * (v.nc1 + 1), refs + nq * (v.nc1 + 1) + nq * v.nc1,
+                     refs + nq * (v.nc1 + 1) + 2 * nq * v.nc1};
+  const int ncol = 6 * v.N * v.N;
+  fp64::k_change_to_perturbation<<<fp64::nblk(ncol, 64), 64, 0, (cudaStream_t)stream>>>(v, w, r);
+  return fp64::check_launch();
+}
+
+int launch_restore_from_perturbation(const DevView& v, double* w, double* wl, double* wr,
+                                     double* refs, void* stream) {
+  const size_t nq = (size_t)6 * v.nc3 * v.nc2;
+  fp64::DecompRefs r{refs, refs + nq * (v.nc1 + 1), refs + nq * (v.nc1 + 1) + nq * v.nc1,
+                     refs + nq * (v.nc1 + 1) + 2 * nq * v.nc1};
+  const int ncol = 6 * v.N * v.N;
+  fp64::k_restore_from_perturbation<<<fp64::nblk(ncol, 64), 64, 0, (cudaStream_t)stream>>>(
+      v, w, wl, wr, r);
+  return fp64::check_launch();
+}
+
+size_t decomposition_refs_doubles(const DevView& v) {
+  const size_t nq = (size_t)6 * v.nc3 * v.nc2;
+  return nq * (v.nc1 + 1) + 2 * nq * v.nc1 + 2 * nq;
+}
 
 int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
                             const double* x1f, const double* x1v, const double* dx1f, double dt,

@@ -166,6 +166,23 @@ int exo_boundary(exo_ctx* ctx);
    own primitive and update arrays: load a state (exo_set_primitive) before
    stepping the context again. */
 int exo_solve_implicit_3d(exo_ctx* ctx, double* du_host, const double* w_host, double dt);
+/* Decomposition::ChangeToPerturbation(w, ...) (change_to_perturbation.cpp:
+   39-157) on every radial column: w_host (six AthenaArray(NHYDRO, nc3, nc2,
+   nc1) blocks, ghosts included; interior columns used) has the hydrostatic
+   pressure (log mean of the face pressures integrated down from the top) and
+   the isentropic reference density subtracted in place.  The context keeps
+   the face pressures, the original pressure and density and each column's
+   gamma and entropy for the restore (device memory allocated on the first
+   call, freed by exo_destroy).  No-op without gravity, as in the reference. */
+int exo_change_to_perturbation(exo_ctx* ctx, double* w_host);
+/* Decomposition::RestoreFromPerturbation(w, wl, wr, k, j, il, iu)
+   (:159-222) on every column: w_host gets its pressure and density back as
+   they were before exo_change_to_perturbation; the x1 face states wl_host
+   and wr_host (same layout as w; entry i is the face between cells i-1 and
+   i, faces is..ie+1 used) get the face pressure and isentropic face density
+   added back with the reference's positivity fallbacks.  Both calls work in
+   the context's own device arrays: load a state before stepping again. */
+int exo_restore_from_perturbation(exo_ctx* ctx, double* w_host, double* wl_host, double* wr_host);
 int exo_get_time(exo_ctx* ctx, double* time, int64_t* ncycle);
 
 /* Sticky device-side validity flag (MeshBlock::Impl::SetStateInvalid,

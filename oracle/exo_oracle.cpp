@@ -212,6 +212,8 @@ struct Oracle {
   double dt, time;
   int64_t ncycle;
   int invalid;
+  // ora_change_to_perturbation's column data for ora_restore_from_perturbation
+  std::vector<double> dec_psf, dec_pres, dec_dens, dec_gam, dec_ent;
 
   size_t at(int p, int n, int k, int j, int i) const {
     return ((((size_t)p * NV + n) * nc3 + k) * nc2 + j) * nc1 + i;
@@ -1689,6 +1691,74 @@ void ora_solve_implicit_3d(void* h, double* du, const double* w, double dt) {
   std::memcpy(o.du.data(), du, o.du.size() * sizeof(double));
   implicit_x1(o, dt);
   std::memcpy(du, o.du.data(), o.du.size() * sizeof(double));
+}
+
+// Decomposition::ChangeToPerturbation on whole arrays (AthenaArray layout of
+// six panels, ghosts included): the interior columns of w are decomposed in
+// place; the face pressures, original pressure and density and the column
+// constants are kept for ora_restore_from_perturbation.
+void ora_change_to_perturbation(void* h, double* w) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  if (o.cfg.grav == 0.) return;
+  size_t nq = (size_t)6 * o.nc3 * o.nc2;
+  o.dec_psf.assign(nq * (o.nc1 + 1), 0.);
+  o.dec_pres.assign(nq * o.nc1, 0.);
+  o.dec_dens.assign(nq * o.nc1, 0.);
+  o.dec_gam.assign(nq, 0.);
+  o.dec_ent.assign(nq, 0.);
+  for (int p = 0; p < 6; ++p)
+    for (int k = o.ks; k <= o.ke; ++k)
+      for (int j = o.js; j <= o.je; ++j) {
+        size_t q = ((size_t)p * o.nc3 + k) * o.nc2 + j;
+        std::vector<double> col((size_t)o.NV * o.nc1);
+        for (int n = 0; n < o.NV; ++n)
+          for (int i = 0; i < o.nc1; ++i) col[(size_t)n * o.nc1 + i] = w[o.at(p, n, k, j, i)];
+        for (int i = 0; i < o.nc1; ++i) {
+          o.dec_pres[q * o.nc1 + i] = col[(size_t)IPR * o.nc1 + i];
+          o.dec_dens[q * o.nc1 + i] = col[(size_t)IDN * o.nc1 + i];
+        }
+        ColumnDecomp cd;
+        decompose_column(o, p, k, j, cd, col.data());
+        std::copy(cd.psf.begin(), cd.psf.end(), o.dec_psf.begin() + q * (o.nc1 + 1));
+        o.dec_gam[q] = cd.gam;
+        o.dec_ent[q] = cd.ent;
+        for (int n = 0; n < o.NV; ++n)
+          for (int i = 0; i < o.nc1; ++i) w[o.at(p, n, k, j, i)] = col[(size_t)n * o.nc1 + i];
+      }
+}
+
+// Decomposition::RestoreFromPerturbation on whole arrays: w gets its kept
+// pressure and density back; the x1 face states wl, wr (same layout, faces
+// is..ie+1) get the face pressure and density added back.
+void ora_restore_from_perturbation(void* h, double* w, double* wl, double* wr) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  if (o.cfg.grav == 0. || o.dec_gam.empty()) return;
+  for (int p = 0; p < 6; ++p)
+    for (int k = o.ks; k <= o.ke; ++k)
+      for (int j = o.js; j <= o.je; ++j) {
+        size_t q = ((size_t)p * o.nc3 + k) * o.nc2 + j;
+        for (int i = 0; i < o.nc1; ++i) {
+          w[o.at(p, IPR, k, j, i)] = o.dec_pres[q * o.nc1 + i];
+          w[o.at(p, IDN, k, j, i)] = o.dec_dens[q * o.nc1 + i];
+        }
+        ColumnDecomp cd;
+        cd.psf.assign(o.dec_psf.begin() + q * (o.nc1 + 1),
+                      o.dec_psf.begin() + (q + 1) * (o.nc1 + 1));
+        cd.gam = o.dec_gam[q];
+        cd.ent = o.dec_ent[q];
+        for (int i = o.is; i <= o.ie + 1; ++i) {
+          double wlf[5], wrf[5];
+          for (int n = 0; n < o.NV; ++n) {
+            wlf[n] = wl[o.at(p, n, k, j, i)];
+            wrf[n] = wr[o.at(p, n, k, j, i)];
+          }
+          restore_faces(o, cd, wlf, wrf, i);
+          for (int n = 0; n < o.NV; ++n) {
+            wl[o.at(p, n, k, j, i)] = wlf[n];
+            wr[o.at(p, n, k, j, i)] = wrf[n];
+          }
+        }
+      }
 }
 
 // geometry exports for the tests

@@ -72,6 +72,8 @@ def lib():
         L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
         L.ora_implicit_columns.argtypes = [i, i, dp, dp, dp, dp, dp, dp, d, d, d]
         L.ora_solve_implicit_3d.argtypes = [p, dp, dp, d]
+        L.ora_change_to_perturbation.argtypes = [p, dp]
+        L.ora_restore_from_perturbation.argtypes = [p, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -148,6 +150,17 @@ class Oracle:
 
     def invalid(self):
         return lib().ora_get_invalid(self._h)
+
+    def change_to_perturbation(self, w):
+        """ChangeToPerturbation on w (whole-array layout, in place)."""
+        assert w.flags.c_contiguous and w.dtype == np.float64 and w.shape == self.shape
+        lib().ora_change_to_perturbation(self._h, _ptr(w))
+
+    def restore_from_perturbation(self, w, wl, wr):
+        """RestoreFromPerturbation: w and the x1 face states wl, wr in place."""
+        for a in (w, wl, wr):
+            assert a.flags.c_contiguous and a.dtype == np.float64 and a.shape == self.shape
+        lib().ora_restore_from_perturbation(self._h, _ptr(w), _ptr(wl), _ptr(wr))
 
     def solve_implicit_3d(self, du, w, dt):
         """SolveImplicit3D: du (whole-array layout) corrected in place."""
