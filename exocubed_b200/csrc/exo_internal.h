@@ -178,7 +178,8 @@ int view_refresh_self(DevView& v, void* stream, std::string* err);
   int launch_set_dt(const DevView& v, double dt, void* stream);                      \
   int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);          \
   int launch_batched_step(const BatchPlan& plan, void* stream);                     \
-  int prepare_kernels();
+  int prepare_kernels();                                                            \
+  bool x23_lines();
 namespace fp64 { EXO_DECLARE_STEP_LAUNCHERS }
 namespace mixed { EXO_DECLARE_STEP_LAUNCHERS }
 #undef EXO_DECLARE_STEP_LAUNCHERS

@@ -31,6 +31,11 @@
 
 #include "exo_internal.h"
 
+// x2/x3 fluxes: 1 = one thread per line of faces (sliding stencil window),
+// 0 = one thread per face
+#ifndef EXO_X23_LINES
+#define EXO_X23_LINES EXO_MIXED
+#endif
 // 1: the implicit solve keeps (A c)_{i-1} in shared memory instead of registers
 #ifndef EXO_IMPL_AP_SMEM
 #define EXO_IMPL_AP_SMEM 0
@@ -926,8 +931,8 @@ __device__ __forceinline__ void flux_x23_lines(const DevView& v, unsigned blk) {
 
 template <class T>
 __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
-  if constexpr (sizeof(T) == sizeof(double)) flux_x23_faces<T>(v, blk);
-  else flux_x23_lines<T>(v, blk);
+  if constexpr (EXO_X23_LINES) flux_x23_lines<T>(v, blk);
+  else flux_x23_faces<T>(v, blk);
 }
 
 // --------------------------------------------------------------- k_update -
@@ -2050,6 +2055,8 @@ inline unsigned member_block_count(const DevView& v, int kind) {
   member_blocks(v, v.tiles, b);
   return b[kind];
 }
+
+bool x23_lines() { return EXO_X23_LINES != 0; }
 
 int prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(kb_implicit, cudaFuncAttributeMaxDynamicSharedMemorySize,
