@@ -76,3 +76,26 @@ def test_hllc_rest_state_balanced(oracle_mod):
     o.set_primitive(W.dry_atmosphere_state(cfg, seed=0, temp_sigma=0., wind_sigma=0.))
     o.step(2, 600.)
     assert np.abs(W.interior(o.primitive())[:, 2:4]).max() < 1.0
+
+
+def test_oracle_decomposition_round_trip(oracle_mod):
+    """ChangeToPerturbation then RestoreFromPerturbation: the cell values come
+    back to the bit, the perturbation pressure is small against the pressure
+    (the hydrostatic part is removed) and restored face states stay positive."""
+    from exocubed_b200 import workloads as W
+    cfg = W.dry_atmosphere_config(N=6, L=12)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(W.dry_atmosphere_state(cfg, seed=2))
+    w0 = o.primitive()
+    w = w0.copy()
+    o.change_to_perturbation(w)
+    pi, p0 = W.interior(w)[:, 4], W.interior(w0)[:, 4]
+    assert (np.abs(pi) < 0.02 * np.abs(p0)).all()
+    wl = np.zeros_like(w)
+    wr = np.zeros_like(w)
+    wl[:, 4] = -1e9                  # a face state that must fall back to psf
+    o.restore_from_perturbation(w, wl, wr)
+    assert np.array_equal(W.interior(w), W.interior(w0))
+    faces = (slice(None), slice(None), slice(3, -3), slice(3, -3), slice(3, -2))
+    assert (wl[faces][:, 4] > 0).all() and (wr[faces][:, 4] > 0).all()
+    assert (wl[faces][:, 0] > 0).all()
