@@ -36,6 +36,11 @@
 #ifndef EXO_X23_LINES
 #define EXO_X23_LINES EXO_MIXED
 #endif
+// 1: the implicit solve's back substitution prefetches two levels through
+// shared memory
+#ifndef EXO_IMPL_BWD_SMEM
+#define EXO_IMPL_BWD_SMEM 0
+#endif
 // 1: the implicit solve keeps (A c)_{i-1} in shared memory instead of registers
 #ifndef EXO_IMPL_AP_SMEM
 #define EXO_IMPL_AP_SMEM 0
@@ -1166,6 +1171,9 @@ __device__ __forceinline__ void cp_async_commit() {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_wait_one() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
 
 // compile-time loops (the matrix entries live in registers, so every index
 // has to be a constant)
@@ -1638,6 +1646,57 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
     c0 = cp;
     cur = nxt;
   }
+#if EXO_IMPL_BWD_SMEM
+  // back substitution: delta_i -= (A c)_i delta_{i+1}.  The factors and the
+  // state of the next two levels are copied asynchronously into this
+  // thread's shared memory (two slots of 35 doubles, free once the forward
+  // sweep is done) while a level is finished.
+  {
+    double u_ie[5];
+    io.uload(ie, u_ie);
+    io.ustore(ie, u_ie, dp);
+  }
+  auto issue = [&](int i, int slot) {
+    double* d = sm + slot * 35;
+#pragma unroll
+    for (int e = 0; e < 30; ++e) cp_async8(d + e, &io.scr(i - is, e));
+    if (IO::kLoadsU) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) cp_async8(d + 30 + n, io.uptr(i, n));
+    }
+    cp_async_commit();
+  };
+  if (ie - 1 >= is) issue(ie - 1, 0);
+  if (ie - 2 >= is) issue(ie - 2, 1);
+  int slot = 0;
+#pragma unroll 1
+  for (int i = ie - 1; i >= is; --i) {
+    if (i - 1 >= is) cp_async_wait_one();
+    else cp_async_wait_all();
+    const double* d = sm + slot * 35;
+    double cs[30], cu[5];
+#pragma unroll
+    for (int e = 0; e < 30; ++e) cs[e] = d[e];
+    if (IO::kLoadsU) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) cu[n] = d[30 + n];
+    }
+    double dl[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double ad = cs[r * 5] * dp[0];
+#pragma unroll
+      for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
+      dl[r] = cs[25 + r] - ad;
+    }
+#pragma unroll
+    for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+    io.ustore(i, cu, dp);
+    if (i - 2 >= is) issue(i - 2, slot);
+    slot ^= 1;
+  }
+}
+#else
   // back substitution: delta_i -= (A c)_i delta_{i+1}, software-pipelined:
   // the next level's scratch and state are in flight while this level ends
   double cur_s[30], cur_u[5];
@@ -1675,6 +1734,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
     }
   }
 }
+#endif
 #undef EXO_AP
 
 // UpdateAllConserved on the last stage with NVAPOR = NCLOUD = 0: the
@@ -1743,7 +1803,7 @@ constexpr int IMPL_MAX_THREADS = 128;
 // each thread's doubles are contiguous (60, or 85 with (A c)_{i-1} kept
 // there), threads IMPL_SM_STRIDE doubles apart: an odd stride keeps a
 // half-warp's 8-byte accesses on distinct banks
-constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : 61;
+constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : (EXO_IMPL_BWD_SMEM ? 71 : 61);
 // per block: the threads' slices, then x1f (nc1+1), x1v (nc1), dx1f (nc1)
 constexpr size_t impl_smem(int threads, int nc1) {
   return ((size_t)IMPL_SM_STRIDE * threads + 3 * (size_t)(nc1 + 1)) * sizeof(double);
@@ -1795,6 +1855,8 @@ struct StepColumnIO {
   __device__ __forceinline__ double& scr(int lev, int e) const {
     return scr0[(lev * 30 + e) * 32];
   }
+  static constexpr bool kLoadsU = true;
+  __device__ __forceinline__ const double* uptr(int i, int n) const { return uc + n * vs + i; }
   __device__ __forceinline__ void uload(int i, double* u) const {
     if (stage < 0) return;
 #pragma unroll

@@ -37,6 +37,8 @@ struct HookColumnIO {
   __device__ __forceinline__ double& scr(int lev, int e) const {
     return scr0[((size_t)lev * 30 + e) * nslot];
   }
+  static constexpr bool kLoadsU = false;
+  __device__ __forceinline__ const double* uptr(int, int) const { return nullptr; }
   __device__ __forceinline__ void uload(int, double*) const {}
   __device__ __forceinline__ void ustore(int i, const double*, const double* dl) const {
 #pragma unroll
