@@ -37,9 +37,10 @@
 #define EXO_X23_LINES EXO_MIXED
 #endif
 // 1: the implicit solve's back substitution prefetches two levels through
-// shared memory
+// shared memory (FP64: 3% faster at 6x192^2x96; mixed: 1% slower, since its
+// 204-register cap already keeps a level in flight)
 #ifndef EXO_IMPL_BWD_SMEM
-#define EXO_IMPL_BWD_SMEM 0
+#define EXO_IMPL_BWD_SMEM (!EXO_MIXED)
 #endif
 // 1: the implicit solve keeps (A c)_{i-1} in shared memory instead of registers
 #ifndef EXO_IMPL_AP_SMEM
