@@ -49,6 +49,7 @@ BYTES_PER_CELL_UPDATE = 320  # 8 registers x 5 vars x 8 B per SSPRK(3,3) step
 
 RSOLVER = {1: "LMARS", 2: "HLLC"}
 _RS = [None]  # the --rsolver choice for exo3 workloads (None: LMARS)
+_IMP = [None]  # the --implicit-flag choice for exo3 workloads (None: 9)
 
 
 def workload_config(name, precision=0):
@@ -56,6 +57,9 @@ def workload_config(name, precision=0):
     if _RS[0] is not None and cfg["eqn"] == 1:
         cfg = dict(cfg, rsolver=_RS[0])
         desc = desc.replace("LMARS", RSOLVER[_RS[0]])
+    if _IMP[0] is not None and cfg["eqn"] == 1:
+        cfg = dict(cfg, implicit_flag=_IMP[0])
+        desc = desc.replace("implicit(9)", f"implicit({_IMP[0]})")
     if precision == 1:
         cfg = dict(cfg, precision=1)
         desc = desc.replace("FP64", "mixed FP32/FP64")
@@ -212,6 +216,8 @@ def run_cpu(workload, steps, warmup):
            "--cpu-steps", str(steps), "--cpu-warmup", str(warmup)]
     if _RS[0] is not None:
         cmd += ["--rsolver", str(_RS[0])]
+    if _IMP[0] is not None:
+        cmd += ["--implicit-flag", str(_IMP[0])]
     r = subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
     return json.loads(r.stdout.strip().splitlines()[-1])
 
@@ -219,13 +225,15 @@ def run_cpu(workload, steps, warmup):
 # -------------------------------------------------------------- our arm --
 # algorithmic DRAM bytes per interior cell and launch, by kernel and flux type
 # (each array element read or written once; the implicit solve's factors
-# (A c)_i and delta_i, 30 doubles per level, are written and read back)
-def alg_bytes_per_cell(kernel, precision):
+# (A c)_i and delta_i, 30 doubles per level with the full correction and 12
+# with the partial one, are written and read back)
+def alg_bytes_per_cell(kernel, precision, implicit_flag=9):
     t = 4 if precision == 1 else 8
     # mixed flux_x23: one thread per line of faces reads every cell once per direction
     x23 = 10 * t + 10 * t if precision == 1 else 5 * t + 10 * t
+    factors = 480 if implicit_flag & 8 else 192
     return {"flux_x1": 40 + 5 * t, "flux_x23": x23, "update": 120 + 15 * t + 80,
-            "implicit": 160 + 480, "prim_ghost": 80 + (20 if precision == 1 else 0),
+            "implicit": 160 + factors, "prim_ghost": 80 + (20 if precision == 1 else 0),
             "other": 0}[kernel]
 
 
@@ -383,13 +391,17 @@ def run_ours(args):
     dom = max((k for k in prof if k != "other"), key=lambda k: prof[k][1])
     n_l, t_l = prof[dom]
     avg_ms = t_l / max(n_l, 1)
-    alg_bytes = alg_bytes_per_cell(dom, prec) * cells
+    iflag = cfg.get("implicit_flag", 9)
+    alg_bytes = alg_bytes_per_cell(dom, prec, iflag) * cells
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        tr = json.load(open(tp)).get(f"{dom}:{'mixed' if prec == 1 else 'fp64'}")
+        key = f"{dom}:{'mixed' if prec == 1 else 'fp64'}"
+        if dom == "implicit" and not iflag & 8:
+            key += ":partial"
+        tr = json.load(open(tp)).get(key)
         if tr:  # DRAM bytes per cell measured by ncu, scaled to this launch
             traffic = tr["bytes_per_cell"] * cells
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
@@ -654,8 +666,11 @@ def main():
                     help="run N steps mixed vs FP64 and report the field errors")
     ap.add_argument("--rsolver", type=int, default=None, choices=[1, 2],
                     help="Riemann solver of exo3 workloads: 1 LMARS (default), 2 HLLC")
+    ap.add_argument("--implicit-flag", type=int, default=None, choices=[1, 9],
+                    help="implicit_flag of exo3 workloads: 9 full 5x5 (default), 1 partial 3x3")
     args = ap.parse_args()
     _RS[0] = args.rsolver
+    _IMP[0] = args.implicit_flag
     if args.cpu_worker:
         cpu_worker(args)
     elif args.accuracy > 0:

@@ -37,7 +37,7 @@ EXPORTED = [
     "exo_stage", "exo_boundary", "exo_solve_implicit_3d", "exo_change_to_perturbation",
     "exo_restore_from_perturbation",
     "exo_ensemble_get_stream",
-    "exo_implicit_columns", "exo_implicit_columns_noalloc",
+    "exo_implicit_columns", "exo_partial_correction_columns", "exo_implicit_columns_noalloc",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
 
@@ -107,6 +107,7 @@ def lib():
     L.exo_riemann.argtypes = [i, i, i, i, d, p, p, p, p, p, p, p, p]
     L.exo_weno5.argtypes = [i, p, p, p, p, p, p, p]
     L.exo_implicit_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
+    L.exo_partial_correction_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
     L.exo_implicit_columns_noalloc.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p]
     sz = ctypes.c_size_t
     L.exo_ensemble_create.argtypes = [i, i, sz, ctypes.POINTER(p)]

@@ -223,9 +223,7 @@ bool validate_config(const exo_config& c, std::string* err) {
   if (c.precision != EXO_PREC_FP64 && c.precision != EXO_PREC_MIXED)
     return bad("precision must be EXO_PREC_FP64 or EXO_PREC_MIXED");
   if (!shallow && (c.implicit_flag & ~9))
-    return bad("implicit_flag: only bits 1 (x1) and 8 (full 5x5) are supported");
-  if (!shallow && (c.implicit_flag & 1) && !(c.implicit_flag & 8))
-    return bad("implicit_flag 1 (partial 3x3 correction) is not available; use 9");
+    return bad("implicit_flag: only bits 1 (x1) and 8 (full 5x5 instead of partial 3x3) are supported");
   if (!(c.cfl > 0.) || !(c.gamma > 1.) || !(c.x1max > c.x1min))
     return bad("cfl, gamma or x1 range out of range");
   if (c.N < 6 || (c.N % 2) != 0) return bad("N must be even and >= 6");
@@ -716,7 +714,7 @@ int exo_restore_from_perturbation(exo_ctx* c, double* w_host, double* wl_host, d
 int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, double dt) {
   if (!c || !du_host || !w_host) return fail(EXO_ERR_ARG, "NULL argument");
   if (c->v.eqn == EXO_EQN_SHALLOW_YZ || !(c->v.implicit_flag & 1))
-    return fail(EXO_ERR_ARG, "the context has no implicit x1 solve (ideal gas, implicit_flag 9)");
+    return fail(EXO_ERR_ARG, "the context has no implicit x1 solve (ideal gas, implicit_flag 1 or 9)");
   if (!(dt > 0.)) return fail(EXO_ERR_ARG, "dt must be positive");
   size_t bytes = c->state_elems * sizeof(double);
   CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
@@ -867,7 +865,21 @@ int exo_implicit_columns(int ncol, int L, const double* w, double* du, const dou
     return fail(EXO_ERR_ARG, "NULL array");
   if (!(dt > 0.) || !(gamma > 1.)) return fail(EXO_ERR_ARG, "dt must be > 0 and gamma > 1");
   RK(exo::launch_implicit_columns(ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav,
-                                  scratch, stream));
+                                  scratch, stream, 1));
+  return EXO_OK;
+}
+
+int exo_partial_correction_columns(int ncol, int L, const double* w, double* du,
+                                   const double* colgeo, const double* x1f, const double* x1v,
+                                   const double* dx1f, double dt, double gamma, double grav,
+                                   double* scratch, void* stream) {
+  if (ncol < 0 || L < 1) return fail(EXO_ERR_ARG, "ncol must be >= 0 and L >= 1");
+  if (ncol == 0) return EXO_OK;
+  if (!w || !du || !colgeo || !x1f || !x1v || !dx1f || !scratch)
+    return fail(EXO_ERR_ARG, "NULL array");
+  if (!(dt > 0.) || !(gamma > 1.)) return fail(EXO_ERR_ARG, "dt must be > 0 and gamma > 1");
+  RK(exo::launch_implicit_columns(ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav,
+                                  scratch, stream, 0));
   return EXO_OK;
 }
 

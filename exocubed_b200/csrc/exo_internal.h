@@ -193,7 +193,7 @@ int launch_weno5(int n, const double* a, const double* b, const double* c,
                  const double* d, const double* e, double* out, void* stream);
 int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
                             const double* x1f, const double* x1v, const double* dx1f, double dt,
-                            double gamma, double grav, double* scratch, void* stream);
+                            double gamma, double grav, double* scratch, void* stream, int full);
 // Decomposition hooks on whole arrays of one atmosphere (refs: face
 // pressures, original pressure and density, column constants)
 int launch_change_to_perturbation(const DevView& v, double* w, double* refs, void* stream);

@@ -1738,6 +1738,238 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
 #endif
 #undef EXO_AP
 
+// ImplicitSolver::PartialCorrection (partial_correction.cpp:26-173) of one
+// radial column, one thread per column: the 3x3 block-tridiagonal system of
+// (rho, m1, E) -- the rows and columns IDN, IVX, IEN of FullCorrection's
+// matrices, the same face and cell Jacobians -- solved by ForwardSweep /
+// BackwardSubstitution with 3-row blocks (forward_backward.hpp:15-126).  The
+// tangential momenta keep their explicit update; the reference's flux
+// correction corr is zero (its computation is commented out there).  Each
+// 3x3 block is inverted as its adjugate over its determinant, the closed form
+// a fixed-size 3x3 inverse takes.  Scratch per level: (A c)_i (9) and
+// delta_i (3).  IO and arguments as for implicit_column; sm holds the two
+// face blocks (18 doubles) and the prefetched w (5) and du (3) of a level.
+template <class IO>
+__device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, double cos_theta,
+                                                        double sin_theta, double d2, double d3,
+                                                        const double* x1f, const double* x1v,
+                                                        const double* dx1f, int is, int ie,
+                                                        double dt, double gamma, double grav) {
+  constexpr int P[3] = {IDN, IVX, IEN};
+  const double s = sin_theta;
+  const double gm1 = (gamma - 1.) * 1. / 1.;
+  const double gp = (gm1 + 1.) / gm1;
+  const double rdt = 1. / dt;
+  auto cell = [&](const double* w) {
+    ColCell c;
+    c.rho = w[IDN];
+    c.v1 = w[IVX];
+    c.v2 = w[IVY] + w[IVZ] * cos_theta;
+    c.v3 = w[IVZ] * sin_theta;
+    c.p = w[IPR];
+    c.s2 = c.v1 * c.v1 + c.v2 * c.v2 + c.v3 * c.v3;
+#if EXO_MIXED
+    c.hr = gp * c.p * (1. / c.rho);
+#else
+    c.hr = gp * c.p / c.rho;
+#endif
+    return c;
+  };
+  auto AMs = [&](int slot, int r, int q) -> double& { return sm[slot * 9 + r * 3 + q]; };
+  auto face = [&](const ColCell& lo, const ColCell& hi, int slot) {
+    double A[5][5];
+    abs_jacobian(lo, hi, gm1, gamma, A);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) AMs(slot, r, q) = A[P[r]][P[q]];
+  };
+  double* pw = sm + 18;
+  double* pdu = sm + 23;
+  auto prefetch = [&](int iw, int idu) {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) cp_async8(pw + n, io.wptr(iw, n));
+    if (idu >= 0) {
+#pragma unroll
+      for (int m = 0; m < 3; ++m) cp_async8(pdu + m, io.duptr(idu, P[m]));
+    }
+    cp_async_commit();
+  };
+  double raw[5];
+  io.w(is - 1, raw);
+  ColCell cm = cell(raw);
+  io.w(is, raw);
+  ColCell c0 = cell(raw);
+  prefetch(is + 1, is);
+  face(cm, c0, 0);
+  double Ap[3][3];  // (A c)_{i-1}
+  double dp[3];     // delta_{i-1}
+  int cur = 0;
+  for (int i = is; i <= ie; ++i) {
+    cp_async_wait_all();
+    double rhs[3];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) raw[n] = pw[n];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) rhs[m] = pdu[m];
+    ColCell cp = cell(raw);
+    prefetch(i + 2, i < ie ? i + 1 : -1);
+    const int nxt = cur ^ 1;
+    face(c0, cp, nxt);
+    const double aleft = d2 * d3 * x1f[i] * x1f[i] * s;
+    const double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
+    const double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
+#if EXO_MIXED
+    const double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
+#endif
+    const bool first = (i == is), last = (i == ie);
+    double t[3][3], cc[3][3], x[3];
+    unroll<3>([&](auto R) {
+      constexpr int r = decltype(R)::value;
+      constexpr int pr = P[r];
+      double brow[3];
+      unroll<3>([&](auto Q) {
+        constexpr int q = decltype(Q)::value;
+        constexpr int pq = P[q];
+        const double am = AMs(cur, r, q), ap = AMs(nxt, r, q);
+        // Phi << 0,0,0, grav,0,0, 0,grav,0 and Bnd = diag(1,-1,1)
+        constexpr bool phi = (r == 1 && q == 0) || (r == 2 && q == 1);
+#if EXO_MIXED
+        double a = am * bl + ap * cr;
+        if constexpr (fj_nz(pr, pq)) a += dd * fj_entry<pr, pq>(c0, gm1);
+        if constexpr (r == q) a += rdt;
+        if constexpr (phi) a -= grav;
+        double bm = am;
+        if constexpr (fj_nz(pr, pq)) bm += fj_entry<pr, pq>(cm, gm1);
+        double b = -bm * bl;
+        double cmv = ap;
+        if constexpr (fj_nz(pr, pq)) cmv -= fj_entry<pr, pq>(cp, gm1);
+        double c = -cmv * cr;
+        if (first) a += (q == 1) ? -b : b;
+        if (last) a += (q == 1) ? -c : c;
+#else
+        double num = am * aleft + ap * aright;
+        if constexpr (fj_nz(pr, pq)) num = num + (aright - aleft) * fj_entry<pr, pq>(c0, gm1);
+        double a = num / (2. * vol);
+        if constexpr (r == q) a = a + rdt;
+        if constexpr (phi) a = a - grav;
+        double bm = am;
+        if constexpr (fj_nz(pr, pq)) bm = am + fj_entry<pr, pq>(cm, gm1);
+        double b = -bm * aleft / (2. * vol);
+        double cmv = ap;
+        if constexpr (fj_nz(pr, pq)) cmv = ap - fj_entry<pr, pq>(cp, gm1);
+        double c = -cmv * aright / (2. * vol);
+        if (first) a = a + ((q == 1) ? -b : b);
+        if (last) a = a + ((q == 1) ? -c : c);
+#endif
+        brow[q] = b;
+        t[r][q] = a;
+        cc[r][q] = c;
+      });
+#if EXO_MIXED
+      x[r] = rhs[r] * rdt;
+#else
+      x[r] = rhs[r] / dt;
+#endif
+      if (!first) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          double ba = brow[0] * Ap[0][q];
+#pragma unroll
+          for (int k = 1; k < 3; ++k) ba += brow[k] * Ap[k][q];
+          t[r][q] = t[r][q] - ba;
+        }
+        double bd = brow[0] * dp[0];
+#pragma unroll
+        for (int k = 1; k < 3; ++k) bd += brow[k] * dp[k];
+        x[r] = x[r] - bd;
+      }
+    });
+    // B = t^-1 = adj(t) / det(t): cofactor (i,j) from the cyclic neighbours
+    // of row i and column j (which carries its sign), det along column 0
+    auto cof = [&](int i0, int j0) {
+      const int i1 = (i0 + 1) % 3, i2 = (i0 + 2) % 3, j1 = (j0 + 1) % 3, j2 = (j0 + 2) % 3;
+      return t[i1][j1] * t[i2][j2] - t[i1][j2] * t[i2][j1];
+    };
+    double B[3][3];
+    {
+      const double c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
+      const double det = c00 * t[0][0] + c10 * t[1][0] + c20 * t[2][0];
+      const double id = 1.0 / det;
+      B[0][0] = c00 * id;
+      B[0][1] = c10 * id;
+      B[0][2] = c20 * id;
+#pragma unroll
+      for (int r = 1; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) B[r][q] = cof(q, r) * id;
+    }
+    // delta_i = B x, (A c)_i = B c_i
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double acc = B[r][0] * x[0];
+#pragma unroll
+      for (int k = 1; k < 3; ++k) acc += B[r][k] * x[k];
+      dp[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        double acc = B[r][0] * cc[0][q];
+#pragma unroll
+        for (int k = 1; k < 3; ++k) acc += B[r][k] * cc[k][q];
+        Ap[r][q] = acc;
+      }
+    if (!last) {
+      const int lev = i - is;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) io.scr(lev, r * 3 + q) = Ap[r][q];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) io.scr(lev, 9 + r) = dp[r];
+    }
+    cm = c0;
+    c0 = cp;
+    cur = nxt;
+  }
+  // back substitution: delta_i -= (A c)_i delta_{i+1}; the update of level i
+  // takes delta for rho, m1, E and the explicit du for m2, m3
+  auto store = [&](int i, const double* u) {
+    double dl[5];
+    dl[IDN] = dp[0];
+    dl[IVX] = dp[1];
+    dl[IVY] = *io.duptr(i, IVY);
+    dl[IVZ] = *io.duptr(i, IVZ);
+    dl[IEN] = dp[2];
+    io.ustore(i, u, dl);
+  };
+  {
+    double u_ie[5];
+    io.uload(ie, u_ie);
+    store(ie, u_ie);
+  }
+#pragma unroll 1
+  for (int i = ie - 1; i >= is; --i) {
+    double cs[12], u[5];
+#pragma unroll
+    for (int e = 0; e < 12; ++e) cs[e] = io.scr(i - is, e);
+    io.uload(i, u);
+    double dl[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double ad = cs[r * 3] * dp[0];
+#pragma unroll
+      for (int k = 1; k < 3; ++k) ad += cs[r * 3 + k] * dp[k];
+      dl[r] = cs[9 + r] - ad;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) dp[r] = dl[r];
+    store(i, u);
+  }
+}
+
 // UpdateAllConserved on the last stage with NVAPOR = NCLOUD = 0: the
 // AirParcel round trip MassConc -> MoleFrac -> MassConc of one cell
 // (impl.cpp:138-304, air_parcel.cpp:190-278)
@@ -1904,9 +2136,15 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   double* scr0 = v.scratch + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
   StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
                   v.du + base};
-  implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
-                  geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), x1f,
-                  x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+  if (v.implicit_flag & 8)
+    implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
+                    geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), x1f,
+                    x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+  else
+    implicit_column_partial(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
+                            geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
+                            geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma,
+                            v.grav);
 }
 
 // last-stage round trip when the implicit solver is off

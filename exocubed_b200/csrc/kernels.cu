@@ -14,8 +14,8 @@ namespace exo {
 namespace fp64 {
 namespace {
 
-// ImplicitSolver::FullCorrection over a batch of independent columns given
-// as plain arrays: w [ncol][5][L+6] primitives with ghosts, du [ncol][5][L]
+// ImplicitSolver::FullCorrection (full != 0) or PartialCorrection over a
+// batch of independent columns given as plain arrays: w [ncol][5][L+6] primitives with ghosts, du [ncol][5][L]
 // explicit update (overwritten by the corrected one), colgeo [ncol][4] =
 // (cos, sin, dx2f_ang, dx3f_ang), scratch ncol*L*30 doubles.
 // A column of exo_implicit_columns: w [5][L+6] and du [5][L] of this column,
@@ -49,7 +49,7 @@ struct HookColumnIO {
 __global__ void EXO_IMPL_BOUNDS k_implicit_columns(
     int ncol, int L, const double* w, double* du, const double* colgeo, const double* x1f,
     const double* x1v, const double* dx1f, double dt, double gamma, double grav,
-    double* scratch) {
+    double* scratch, int full) {
   extern __shared__ double ism[];
   const int col = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int nc1 = L + 2 * G;
@@ -59,8 +59,12 @@ __global__ void EXO_IMPL_BOUNDS k_implicit_columns(
   HookColumnIO io{w + (size_t)col * 5 * nc1, du + (size_t)col * 5 * L, nc1, L, scratch + col,
                   (size_t)ncol};
   const double* g4 = colgeo + (size_t)col * 4;
-  implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3], sx1f, sx1v,
-                  sdx1f, G, G + L - 1, dt, gamma, grav);
+  if (full)
+    implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3], sx1f,
+                    sx1v, sdx1f, G, G + L - 1, dt, gamma, grav);
+  else
+    implicit_column_partial(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3],
+                            sx1f, sx1v, sdx1f, G, G + L - 1, dt, gamma, grav);
 }
 
 __global__ void k_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
@@ -198,12 +202,12 @@ size_t decomposition_refs_doubles(const DevView& v) {
 
 int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
                             const double* x1f, const double* x1v, const double* dx1f, double dt,
-                            double gamma, double grav, double* scratch, void* stream) {
+                            double gamma, double grav, double* scratch, void* stream, int full) {
   if (ncol <= 0) return 0;
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
                               fp64::impl_smem(fp64::IMPL_THREADS, L + 2 * G),
                               (cudaStream_t)stream>>>(
-      ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
+      ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch, full);
   return fp64::check_launch();
 }
 
@@ -255,7 +259,7 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
                               fp64::impl_smem(fp64::IMPL_THREADS, L + 2 * G),
                               (cudaStream_t)stream>>>(
-      ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch);
+      ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch, 1);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     *err = std::string("k_implicit_columns: ") + cudaGetErrorString(e);

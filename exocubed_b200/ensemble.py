@@ -39,6 +39,12 @@ class Ensemble:
             nat.lib().exo_ensemble_destroy(self._h)
             self._h = ctypes.c_void_p()
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def __del__(self):
         try:
             self.close()

@@ -71,7 +71,8 @@ typedef struct exo_config {
   int L;              /* radial levels (nx1)                                      */
   int eqn;            /* EXO_EQN_*                                                */
   int rsolver;        /* EXO_RS_*                                                 */
-  int implicit_flag;  /* <hydro> implicit_flag bits: 1 = x1, 8 = full 5x5 solve  */
+  int implicit_flag;  /* <hydro> implicit_flag bits: 1 = x1 (3x3 partial       */
+                      /* correction), + 8 = full 5x5 correction                   */
   int precision;      /* EXO_PREC_*                                               */
   int coriolis;       /* EXO_CORIOLIS_*                                           */
   int reserved0;
@@ -267,6 +268,18 @@ int exo_implicit_columns(int ncol, int L, const double* w, double* du,
                          const double* colgeo, const double* x1f, const double* x1v,
                          const double* dx1f, double dt, double gamma, double grav,
                          double* scratch, void* stream);
+
+/* ImplicitSolver::PartialCorrection with SolveImplicit3D's velocity
+   projection (src/snap/implicit/solve_implicit_3d.cpp:102-179,
+   partial_correction.cpp:26-173, forward_backward.hpp:15-126) over ncol
+   independent radial columns: the 3x3 block-tridiagonal system of
+   (rho, x1 momentum, energy).  Arguments as for exo_implicit_columns; the
+   x2 and x3 momentum rows of du are left as they came in. */
+int exo_partial_correction_columns(int ncol, int L, const double* w, double* du,
+                                   const double* colgeo, const double* x1f,
+                                   const double* x1v, const double* dx1f, double dt,
+                                   double gamma, double grav, double* scratch,
+                                   void* stream);
 
 /* Allocation-free form of exo_implicit_columns.  This entry point has no
    counterpart in the reference: it exists for callers that cannot allocate

@@ -18,8 +18,8 @@
 //   decomposition       src/snap/decomposition/change_to_perturbation.cpp:20-222,
 //                       decomposition.cpp:341-388
 //   implicit solver     src/snap/implicit/solve_implicit_3d.cpp:102-179,
-//                       full_correction.cpp:32-165, flux_decomposition.hpp:14-120,
-//                       forward_backward.hpp:15-126
+//                       full_correction.cpp:32-165, partial_correction.cpp:26-173,
+//                       flux_decomposition.hpp:14-120, forward_backward.hpp:15-126
 //   stage tasks         src/tasklist/implicit_hydro_tasks.cpp:129-301, patches/24,25
 //   AirParcel round trip src/impl.cpp:138-304, src/air_parcel.cpp:190-278
 //   W92 Coriolis        examples/2023-Chen-exo3/W92.cpp:48-70, cubed_sphere.cpp:78-162,226-262
@@ -36,6 +36,9 @@
 //     algorithm.
 //   * 5x5 inverse: Gauss-Jordan with partial pivoting (Eigen's PartialPivLU
 //     order is not reproducible without Eigen).
+//   * 3x3 inverse (PartialCorrection): adjugate over determinant, the
+//     closed form Eigen takes for fixed 3x3 matrices; cofactor and product
+//     order are this restatement's own.
 // Parity against the reference itself is therefore pinned only by the KATs
 // of tests/test_weno.cpp and tests/test_transform.cpp ("partially pinned").
 //
@@ -1402,7 +1405,151 @@ void implicit_column(const double* wcol_in, double* ducol, int nc1, int is, int 
     for (int n = 0; n < 5; ++n) ducol[n * nc1 + i] = delta[i].a[n];
 }
 
-// SolveImplicit3D, X1 branch with FullCorrection (flag bit 3)
+// ------------------------------------------------- 3x3 block tridiagonal -
+// PartialCorrection works on the (rho, x1 momentum, energy) rows and columns
+// of the same matrices; P maps its 3 indices to the 5 variables.
+constexpr int P3[3] = {IDN, IVX, IEN};
+struct M3 { double a[3][3]; };
+struct V3 { double a[3]; };
+inline M3 sub3(const M5& A) {
+  M3 m;
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q) m.a[r][q] = A.a[P3[r]][P3[q]];
+  return m;
+}
+inline M3 mmul3(const M3& A, const M3& B) {
+  M3 C;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double s = A.a[r][0] * B.a[0][c];
+      for (int k = 1; k < 3; ++k) s += A.a[r][k] * B.a[k][c];
+      C.a[r][c] = s;
+    }
+  return C;
+}
+inline V3 mvmul3(const M3& A, const V3& x) {
+  V3 y;
+  for (int r = 0; r < 3; ++r) {
+    double s = A.a[r][0] * x.a[0];
+    for (int k = 1; k < 3; ++k) s += A.a[r][k] * x.a[k];
+    y.a[r] = s;
+  }
+  return y;
+}
+// 3x3 inverse as the adjugate over the determinant (the closed form a
+// fixed-size 3x3 inverse takes): cofactor (i,j) from the cyclic neighbours
+// of row i and column j, which carries its sign; det expanded along column 0.
+inline double cof3(const M3& m, int i, int j) {
+  int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+  return m.a[i1][j1] * m.a[i2][j2] - m.a[i1][j2] * m.a[i2][j1];
+}
+inline M3 minv3(const M3& m) {
+  double c00 = cof3(m, 0, 0), c10 = cof3(m, 1, 0), c20 = cof3(m, 2, 0);
+  double det = c00 * m.a[0][0] + c10 * m.a[1][0] + c20 * m.a[2][0];
+  double id = 1.0 / det;
+  M3 r;
+  r.a[0][0] = c00 * id;
+  r.a[0][1] = c10 * id;
+  r.a[0][2] = c20 * id;
+  for (int i = 1; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.a[i][j] = cof3(m, j, i) * id;
+  return r;
+}
+
+// One radial column of SolveImplicit3D's X1 branch with PartialCorrection
+// (partial_correction.cpp:26-173; ForwardSweep / BackwardSubstitution with
+// 3-row blocks, forward_backward.hpp:15-126): the 3x3 block-tridiagonal
+// system of (rho, m1, E); the tangential momenta keep their explicit update.
+// The flux correction term corr is zero in the reference (its computation is
+// commented out), so rhs - corr = rhs.  Arguments as for implicit_column.
+void implicit_column_partial(const double* wcol_in, double* ducol, int nc1, int is, int ie,
+                             double cos_theta, double sin_theta, double dx2a, double dx3a,
+                             const double* x1f, const double* x1v, const double* dx1f,
+                             double dt, double gamma, double grav) {
+  std::vector<double> wc(wcol_in, wcol_in + (size_t)5 * nc1), gmm1(nc1);
+  std::vector<M3> a(nc1), b(nc1), c(nc1), dfdq2(nc1);
+  std::vector<V3> delta(nc1);
+  for (int i = 0; i < nc1; ++i) {
+    wc[IVY * nc1 + i] += wc[IVZ * nc1 + i] * cos_theta;
+    wc[IVZ * nc1 + i] *= sin_theta;
+  }
+  auto W = [&](int i, double* out) { for (int n = 0; n < 5; ++n) out[n] = wc[(size_t)n * nc1 + i]; };
+  auto area1 = [&](int i) { return dx2a * dx3a * x1f[i] * x1f[i] * sin_theta; };
+  auto volume = [&](int i) { return dx1f[i] * dx2a * dx3a * x1v[i] * x1v[i] * sin_theta; };
+  // Phi << 0,0,0, grav,0,0, 0,grav,0
+  M3 Phi = {{{0., 0., 0.}, {grav, 0., 0.}, {0., grav, 0.}}};
+  double wl[5], wr[5], prim[5];
+  for (int i = is - 2; i <= ie + 1; ++i) {
+    W(i, wr);
+    double fsig = 1., feps = 1.;
+    gmm1[i] = (gamma - 1.) * feps / fsig;
+    dfdq2[i] = sub3(flux_jacobian(gmm1[i], wr));
+  }
+  W(is - 2, wl); W(is - 1, wr);
+  double gm1 = 0.5 * (gmm1[is - 2] + gmm1[is - 1]);
+  roe_average(prim, gm1, wl, wr);
+  double fsig = 1., feps = 1.;
+  double cs = std::sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
+  M3 Am2 = sub3(abs_jacobian(prim, cs, gm1)), Ap2;
+  for (int i = is - 1; i <= ie; ++i) {
+    W(i, wl); W(i + 1, wr);
+    gm1 = 0.5 * (gmm1[i] + gmm1[i + 1]);
+    roe_average(prim, gm1, wl, wr);
+    cs = std::sqrt((1. + (gamma - 1) * feps / fsig) * prim[IPR] / prim[IDN]);
+    Ap2 = sub3(abs_jacobian(prim, cs, gm1));
+    double aleft = area1(i), aright = area1(i + 1);
+    double vol = volume(i);
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q) {
+        double Dt = (r == q) ? 1. / dt : 0.;
+        a[i].a[r][q] = (Am2.a[r][q] * aleft + Ap2.a[r][q] * aright +
+                        (aright - aleft) * dfdq2[i].a[r][q]) / (2. * vol) + Dt - Phi.a[r][q];
+        b[i].a[r][q] = -(Am2.a[r][q] + dfdq2[i - 1].a[r][q]) * aleft / (2. * vol);
+        c[i].a[r][q] = -(Ap2.a[r][q] - dfdq2[i + 1].a[r][q]) * aright / (2. * vol);
+      }
+    Am2 = Ap2;
+  }
+  // reflecting boundaries: Bnd = diag(1,-1,1)
+  M3 B = {{{1., 0., 0.}, {0., -1., 0.}, {0., 0., 1.}}};
+  {
+    M3 t = mmul3(b[is], B);
+    for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) a[is].a[r][q] += t.a[r][q];
+    t = mmul3(c[ie], B);
+    for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) a[ie].a[r][q] += t.a[r][q];
+  }
+  for (int i = is; i <= ie; ++i) {
+    V3 rhs;
+    rhs.a[0] = ducol[IDN * nc1 + i];
+    rhs.a[0] /= dt;
+    rhs.a[1] = ducol[IVX * nc1 + i] / dt;
+    rhs.a[2] = ducol[IEN * nc1 + i] / dt;
+    if (i == is) {
+      a[i] = minv3(a[i]);
+      delta[i] = mvmul3(a[i], rhs);
+    } else {
+      M3 ba = mmul3(b[i], a[i - 1]);
+      M3 t;
+      for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) t.a[r][q] = a[i].a[r][q] - ba.a[r][q];
+      a[i] = minv3(t);
+      V3 bd = mvmul3(b[i], delta[i - 1]), x;
+      for (int r = 0; r < 3; ++r) x.a[r] = rhs.a[r] - bd.a[r];
+      delta[i] = mvmul3(a[i], x);
+    }
+    a[i] = mmul3(a[i], c[i]);
+  }
+  for (int i = ie - 1; i >= is; --i) {
+    V3 ad = mvmul3(a[i], delta[i + 1]);
+    for (int r = 0; r < 3; ++r) delta[i].a[r] -= ad.a[r];
+  }
+  for (int i = is; i <= ie; ++i) {
+    ducol[IDN * nc1 + i] = delta[i].a[0];
+    ducol[IVX * nc1 + i] = delta[i].a[1];
+    ducol[IEN * nc1 + i] = delta[i].a[2];
+  }
+}
+
+// SolveImplicit3D, X1 branch: FullCorrection when flag bit 3 is set, else
+// PartialCorrection (solve_implicit_3d.cpp:131-135)
 void implicit_x1(Oracle& o, double dt) {
   int nc1 = o.nc1;
 #pragma omp parallel for collapse(2)
@@ -1417,9 +1564,10 @@ void implicit_x1(Oracle& o, double dt) {
             wc[(size_t)n * nc1 + i] = o.w[o.at(p, n, k, j, i)];
             dc[(size_t)n * nc1 + i] = o.du[o.at(p, n, k, j, i)];
           }
-        implicit_column(wc.data(), dc.data(), nc1, o.is, o.ie, g.cosc[q], g.sinc[q], g.dx2a[q],
-                        g.dx3a[q], o.x1f.data(), o.x1v.data(), o.dx1f.data(), dt, o.cfg.gamma,
-                        o.cfg.grav);
+        auto column = (o.cfg.implicit_flag & 8) ? implicit_column : implicit_column_partial;
+        column(wc.data(), dc.data(), nc1, o.is, o.ie, g.cosc[q], g.sinc[q], g.dx2a[q],
+               g.dx3a[q], o.x1f.data(), o.x1v.data(), o.dx1f.data(), dt, o.cfg.gamma,
+               o.cfg.grav);
         for (int n = 0; n < 5; ++n)
           for (int i = o.is; i <= o.ie; ++i) o.du[o.at(p, n, k, j, i)] = dc[(size_t)n * nc1 + i];
       }
@@ -1769,20 +1917,22 @@ void ora_get_mesh(void* h, int panel, double* x1f, double* x2f, double* x3f) {
   std::memcpy(x3f, o.pg[panel].x3f.data(), o.pg[panel].x3f.size() * sizeof(double));
 }
 
-// FullCorrection over a batch of columns: w [ncol][5][L+6], du [ncol][5][L]
-// (in/out), colgeo [ncol][4] = (cos, sin, dx2f_ang, dx3f_ang)
-void ora_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
-                          const double* x1f, const double* x1v, const double* dx1f, double dt,
-                          double gamma, double grav) {
+// FullCorrection (full != 0) or PartialCorrection over a batch of columns:
+// w [ncol][5][L+6], du [ncol][5][L] (in/out), colgeo [ncol][4] = (cos, sin,
+// dx2f_ang, dx3f_ang)
+void ora_correction_columns(int full, int ncol, int L, const double* w, double* du,
+                            const double* colgeo, const double* x1f, const double* x1v,
+                            const double* dx1f, double dt, double gamma, double grav) {
   int nc1 = L + 2 * G;
+  auto column = full ? implicit_column : implicit_column_partial;
 #pragma omp parallel for
   for (int c = 0; c < ncol; ++c) {
     std::vector<double> dc((size_t)5 * nc1, 0.);
     for (int n = 0; n < 5; ++n)
       for (int i = 0; i < L; ++i) dc[(size_t)n * nc1 + G + i] = du[((size_t)c * 5 + n) * L + i];
     const double* g4 = colgeo + (size_t)c * 4;
-    implicit_column(w + (size_t)c * 5 * nc1, dc.data(), nc1, G, G + L - 1, g4[0], g4[1], g4[2],
-                    g4[3], x1f, x1v, dx1f, dt, gamma, grav);
+    column(w + (size_t)c * 5 * nc1, dc.data(), nc1, G, G + L - 1, g4[0], g4[1], g4[2], g4[3],
+           x1f, x1v, dx1f, dt, gamma, grav);
     for (int n = 0; n < 5; ++n)
       for (int i = 0; i < L; ++i) du[((size_t)c * 5 + n) * L + i] = dc[(size_t)n * nc1 + G + i];
   }

@@ -70,7 +70,7 @@ def lib():
         L.ora_step.argtypes = [p, i, d]
         L.ora_get_mesh.argtypes = [p, i, dp, dp, dp]
         L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
-        L.ora_implicit_columns.argtypes = [i, i, dp, dp, dp, dp, dp, dp, d, d, d]
+        L.ora_correction_columns.argtypes = [i, i, i, dp, dp, dp, dp, dp, dp, d, d, d]
         L.ora_solve_implicit_3d.argtypes = [p, dp, dp, d]
         L.ora_change_to_perturbation.argtypes = [p, dp]
         L.ora_restore_from_perturbation.argtypes = [p, dp, dp, dp]
@@ -206,13 +206,14 @@ def riemann_face(rsolver, eqn, ivx, gamma, wl, wr, cosf=0.0, sinf=1.0, cthp=0.0,
     return f
 
 
-def implicit_columns(w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav):
-    """FullCorrection over a batch of columns; returns the corrected du."""
+def implicit_columns(w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, full=True):
+    """FullCorrection (full=True) or PartialCorrection over a batch of
+    columns; returns the corrected du."""
     w = np.ascontiguousarray(w, dtype=np.float64)
     out = np.ascontiguousarray(du, dtype=np.float64).copy()
     colgeo = np.ascontiguousarray(colgeo, dtype=np.float64)
     ncol, _, L = out.shape
-    lib().ora_implicit_columns(ncol, L, _ptr(w), _ptr(out), _ptr(colgeo),
-                               _ptr(np.ascontiguousarray(x1f)), _ptr(np.ascontiguousarray(x1v)),
-                               _ptr(np.ascontiguousarray(dx1f)), dt, gamma, grav)
+    lib().ora_correction_columns(int(bool(full)), ncol, L, _ptr(w), _ptr(out), _ptr(colgeo),
+                                 _ptr(np.ascontiguousarray(x1f)), _ptr(np.ascontiguousarray(x1v)),
+                                 _ptr(np.ascontiguousarray(dx1f)), dt, gamma, grav)
     return out
