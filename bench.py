@@ -80,6 +80,10 @@ def _workload(name):
     if name == "c3":
         return (W.dry_atmosphere_config(N=192, L=96, rsolver=1),
                 "exo3 dry ideal gas 6x192x192x96 FP64 WENO5+LMARS+implicit(9), SSPRK3, CFL 0.4")
+    if name == "hs94":  # examples/2023-Chen-exo3/hs94.inp
+        return (W.hs94_config(),
+                "exo3 Held-Suarez 6x40x40x40 FP64 WENO5+HLLC+implicit(1)+HS94 forcing, "
+                "SSPRK3, CFL 0.9")
     raise ValueError(name)
 
 
@@ -87,6 +91,8 @@ def make_state(cfg, seed):
     from exocubed_b200 import workloads as W
     if cfg["eqn"] == 0:
         return W.shallow_water_state(cfg, seed=seed)
+    if cfg.get("forcing", 0) == 1:
+        return W.hs94_state(cfg, seed=seed)
     return W.dry_atmosphere_state(cfg, seed=seed)
 
 
@@ -641,7 +647,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c2s", "c3", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c2s", "c3", "c4", "hs94"])
     ap.add_argument("--members", type=int, default=64, help="ensemble members (c4)")
     ap.add_argument("--serve", default="", help="comma-separated arrival rates (req/s): serving sweep")
     ap.add_argument("--requests", type=int, default=24, help="requests per rate (serving)")

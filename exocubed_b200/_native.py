@@ -15,7 +15,8 @@ EXO_OK = 0
 EXO_EQN_SHALLOW_YZ, EXO_EQN_IDEAL = 0, 1
 EXO_RS_ROE_SHALLOW, EXO_RS_LMARS, EXO_RS_HLLC, EXO_RS_LMARS_SHALLOW = 0, 1, 2, 3
 EXO_PREC_FP64, EXO_PREC_MIXED = 0, 1
-EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92 = 0, 1
+EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92, EXO_CORIOLIS_3D = 0, 1, 2
+EXO_FORCING_NONE, EXO_FORCING_HS94 = 0, 1
 NGHOST = 3
 EXO_TILE_COUNT = 6
 EXO_K_FLUX_X1, EXO_K_FLUX_X23, EXO_K_UPDATE, EXO_K_IMPLICIT, EXO_K_PRIM_GHOST, EXO_K_OTHER = range(6)
@@ -48,11 +49,14 @@ class ExoConfig(ctypes.Structure):
         ("N", ctypes.c_int), ("L", ctypes.c_int), ("eqn", ctypes.c_int),
         ("rsolver", ctypes.c_int), ("implicit_flag", ctypes.c_int),
         ("precision", ctypes.c_int), ("coriolis", ctypes.c_int),
-        ("reserved0", ctypes.c_int),
+        ("forcing", ctypes.c_int),
         ("x1min", ctypes.c_double), ("x1max", ctypes.c_double),
         ("gamma", ctypes.c_double), ("Rd", ctypes.c_double),
         ("grav", ctypes.c_double), ("cfl", ctypes.c_double),
         ("omega", ctypes.c_double), ("reserved1", ctypes.c_double),
+        ("hs_p0", ctypes.c_double), ("hs_Ts", ctypes.c_double), ("hs_dT", ctypes.c_double),
+        ("hs_dtheta", ctypes.c_double), ("hs_Kf", ctypes.c_double), ("hs_Ka", ctypes.c_double),
+        ("hs_Ks", ctypes.c_double), ("hs_sigmab", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -226,6 +226,15 @@ bool validate_config(const exo_config& c, std::string* err) {
     return bad("implicit_flag: only bits 1 (x1) and 8 (full 5x5 instead of partial 3x3) are supported");
   if (!(c.cfl > 0.) || !(c.gamma > 1.) || !(c.x1max > c.x1min))
     return bad("cfl, gamma or x1 range out of range");
+  if (c.coriolis < EXO_CORIOLIS_NONE || c.coriolis > EXO_CORIOLIS_3D)
+    return bad("unknown Coriolis source");
+  if (shallow && c.coriolis == EXO_CORIOLIS_3D)
+    return bad("the 3D Coriolis source needs the ideal gas");
+  if (c.forcing != EXO_FORCING_NONE && c.forcing != EXO_FORCING_HS94)
+    return bad("unknown forcing");
+  if (c.forcing == EXO_FORCING_HS94 &&
+      (shallow || !(c.hs_p0 > 0.) || !(c.hs_sigmab < 1.) || !(c.Rd > 0.)))
+    return bad("HS94 forcing needs the ideal gas, hs_p0 > 0, hs_sigmab < 1 and Rd > 0");
   if (c.N < 6 || (c.N % 2) != 0) return bad("N must be even and >= 6");
   if (c.L < 1 || c.L > 250) return bad("L must be in [1, 250]");
   return true;
@@ -282,6 +291,22 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
   v.implicit_flag = shallow ? 0 : cfg.implicit_flag;
   v.coriolis = cfg.coriolis;
   v.precision = cfg.precision;
+  v.forcing = shallow ? EXO_FORCING_NONE : cfg.forcing;
+  if (v.forcing == EXO_FORCING_HS94) {
+    // Mesh::InitUserMeshData (hs94.cpp:212-243): cp from gamma, rates per day
+    const double day_to_s = 8.64E4;
+    const double cp = cfg.gamma / (cfg.gamma - 1.) * cfg.Rd;
+    v.hs[HS_P0] = cfg.hs_p0;
+    v.hs[HS_TS] = cfg.hs_Ts;
+    v.hs[HS_DT] = cfg.hs_dT;
+    v.hs[HS_DTHETA] = cfg.hs_dtheta;
+    v.hs[HS_KF] = cfg.hs_Kf / day_to_s;
+    v.hs[HS_KA] = cfg.hs_Ka / day_to_s;
+    v.hs[HS_KS] = cfg.hs_Ks / day_to_s;
+    v.hs[HS_SIGMAB] = cfg.hs_sigmab;
+    v.hs[HS_KAPPA] = cfg.Rd / cp;
+    v.hs[HS_CVM] = cp - cfg.Rd;
+  }
   v.gamma = cfg.gamma;
   v.Rd = cfg.Rd;
   v.grav = shallow ? 0. : cfg.grav;
@@ -481,6 +506,17 @@ int exo_config_default(exo_config* cfg, int eqn) {
   } else {
     return fail(EXO_ERR_ARG, "unknown equation set");
   }
+  // Held-Suarez parameters of examples/2023-Chen-exo3/hs94.inp (used only
+  // with forcing = EXO_FORCING_HS94)
+  cfg->forcing = EXO_FORCING_NONE;
+  cfg->hs_p0 = 1.E5;
+  cfg->hs_Ts = 315.;
+  cfg->hs_dT = 60.;
+  cfg->hs_dtheta = 10.;
+  cfg->hs_Kf = 1.;
+  cfg->hs_Ka = 0.025;
+  cfg->hs_Ks = 0.25;
+  cfg->hs_sigmab = 0.7;
   return EXO_OK;
 }
 

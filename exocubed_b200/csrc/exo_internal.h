@@ -24,7 +24,18 @@ enum Geo2D {
   GFCOR,                                           // Coriolis parameter 2*Omega*sin(lat)
   GCR0, GCR1, GCR2, GCR3,                          // cell (V2,V3) -> (U,V)
   GCQ0, GCQ1, GCQ2, GCQ3,                          // cell (U,V) -> (V2,V3)
+  GSLAT2, GCLAT2, GCLAT4,                          // sin^2, cos^2, cos^4 of the latitude
+  GTANX, GTANY, GC3C, GC3D, GC3A,                  // CalculateCoriolisForce3: x, y, C, D,
+                                                   // 2 Omega C D / delta^2
   NGEO2D
+};
+
+// Held-Suarez forcing constants of a DevView (host-computed, hs94.cpp:212-243)
+enum HsParam {
+  HS_P0 = 0, HS_TS, HS_DT, HS_DTHETA, HS_KF, HS_KA, HS_KS, HS_SIGMAB,  // Kf, Ka, Ks in 1/s
+  HS_KAPPA,                                                            // Rd / cp
+  HS_CVM,                                                              // cp - Rd
+  NHS
 };
 
 // One ghost-band cell of a receiving panel (independent of i and n).  Its
@@ -87,8 +98,9 @@ struct alignas(16) DevView {
   int N, L, nv, nc1, nc2, nc3;
   int is, ie, js, je, ks, ke;
   int eqn, rsolver, implicit_flag, coriolis;
-  int precision;
+  int precision, forcing;
   double gamma, Rd, grav, cfl;
+  double hs[NHS];                  // Held-Suarez constants (forcing == EXO_FORCING_HS94)
   size_t cells;                    // nc3*nc2*nc1 (one variable of one panel)
   // state
   double* u;

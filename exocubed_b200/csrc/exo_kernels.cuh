@@ -1079,6 +1079,64 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
       out[IVY] += wght * rho * a2c;
       out[IVZ] += wght * rho * a3c;
     }
+    // CubedSphere::CalculateCoriolisForce3 (cubed_sphere.cpp:197-231): blocks
+    // 1 and 5 (panels 0 and 4) carry the rotation axis through their centre
+    if (v.coriolis == EXO_CORIOLIS_3D) {
+      const double A = G2(GC3A, 0) * rho;
+      const double x = G2(GTANX, 0), y = G2(GTANY, 0), C = G2(GC3C, 0), D = G2(GC3D, 0);
+      double cF1, cF2, cF3;
+      if (p == 0 || p == 4) {
+        cF1 = A * (y * C * v2 - x * D * v3);
+        cF2 = A * (-y * C * v1 - v3);
+        cF3 = A * (x * D * v1 + v2);
+      } else {
+        cF1 = -A * D * v3;
+        cF2 = A * x * v3;
+        cF3 = A * (D * v1 - x * v2);
+      }
+      out[IVX] += wght * cF1;
+      out[IVY] += wght * cF2;
+      out[IVZ] += wght * cF3;
+    }
+    // Held-Suarez forcing (examples/2023-Chen-exo3/hs94.cpp:59-155)
+    if (v.forcing == EXO_FORCING_HS94) {
+      // Coriolis on the momenta in latitude-longitude (hs94.cpp:82-104)
+      {
+        double f = G2(GFCOR, 0);
+        double U = G2(GCR0, 0) * v2 + G2(GCR1, 0) * v3;
+        double V = G2(GCR2, 0) * v2 + G2(GCR3, 0) * v3;
+        U = -U;
+        double m2 = rho * U, m3 = rho * V;
+        double llU = f * m3, llV = -f * m2;
+        double mU = -llU;
+        double acc2 = G2(GCQ0, 0) * mU + G2(GCQ1, 0) * llV;
+        double acc3 = G2(GCQ2, 0) * mU + G2(GCQ3, 0) * llV;
+        double a2c = acc2 + acc3 * cosine, a3c = acc3 + acc2 * cosine;
+        out[IVY] += wght * a2c;
+        out[IVZ] += wght * a3c;
+      }
+      // Rayleigh drag and Newtonian cooling (hs94.cpp:110-153)
+      {
+        const double* hs = v.hs;
+        double scaled_z = pr / hs[HS_P0];
+        double sigma = pr / hs[HS_P0];
+        double sigma_p = (sigma - hs[HS_SIGMAB]) / (1. - hs[HS_SIGMAB]);
+        double Kv = (sigma_p < 0.0) ? 0.0 : sigma_p * hs[HS_KF];
+        double Teq_p = hs[HS_TS] - hs[HS_DT] * G2(GSLAT2, 0) -
+                       hs[HS_DTHETA] * log(scaled_z) * G2(GCLAT2, 0);
+        Teq_p *= pow(scaled_z, hs[HS_KAPPA]);
+        double Teq = (Teq_p > 200.) ? Teq_p : 200.;
+        double temp = pr / rho / v.Rd;
+        sigma_p = (sigma_p < 0.0) ? 0.0 : sigma_p * G2(GCLAT4, 0);
+        double Kt = hs[HS_KA] + (hs[HS_KS] - hs[HS_KA]) * sigma_p;
+        double m1 = rho * v1, m2 = rho * v2, m3 = rho * v3;
+        double m2c = m2 + m3 * cosine, m3c = m3 + m2 * cosine;
+        out[IVX] += -wght * Kv * m1;
+        out[IVY] += -wght * Kv * m2c;
+        out[IVZ] += -wght * Kv * m3c;
+        out[IEN] += -wght * hs[HS_CVM] * rho * Kt * (temp - Teq);
+      }
+    }
   }
   double* uout = v.u + c0;
   if (shallow) {

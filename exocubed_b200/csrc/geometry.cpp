@@ -235,6 +235,24 @@ static void build_metric(const exo_config& cfg, HostTables& t) {
         double lat, lon;
         rll_from_xyp(dY, -dX, p, lon, lat);
         G2(GFCOR) = 2. * cfg.omega * sin(lat);
+        // Held-Suarez forcing: hs94.cpp:130-138 (_sqr, _qur of sin/cos(lat))
+        {
+          double sl = sin(lat), cl = cos(lat);
+          G2(GSLAT2) = sl * sl;
+          G2(GCLAT2) = cl * cl;
+          G2(GCLAT4) = cl * cl * cl * cl;
+        }
+        // CalculateCoriolisForce3 (cubed_sphere.cpp:197-231): A = 2 Omega C D
+        // / delta / delta, times the density on the device
+        {
+          double C = sqrt(dX * dX + 1), D = sqrt(dY * dY + 1);
+          double delta = sqrt(dX * dX + dY * dY + 1);
+          G2(GTANX) = dX;
+          G2(GTANY) = dY;
+          G2(GC3C) = C;
+          G2(GC3D) = D;
+          G2(GC3A) = 2 * cfg.omega * C * D / delta / delta;
+        }
         double c[4];
         rll_from_abp_coef(dX, dY, p + 1, c);
         G2(GCR0) = c[0]; G2(GCR1) = c[1]; G2(GCR2) = c[2]; G2(GCR3) = c[3];

@@ -190,3 +190,53 @@ def ensemble_member(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS
     w[:, 2][sl] = m[..., 0, None] * U + m[..., 1, None] * V
     w[:, 3][sl] = m[..., 2, None] * U + m[..., 3, None] * V
     return cfg, w
+
+
+def hs94_config(N=40, L=40, precision=nat.EXO_PREC_FP64, **kw):
+    """The Held-Suarez benchmark of examples/2023-Chen-exo3/hs94.inp: six
+    40x40 panels, 40 levels from 6371 to 6396 km, implicit_flag 1 (the
+    partial vertical correction), CFL 0.9, gamma 1.4, g = 9.81, Rd = 287,
+    Omega = 7.292e-5 and the HS94 forcing parameters of its <problem> and
+    <thermodynamics> blocks.  The Riemann solver is HLLC, the one an exo3
+    build compiles in (cmake/exo3.cmake: RSOLVER hllc_transform); the
+    "--flux=lmars" of the input file's configure comment names an older
+    build.  (LMARS has no cubed-sphere projection, lmars.cpp:24-110, so a
+    resting atmosphere does not stay at rest with it on this grid.)"""
+    cfg = dict(N=N, L=L, eqn=nat.EXO_EQN_IDEAL, rsolver=nat.EXO_RS_HLLC, implicit_flag=1,
+               precision=precision, coriolis=nat.EXO_CORIOLIS_NONE,
+               forcing=nat.EXO_FORCING_HS94, x1min=6.371e6, x1max=6.396e6, gamma=1.4,
+               Rd=287., grav=-9.81, cfl=0.9, omega=7.292e-5,
+               hs_p0=1.e5, hs_Ts=315., hs_dT=60., hs_dtheta=10., hs_Kf=1., hs_Ka=0.025,
+               hs_Ks=0.25, hs_sigmab=0.7)
+    cfg.update(kw)
+    return cfg
+
+
+def hs94_state(cfg, seed=0, z_iso=2.e4, wind_sigma=10.):
+    """MeshBlock::ProblemGenerator of hs94.cpp:246-291 restated: a dry adiabat
+    from (Ts, p0) up to z_iso, isothermal above (Ttop = Ts + grav z_iso / cp),
+    and wind noise of wind_sigma m/s in v2 and v3 of the adiabatic cells; the
+    isothermal cells of a column keep the noise of its top adiabatic cell, as
+    the reference's level loop leaves them.  Noise from a PCG64 generator."""
+    c = make_config(**cfg) if isinstance(cfg, dict) else cfg
+    N, L, Rd, g = c.N, c.L, c.Rd, -c.grav
+    cp = c.gamma / (c.gamma - 1.) * Rd
+    Ts, p0 = c.hs_Ts, c.hs_p0
+    Ttop = Ts - g * z_iso / cp
+    _, _, _, x1v = cell_geometry(c)
+    z = x1v - c.x1min
+    T, p = _adiabat_isothermal(z, Ts, Ttop, g, Rd, c.gamma, p0)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    v2 = wind_sigma * rng.standard_normal((6, N, N, L))
+    v3 = wind_sigma * rng.standard_normal((6, N, N, L))
+    top = int(np.searchsorted(z, z_iso, side="right"))  # first isothermal level
+    if 0 < top < L:
+        v2[..., top:] = v2[..., top - 1:top]
+        v3[..., top:] = v3[..., top - 1:top]
+    w = np.zeros((6, 5, N + 2 * G, N + 2 * G, L + 2 * G))
+    sl = (slice(None), slice(G, G + N), slice(G, G + N), slice(G, G + L))
+    w[:, 4][sl] = p[None, None, None, :]
+    w[:, 0][sl] = (p / (Rd * T))[None, None, None, :]
+    w[:, 2][sl] = v2
+    w[:, 3][sl] = v3
+    return w

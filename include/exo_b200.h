@@ -63,8 +63,17 @@ enum {
                          FP64 decomposition, implicit solve and RK accumulation */
 };
 
-/* source terms */
-enum { EXO_CORIOLIS_NONE = 0, EXO_CORIOLIS_W92 = 1 };
+/* Coriolis source (a user explicit source of the reference's examples):
+   W92: the lat-lon f-plane form of examples/2023-Chen-exo3/W92.cpp:48-70;
+   3D:  CubedSphere::CalculateCoriolisForce3 (src/exo3/cubed_sphere.cpp:197-231),
+        the full rotation vector on every panel, all three momenta */
+enum { EXO_CORIOLIS_NONE = 0, EXO_CORIOLIS_W92 = 1, EXO_CORIOLIS_3D = 2 };
+/* user forcing, added with the sources of each stage:
+   HS94: examples/2023-Chen-exo3/hs94.cpp:59-155 -- Coriolis on the momenta in
+         latitude-longitude, Rayleigh drag below sigmab and Newtonian cooling
+         toward the Held-Suarez equilibrium temperature (uses omega, gamma,
+         Rd and the hs_* parameters) */
+enum { EXO_FORCING_NONE = 0, EXO_FORCING_HS94 = 1 };
 
 typedef struct exo_config {
   int N;              /* cells along a panel edge (meshblock nx2 = nx3)          */
@@ -75,7 +84,7 @@ typedef struct exo_config {
                       /* correction), + 8 = full 5x5 correction                   */
   int precision;      /* EXO_PREC_*                                               */
   int coriolis;       /* EXO_CORIOLIS_*                                           */
-  int reserved0;
+  int forcing;        /* EXO_FORCING_*                                            */
   double x1min;       /* inner radius [m]                                         */
   double x1max;       /* outer radius [m]                                         */
   double gamma;       /* <hydro> gamma                                            */
@@ -84,6 +93,15 @@ typedef struct exo_config {
   double cfl;         /* <time> cfl_number                                        */
   double omega;       /* planetary rotation rate for the Coriolis source [1/s]    */
   double reserved1;
+  /* Held-Suarez forcing (hs94.inp <problem> and <thermodynamics> blocks) */
+  double hs_p0;       /* p0: reference surface pressure [Pa]                      */
+  double hs_Ts;       /* Ts: equatorial surface temperature [K]                   */
+  double hs_dT;       /* dT: equator-to-pole temperature difference [K]           */
+  double hs_dtheta;   /* dtheta: vertical potential temperature difference [K]    */
+  double hs_Kf;       /* Kf: boundary-layer Rayleigh drag rate [1/day]            */
+  double hs_Ka;       /* Ka: free-atmosphere Newtonian cooling rate [1/day]       */
+  double hs_Ks;       /* Ks: surface Newtonian cooling rate [1/day]               */
+  double hs_sigmab;   /* sigmab: top of the boundary layer, in p/p0               */
 } exo_config;
 
 typedef struct exo_ctx exo_ctx;

@@ -23,6 +23,8 @@
 //   stage tasks         src/tasklist/implicit_hydro_tasks.cpp:129-301, patches/24,25
 //   AirParcel round trip src/impl.cpp:138-304, src/air_parcel.cpp:190-278
 //   W92 Coriolis        examples/2023-Chen-exo3/W92.cpp:48-70, cubed_sphere.cpp:78-162,226-262
+//   3D Coriolis         cubed_sphere.cpp:197-231 (CalculateCoriolisForce3)
+//   HS94 forcing        examples/2023-Chen-exo3/hs94.cpp:59-155, 212-243
 //   CFL time step       patches/21.new_blockdt.patch:23-35
 //
 // Pieces owned by the un-vendored Athena++ fork (chengcli/athenapp, tag
@@ -203,6 +205,8 @@ struct PanelGeo {
   std::vector<double> cthp1, cthp2, cthp3;
   // W92 Coriolis pieces per (k,j): f and the cell's (X,Y)
   std::vector<double> fcor, X, Y;
+  // HS94 forcing: sin^2, cos^2, cos^4 of the cell-centre latitude
+  std::vector<double> slat2, clat2, clat4;
 };
 
 struct Oracle {
@@ -294,7 +298,7 @@ void build_geometry(Oracle& o) {
     PanelGeo& g = o.pg[p];
     for (auto* v : {&g.cosc, &g.sinc, &g.cosf2, &g.sinf2, &g.cosf3, &g.sinf3,
                     &g.dx2a, &g.dx3a, &g.dx2a_f3, &g.dx3a_f2, &g.cthp1,
-                    &g.cthp2, &g.cthp3, &g.fcor, &g.X, &g.Y})
+                    &g.cthp2, &g.cthp3, &g.fcor, &g.X, &g.Y, &g.slat2, &g.clat2, &g.clat4})
       v->assign(n2, 0.);
     for (int k = 0; k < o.nc3; ++k)
       for (int j = 0; j < o.nc2; ++j) {
@@ -346,6 +350,11 @@ void build_geometry(Oracle& o) {
           g.fcor[q] = 2. * o.cfg.omega * sin(lat);
           g.X[q] = dX;
           g.Y[q] = dY;
+          // hs94.cpp:130-138: _sqr(sin(lat)), _sqr(cos(lat)), _qur(cos(lat))
+          double sl = sin(lat), cl = cos(lat);
+          g.slat2[q] = sl * sl;
+          g.clat2[q] = cl * cl;
+          g.clat4[q] = cl * cl * cl * cl;
         }
       }
   }
@@ -1138,6 +1147,110 @@ void calculate_fluxes(Oracle& o) {
 // Athena++ AddFluxDivergence + GnomonicEquiangle::AddCoordTermsDivergence
 // into `out` (u for the shallow-water task list, du for ImplicitHydroTasks),
 // then the source terms.
+// The user explicit sources of the reference's examples, added after the
+// geometric and gravity terms of cell column (p,k,j) (HydroSourceTerms calls
+// the enrolled user function last).
+void add_user_sources(const Oracle& o, int p, int k, int j, std::vector<double>& out,
+                      double wght) {
+  const PanelGeo& g = o.pg[p];
+  // user source: W92 Coriolis (examples/2023-Chen-exo3/W92.cpp:48-70)
+  if (o.cfg.coriolis == EXO_CORIOLIS_W92) {
+    size_t q = o.kj(k, j);
+    double X = g.X[q], Y = g.Y[q], f = g.fcor[q];
+    double C = sqrt(X * X + 1), D = sqrt(Y * Y + 1), delta = sqrt(X * X + Y * Y + 1);
+    double cth = -X * Y / (C * D);
+    for (int i = o.is; i <= o.ie; ++i) {
+      double U, V, acc2, acc3;
+      vec_rll_from_abp(X, Y, p + 1, o.w[o.at(p, IVY, k, j, i)], o.w[o.at(p, IVZ, k, j, i)], &U, &V);
+      U = -U;
+      double llU = f * V, llV = -f * U;
+      vec_abp_from_rll(X, Y, p + 1, -llU, llV, &acc2, &acc3);
+      double a2c = acc2 + acc3 * cth, a3c = acc3 + acc2 * cth;
+      out[o.at(p, IVY, k, j, i)] += wght * o.w[o.at(p, IDN, k, j, i)] * a2c;
+      out[o.at(p, IVZ, k, j, i)] += wght * o.w[o.at(p, IDN, k, j, i)] * a3c;
+    }
+    (void)delta;
+  }
+  // CubedSphere::CalculateCoriolisForce3 (cubed_sphere.cpp:197-231),
+  // u(IMn) += dt * cFn as in the commented form of hs94.cpp:66-78
+  if (o.cfg.coriolis == EXO_CORIOLIS_3D) {
+    size_t q = o.kj(k, j);
+    double x = g.X[q], y = g.Y[q];
+    double C = sqrt(x * x + 1), D = sqrt(y * y + 1), delta = sqrt(x * x + y * y + 1);
+    for (int i = o.is; i <= o.ie; ++i) {
+      double den = o.w[o.at(p, IDN, k, j, i)];
+      double v1 = o.w[o.at(p, IVX, k, j, i)], v2 = o.w[o.at(p, IVY, k, j, i)],
+             v3 = o.w[o.at(p, IVZ, k, j, i)];
+      double A = 2 * o.cfg.omega * C * D / delta / delta * den;
+      double cF1, cF2, cF3;
+      int blockID = p + 1;
+      if (blockID == 1 || blockID == 5) {
+        cF1 = A * (y * C * v2 - x * D * v3);
+        cF2 = A * (-y * C * v1 - v3);
+        cF3 = A * (x * D * v1 + v2);
+      } else {
+        cF1 = -A * D * v3;
+        cF2 = A * x * v3;
+        cF3 = A * (D * v1 - x * v2);
+      }
+      out[o.at(p, IVX, k, j, i)] += wght * cF1;
+      out[o.at(p, IVY, k, j, i)] += wght * cF2;
+      out[o.at(p, IVZ, k, j, i)] += wght * cF3;
+    }
+  }
+  // Held-Suarez forcing (examples/2023-Chen-exo3/hs94.cpp:59-155) with
+  // the constants of Mesh::InitUserMeshData (hs94.cpp:212-243)
+  if (o.cfg.forcing == EXO_FORCING_HS94) {
+    const double day_to_s = 8.64E4;
+    const double Rd = o.cfg.Rd, cp = o.cfg.gamma / (o.cfg.gamma - 1.) * Rd;
+    const double p0 = o.cfg.hs_p0, Ts = o.cfg.hs_Ts, dT = o.cfg.hs_dT;
+    const double dtheta = o.cfg.hs_dtheta, sigmab = o.cfg.hs_sigmab;
+    const double Kf = o.cfg.hs_Kf / day_to_s, Ka = o.cfg.hs_Ka / day_to_s,
+                 Ks = o.cfg.hs_Ks / day_to_s;
+    const double kappa = Rd / cp;
+    size_t q = o.kj(k, j);
+    double X = g.X[q], Y = g.Y[q], f = g.fcor[q];
+    double C = sqrt(X * X + 1), D = sqrt(Y * Y + 1);
+    double cth = -X * Y / (C * D);
+    // Coriolis on the momenta in latitude-longitude
+    for (int i = o.is; i <= o.ie; ++i) {
+      double U, V, acc2, acc3;
+      double rho = o.w[o.at(p, IDN, k, j, i)];
+      vec_rll_from_abp(X, Y, p + 1, o.w[o.at(p, IVY, k, j, i)], o.w[o.at(p, IVZ, k, j, i)],
+                       &U, &V);
+      U = -U;
+      double m2 = rho * U, m3 = rho * V;
+      double llU = f * m3, llV = -f * m2;
+      vec_abp_from_rll(X, Y, p + 1, -llU, llV, &acc2, &acc3);
+      double a2c = acc2 + acc3 * cth, a3c = acc3 + acc2 * cth;
+      out[o.at(p, IVY, k, j, i)] += wght * a2c;
+      out[o.at(p, IVZ, k, j, i)] += wght * a3c;
+    }
+    // Rayleigh drag and Newtonian cooling
+    for (int i = o.is; i <= o.ie; ++i) {
+      double rho = o.w[o.at(p, IDN, k, j, i)], pres = o.w[o.at(p, IPR, k, j, i)];
+      double scaled_z = pres / p0;
+      double sigma = pres / p0;
+      double sigma_p = (sigma - sigmab) / (1. - sigmab);
+      double Kv = (sigma_p < 0.0) ? 0.0 : sigma_p * Kf;
+      double Teq_p = Ts - dT * g.slat2[q] - dtheta * log(scaled_z) * g.clat2[q];
+      Teq_p *= pow(scaled_z, kappa);
+      double Teq = (Teq_p > 200.) ? Teq_p : 200.;
+      double temp = pres / rho / Rd;
+      sigma_p = (sigma_p < 0.0) ? 0.0 : sigma_p * g.clat4[q];
+      double Kt = Ka + (Ks - Ka) * sigma_p;
+      double m1 = rho * o.w[o.at(p, IVX, k, j, i)];
+      double m2 = rho * o.w[o.at(p, IVY, k, j, i)];
+      double m3 = rho * o.w[o.at(p, IVZ, k, j, i)];
+      double m2c = m2 + m3 * cth, m3c = m3 + m2 * cth;
+      out[o.at(p, IVX, k, j, i)] += -wght * Kv * m1;
+      out[o.at(p, IVY, k, j, i)] += -wght * Kv * m2c;
+      out[o.at(p, IVZ, k, j, i)] += -wght * Kv * m3c;
+      out[o.at(p, IEN, k, j, i)] += -wght * (cp - Rd) * rho * Kt * (temp - Teq);
+    }
+  }
+}
+
 void add_divergence_and_sources(Oracle& o, std::vector<double>& out, double wght) {
   int NV = o.NV;
   bool shallow = (o.cfg.eqn == EXO_EQN_SHALLOW_YZ);
@@ -1196,24 +1309,7 @@ void add_divergence_and_sources(Oracle& o, std::vector<double>& out, double wght
             if (!shallow) out[o.at(p, IEN, k, j, i)] += src * o.w[o.at(p, IVX, k, j, i)];
           }
         }
-        // user source: W92 Coriolis (examples/2023-Chen-exo3/W92.cpp:48-70)
-        if (o.cfg.coriolis == EXO_CORIOLIS_W92) {
-          size_t q = o.kj(k, j);
-          double X = g.X[q], Y = g.Y[q], f = g.fcor[q];
-          double C = sqrt(X * X + 1), D = sqrt(Y * Y + 1), delta = sqrt(X * X + Y * Y + 1);
-          double cth = -X * Y / (C * D);
-          for (int i = o.is; i <= o.ie; ++i) {
-            double U, V, acc2, acc3;
-            vec_rll_from_abp(X, Y, p + 1, o.w[o.at(p, IVY, k, j, i)], o.w[o.at(p, IVZ, k, j, i)], &U, &V);
-            U = -U;
-            double llU = f * V, llV = -f * U;
-            vec_abp_from_rll(X, Y, p + 1, -llU, llV, &acc2, &acc3);
-            double a2c = acc2 + acc3 * cth, a3c = acc3 + acc2 * cth;
-            out[o.at(p, IVY, k, j, i)] += wght * o.w[o.at(p, IDN, k, j, i)] * a2c;
-            out[o.at(p, IVZ, k, j, i)] += wght * o.w[o.at(p, IDN, k, j, i)] * a3c;
-          }
-          (void)delta;
-        }
+        add_user_sources(o, p, k, j, out, wght);
       }
 }
 
@@ -1829,6 +1925,18 @@ void ora_step(void* h, int nsteps, double dt_fixed) {
       o.dt = std::min(2.0 * o.dt, nd);
     }
   }
+}
+
+// The user explicit sources alone (Coriolis, HS94 forcing) of primitives w,
+// added to out (AthenaArray layout of six panels) with weight wght
+void ora_user_sources(void* h, const double* w, double* out, double wght) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  std::memcpy(o.w.data(), w, o.w.size() * sizeof(double));
+  std::vector<double> acc(out, out + o.w.size());
+  for (int p = 0; p < 6; ++p)
+    for (int k = o.ks; k <= o.ke; ++k)
+      for (int j = o.js; j <= o.je; ++j) add_user_sources(o, p, k, j, acc, wght);
+  std::memcpy(out, acc.data(), acc.size() * sizeof(double));
 }
 
 // ImplicitSolver::SolveImplicit3D on whole arrays: du (in/out, interior) and

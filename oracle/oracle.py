@@ -25,11 +25,14 @@ class ExoConfig(ctypes.Structure):
         ("N", ctypes.c_int), ("L", ctypes.c_int), ("eqn", ctypes.c_int),
         ("rsolver", ctypes.c_int), ("implicit_flag", ctypes.c_int),
         ("precision", ctypes.c_int), ("coriolis", ctypes.c_int),
-        ("reserved0", ctypes.c_int),
+        ("forcing", ctypes.c_int),
         ("x1min", ctypes.c_double), ("x1max", ctypes.c_double),
         ("gamma", ctypes.c_double), ("Rd", ctypes.c_double),
         ("grav", ctypes.c_double), ("cfl", ctypes.c_double),
         ("omega", ctypes.c_double), ("reserved1", ctypes.c_double),
+        ("hs_p0", ctypes.c_double), ("hs_Ts", ctypes.c_double), ("hs_dT", ctypes.c_double),
+        ("hs_dtheta", ctypes.c_double), ("hs_Kf", ctypes.c_double), ("hs_Ka", ctypes.c_double),
+        ("hs_Ks", ctypes.c_double), ("hs_sigmab", ctypes.c_double),
     ]
 
 
@@ -72,6 +75,7 @@ def lib():
         L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
         L.ora_correction_columns.argtypes = [i, i, i, dp, dp, dp, dp, dp, dp, d, d, d]
         L.ora_solve_implicit_3d.argtypes = [p, dp, dp, d]
+        L.ora_user_sources.argtypes = [p, dp, dp, d]
         L.ora_change_to_perturbation.argtypes = [p, dp]
         L.ora_restore_from_perturbation.argtypes = [p, dp, dp, dp]
         _lib = L
@@ -161,6 +165,14 @@ class Oracle:
         for a in (w, wl, wr):
             assert a.flags.c_contiguous and a.dtype == np.float64 and a.shape == self.shape
         lib().ora_restore_from_perturbation(self._h, _ptr(w), _ptr(wl), _ptr(wr))
+
+    def user_sources(self, w, wght, out=None):
+        """The user explicit sources alone (Coriolis, HS94 forcing) of
+        primitives w, times wght, added to out (zeros if None)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        out = np.zeros(self.shape) if out is None else np.ascontiguousarray(out, dtype=np.float64).copy()
+        lib().ora_user_sources(self._h, _ptr(w), _ptr(out), float(wght))
+        return out
 
     def solve_implicit_3d(self, du, w, dt):
         """SolveImplicit3D: du (whole-array layout) corrected in place."""
