@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(_HERE, "libexo_b200.so")
 
 EXO_OK = 0
 EXO_EQN_SHALLOW_YZ, EXO_EQN_IDEAL = 0, 1
+(EXO_OK, EXO_ERR_ARG, EXO_ERR_SHAPE, EXO_ERR_CUDA, EXO_ERR_NONFINITE, EXO_ERR_TIMEOUT,
+ EXO_ERR_NOGPU, EXO_ERR_CAPACITY) = range(8)
 EXO_RS_ROE_SHALLOW, EXO_RS_LMARS, EXO_RS_HLLC, EXO_RS_LMARS_SHALLOW = 0, 1, 2, 3
 EXO_PREC_FP64, EXO_PREC_MIXED = 0, 1
 EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92, EXO_CORIOLIS_3D = 0, 1, 2
@@ -39,6 +41,9 @@ EXPORTED = [
     "exo_restore_from_perturbation",
     "exo_ensemble_get_stream",
     "exo_implicit_columns", "exo_partial_correction_columns", "exo_implicit_columns_noalloc",
+    "exo_checkpoint_bytes", "exo_checkpoint_save", "exo_checkpoint_load",
+    "exo_ensemble_checkpoint_bytes", "exo_ensemble_checkpoint_save",
+    "exo_ensemble_add_checkpoint", "exo_set_max_redo", "exo_redo_count",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
 
@@ -61,6 +66,17 @@ class ExoConfig(ctypes.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class CheckpointHeader(ctypes.Structure):
+    """exo_checkpoint_header of include/exo_b200.h (512 bytes)."""
+    _fields_ = [
+        ("magic", ctypes.c_char * 8), ("version", ctypes.c_uint32),
+        ("header_bytes", ctypes.c_uint32), ("values", ctypes.c_uint64),
+        ("time", ctypes.c_double), ("dt", ctypes.c_double), ("ncycle", ctypes.c_int64),
+        ("invalid", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("cfg", ExoConfig), ("pad", ctypes.c_uint8 * (512 - 56 - ctypes.sizeof(ExoConfig))),
+    ]
 
 
 class ExoError(RuntimeError):
@@ -136,6 +152,14 @@ def lib():
     L.exo_ensemble_set_tiles.argtypes = [p, ip]
     L.exo_ensemble_get_tiles.argtypes = [p, ip]
     L.exo_ensemble_check_state.argtypes = [p, i, ctypes.POINTER(i)]
+    L.exo_set_max_redo.argtypes = [p, i]
+    L.exo_redo_count.argtypes = [p, ctypes.POINTER(ctypes.c_int64)]
+    L.exo_checkpoint_bytes.argtypes = [p, ctypes.POINTER(sz)]
+    L.exo_checkpoint_save.argtypes = [p, p, sz]
+    L.exo_checkpoint_load.argtypes = [p, p, sz]
+    L.exo_ensemble_checkpoint_bytes.argtypes = [p, i, ctypes.POINTER(sz)]
+    L.exo_ensemble_checkpoint_save.argtypes = [p, i, p, sz]
+    L.exo_ensemble_add_checkpoint.argtypes = [p, p, sz, ctypes.POINTER(i)]
     L.exo_ensemble_stats.argtypes = [p, ctypes.POINTER(i), ctypes.POINTER(sz),
                                      ctypes.POINTER(ctypes.c_int64)]
     L.exo_ensemble_get_stream.argtypes = [p, ctypes.POINTER(p)]
@@ -155,3 +179,15 @@ def check(rc):
 
 def dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def checkpoint_header(image):
+    """The exo_checkpoint_header of a checkpoint image (bytes-like) as a dict:
+    magic, version, time, dt, ncycle, invalid and the configuration."""
+    mv = memoryview(image).cast("B")
+    if len(mv) < ctypes.sizeof(CheckpointHeader):
+        raise ValueError("shorter than a checkpoint header")
+    h = CheckpointHeader.from_buffer_copy(bytes(mv[:ctypes.sizeof(CheckpointHeader)]))
+    return {"magic": bytes(h.magic), "version": h.version, "values": h.values,
+            "time": h.time, "dt": h.dt, "ncycle": h.ncycle, "invalid": h.invalid,
+            "cfg": h.cfg.as_dict()}

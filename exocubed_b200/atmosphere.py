@@ -12,6 +12,7 @@ Arrays follow AthenaArray(n,k,j,i) per panel, six panels stacked:
 shape (6, nvar, N+6, N+6, L+6).
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -128,6 +129,55 @@ class CubedSphereAtmosphere:
         nat.check(nat.lib().exo_restore_from_perturbation(self._ctx, nat.dptr(w), nat.dptr(wl),
                                                           nat.dptr(wr)))
 
+    def set_max_redo(self, max_redo):
+        """Redo of failed steps with half the time step (the reference's
+        max_redo; 0 turns it off)."""
+        nat.check(nat.lib().exo_set_max_redo(self._ctx, int(max_redo)))
+
+    @property
+    def redo_count(self):
+        n = ctypes.c_int64()
+        nat.check(nat.lib().exo_redo_count(self._ctx, ctypes.byref(n)))
+        return n.value
+
+    def checkpoint(self):
+        """The run's checkpoint image (numpy uint8 array): configuration,
+        clock, conserved and primitive arrays.  restore() or
+        Ensemble.add_checkpoint() continue it bit for bit."""
+        n = ctypes.c_size_t()
+        nat.check(nat.lib().exo_checkpoint_bytes(self._ctx, ctypes.byref(n)))
+        img = np.empty(n.value, dtype=np.uint8)
+        nat.check(nat.lib().exo_checkpoint_save(self._ctx, img.ctypes.data, n.value))
+        return img
+
+    def restore(self, image):
+        """Continue from a checkpoint image of this configuration (the
+        precision may differ)."""
+        img = np.ascontiguousarray(np.frombuffer(image, dtype=np.uint8))
+        nat.check(nat.lib().exo_checkpoint_load(self._ctx, img.ctypes.data, img.size))
+
+    def save_checkpoint(self, path):
+        """Write the checkpoint image to a file."""
+        img = self.checkpoint()
+        with open(path, "wb") as f:
+            f.write(img.tobytes())
+
+    @classmethod
+    def from_checkpoint(cls, path_or_image, precision=None):
+        """A context built from a checkpoint's configuration and resumed from
+        it; precision overrides the one it was written with."""
+        if isinstance(path_or_image, (str, os.PathLike)):
+            with open(path_or_image, "rb") as f:
+                image = f.read()
+        else:
+            image = path_or_image
+        cfg = dict(nat.checkpoint_header(image)["cfg"])
+        if precision is not None:
+            cfg["precision"] = precision
+        a = cls(make_config(**cfg))
+        a.restore(image)
+        return a
+
     def synchronize(self):
         nat.check(nat.lib().exo_synchronize(self._ctx))
 
@@ -145,6 +195,13 @@ class CubedSphereAtmosphere:
         t, n = ctypes.c_double(), ctypes.c_int64()
         nat.check(nat.lib().exo_get_time(self._ctx, ctypes.byref(t), ctypes.byref(n)))
         return t.value
+
+    @property
+    def ncycle(self):
+        """Steps taken."""
+        t, n = ctypes.c_double(), ctypes.c_int64()
+        nat.check(nat.lib().exo_get_time(self._ctx, ctypes.byref(t), ctypes.byref(n)))
+        return n.value
 
     @property
     def tiles(self):

@@ -90,6 +90,12 @@ struct exo_ctx {
   // column constants between the two calls (allocated on the first call)
   double* dec_refs = nullptr;
   bool dec_done = false;
+  // Redo of failed steps: budget, redos taken, the pre-step copy of u, w and
+  // the clock (allocated by exo_set_max_redo)
+  int max_redo = 0;
+  int64_t redo_attempts = 0;
+  double* redo_state = nullptr;
+  exo::DevScalars* redo_sc = nullptr;
 };
 
 
@@ -670,10 +676,102 @@ int exo_device_state(exo_ctx* c, double** u_dev, double** w_dev) {
   return EXO_OK;
 }
 
+// One step: the captured CFL graph, or the launches of one_step when
+// profiling or with a fixed dt.
+static int step_once(exo_ctx* c, double dt_fixed) {
+  if (!c->profiling && dt_fixed <= 0.) {
+    int rc = capture_step(c);
+    if (rc) return rc;
+    CK(cudaGraphLaunch(c->step_graph, c->stream));
+    c->launches += c->graph_launches;
+    return EXO_OK;
+  }
+  return one_step(c, dt_fixed);
+}
+
+static int read_scalars(exo_ctx* c, const exo::DevScalars* src, exo::DevScalars* s) {
+  CK(cudaMemcpyAsync(s, src, sizeof(*s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+// copy u, w and the clock: to the redo copy (save) or back (!save)
+static int redo_copy(exo_ctx* c, bool save) {
+  const size_t b = c->state_elems * sizeof(double);
+  double* keep_u = c->redo_state;
+  double* keep_w = c->redo_state + c->state_elems;
+  auto cp = [&](void* dst, const void* src, size_t n) {
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, c->stream);
+  };
+  if (save) {
+    CK(cp(keep_u, c->v.u, b));
+    CK(cp(keep_w, c->v.w, b));
+    CK(cp(c->redo_sc, c->v.sc, sizeof(exo::DevScalars)));
+  } else {
+    CK(cp(c->v.u, keep_u, b));
+    CK(cp(c->v.w, keep_w, b));
+    CK(cp(c->v.sc, c->redo_sc, sizeof(exo::DevScalars)));
+  }
+  return EXO_OK;
+}
+
+// The main loop's redo (main.cpp.in:126-157, mesh_redo.cpp:12-46): keep the
+// state, take the step, and while the state came out invalid put the kept
+// state back and take the step again with half the time step.  The budget
+// counts redos over the whole run, `attempts++ > max_redo` as there.
+static int step_with_redo(exo_ctx* c, double dt_fixed) {
+  exo::DevScalars s;
+  int rc = read_scalars(c, c->v.sc, &s);
+  if (rc) return rc;
+  if (s.invalid) return fail(EXO_ERR_NONFINITE, "the state is invalid before the step");
+  if ((rc = redo_copy(c, true))) return rc;
+  // the step in use: the fixed one, or the CFL step the previous step chose
+  double dt_step = dt_fixed > 0. ? dt_fixed : s.dt;
+  if ((rc = step_once(c, dt_fixed))) return rc;
+  if ((rc = read_scalars(c, c->v.sc, &s))) return rc;
+  while (s.invalid) {
+    // LoadAllStates (the kept copy holds the pre-step clock), DecreaseTimeStep
+    if ((rc = redo_copy(c, false))) return rc;
+    dt_step *= 0.5;
+    if (dt_fixed <= 0.) RK(STEP(launch_set_dt, c->v, dt_step, c->stream));
+    if (c->redo_attempts++ > c->max_redo)
+      return fail(EXO_ERR_NONFINITE, "too many attempts to redo the step");
+    if ((rc = step_once(c, dt_fixed > 0. ? dt_step : 0.))) return rc;
+    if ((rc = read_scalars(c, c->v.sc, &s))) return rc;
+  }
+  return EXO_OK;
+}
+
+int exo_set_max_redo(exo_ctx* c, int max_redo) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (max_redo < 0) return fail(EXO_ERR_ARG, "max_redo < 0");
+  if (max_redo > 0 && !c->redo_state) {
+    CK(cudaMalloc((void**)&c->redo_state, 2 * c->state_elems * sizeof(double)));
+    c->owned.push_back(c->redo_state);
+    CK(cudaMalloc((void**)&c->redo_sc, sizeof(exo::DevScalars)));
+    c->owned.push_back(c->redo_sc);
+  }
+  c->max_redo = max_redo;
+  return EXO_OK;
+}
+
+int exo_redo_count(exo_ctx* c, int64_t* redos) {
+  if (!c || !redos) return fail(EXO_ERR_ARG, "NULL argument");
+  *redos = c->redo_attempts;
+  return EXO_OK;
+}
+
 int exo_step(exo_ctx* c, int nsteps, double dt_fixed) {
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
   if (nsteps < 0) return fail(EXO_ERR_ARG, "nsteps < 0");
+  if (c->max_redo > 0) {
+    for (int n = 0; n < nsteps; ++n) {
+      int rc = step_with_redo(c, dt_fixed);
+      if (rc) return rc;
+    }
+    return EXO_OK;
+  }
   if (!c->profiling && dt_fixed <= 0. && nsteps > 0) {
     // the CFL step is replayed from its graph: one launch per step on the host
     int rc = capture_step(c);
@@ -760,6 +858,40 @@ int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, dou
   if (rc) return fail(rc, "implicit launch failed");
   CK(cudaMemcpyAsync(du_host, c->v.du, bytes, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return EXO_OK;
+}
+
+int exo_checkpoint_bytes(const exo_ctx* c, size_t* bytes) {
+  if (!c || !bytes) return fail(EXO_ERR_ARG, "NULL argument");
+  *bytes = exo::checkpoint_bytes(c->v);
+  return EXO_OK;
+}
+
+int exo_checkpoint_save(exo_ctx* c, void* image, size_t bytes) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
+  std::string err;
+  int rc = exo::checkpoint_save(c->cfg, c->v, c->stream, image, bytes, &err);
+  return rc ? fail(rc, err) : EXO_OK;
+}
+
+int exo_checkpoint_load(exo_ctx* c, const void* image, size_t bytes) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  exo_checkpoint_header h;
+  std::string err;
+  int rc = exo::checkpoint_parse(image, bytes, &h, &err);
+  if (rc) return fail(rc, err);
+  if (!exo::same_config_but_precision(h.cfg, c->cfg))
+    return fail(EXO_ERR_ARG, "the checkpoint was written with another configuration");
+  CK(cudaStreamSynchronize(c->stream));
+  rc = exo::checkpoint_restore(c->v, c->stream, image, &err);
+  if (rc) return fail(rc, err);
+  // the primitives (and their FP32 copy in the mixed build) from u, as the
+  // end of every step computes them
+  rc = boundary_and_prim(c, false);
+  if (rc) return fail(rc, "recomputing the primitives failed");
+  CK(cudaStreamSynchronize(c->stream));
+  c->has_state = true;
   return EXO_OK;
 }
 

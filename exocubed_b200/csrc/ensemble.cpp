@@ -77,6 +77,8 @@ int launch_single(int precision, int which, const DevView& v, void* st, double a
     case 1: return mixed ? exo::mixed::launch_dt_reset(v, st) : exo::fp64::launch_dt_reset(v, st);
     case 2: return mixed ? exo::mixed::launch_prim_ghost(v, true, st)
                          : exo::fp64::launch_prim_ghost(v, true, st);
+    case 4: return mixed ? exo::mixed::launch_prim_ghost(v, false, st)
+                         : exo::fp64::launch_prim_ghost(v, false, st);
     default: return mixed ? exo::mixed::launch_dt_finalize(v, arg, false, st)
                           : exo::fp64::launch_dt_finalize(v, arg, false, st);
   }
@@ -231,8 +233,13 @@ void exo_ensemble_destroy(exo_ensemble* e) {
   delete e;
 }
 
-int exo_ensemble_add(exo_ensemble* e, const exo_config* cfg, const double* w_host, int* slot) {
-  if (!e || !cfg || !w_host || !slot) return efail(EXO_ERR_ARG, "NULL argument");
+namespace {
+
+// Admission of a member: slot, budget, tables, device memory; then its
+// state from the primitives w_host (PrimitiveToConserved, ghosts,
+// primitives, first dt) or from a checkpoint image.
+int admit(exo_ensemble* e, const exo_config* cfg, const double* w_host, const void* image,
+          int* slot) {
   *slot = -1;
   std::string err;
   if (!exo::validate_config(*cfg, &err)) return efail(EXO_ERR_ARG, err);
@@ -257,30 +264,87 @@ int exo_ensemble_add(exo_ensemble* e, const exo_config* cfg, const double* w_hos
     delete m;
     return efail(rc, err);
   }
-  // the initial state: PrimitiveToConserved, ghosts, primitives, first dt
-  size_t bytes = (size_t)6 * m->v.nv * m->v.cells * sizeof(double);
-  cudaError_t ce = cudaMemcpyAsync(m->v.w, w_host, bytes, cudaMemcpyHostToDevice, e->stream);
-  if (ce != cudaSuccess) {
-    for (void* p : m->owned) cudaFreeAsync(p, e->stream);
-    delete m;
-    return cuda_efail(ce, "cudaMemcpyAsync(initial state)");
+  if (image) {
+    // u, w and the clock; the primitives (and their FP32 copy in the mixed
+    // build) are recomputed from u as the end of every step computes them
+    rc = exo::checkpoint_restore(m->v, e->stream, image, &err);
+    if (!rc && launch_single(e->precision, 4, m->v, e->stream, 0., nullptr)) {
+      rc = EXO_ERR_CUDA;
+      err = "recomputing the member's primitives failed";
+    }
+    if (!rc) {
+      cudaError_t ce = cudaStreamSynchronize(e->stream);
+      if (ce != cudaSuccess) {
+        rc = EXO_ERR_CUDA;
+        err = std::string("exo_ensemble_add_checkpoint: ") + cudaGetErrorString(ce);
+      }
+    }
+    if (rc) {
+      for (void* p : m->owned) cudaFreeAsync(p, e->stream);
+      delete m;
+      return efail(rc, err);
+    }
+    e->launches += 1;
+  } else {
+    // the initial state: PrimitiveToConserved, ghosts, primitives, first dt
+    size_t bytes = (size_t)6 * m->v.nv * m->v.cells * sizeof(double);
+    cudaError_t ce = cudaMemcpyAsync(m->v.w, w_host, bytes, cudaMemcpyHostToDevice, e->stream);
+    if (ce != cudaSuccess) {
+      for (void* p : m->owned) cudaFreeAsync(p, e->stream);
+      delete m;
+      return cuda_efail(ce, "cudaMemcpyAsync(initial state)");
+    }
+    if (launch_single(e->precision, 0, m->v, e->stream, 0., m->v.w) ||
+        launch_single(e->precision, 1, m->v, e->stream, 0., nullptr) ||
+        launch_single(e->precision, 2, m->v, e->stream, 0., nullptr) ||
+        launch_single(e->precision, 3, m->v, e->stream, 0., nullptr)) {
+      for (void* p : m->owned) cudaFreeAsync(p, e->stream);
+      delete m;
+      return efail(EXO_ERR_CUDA, "initialising the member failed");
+    }
+    ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return cuda_efail(ce, "exo_ensemble_add");
+    e->launches += 4;
   }
-  if (launch_single(e->precision, 0, m->v, e->stream, 0., m->v.w) ||
-      launch_single(e->precision, 1, m->v, e->stream, 0., nullptr) ||
-      launch_single(e->precision, 2, m->v, e->stream, 0., nullptr) ||
-      launch_single(e->precision, 3, m->v, e->stream, 0., nullptr)) {
-    for (void* p : m->owned) cudaFreeAsync(p, e->stream);
-    delete m;
-    return efail(EXO_ERR_CUDA, "initialising the member failed");
-  }
-  ce = cudaStreamSynchronize(e->stream);
-  if (ce != cudaSuccess) return cuda_efail(ce, "exo_ensemble_add");
-  e->launches += 4;
   e->slots[free_slot] = m;
   e->used += need;
   e->dirty = true;
   *slot = free_slot;
   return EXO_OK;
+}
+
+}  // namespace
+
+int exo_ensemble_add(exo_ensemble* e, const exo_config* cfg, const double* w_host, int* slot) {
+  if (!e || !cfg || !w_host || !slot) return efail(EXO_ERR_ARG, "NULL argument");
+  return admit(e, cfg, w_host, nullptr, slot);
+}
+
+int exo_ensemble_add_checkpoint(exo_ensemble* e, const void* image, size_t bytes, int* slot) {
+  if (!e || !slot) return efail(EXO_ERR_ARG, "NULL argument");
+  *slot = -1;
+  exo_checkpoint_header h;
+  std::string err;
+  int rc = exo::checkpoint_parse(image, bytes, &h, &err);
+  if (rc) return efail(rc, err);
+  exo_config cfg = h.cfg;
+  cfg.precision = e->precision;
+  return admit(e, &cfg, nullptr, image, slot);
+}
+
+int exo_ensemble_checkpoint_bytes(exo_ensemble* e, int slot, size_t* bytes) {
+  Member* m = member_at(e, slot);
+  if (!m || !bytes) return efail(EXO_ERR_ARG, "bad slot or NULL argument");
+  *bytes = exo::checkpoint_bytes(m->v);
+  return EXO_OK;
+}
+
+int exo_ensemble_checkpoint_save(exo_ensemble* e, int slot, void* image, size_t bytes) {
+  Member* m = member_at(e, slot);
+  if (!m) return efail(EXO_ERR_ARG, "no member in that slot");
+  std::string err;
+  int rc = exo::checkpoint_save(m->cfg, m->v, e->stream, image, bytes, &err);
+  return rc ? efail(rc, err) : EXO_OK;
 }
 
 int exo_ensemble_remove(exo_ensemble* e, int slot) {

@@ -218,6 +218,17 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
                                     void* stream, std::string* err);
 
 
+// checkpoint.cpp: images of one atmosphere (exo_checkpoint_header, u, w)
+size_t checkpoint_bytes(const DevView& v);
+bool same_config_but_precision(const exo_config& a, const exo_config& b);
+int checkpoint_save(const exo_config& cfg, const DevView& v, void* stream, void* image,
+                    size_t bytes, std::string* err);
+// checks magic, version, configuration and size; copies the header out
+int checkpoint_parse(const void* image, size_t bytes, exo_checkpoint_header* h,
+                     std::string* err);
+// u, w and the clock of an image already parsed into the atmosphere v
+int checkpoint_restore(const DevView& v, void* stream, const void* image, std::string* err);
+
 // capi.cpp: shared by the single-atmosphere context and the ensemble
 bool validate_config(const exo_config& cfg, std::string* err);
 size_t view_footprint(const exo_config& cfg);

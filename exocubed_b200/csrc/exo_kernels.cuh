@@ -1992,6 +1992,7 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
     c0 = cp;
     cur = nxt;
   }
+  cp_async_wait_all();  // the last level's prefetch (unused) lands before the slice is reused
   // back substitution: delta_i -= (A c)_i delta_{i+1}; the update of level i
   // takes delta for rho, m1, E and the explicit du for m2, m3
   auto store = [&](int i, const double* u) {

@@ -65,6 +65,31 @@ class Ensemble:
         self.cfgs[slot.value] = {f: getattr(c, f) for f, _ in nat.ExoConfig._fields_}
         return slot.value
 
+    def add_checkpoint(self, image):
+        """Admit a member from a checkpoint image (CubedSphereAtmosphere.
+        checkpoint or Ensemble.checkpoint); it continues the run that wrote
+        it, in this ensemble's precision.  Returns its slot."""
+        img = np.ascontiguousarray(np.frombuffer(image, dtype=np.uint8))
+        slot = ctypes.c_int()
+        nat.check(nat.lib().exo_ensemble_add_checkpoint(self._h, img.ctypes.data, img.size,
+                                                        ctypes.byref(slot)))
+        h = nat.checkpoint_header(img)
+        c = dict(h["cfg"], precision=self.precision)
+        nv = 4 if c["eqn"] == nat.EXO_EQN_SHALLOW_YZ else 5
+        n2 = c["N"] + 6
+        self.shapes[slot.value] = (6, nv, n2, n2, c["L"] + 6)
+        self.cfgs[slot.value] = c
+        return slot.value
+
+    def checkpoint(self, slot):
+        """Checkpoint image of one member (numpy uint8 array)."""
+        n = ctypes.c_size_t()
+        nat.check(nat.lib().exo_ensemble_checkpoint_bytes(self._h, slot, ctypes.byref(n)))
+        img = np.empty(n.value, dtype=np.uint8)
+        nat.check(nat.lib().exo_ensemble_checkpoint_save(self._h, slot, img.ctypes.data,
+                                                         n.value))
+        return img
+
     def try_add(self, cfg, w):
         try:
             return self.add(cfg, w)

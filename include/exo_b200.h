@@ -377,6 +377,68 @@ int exo_ensemble_stats(exo_ensemble* ens, int* members, size_t* bytes_in_use,
                        int64_t* launches);
 int exo_ensemble_get_stream(exo_ensemble* ens, void** stream);
 
+/* ------------------------------------------------------ redo of a step */
+
+/* The main loop's redo of failed steps (main.cpp.in:126-157,
+   src/mesh_redo.cpp:12-46): with max_redo > 0 every exo_step step first
+   keeps a device copy of u, w and the clock; a step that leaves the state
+   invalid (rho or p negative or not finite, exo_check_state) is taken again
+   from that copy with half the time step (half the fixed dt when one is
+   given), as often as needed.  As in the reference the budget counts redos
+   over the whole run and `attempts++ > max_redo` ends it: the step returns
+   EXO_ERR_NONFINITE with the kept state back in place and its dt halved.
+   A step that starts from an invalid state returns EXO_ERR_NONFINITE at
+   once.  Each step then waits for the device once (the flag read); the
+   default 0, the reference's, keeps steps asynchronous.  The first call with
+   max_redo > 0 allocates the copy (2 x the state). */
+int exo_set_max_redo(exo_ctx* ctx, int max_redo);
+/* Redos taken so far. */
+int exo_redo_count(exo_ctx* ctx, int64_t* redos);
+
+/* ----------------------------------------------------------- checkpoints */
+
+/* A checkpoint image holds what a run needs to continue exactly where it
+   stopped: the configuration, the clock (time, steps taken, the dt of the
+   next step) and the conserved and primitive arrays with their ghosts.  It
+   replaces the hydro part of an Athena++ restart file (src/mesh_setup.cpp:
+   25-97, written by <output> file_type = rst in hs94.inp) and of the
+   in-memory copy MeshBlock::Impl::SaveAllStates / LoadAllStates keeps
+   (src/impl.cpp:306-332).  A run resumed from an image takes, step for step,
+   the bits the uninterrupted run takes.
+   Layout: exo_checkpoint_header (512 bytes), then u, then w, each
+   header.values doubles in the context's (panel, variable, k, j, i) order,
+   in the byte order of the machine that wrote it. */
+#define EXO_CHECKPOINT_VERSION 1
+typedef struct exo_checkpoint_header {
+  char magic[8];          /* "EXOCKPT1" (not NUL-terminated)                  */
+  uint32_t version;       /* EXO_CHECKPOINT_VERSION                           */
+  uint32_t header_bytes;  /* sizeof(exo_checkpoint_header) = 512              */
+  uint64_t values;        /* doubles in each of u and w: 6*nvar*nc3*nc2*nc1   */
+  double time;            /* simulated time                                   */
+  double dt;              /* the step the run takes next                      */
+  int64_t ncycle;         /* steps taken                                      */
+  int32_t invalid;        /* sticky invalid-state flag at the time of writing */
+  int32_t reserved;
+  exo_config cfg;         /* the configuration the state belongs to           */
+  uint8_t pad[512 - 56 - sizeof(exo_config)];
+} exo_checkpoint_header;
+
+/* Bytes of a checkpoint image of this context (header + u + w). */
+int exo_checkpoint_bytes(const exo_ctx* ctx, size_t* bytes);
+/* Write the context's image into image[0, bytes): waits for the context's
+   queued work.  EXO_ERR_SHAPE if bytes is smaller than exo_checkpoint_bytes. */
+int exo_checkpoint_save(exo_ctx* ctx, void* image, size_t bytes);
+/* Continue from an image: its configuration must equal the context's in
+   every field except precision (a run may resume in the other build);
+   EXO_ERR_ARG for a foreign or damaged image or another configuration. */
+int exo_checkpoint_load(exo_ctx* ctx, const void* image, size_t bytes);
+/* The same for one member of an ensemble, and admission of a new member
+   from an image (in the ensemble's precision), which then continues the run
+   that wrote it. */
+int exo_ensemble_checkpoint_bytes(exo_ensemble* ens, int slot, size_t* bytes);
+int exo_ensemble_checkpoint_save(exo_ensemble* ens, int slot, void* image, size_t bytes);
+int exo_ensemble_add_checkpoint(exo_ensemble* ens, const void* image, size_t bytes, int* slot);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,7 +43,7 @@ def test_coriolis3_without_gravity_bitwise(oracle_mod):
 
 @pytest.mark.parametrize("implicit_flag", [1, 9])
 def test_hs94_steps(oracle_mod, implicit_flag):
-    cfg = W.hs94_config(N=8, L=12, cfl=0.4, implicit_flag=implicit_flag)
+    cfg = W.hs94_config(N=8, L=20, cfl=0.4, implicit_flag=implicit_flag)
     state = W.hs94_state(cfg, seed=2)
     o, g = _pair(oracle_mod, cfg, state)
     o.step(3)
@@ -78,7 +78,7 @@ def test_hs94_mixed_close_to_oracle(oracle_mod):
 
 @pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
 def test_forced_and_unforced_members_in_one_batch(precision):
-    cfgs = [dict(W.hs94_config(N=8, L=12, cfl=0.4), precision=precision),
+    cfgs = [dict(W.hs94_config(N=8, L=20, cfl=0.4), precision=precision),
             dict(W.dry_atmosphere_config(N=10, L=8, rsolver=nat.EXO_RS_HLLC,
                                          coriolis=nat.EXO_CORIOLIS_3D, omega=7.292e-5),
                  precision=precision),
