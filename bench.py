@@ -604,6 +604,60 @@ def run_serving(args):
             "continuous_batching_mixed": mixed, "one_at_a_time_fp64": base}}), flush=True)
 
 
+def run_mcmc(args):
+    """MCMC driver: the stretch-move sampler with args.mcmc walkers over the
+    temperature-profile problem (each forward model a 6 x 32^2 x 48
+    atmosphere run args.mcmc_steps steps), its forward models batched in one
+    mixed-precision ensemble, against the same sampler evaluating them one
+    at a time on FP64 contexts (the reference's order).  Reports walker
+    evaluations per second and cell-updates per second of both."""
+    import time
+
+    import numpy as np
+    import torch
+
+    from exocubed_b200.inversion import (EnsembleForward, SequentialForward, StretchSampler,
+                                         profile_problem)
+    torch.cuda.init()
+    nw, steps, iters = args.mcmc, args.mcmc_steps, args.mcmc_iters
+    build, observe, nvalue = profile_problem(N=32, L=48, steps=steps)
+    obs = SequentialForward(build, observe, nvalue, steps, precision=0)(
+        np.array([[285., 205.]]))[0]
+
+    def log_prob(theta, val):
+        Ts, Ttop = theta
+        if not (200. < Ts < 350. and 150. < Ttop < Ts) or np.isnan(val).any():
+            return -np.inf
+        return float(-0.5 * (((val - obs) / 2.0) ** 2).sum())
+
+    rng = np.random.default_rng(0)
+    pos = np.stack([280. + 5 * rng.standard_normal(nw), 200. + 5 * rng.standard_normal(nw)], 1)
+    out = {}
+    for name, fwd in (("batched_mixed", EnsembleForward(build, observe, nvalue, steps,
+                                                        precision=1, capacity=nw)),
+                      ("one_at_a_time_fp64", SequentialForward(build, observe, nvalue, steps,
+                                                               precision=0))):
+        fwd(pos[:2])  # warm-up: contexts, pools, graph capture
+        fwd.cell_updates = 0
+        sampler = StretchSampler(fwd, log_prob, nw, 2, nvalue, seed=1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rec = sampler.run(pos, iters)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        out[name] = {"seconds": el, "evaluations": sampler.evaluations,
+                     "evaluations_per_s": sampler.evaluations / el,
+                     "cell_updates_per_s": fwd.cell_updates / el,
+                     "acceptance": rec.acceptance_fraction(),
+                     "best_theta": [float(x) for x in rec.opt_par]}
+        if hasattr(fwd, "close"):
+            fwd.close()
+    print(json.dumps({"mcmc": {
+        "walkers": nw, "iterations": iters, "forward": f"6x32x32x48 dry atmosphere, {steps} steps",
+        "speedup": out["batched_mixed"]["evaluations_per_s"] /
+        out["one_at_a_time_fp64"]["evaluations_per_s"], **out}}), flush=True)
+
+
 def run_accuracy(args):
     """Mixed precision against the FP64 path after args.accuracy steps."""
     import torch  # noqa: F401  (CUDA context)
@@ -672,6 +726,10 @@ def main():
                     help="run N steps mixed vs FP64 and report the field errors")
     ap.add_argument("--rsolver", type=int, default=None, choices=[1, 2],
                     help="Riemann solver of exo3 workloads: 1 LMARS (default), 2 HLLC")
+    ap.add_argument("--mcmc", type=int, default=0,
+                    help="walkers: run the MCMC driver comparison instead of a step benchmark")
+    ap.add_argument("--mcmc-steps", type=int, default=50, help="steps per forward model (mcmc)")
+    ap.add_argument("--mcmc-iters", type=int, default=3, help="sampler iterations (mcmc)")
     ap.add_argument("--implicit-flag", type=int, default=None, choices=[1, 9],
                     help="implicit_flag of exo3 workloads: 9 full 5x5 (default), 1 partial 3x3")
     args = ap.parse_args()
@@ -683,6 +741,8 @@ def main():
         run_accuracy(args)
     elif args.serve:
         run_serving(args)
+    elif args.mcmc:
+        run_mcmc(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "c4":
