@@ -41,6 +41,18 @@ def cell_geometry(cfg):
     return lat, lon, m, x1v
 
 
+def mesh(cfg, panel):
+    """(x1f, x2f, x3f) face coordinates of a panel, ghosts included; no GPU
+    needed."""
+    cfg = cfg if isinstance(cfg, nat.ExoConfig) else make_config(**cfg)
+    x1f = np.empty(cfg.L + 7)
+    x2f = np.empty(cfg.N + 7)
+    x3f = np.empty(cfg.N + 7)
+    nat.check(nat.lib().exo_mesh(ctypes.byref(cfg), int(panel), nat.dptr(x1f), nat.dptr(x2f),
+                                 nat.dptr(x3f)))
+    return x1f, x2f, x3f
+
+
 class CubedSphereAtmosphere:
     """Six-panel cubed-sphere atmosphere advanced on the current CUDA device."""
 
@@ -139,6 +151,13 @@ class CubedSphereAtmosphere:
         n = ctypes.c_int64()
         nat.check(nat.lib().exo_redo_count(self._ctx, ctypes.byref(n)))
         return n.value
+
+    def write_netcdf(self, basename, file_id="out2", number=0, directory="."):
+        """Primitive output in the reference's per-block NetCDF layout (one
+        file per panel; exocubed_b200.netcdf)."""
+        from . import netcdf
+        return netcdf.write_prim_output(self.primitive(), lambda p: mesh(self.cfg, p), basename,
+                                        file_id, number, self.time, directory)
 
     def checkpoint(self):
         """The run's checkpoint image (numpy uint8 array): configuration,

@@ -117,3 +117,19 @@ def test_load_rejects_foreign_images():
         # the context still runs after the refused loads
         a.step(1)
         assert a.invalid() == 0
+
+
+def test_netcdf_output_of_a_run(tmp_path):
+    from scipy.io import netcdf_file
+    cfg = W.dry_atmosphere_config(N=8, L=12)
+    with CubedSphereAtmosphere(cfg) as a:
+        a.set_primitive(W.dry_atmosphere_state(cfg, seed=0))
+        a.step(2)
+        paths = a.write_netcdf("exo3", "out2", 1, directory=str(tmp_path))
+        w = a.primitive()
+        t = a.time
+    f = netcdf_file(paths[2], "r", mmap=False)
+    assert np.array_equal(f.variables["press"][0],
+                          W.interior(w)[2, 4].transpose(2, 1, 0).astype(np.float32))
+    assert f.variables["time"][0] == np.float32(t)
+    f.close()
