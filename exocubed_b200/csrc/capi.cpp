@@ -16,6 +16,10 @@
 #include <vector>
 
 #include "exo_internal.h"
+#include "nvtx3/nvToolsExt.h"
+
+exo::Range::Range(const char* name) { nvtxRangePushA(name); }
+exo::Range::~Range() { nvtxRangePop(); }
 
 using exo::DevScalars;
 using exo::DevView;
@@ -142,6 +146,8 @@ static int boundary_and_prim(exo_ctx* c, bool dt) {
 // correction, boundaries and primitives (with the CFL candidate on the last
 // stage unless the step is fixed).
 static int one_stage(exo_ctx* c, int s, bool cfl) {
+  static const char* kStage[3] = {"exo stage 0", "exo stage 1", "exo stage 2"};
+  exo::Range range(kStage[s]);
   const DevView& v = c->v;
   bool shallow = v.eqn == EXO_EQN_SHALLOW_YZ;
   bool implicit = !shallow && (v.implicit_flag & 1);
@@ -730,6 +736,7 @@ static int step_with_redo(exo_ctx* c, double dt_fixed) {
   if ((rc = step_once(c, dt_fixed))) return rc;
   if ((rc = read_scalars(c, c->v.sc, &s))) return rc;
   while (s.invalid) {
+    exo::Range redo("exo redo");
     // LoadAllStates (the kept copy holds the pre-step clock), DecreaseTimeStep
     if ((rc = redo_copy(c, false))) return rc;
     dt_step *= 0.5;
@@ -762,6 +769,7 @@ int exo_redo_count(exo_ctx* c, int64_t* redos) {
 }
 
 int exo_step(exo_ctx* c, int nsteps, double dt_fixed) {
+  exo::Range range("exo_step");
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
   if (nsteps < 0) return fail(EXO_ERR_ARG, "nsteps < 0");
@@ -868,6 +876,7 @@ int exo_checkpoint_bytes(const exo_ctx* c, size_t* bytes) {
 }
 
 int exo_checkpoint_save(exo_ctx* c, void* image, size_t bytes) {
+  exo::Range range("exo_checkpoint_save");
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   if (!c->has_state) return fail(EXO_ERR_ARG, "no state loaded (exo_set_primitive)");
   std::string err;
@@ -876,6 +885,7 @@ int exo_checkpoint_save(exo_ctx* c, void* image, size_t bytes) {
 }
 
 int exo_checkpoint_load(exo_ctx* c, const void* image, size_t bytes) {
+  exo::Range range("exo_checkpoint_load");
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   exo_checkpoint_header h;
   std::string err;

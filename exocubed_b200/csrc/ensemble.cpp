@@ -359,6 +359,7 @@ int exo_ensemble_remove(exo_ensemble* e, int slot) {
 }
 
 int exo_ensemble_step(exo_ensemble* e, int nsteps) {
+  exo::Range range("exo_ensemble_step");
   if (!e) return efail(EXO_ERR_ARG, "NULL ensemble");
   if (nsteps < 0) return efail(EXO_ERR_ARG, "nsteps < 0");
   if (e->dirty) {

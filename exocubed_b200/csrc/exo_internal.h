@@ -12,6 +12,16 @@
 
 namespace exo {
 
+// NVTX range for the host side of a call (steps, stages, redos, checkpoints):
+// visible in Nsight Systems and Nsight Compute timelines, free when no
+// profiler is attached.  Defined in capi.cpp.
+struct Range {
+  explicit Range(const char* name);
+  ~Range();
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
+
 constexpr int G = EXO_NGHOST;
 constexpr int IDN = 0, IVX = 1, IVY = 2, IVZ = 3, IPR = 4, IEN = 4;
 enum Side { UP = 0, DOWN = 1, LEFT = 2, RIGHT = 3 };

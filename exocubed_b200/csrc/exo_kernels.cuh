@@ -36,6 +36,11 @@
 #ifndef EXO_X23_LINES
 #define EXO_X23_LINES EXO_MIXED
 #endif
+// 1: the sliding window computes each cell's WENO smoothness indicators once
+// for both of its faces (mixed build; the FP64 build keeps weno5's order)
+#ifndef EXO_X23_SHARED_BETA
+#define EXO_X23_SHARED_BETA EXO_MIXED
+#endif
 // 1: the implicit solve's back substitution prefetches two levels through
 // shared memory (FP64: 3% faster at 6x192^2x96; mixed: 1% slower, since its
 // 204-register cap already keeps a level in flight)
@@ -101,6 +106,44 @@ __device__ __forceinline__ T weno5(T phip2, T phip1, T phi, T phim1, T phim2) {
   T a0 = T(0.1) / ((b0 + eps) * (b0 + eps));
   T a1 = T(0.6) / ((b1 + eps) * (b1 + eps));
   T a2 = T(0.3) / ((b2 + eps) * (b2 + eps));
+  return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+}
+
+// The same reconstruction split so that a cell's smoothness indicators serve
+// both of its faces: the right-face value of cell c uses the weights
+// 1/(beta_k + eps)^2 of its left, centre and right candidate stencils in that
+// order, the left-face value the same three in mirror order.  a..e are the
+// cells c-2..c+2.  (A sliding window over a line of faces computes each
+// cell's indicators once instead of twice; the indicators of the mirrored
+// stencils are the same sums taken in the other order, so results agree
+// with weno5 to rounding.)
+template <class T>
+struct WenoCell {
+  T i0, i1, i2;  // 1/(beta+eps)^2 of the stencils {c-2..c}, {c-1..c+1}, {c..c+2}
+};
+template <class T>
+__device__ __forceinline__ WenoCell<T> weno_cell(T a, T b, T c, T d, T e) {
+  const T eps = T(WENO_EPS);
+  T b0 = T(13. / 12.) * sqr(a - T(2.) * b + c) + T(.25) * sqr(a - T(4.) * b + T(3.) * c);
+  T b1 = T(13. / 12.) * sqr(b - T(2.) * c + d) + T(.25) * sqr(b - d);
+  T b2 = T(13. / 12.) * sqr(c - T(2.) * d + e) + T(.25) * sqr(T(3.) * c - T(4.) * d + e);
+  return {T(1.) / ((b0 + eps) * (b0 + eps)), T(1.) / ((b1 + eps) * (b1 + eps)),
+          T(1.) / ((b2 + eps) * (b2 + eps))};
+}
+template <class T>
+__device__ __forceinline__ T weno_right(const WenoCell<T>& w, T a, T b, T c, T d, T e) {
+  T p0 = T(1.0 / 3.0) * a - T(7.0 / 6.0) * b + T(11.0 / 6.0) * c;
+  T p1 = T(-1.0 / 6.0) * b + T(5.0 / 6.0) * c + T(1.0 / 3.0) * d;
+  T p2 = T(1.0 / 3.0) * c + T(5.0 / 6.0) * d - T(1.0 / 6.0) * e;
+  T a0 = T(0.1) * w.i0, a1 = T(0.6) * w.i1, a2 = T(0.3) * w.i2;
+  return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+}
+template <class T>
+__device__ __forceinline__ T weno_left(const WenoCell<T>& w, T a, T b, T c, T d, T e) {
+  T p0 = T(1.0 / 3.0) * e - T(7.0 / 6.0) * d + T(11.0 / 6.0) * c;
+  T p1 = T(-1.0 / 6.0) * d + T(5.0 / 6.0) * c + T(1.0 / 3.0) * b;
+  T p2 = T(1.0 / 3.0) * c + T(5.0 / 6.0) * b - T(1.0 / 6.0) * a;
+  T a0 = T(0.1) * w.i2, a1 = T(0.6) * w.i1, a2 = T(0.3) * w.i0;
   return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
 }
 
@@ -894,13 +937,28 @@ __device__ __forceinline__ void flux_x23_lines(const DevView& v, unsigned blk) {
 #pragma unroll
     for (int m = 0; m < 6; ++m) q[n][m] = T(__ldg(W + n * vs + (long)(c0 - 3 + m) * s));
   }
+#if EXO_X23_SHARED_BETA
+  WenoCell<T> wprev[5];  // indicators of cell c - 1
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    if (n >= nv) break;
+    wprev[n] = weno_cell<T>(q[n][0], q[n][1], q[n][2], q[n][3], q[n][4]);
+  }
+#endif
   for (int c = c0; c <= c1 + 1; ++c) {
     T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       if (n >= nv) break;
+#if EXO_X23_SHARED_BETA
+      const WenoCell<T> wcur = weno_cell<T>(q[n][1], q[n][2], q[n][3], q[n][4], q[n][5]);
+      wl[n] = weno_right<T>(wprev[n], q[n][0], q[n][1], q[n][2], q[n][3], q[n][4]);
+      wr[n] = weno_left<T>(wcur, q[n][1], q[n][2], q[n][3], q[n][4], q[n][5]);
+      wprev[n] = wcur;
+#else
       wl[n] = weno5<T>(q[n][4], q[n][3], q[n][2], q[n][1], q[n][0]);  // weno_r of cell c-1
       wr[n] = weno5<T>(q[n][1], q[n][2], q[n][3], q[n][4], q[n][5]);  // weno_l of cell c
+#endif
     }
     const int k = dir == 1 ? v.ks + a : c;
     const int j = dir == 1 ? c : v.js + a;
