@@ -2139,9 +2139,12 @@ constexpr int IMPL_MAX_THREADS = 128;
 #ifndef EXO_IMPL_MINB
 #define EXO_IMPL_MINB 2  // resident 128-thread blocks per SM the register budget is sized for
 #endif
-// the mixed build's solve fits 204 registers without spilling: 5 blocks of
-// 64 columns per SM instead of 4 (measured 18 % faster at 6x192^2x96); the
-// FP64 build spills there and keeps the full register file
+// the mixed build's solve is capped at 204 registers (8 bytes of spill),
+// measured 18 % faster at 6x192^2x96 than uncapped; with the per-warp
+// register rounding that still leaves 4 blocks of 64 columns per SM (8 warps).
+// 200 registers fit a fifth block but measured 1-3 % slower, so the forward
+// sweep is bound by its FP64 dependency chains, not by resident warps.  The
+// FP64 build spills below 254 registers and keeps the full register file.
 #if !defined(EXO_IMPL_MAXNREG) && EXO_MIXED
 #define EXO_IMPL_MAXNREG 204
 #endif
