@@ -1763,6 +1763,9 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
     c0 = cp;
     cur = nxt;
   }
+  // the last level's prefetch (unused) must land before the back substitution
+  // reuses this thread's slots of shared memory
+  cp_async_wait_all();
 #if EXO_IMPL_BWD_SMEM
   // back substitution: delta_i -= (A c)_i delta_{i+1}.  The factors and the
   // state of the next two levels are copied asynchronously into this
