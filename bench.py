@@ -238,7 +238,8 @@ def alg_bytes_per_cell(kernel, precision, implicit_flag=9):
     # mixed flux_x23: one thread per line of faces reads every cell once per direction
     x23 = 10 * t + 10 * t if precision == 1 else 5 * t + 10 * t
     factors = 480 if implicit_flag & 8 else 192
-    return {"flux_x1": 40 + 5 * t, "flux_x23": x23, "update": 120 + 15 * t + 80,
+    # the x1 fluxes are FP64 in both builds (5 values of 8 bytes per cell)
+    return {"flux_x1": 40 + 40, "flux_x23": x23, "update": 120 + 40 + 10 * t + 80,
             "implicit": 160 + factors, "prim_ghost": 80 + (20 if precision == 1 else 0),
             "other": 0}[kernel]
 

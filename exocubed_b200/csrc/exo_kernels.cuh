@@ -36,6 +36,14 @@
 #ifndef EXO_X23_LINES
 #define EXO_X23_LINES EXO_MIXED
 #endif
+// 1: the x1 (radial) Riemann flux, its storage and its divergence stay FP64
+// in the mixed build (the reconstruction of the perturbations stays FP32):
+// the radial momentum flux carries the full hydrostatic pressure, whose
+// difference across a cell is a few per cent of it, so FP32 storage of the
+// flux loses the balance against gravity to cancellation
+#ifndef EXO_X1_FLUX64
+#define EXO_X1_FLUX64 EXO_MIXED
+#endif
 // 1: the sliding window computes each cell's WENO smoothness indicators once
 // for both of its faces (mixed build; the FP64 build keeps weno5's order)
 #ifndef EXO_X23_SHARED_BETA
@@ -82,6 +90,9 @@ template <> __device__ __forceinline__ double* flux_array<double>(const DevView&
 template <> __device__ __forceinline__ float* flux_array<float>(const DevView& v, int d) {
   return v.flux32[d];
 }
+// the type of the x1 face fluxes for a build whose flux type is T
+template <class T>
+using X1Flux = std::conditional_t<(EXO_X1_FLUX64 != 0), double, T>;
 template <class T> __device__ __forceinline__ const T* prim_array(const DevView& v);
 template <> __device__ __forceinline__ const double* prim_array<double>(const DevView& v) {
   return v.w;
@@ -748,7 +759,8 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
 #endif
     __syncthreads();
   }
-  T* F = flux_array<T>(v, 0);
+  using TF = X1Flux<T>;
+  TF* F = flux_array<TF>(v, 0);
   const float inv_faces = 1.f / (float)(L + 1);
   for (int t = threadIdx.x; t < ncb * (L + 1); t += blockDim.x) {
     int c, f;
@@ -756,15 +768,16 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
     const double* wc = WC(c);
     const double* psf = PSF(c);
     const int i = v.is + f;
-    FaceGeo<T> fg{T(0.), T(1.), T(s_cthp[c]), T(s_cosc[c])};
-    // perturbations are formed in FP64 above; WENO5 and the Riemann solve run in T
-    T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
+    FaceGeo<TF> fg{TF(0.), TF(1.), TF(s_cthp[c]), TF(s_cosc[c])};
+    // perturbations are formed in FP64 above; WENO5 runs in T, the restore in
+    // FP64 and the Riemann solve in TF
+    TF wl[5], wr[5], fx[5] = {TF(0.), TF(0.), TF(0.), TF(0.), TF(0.)};
     #pragma unroll
     for (int n = 0; n < 5; ++n) {
       if (n >= nv) break;
       const double* q = wc + n * nc1;
-      wl[n] = weno_r<T>(q, 1, i - 1);
-      wr[n] = weno_l<T>(q, 1, i);
+      wl[n] = TF(weno_r<T>(q, 1, i - 1));
+      wr[n] = TF(weno_l<T>(q, 1, i));
     }
     if (decomp) {
       // RestoreFromPerturbation (change_to_perturbation.cpp:159-222), in FP64
@@ -784,15 +797,15 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       if (dr < 0.) dr = dsf;
       dl += dsf;
       if (dl < 0.) dl = dsf;
-      wr[IPR] = T(xr);
-      wl[IPR] = T(xl);
-      wr[IDN] = T(dr);
-      wl[IDN] = T(dl);
+      wr[IPR] = TF(xr);
+      wl[IPR] = TF(xl);
+      wr[IDN] = TF(dr);
+      wl[IDN] = TF(dl);
     }
     // x1 runs for the ideal gas only: LMARS or HLLC
-    if (v.rsolver == EXO_RS_HLLC) riemann_hllc<T>(v.gamma, IVX, fg, wl, wr, fx);
-    else riemann_lmars<T>(v.gamma, IVX, wl, wr, fx);
-    T* Fc = F + (size_t)s_base[c] + i;
+    if (v.rsolver == EXO_RS_HLLC) riemann_hllc<TF>(v.gamma, IVX, fg, wl, wr, fx);
+    else riemann_lmars<TF>(v.gamma, IVX, wl, wr, fx);
+    TF* Fc = F + (size_t)s_base[c] + i;
     #pragma unroll
     for (int n = 0; n < 5; ++n) {
       if (n >= nv) break;
@@ -1023,20 +1036,21 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   const double* uin = v.u + c0;  // read here, written below
   const double* u1in = v.u1 + c0;
   const double* __restrict__ win = v.w + c0;
-  const T* __restrict__ F0 = flux_array<T>(v, 0) + c0;
+  const X1Flux<T>* __restrict__ F0 = flux_array<X1Flux<T>>(v, 0) + c0;
   const T* __restrict__ F1 = flux_array<T>(v, 1) + c0;
   const T* __restrict__ F2 = flux_array<T>(v, 2) + c0;
   // every input of the cell is requested before any is used
   double uu[5], u1v[5], wv[5];
-  T f0l[5], f0r[5], f1l[5], f1r[5], f2l[5], f2r[5];
+  X1Flux<T> f0l[5], f0r[5];
+  T f1l[5], f1r[5], f2l[5], f2r[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     if (n >= nv) break;
     uu[n] = uin[n * vs];
     u1v[n] = stage ? u1in[n * vs] : 0.;
     wv[n] = __ldg(win + n * vs);
-    f0l[n] = shallow ? T(0.) : __ldg(F0 + n * vs);
-    f0r[n] = shallow ? T(0.) : __ldg(F0 + n * vs + 1);
+    f0l[n] = shallow ? X1Flux<T>(0.) : __ldg(F0 + n * vs);
+    f0r[n] = shallow ? X1Flux<T>(0.) : __ldg(F0 + n * vs + 1);
     f1l[n] = __ldg(F1 + n * vs);
     f1r[n] = __ldg(F1 + n * vs + sj);
     f2l[n] = __ldg(F2 + n * vs);
@@ -1071,18 +1085,27 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   const double a3p = x1vi * dx2f3p * dx1fi;
   const double vol = dx1fi * d2 * d3 * x1vi * x1vi * s;
   double du[5];
-  // flux divergence in T; the conserved state accumulates in FP64
+  // flux divergence in T (the x1 part in FP64 where its fluxes are); the
+  // conserved state accumulates in FP64
   const T A1 = T(a1), A1p = T(a1p), A2 = T(a2), A2p = T(a2p), A3 = T(a3), A3p = T(a3p);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     if (n >= nv) break;
-    T dflx = (A1p * f0r[n] - A1 * f0l[n]);
-    dflx += (A2p * f1r[n] - A2 * f1l[n]);
-    dflx += (A3p * f2r[n] - A3 * f2l[n]);
     double change;
     if constexpr (sizeof(T) == sizeof(double)) {
+      T dflx = (A1p * f0r[n] - A1 * f0l[n]);
+      dflx += (A2p * f1r[n] - A2 * f1l[n]);
+      dflx += (A3p * f2r[n] - A3 * f2l[n]);
       change = wght * dflx / vol;
+    } else if constexpr (sizeof(X1Flux<T>) == sizeof(double)) {
+      T d23 = (A2p * f1r[n] - A2 * f1l[n]);
+      d23 += (A3p * f2r[n] - A3 * f2l[n]);
+      const double d1 = a1p * f0r[n] - a1 * f0l[n];
+      change = wght * ((d1 + (double)d23) / vol);
     } else {
+      T dflx = (A1p * f0r[n] - A1 * f0l[n]);
+      dflx += (A2p * f1r[n] - A2 * f1l[n]);
+      dflx += (A3p * f2r[n] - A3 * f2l[n]);
       change = wght * (double)(dflx / T(vol));
     }
     if (shallow) {
