@@ -689,7 +689,61 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
   __syncthreads();
   const bool decomp = (v.grav != 0.);
   if (decomp) {
-    // Decomposition::ChangeToPerturbation (change_to_perturbation.cpp:39-157),
+    // Decomposition::ChangeToPerturbation (change_to_perturbation.cpp:39-157).
+#if EXO_MIXED
+    // The downward scan psf[i] = psf[i+1] + g rho_i dx1f_i as a suffix sum,
+    // one warp per column: each lane sums a chunk of levels, the lanes'
+    // sums are scanned with shuffles, then each lane fills its chunk (FP64
+    // throughout; only the order of the additions differs from the serial
+    // scan of the FP64 build)
+    {
+      const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
+      const int nwarps = (int)blockDim.x >> 5;
+      const int is = v.is, ie = v.ie;
+      const int chunk = (L + 31) >> 5;
+      const double grav = -v.grav;
+      for (int c = warp; c < ncb; c += nwarps) {
+        double* wc = WC(c);
+        double* psf = PSF(c);
+        const double* wd = wc + IDN * nc1;
+        const double* wp = wc + IPR * nc1;
+        const int m0 = is + lane * chunk, m1 = min(m0 + chunk, ie + 1);
+        double part = 0.;
+        for (int m = m0; m < m1; ++m) part += grav * wd[m] * v.dx1f[m];
+        // sum of the parts of the lanes above this one
+        double above = part;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const double y = __shfl_down_sync(0xffffffffu, above, off);
+          if (lane + off < 32) above += y;
+        }
+        above = __shfl_down_sync(0xffffffffu, above, 1);
+        if (lane == 31) above = 0.;
+        double top = 0.;
+        if (lane == 0) {
+          const double RdTv = wp[ie] / wd[ie];
+          top = wp[ie] * exp(-grav * v.dx1f[ie] / (2 * RdTv));
+          psf[ie + 1] = top;
+        }
+        top = __shfl_sync(0xffffffffu, top, 0);
+        double run = top + above;
+        for (int m = m1 - 1; m >= m0; --m) {
+          run += grav * wd[m] * v.dx1f[m];
+          psf[m] = run;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          for (int i = 1; i <= G; ++i) psf[is - i] = psf[is + i];
+          for (int i = 1; i <= G; ++i) psf[ie + i + 1] = psf[ie + 1 - i];
+          double gammad = v.gamma, fsig = 1., feps = 1.;
+          double gam = 1. + (gammad - 1.) * feps / fsig;
+          double ent = log(wp[is]) - gam * log(wd[is]);
+          s_gam[c] = gam;
+          s_expf[c] = exp(-ent / gam);
+        }
+      }
+    }
+#else
     // one thread per column for the downward scan
     if ((int)threadIdx.x < ncb) {
       const int c = threadIdx.x;
@@ -710,6 +764,7 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       s_gam[c] = gam;
       s_expf[c] = exp(-ent / gam);
     }
+#endif
     __syncthreads();
     const float inv_nc1 = 1.f / (float)nc1;
 #if EXO_MIXED
