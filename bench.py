@@ -7,15 +7,17 @@ Default workload (c3): the exo3 dry ideal-gas atmosphere, 6 panels x 192 x
 A "step" is one SSPRK(3,3) step of the whole atmosphere; one cell-update is
 one interior cell advanced one step (6*N*N*L per step).
 
-The line's value is the mixed-precision path (FP32 reconstruction, Riemann
-fluxes and flux divergence; FP64 decomposition, implicit solve and state);
+The line's value is the mixed-precision path (FP32 reconstruction, x2/x3
+Riemann fluxes and their divergence; FP64 decomposition, x1 fluxes,
+implicit solve, state and RK accumulation; --precision 2 also runs the
+implicit solve's blocks in FP32);
 "fp64" is the plain FP64 path on the same workload in the same run;
 "accuracy" compares the two after --accuracy-steps steps; "serving" is a
 short continuous-batching sample (ensemble-member requests, p50/p99 latency)
 with the FP64 one-at-a-time path beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c1|c2|c2s|c3|c4] [--precision 0|1]
+                  [--workload c1|c2|c2s|c3|c4] [--precision 0|1|2]
   python bench.py --accuracy 1000            (mixed vs FP64 after 1000 steps)
   python bench.py --serve 10,100,2000        (serving sweep, one line per rate)
 
@@ -60,9 +62,10 @@ def workload_config(name, precision=0):
     if _IMP[0] is not None and cfg["eqn"] == 1:
         cfg = dict(cfg, implicit_flag=_IMP[0])
         desc = desc.replace("implicit(9)", f"implicit({_IMP[0]})")
-    if precision == 1:
-        cfg = dict(cfg, precision=1)
-        desc = desc.replace("FP64", "mixed FP32/FP64")
+    if precision in (1, 2):
+        cfg = dict(cfg, precision=precision)
+        desc = desc.replace("FP64", "mixed FP32/FP64" + (" (FP32 implicit blocks)"
+                                                         if precision == 2 else ""))
     return cfg, desc
 
 
@@ -231,16 +234,18 @@ def run_cpu(workload, steps, warmup):
 # -------------------------------------------------------------- our arm --
 # algorithmic DRAM bytes per interior cell and launch, by kernel and flux type
 # (each array element read or written once; the implicit solve's factors
-# (A c)_i and delta_i, 30 doubles per level with the full correction and 12
-# with the partial one, are written and read back)
+# (A c)_i and delta_i, 30 values per level with the full correction and 12
+# with the partial one, FP32 at precision 2 and FP64 otherwise, are written
+# and read back)
 def alg_bytes_per_cell(kernel, precision, implicit_flag=9):
-    t = 4 if precision == 1 else 8
+    mixed = precision in (1, 2)
+    t = 4 if mixed else 8
     # mixed flux_x23: one thread per line of faces reads every cell once per direction
-    x23 = 10 * t + 10 * t if precision == 1 else 5 * t + 10 * t
-    factors = 480 if implicit_flag & 8 else 192
+    x23 = 10 * t + 10 * t if mixed else 5 * t + 10 * t
+    factors = (30 if implicit_flag & 8 else 12) * (4 if precision == 2 else 8) * 2
     # the x1 fluxes are FP64 in both builds (5 values of 8 bytes per cell)
     return {"flux_x1": 40 + 40, "flux_x23": x23, "update": 120 + 40 + 10 * t + 80,
-            "implicit": 160 + factors, "prim_ghost": 80 + (20 if precision == 1 else 0),
+            "implicit": 160 + factors, "prim_ghost": 80 + (20 if mixed else 0),
             "other": 0}[kernel]
 
 
@@ -312,11 +317,9 @@ def measure_e2e(cfg, state, steps, pg):
     return ms, state.nbytes
 
 
-def accuracy(cfg, state, steps):
-    """Mixed precision against the FP64 path on the same state, the FP64
-    path's first CFL step held fixed: relative L2 / Linf per field."""
-    import numpy as np
-
+def fp64_reference(cfg, state, steps):
+    """(dt, interior primitives) of the FP64 path after steps steps of its
+    first CFL step."""
     from exocubed_b200 import workloads as W
     from exocubed_b200.atmosphere import CubedSphereAtmosphere
     ref = CubedSphereAtmosphere(dict(cfg, precision=0))
@@ -325,7 +328,19 @@ def accuracy(cfg, state, steps):
     ref.step(steps, dt)
     wr = W.interior(ref.primitive())
     ref.close()
-    mix = CubedSphereAtmosphere(dict(cfg, precision=1))
+    return dt, wr
+
+
+def accuracy(cfg, state, steps, precision=1, ref=None):
+    """A mixed precision (1 or 2) against the FP64 path on the same state,
+    the FP64 path's first CFL step held fixed: relative L2 / Linf per field.
+    ref: fp64_reference(cfg, state, steps), computed here when None."""
+    import numpy as np
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
+    dt, wr = ref if ref is not None else fp64_reference(cfg, state, steps)
+    mix = CubedSphereAtmosphere(dict(cfg, precision=precision))
     mix.set_primitive(state)
     mix.step(steps, dt)
     wm = W.interior(mix.primitive())
@@ -342,7 +357,8 @@ def accuracy(cfg, state, steps):
                      else float(np.linalg.norm(d)),
                      "linf": float(np.abs(d).max()),
                      "rel_linf": float(np.abs(d).max() / max(np.abs(wr[:, n]).max(), 1e-300))}
-    return {"steps": steps, "dt": dt, "simulated_seconds": dt * steps, "fields": err,
+    return {"steps": steps, "precision": precision, "dt": dt, "simulated_seconds": dt * steps,
+            "fields": err,
             "state_valid": invalid == 0}
 
 
@@ -390,6 +406,11 @@ def run_ours(args):
     if prec == 1 and not args.no_fp64:
         plain = measure_path(dict(cfg, precision=0), state, args.steps, args.warmup, pg, local,
                              False)
+    # the same workload with the implicit solve's blocks in FP32 as well
+    f32s = None
+    if prec == 1 and not args.no_f32_solve and cfg["eqn"] == 1 and cfg["implicit_flag"] & 1:
+        f32s = measure_path(dict(cfg, precision=2), state, args.steps, args.warmup, pg, local,
+                            False)
     value = world * cells * args.steps / (main["ms"] / 1e3)
     e2e_value = world * cells * args.steps / (ms_e2e / 1e3)
 
@@ -405,7 +426,9 @@ def run_ours(args):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        key = f"{dom}:{'mixed' if prec == 1 else 'fp64'}"
+        key = f"{dom}:{'mixed' if prec in (1, 2) else 'fp64'}"
+        if dom == "implicit" and prec == 2:
+            key += "_f32_solve"
         if dom == "implicit" and not iflag & 8:
             key += ":partial"
         tr = json.load(open(tp)).get(key)
@@ -415,9 +438,12 @@ def run_ours(args):
 
     extra = {}
     if rank == 0 and world == 1:
-        if args.accuracy_steps > 0 and prec == 1:
-            extra["accuracy"] = accuracy(workload_config(args.workload, 0)[0], state,
-                                         args.accuracy_steps)
+        if args.accuracy_steps > 0 and prec in (1, 2):
+            c0 = workload_config(args.workload, 0)[0]
+            ref = fp64_reference(c0, state, args.accuracy_steps)
+            extra["accuracy"] = accuracy(c0, state, args.accuracy_steps, prec, ref)
+            if f32s is not None:
+                extra["accuracy_f32_solve"] = accuracy(c0, state, args.accuracy_steps, 2, ref)
         if args.serve_requests > 0:
             extra["serving"] = serving_sample(args.serve_rate, args.serve_requests,
                                               args.serve_steps, not args.no_fp64_baseline)
@@ -446,6 +472,13 @@ def run_ours(args):
             "value": world * cells * args.steps / (plain["ms"] / 1e3),
             "ms_per_step": plain["ms"] / args.steps,
             "note": "the plain FP64 path on the same workload, same run"},
+        "mixed_f32_solve": None if f32s is None else {
+            "value": world * cells * args.steps / (f32s["ms"] / 1e3),
+            "ms_per_step": f32s["ms"] / args.steps,
+            "accuracy_rel_l2": {k: v["rel_l2"] for k, v in
+                                extra.get("accuracy_f32_solve", {}).get("fields", {}).items()},
+            "note": "--precision 2 on the same workload, same run: the implicit solve's blocks "
+                    "in FP32 as well (state and corrected update FP64)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": dom,
                      "peak_kind": peak_kind,
@@ -663,7 +696,8 @@ def run_accuracy(args):
     """Mixed precision against the FP64 path after args.accuracy steps."""
     import torch  # noqa: F401  (CUDA context)
     cfg, desc = workload_config(args.workload, 0)
-    res = accuracy(cfg, make_state(cfg, seed=0), args.accuracy)
+    res = accuracy(cfg, make_state(cfg, seed=0), args.accuracy,
+                   args.precision if args.precision in (1, 2) else 1)
     res["workload"] = desc.replace("FP64", "mixed vs FP64")
     print(json.dumps({"accuracy": res}))
 
@@ -709,9 +743,12 @@ def main():
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--no-fp64-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tiles")
-    ap.add_argument("--precision", type=int, default=1, choices=[0, 1],
-                    help="0: FP64; 1: FP32 reconstruction/Riemann/divergence, FP64 rest")
+    ap.add_argument("--precision", type=int, default=1, choices=[0, 1, 2],
+                    help="0: FP64; 1: mixed (FP32 reconstruction, x2/x3 Riemann and "
+                         "divergence); 2: mixed with FP32 implicit blocks")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
+    ap.add_argument("--no-f32-solve", action="store_true",
+                    help="skip the leg with FP32 implicit blocks (--precision 2)")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="steps of the mixed-vs-FP64 error check in the bench line (0: none)")
     ap.add_argument("--serve-requests", type=int, default=8,

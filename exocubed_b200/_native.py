@@ -16,7 +16,7 @@ EXO_EQN_SHALLOW_YZ, EXO_EQN_IDEAL = 0, 1
 (EXO_OK, EXO_ERR_ARG, EXO_ERR_SHAPE, EXO_ERR_CUDA, EXO_ERR_NONFINITE, EXO_ERR_TIMEOUT,
  EXO_ERR_NOGPU, EXO_ERR_CAPACITY) = range(8)
 EXO_RS_ROE_SHALLOW, EXO_RS_LMARS, EXO_RS_HLLC, EXO_RS_LMARS_SHALLOW = 0, 1, 2, 3
-EXO_PREC_FP64, EXO_PREC_MIXED = 0, 1
+EXO_PREC_FP64, EXO_PREC_MIXED, EXO_PREC_MIXED_F32_SOLVE = 0, 1, 2
 EXO_CORIOLIS_NONE, EXO_CORIOLIS_W92, EXO_CORIOLIS_3D = 0, 1, 2
 EXO_FORCING_NONE, EXO_FORCING_HS94 = 0, 1
 NGHOST = 3

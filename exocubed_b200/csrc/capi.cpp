@@ -26,7 +26,7 @@ using exo::DevView;
 
 // the step launchers of the context's arithmetic build
 #define STEP(name, ...) \
-  (c->v.precision == EXO_PREC_MIXED ? exo::mixed::name(__VA_ARGS__) : exo::fp64::name(__VA_ARGS__))
+  (exo::mixed_build(c->v.precision) ? exo::mixed::name(__VA_ARGS__) : exo::fp64::name(__VA_ARGS__))
 
 namespace {
 
@@ -232,8 +232,8 @@ bool validate_config(const exo_config& c, std::string* err) {
     return bad("shallow water needs the Roe or LMARS shallow-water solver");
   if (!shallow && c.rsolver != EXO_RS_LMARS && c.rsolver != EXO_RS_HLLC)
     return bad("the ideal gas needs the LMARS or HLLC solver");
-  if (c.precision != EXO_PREC_FP64 && c.precision != EXO_PREC_MIXED)
-    return bad("precision must be EXO_PREC_FP64 or EXO_PREC_MIXED");
+  if (c.precision != EXO_PREC_FP64 && !mixed_build(c.precision))
+    return bad("precision must be EXO_PREC_FP64, EXO_PREC_MIXED or EXO_PREC_MIXED_F32_SOLVE");
   if (!shallow && (c.implicit_flag & ~9))
     return bad("implicit_flag: only bits 1 (x1) and 8 (full 5x5 instead of partial 3x3) are supported");
   if (!(c.cfl > 0.) || !(c.gamma > 1.) || !(c.x1max > c.x1min))
@@ -267,7 +267,7 @@ size_t view_footprint(const exo_config& c) {
   size_t nd = shallow ? 5 : 7;  // u, w, u1, flux x2, x3 (+ du, flux x1)
   size_t bytes = nd * elems * sizeof(double);
   if (!shallow && (c.implicit_flag & 1)) bytes += implicit_scratch_doubles(c.N, c.L) * sizeof(double);
-  if (c.precision == EXO_PREC_MIXED) bytes += (shallow ? 3 : 4) * elems * sizeof(float);
+  if (mixed_build(c.precision)) bytes += (shallow ? 3 : 4) * elems * sizeof(float);
   bytes += (size_t)NGEO2D * 6 * nc2 * nc2 * sizeof(double);       // metric
   bytes += (size_t)6 * nc2 * nc2 * sizeof(int);                   // ghost map
   bytes += (size_t)6 * 12 * c.N * sizeof(GhostEntry) + (size_t)24 * c.N * sizeof(EdgeEntry);
@@ -366,7 +366,7 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
         !alloc((void**)&v.scratch, implicit_scratch_doubles(cfg.N, cfg.L) * sizeof(double), false))
       return EXO_ERR_CAPACITY;
   }
-  if (cfg.precision == EXO_PREC_MIXED) {
+  if (mixed_build(cfg.precision)) {
     if (!alloc((void**)&v.w32, fb, true) || !alloc((void**)&v.flux32[1], fb, true) ||
         !alloc((void**)&v.flux32[2], fb, true))
       return EXO_ERR_CAPACITY;
@@ -448,7 +448,7 @@ void member_blocks(const DevView& v, const int* t, unsigned b[BK_COUNT]) {
   auto nb = [](size_t n, int th) { return (unsigned)((n + th - 1) / th); };
   b[BK_X1] = shallow ? 0u : nb((size_t)6 * v.N * v.N, t[BK_X1]);  // t[BK_X1] columns per block
   // one thread per line of faces or per face, as the build chose
-  const bool lines = v.precision == EXO_PREC_MIXED ? mixed::x23_lines() : fp64::x23_lines();
+  const bool lines = mixed_build(v.precision) ? mixed::x23_lines() : fp64::x23_lines();
   b[BK_X23] = lines ? nb((size_t)2 * 6 * v.N * v.L, t[BK_X23])
                     : nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, t[BK_X23]);
   b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, t[BK_UPDATE]);

@@ -70,7 +70,7 @@ int cuda_efail(cudaError_t e, const char* what) {
 
 int launch_single(int precision, int which, const DevView& v, void* st, double arg,
                   const double* src) {
-  bool mixed = precision == EXO_PREC_MIXED;
+  bool mixed = exo::mixed_build(precision);
   switch (which) {
     case 0: return mixed ? exo::mixed::launch_p2c_interior(v, src, st)
                          : exo::fp64::launch_p2c_interior(v, src, st);
@@ -136,12 +136,13 @@ int rebuild(exo_ensemble* e) {
   pl.x1_smem = x1_smem;
   for (int k = 0; k < exo::BK_COUNT; ++k) pl.threads[k] = e->tiles.t[k];
   pl.max_nc1 = max_nc1;
+  pl.precision = e->precision;
   // count the kernel nodes of one step
   int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 + (tot[exo::BK_IMPLICIT] ? 1 : 0) + 1;
   e->launches_per_step = 3 * per_stage + (tot[exo::BK_ROUNDTRIP] ? 1 : 0) + 1 + 1;
   cudaGraph_t graph;
   ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = e->precision == EXO_PREC_MIXED ? exo::mixed::launch_batched_step(pl, e->stream)
+  int rc = exo::mixed_build(e->precision) ? exo::mixed::launch_batched_step(pl, e->stream)
                                           : exo::fp64::launch_batched_step(pl, e->stream);
   cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
   if (rc) return efail(EXO_ERR_CUDA, "batched step capture failed");
@@ -172,8 +173,9 @@ int exo_ensemble_footprint(const exo_config* cfg, size_t* bytes) {
 int exo_ensemble_create(int precision, int capacity, size_t budget_bytes, exo_ensemble** out) {
   if (!out) return efail(EXO_ERR_ARG, "NULL argument");
   *out = nullptr;
-  if (precision != EXO_PREC_FP64 && precision != EXO_PREC_MIXED)
-    return efail(EXO_ERR_ARG, "precision must be EXO_PREC_FP64 or EXO_PREC_MIXED");
+  if (precision != EXO_PREC_FP64 && !exo::mixed_build(precision))
+    return efail(EXO_ERR_ARG,
+                 "precision must be EXO_PREC_FP64, EXO_PREC_MIXED or EXO_PREC_MIXED_F32_SOLVE");
   if (capacity < 1 || capacity > 4096) return efail(EXO_ERR_ARG, "capacity must be in [1, 4096]");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)

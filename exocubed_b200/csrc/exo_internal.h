@@ -149,6 +149,7 @@ struct BatchPlan {
   size_t x1_smem;                // its dynamic shared memory
   int threads[BK_COUNT];         // tiles of the other kernels
   int max_nc1;                   // largest nc1 of the members (radial tables in shared memory)
+  int precision;                 // EXO_PREC_* of every member
 };
 // Threads per block ("tile") of each batched kernel by BatchKind.  BK_X1
 // takes one radial column per block (its size follows L) and ignores its
@@ -168,9 +169,13 @@ constexpr int X1_MAX_COLUMNS = 8;
 #else
 #define EXO_HD
 #endif
+// the precisions stepped by the mixed build (exo::mixed)
+EXO_HD inline bool mixed_build(int precision) {
+  return precision == EXO_PREC_MIXED || precision == EXO_PREC_MIXED_F32_SOLVE;
+}
 EXO_HD inline int x1_column_doubles(const DevView& v) {
   int faces = v.nc1 + 1;
-  return v.nv * v.nc1 + (v.precision == EXO_PREC_MIXED ? 3 : 1) * faces;
+  return v.nv * v.nc1 + (mixed_build(v.precision) ? 3 : 1) * faces;
 }
 inline int x1_cols(const DevView& v) { return v.tiles[BK_X1] > 0 ? v.tiles[BK_X1] : 1; }
 inline size_t x1_smem_bytes(const DevView& v) {

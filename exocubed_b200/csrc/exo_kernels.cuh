@@ -64,6 +64,18 @@ namespace exo {
 namespace EXO_KNS {
 namespace {
 
+// the implicit solve's block arithmetic is FP64 or FP32 (template argument
+// R): EXO_PREC_MIXED_F32_SOLVE builds and factors its blocks and keeps its
+// back-substitution factors in FP32, EXO_PREC_MIXED and the FP64 build in
+// FP64.  The state, the explicit update it corrects and the corrected state
+// are FP64 in every case.  At the solver's time steps (vertical acoustic
+// Courant numbers of tens) FP32 blocks change a corrected update by a few
+// 1e-7 of itself.
+__device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
+__device__ __forceinline__ double abs_r(double x) { return fabs(x); }
+__device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+
 constexpr double TINY_NUMBER = 1.0e-20;
 constexpr double WENO_EPS = 1.0e-7;
 
@@ -1324,17 +1336,18 @@ __host__ __device__ constexpr bool ri_nz(int r, int c) {
 
 // One cell of a column, velocities projected (v2 += v3 cos, v3 *= sin): the
 // primitives and the two derived quantities of its flux Jacobian.
+template <class R>
 struct ColCell {
-  double rho, v1, v2, v3, p, s2, hr;  // s2 = |v|^2, hr = (g+1)/g * p/rho (g = gamma-1)
+  R rho, v1, v2, v3, p, s2, hr;  // s2 = |v|^2, hr = (g+1)/g * p/rho (g = gamma-1)
 };
 
 // entry (r, q) of dF/dq at a cell, in the reference's expression order
-template <int r, int q>
-__device__ __forceinline__ double fj_entry(const ColCell& c, double gm1) {
-  if constexpr (r == 0) return 1.;
+template <int r, int q, class R>
+__device__ __forceinline__ R fj_entry(const ColCell<R>& c, R gm1) {
+  if constexpr (r == 0) return R(1);
   else if constexpr (r == 1) {
     if constexpr (q == 0) return gm1 * c.s2 / 2 - c.v1 * c.v1;
-    else if constexpr (q == 1) return (2. - gm1) * c.v1;
+    else if constexpr (q == 1) return (R(2) - gm1) * c.v1;
     else if constexpr (q == 2) return -gm1 * c.v2;
     else if constexpr (q == 3) return -gm1 * c.v3;
     else return gm1;
@@ -1387,40 +1400,42 @@ __device__ __forceinline__ void unroll(F&& f) {
 // value is the same; at most the sign of an exact zero differs).  Mixed
 // build: the same matrix as |u| I + (|u-c|-|u|) r0 l0^T + (|u+c|-|u|) r2 l2^T
 // (the three |u| eigenvalues coincide), with shared reciprocals.
-__device__ __forceinline__ void abs_jacobian(const ColCell& L, const ColCell& R_, double gm1,
-                                             double gamma, double A[5][5]) {
-  double wl[5] = {L.rho, L.v1, L.v2, L.v3, L.p};
-  double wr[5] = {R_.rho, R_.v1, R_.v2, R_.v3, R_.p};
+template <class R>
+__device__ __forceinline__ void abs_jacobian(const ColCell<R>& L, const ColCell<R>& R_, R gm1,
+                                             R gamma, R A[5][5]) {
+  R wl[5] = {L.rho, L.v1, L.v2, L.v3, L.p};
+  R wr[5] = {R_.rho, R_.v1, R_.v2, R_.v3, R_.p};
 #if EXO_MIXED
-  double sqrtdl = sqrt(wl[IDN]), sqrtdr = sqrt(wr[IDN]);
-  double isdlpdr = 1.0 / (sqrtdl + sqrtdr);
-  double isl = isdlpdr / sqrtdl, isr = isdlpdr / sqrtdr;
-  double rr = sqrtdl * sqrtdr;
-  double u = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
-  double v = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
-  double w = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
-  double inv_gm1 = 1. / gm1;
-  double el = wl[IPR] * inv_gm1 + 0.5 * wl[IDN] * L.s2;
-  double er = wr[IPR] * inv_gm1 + 0.5 * wr[IDN] * R_.s2;
-  double hbar = (el + wl[IPR]) * isl + (er + wr[IPR]) * isr;
-  double ke = 0.5 * (u * u + v * v + w * w);
-  double p = (hbar - ke) * (gm1 / (gm1 + 1.)) * rr;
-  double irr = 1. / rr;
-  double cs = sqrt(gamma * p * irr);
-  double hp = (gm1 + 1.) * inv_gm1 * p * irr;
-  double h = hp + ke;
-  double ihp = 1. / hp, i2hp = 0.5 * ihp, i2cshp = i2hp / cs;
-  double au = fabs(u), al = fabs(u - cs) - au, ar = fabs(u + cs) - au;
-  double l0[5] = {al * (cs * ke + u * hp) * i2cshp, al * (-hp - cs * u) * i2cshp, -al * v * i2hp,
-                  -al * w * i2hp, al * i2hp};
-  double l2[5] = {ar * (cs * ke - u * hp) * i2cshp, ar * (hp - cs * u) * i2cshp, -ar * v * i2hp,
-                  -ar * w * i2hp, ar * i2hp};
-  double r0[5] = {1., u - cs, v, w, h - u * cs};
-  double r2[5] = {1., u + cs, v, w, h + u * cs};
+  const R one = R(1), half = R(0.5);
+  R sqrtdl = sqrt_r(wl[IDN]), sqrtdr = sqrt_r(wr[IDN]);
+  R isdlpdr = one / (sqrtdl + sqrtdr);
+  R isl = isdlpdr / sqrtdl, isr = isdlpdr / sqrtdr;
+  R rr = sqrtdl * sqrtdr;
+  R u = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
+  R v = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
+  R w = (sqrtdl * wl[IVZ] + sqrtdr * wr[IVZ]) * isdlpdr;
+  R inv_gm1 = one / gm1;
+  R el = wl[IPR] * inv_gm1 + half * wl[IDN] * L.s2;
+  R er = wr[IPR] * inv_gm1 + half * wr[IDN] * R_.s2;
+  R hbar = (el + wl[IPR]) * isl + (er + wr[IPR]) * isr;
+  R ke = half * (u * u + v * v + w * w);
+  R p = (hbar - ke) * (gm1 / (gm1 + one)) * rr;
+  R irr = one / rr;
+  R cs = sqrt_r(gamma * p * irr);
+  R hp = (gm1 + one) * inv_gm1 * p * irr;
+  R h = hp + ke;
+  R ihp = one / hp, i2hp = half * ihp, i2cshp = i2hp / cs;
+  R au = abs_r(u), al = abs_r(u - cs) - au, ar = abs_r(u + cs) - au;
+  R l0[5] = {al * (cs * ke + u * hp) * i2cshp, al * (-hp - cs * u) * i2cshp, -al * v * i2hp,
+              -al * w * i2hp, al * i2hp};
+  R l2[5] = {ar * (cs * ke - u * hp) * i2cshp, ar * (hp - cs * u) * i2cshp, -ar * v * i2hp,
+              -ar * w * i2hp, ar * i2hp};
+  R r0[5] = {one, u - cs, v, w, h - u * cs};
+  R r2[5] = {one, u + cs, v, w, h + u * cs};
 #pragma unroll
   for (int r = 0; r < 5; ++r)
 #pragma unroll
-    for (int c = 0; c < 5; ++c) A[r][c] = (r == c ? au : 0.) + r0[r] * l0[c] + r2[r] * l2[c];
+    for (int c = 0; c < 5; ++c) A[r][c] = (r == c ? au : R(0)) + r0[r] * l0[c] + r2[r] * l2[c];
 #else
   double prim[5];
   roe_average(prim, gm1, wl, wr);
@@ -1465,8 +1480,9 @@ __device__ __forceinline__ void abs_jacobian(const ColCell& L, const ColCell& R_
 // the order 1, 4, 2, 3, 0, threshold row swaps packed 3 bits per step): y
 // holds the right-hand side with its rows in natural order on entry and the
 // solution, unknowns in order, on exit.
-__device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const double (&idg)[5],
-                                              unsigned perm, bool swapped, double* y) {
+template <class R>
+__device__ __forceinline__ void lu_solve_rows(const R (&t)[5][5], const R (&idg)[5],
+                                              unsigned perm, bool swapped, R* y) {
   constexpr int O[5] = {1, 4, 2, 3, 0};
   if (swapped) {
 #pragma unroll
@@ -1475,7 +1491,7 @@ __device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const dou
 #pragma unroll
       for (int r = k + 1; r < 5; ++r) {
         const bool sw = (pk == (unsigned)r);
-        const double a = y[O[k]], b = y[O[r]];
+        const R a = y[O[k]], b = y[O[r]];
         y[O[k]] = sw ? b : a;
         y[O[r]] = sw ? a : b;
       }
@@ -1485,10 +1501,10 @@ __device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const dou
   for (int r = 1; r < 5; ++r)
 #pragma unroll
     for (int k = 0; k < r; ++k) y[O[r]] -= t[O[r]][k] * y[O[k]];
-  double z[5];
+  R z[5];
 #pragma unroll
   for (int r = 4; r >= 0; --r) {
-    double acc = y[O[r]];
+    R acc = y[O[r]];
 #pragma unroll
     for (int q = r + 1; q < 5; ++q) acc -= t[O[r]][q] * z[q];
     z[r] = acc * idg[r];
@@ -1521,47 +1537,53 @@ __device__ __forceinline__ void lu_solve_rows(const double (&t)[5][5], const dou
 //                    for it beforehand (callers that only need d load nothing)
 //   io.wptr(i, n), io.duptr(i, n)  addresses of w and of the explicit update
 //                    du of level i (the inputs are prefetched through shared memory)
-//   sm               this thread's 60 contiguous doubles of shared memory
+//   sa, sp, ss       this thread's shared memory: entry e (0..49) of the two
+//                    face blocks at sa[e * ss], prefetch slot n (0..9) at
+//                    sp[n * ss]
 template <class IO>
-__device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_theta,
-                                                double sin_theta, double d2, double d3,
-                                                const double* x1f, const double* x1v,
+__device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, double* sp, int ss,
+                                                double cos_theta, double sin_theta, double d2,
+                                                double d3, const double* x1f, const double* x1v,
                                                 const double* dx1f, int is, int ie, double dt,
                                                 double gamma, double grav) {
+  using R = typename IO::Real;
+  using ColCell = exo::EXO_KNS::ColCell<R>;
   const double s = sin_theta;
-  const double gm1 = (gamma - 1.) * 1. / 1.;  // gmm1 of every cell; the face average equals it
-  const double gp = (gm1 + 1.) / gm1;
+  // gmm1 of every cell; the face average equals it
+  const R gm1 = R((gamma - 1.) * 1. / 1.);
+  const R gp = (gm1 + R(1)) / gm1;
+  const R gam = R(gamma);
 #if EXO_MIXED
-  const double rdt = 1. / dt;
-#else
-  const double rdt = 1. / dt;  // the reference's Dt = 1/dt, the same value every time
+  const R grv = R(grav);
 #endif
+  // the reference's Dt = 1/dt, the same value every time
+  const R rdt = R(1. / dt);
   auto cell = [&](const double* w) {
     ColCell c;
-    c.rho = w[IDN];
-    c.v1 = w[IVX];
-    c.v2 = w[IVY] + w[IVZ] * cos_theta;
-    c.v3 = w[IVZ] * sin_theta;
-    c.p = w[IPR];
+    c.rho = R(w[IDN]);
+    c.v1 = R(w[IVX]);
+    c.v2 = R(w[IVY] + w[IVZ] * cos_theta);
+    c.v3 = R(w[IVZ] * sin_theta);
+    c.p = R(w[IPR]);
     c.s2 = c.v1 * c.v1 + c.v2 * c.v2 + c.v3 * c.v3;
 #if EXO_MIXED
-    c.hr = gp * c.p * (1. / c.rho);
+    c.hr = gp * c.p * (R(1) / c.rho);
 #else
     c.hr = gp * c.p / c.rho;
 #endif
     return c;
   };
-  auto AMs = [&](int slot, int r, int q) -> double& { return sm[slot * 25 + r * 5 + q]; };
+  auto AMs = [&](int slot, int r, int q) -> R& { return sa[(slot * 25 + r * 5 + q) * ss]; };
 
   // prefetch slots: w(i+1) and du(i) of the next level, copied asynchronously
-  double* pw = sm + 50;
-  double* pdu = sm + 55;
+  auto pw = [&](int n) -> double& { return sp[n * ss]; };
+  auto pdu = [&](int n) -> double& { return sp[(5 + n) * ss]; };
   auto prefetch = [&](int iw, int idu) {
 #pragma unroll
-    for (int n = 0; n < 5; ++n) cp_async8(pw + n, io.wptr(iw, n));
+    for (int n = 0; n < 5; ++n) cp_async8(&pw(n), io.wptr(iw, n));
     if (idu >= 0) {
 #pragma unroll
-      for (int n = 0; n < 5; ++n) cp_async8(pdu + n, io.duptr(idu, n));
+      for (int n = 0; n < 5; ++n) cp_async8(&pdu(n), io.duptr(idu, n));
     }
     cp_async_commit();
   };
@@ -1572,8 +1594,8 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
   ColCell c0 = cell(raw);
   prefetch(is + 1, is);
   {
-    double A[5][5];
-    abs_jacobian(cm, c0, gm1, gamma, A);
+    R A[5][5];
+    abs_jacobian(cm, c0, gm1, gam, A);
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
@@ -1582,28 +1604,29 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
   // (A c)_{i-1} lives in registers, or in this thread's shared memory when
   // EXO_IMPL_AP_SMEM (fewer registers, more resident warps)
 #if EXO_IMPL_AP_SMEM
-  double* const aps = sm + 60;
+  static_assert(sizeof(R) == 8, "(A c)_{i-1} in shared memory takes the FP64 slice layout");
+  double* const aps = sa + 60;
 #define EXO_AP(r, q) aps[(r) * 5 + (q)]
 #else
-  double Ap[5][5];
+  R Ap[5][5];
 #define EXO_AP(r, q) Ap[r][q]
 #endif
-  double dp[5];  // delta_{i-1}
+  R dp[5];  // delta_{i-1}
   int cur = 0;
   for (int i = is; i <= ie; ++i) {
     cp_async_wait_all();
     double rhs[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-      raw[n] = pw[n];
-      rhs[n] = pdu[n];
+      raw[n] = pw(n);
+      rhs[n] = pdu(n);
     }
     ColCell cp = cell(raw);
     prefetch(i + 2, i < ie ? i + 1 : -1);
     const int nxt = cur ^ 1;
     {
-      double A[5][5];
-      abs_jacobian(c0, cp, gm1, gamma, A);
+      R A[5][5];
+      abs_jacobian(c0, cp, gm1, gam, A);
 #pragma unroll
       for (int r = 0; r < 5; ++r)
 #pragma unroll
@@ -1613,31 +1636,32 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
     const double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
     const double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
 #if EXO_MIXED
-    const double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
+    const double i2v = 0.5 / vol;
+    const R bl = R(aleft * i2v), cr = R(aright * i2v), dd = R((aright - aleft) * i2v);
 #endif
     const bool first = (i == is), last = (i == ie);
-    double x[5];
+    R x[5];
     // rows of a, b (and c at the top boundary), then of t = a - b (A c)_{i-1},
     // written over row r of |A|(i-1/2) once that row has been read; and x
-    unroll<5>([&](auto R) {
-      constexpr int r = decltype(R)::value;
-      double brow[5], trow[5];
+    unroll<5>([&](auto Row) {
+      constexpr int r = decltype(Row)::value;
+      R brow[5], trow[5];
       unroll<5>([&](auto Q) {
         constexpr int q = decltype(Q)::value;
-        const double am = AMs(cur, r, q), ap = AMs(nxt, r, q);
+        const R am = AMs(cur, r, q), ap = AMs(nxt, r, q);
 #if EXO_MIXED
-        double a = am * bl + ap * cr;
+        R a = am * bl + ap * cr;
         if constexpr (fj_nz(r, q)) a += dd * fj_entry<r, q>(c0, gm1);
         if constexpr (r == q) a += rdt;
-        if constexpr ((r == IVX && q == IDN) || (r == IEN && q == IVX)) a -= grav;
-        double bm = am;
+        if constexpr ((r == IVX && q == IDN) || (r == IEN && q == IVX)) a -= grv;
+        R bm = am;
         if constexpr (fj_nz(r, q)) bm += fj_entry<r, q>(cm, gm1);
-        double b = -bm * bl;
+        R b = -bm * bl;
         if (first) a += (q == IVX) ? -b : b;
         if (last) {
-          double cmv = ap;
+          R cmv = ap;
           if constexpr (fj_nz(r, q)) cmv -= fj_entry<r, q>(cp, gm1);
-          double c = -cmv * cr;
+          R c = -cmv * cr;
           a += (q == IVX) ? -c : c;
         }
 #else
@@ -1661,19 +1685,19 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
         trow[q] = a;
       });
 #if EXO_MIXED
-      x[r] = rhs[r] * rdt;
+      x[r] = R(rhs[r]) * rdt;
 #else
       x[r] = rhs[r] / dt;
 #endif
       if (!first) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-          double ba = brow[0] * EXO_AP(0, q);
+          R ba = brow[0] * EXO_AP(0, q);
 #pragma unroll
           for (int k = 1; k < 5; ++k) ba += brow[k] * EXO_AP(k, q);
           trow[q] = trow[q] - ba;
         }
-        double bd = brow[0] * dp[0];
+        R bd = brow[0] * dp[0];
 #pragma unroll
         for (int k = 1; k < 5; ++k) bd += brow[k] * dp[k];
         x[r] = x[r] - bd;
@@ -1681,17 +1705,17 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
 #pragma unroll
       for (int q = 0; q < 5; ++q) AMs(cur, r, q) = trow[q];
     });
-    double t[5][5];
+    R t[5][5];
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
       for (int q = 0; q < 5; ++q) t[r][q] = AMs(cur, r, q);
     // c_i column by column, from |A|(i+1/2) in shared memory and the upper cell
-    auto ccol = [&](auto Q, double* c) {
+    auto ccol = [&](auto Q, R* c) {
       constexpr int q = decltype(Q)::value;
-      unroll<5>([&](auto R) {
-        constexpr int r = decltype(R)::value;
-        double cmv = AMs(nxt, r, q);
+      unroll<5>([&](auto Row) {
+        constexpr int r = decltype(Row)::value;
+        R cmv = AMs(nxt, r, q);
 #if EXO_MIXED
         if constexpr (fj_nz(r, q)) cmv -= fj_entry<r, q>(cp, gm1);
         c[r] = -cmv * cr;
@@ -1710,19 +1734,19 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
     constexpr int O[5] = {1, 4, 2, 3, 0};
     unsigned perm = 0;  // 3 bits per step: the position swapped in
     bool swapped = false;
-    double idg[5];
+    R idg[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       if (k < 4) {
-        const double dk = fabs(t[O[k]][k]);
-        double best = dk;
+        const R dk = abs_r(t[O[k]][k]);
+        R best = dk;
         int piv = k;
 #pragma unroll
         for (int r = k + 1; r < 5; ++r) {
-          const double m = fabs(t[O[r]][k]);
+          const R m = abs_r(t[O[r]][k]);
           if (m > best) { best = m; piv = r; }
         }
-        if (dk < 0.1 * best) {
+        if (dk < R(0.1) * best) {
           swapped = true;
           perm |= (unsigned)piv << (3 * k);
 #pragma unroll
@@ -1730,7 +1754,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
             const bool sw = (piv == r);
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-              const double a = t[O[k]][q], b = t[O[r]][q];
+              const R a = t[O[k]][q], b = t[O[r]][q];
               t[O[k]][q] = sw ? b : a;
               t[O[r]][q] = sw ? a : b;
             }
@@ -1739,20 +1763,20 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
           perm |= (unsigned)k << (3 * k);
         }
       }
-      idg[k] = 1. / t[O[k]][k];
+      idg[k] = R(1) / t[O[k]][k];
 #pragma unroll
       for (int r = k + 1; r < 5; ++r) {
-        const double l = t[O[r]][k] * idg[k];
+        const R l = t[O[r]][k] * idg[k];
         t[O[r]][k] = l;
 #pragma unroll
         for (int q = k + 1; q < 5; ++q) t[O[r]][q] -= l * t[O[k]][q];
       }
     }
-    auto solve = [&](double* y) { lu_solve_rows(t, idg, perm, swapped, y); };
+    auto solve = [&](R* y) { lu_solve_rows(t, idg, perm, swapped, y); };
     solve(x);
     unroll<5>([&](auto Q) {
       constexpr int q = decltype(Q)::value;
-      double c[5];
+      R c[5];
       ccol(Q, c);
       solve(c);
 #pragma unroll
@@ -1854,8 +1878,9 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
     io.uload(ie, u_ie);
     io.ustore(ie, u_ie, dp);
   }
+  static_assert(sizeof(R) == 8, "the FP32 solve keeps its back substitution in registers");
   auto issue = [&](int i, int slot) {
-    double* d = sm + slot * 35;
+    double* d = sa + slot * 35;
 #pragma unroll
     for (int e = 0; e < 30; ++e) cp_async8(d + e, &io.scr(i - is, e));
     if (IO::kLoadsU) {
@@ -1871,7 +1896,7 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
   for (int i = ie - 1; i >= is; --i) {
     if (i - 1 >= is) cp_async_wait_one();
     else cp_async_wait_all();
-    const double* d = sm + slot * 35;
+    const double* d = sa + slot * 35;
     double cs[30], cu[5];
 #pragma unroll
     for (int e = 0; e < 30; ++e) cs[e] = d[e];
@@ -1897,9 +1922,16 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
 #else
   // back substitution: delta_i -= (A c)_i delta_{i+1}, software-pipelined:
   // the next level's scratch and state are in flight while this level ends
-  double cur_s[30], cur_u[5];
+  auto store = [&](int i, const double* u) {
+    double d[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) d[n] = dp[n];
+    io.ustore(i, u, d);
+  };
+  R cur_s[30];
+  double cur_u[5];
   io.uload(ie, cur_u);
-  io.ustore(ie, cur_u, dp);
+  store(ie, cur_u);
   if (ie > is) {
 #pragma unroll
     for (int e = 0; e < 30; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
@@ -1907,23 +1939,24 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
   }
 #pragma unroll 1
   for (int i = ie - 1; i >= is; --i) {
-    double nxt_s[30], nxt_u[5];
+    R nxt_s[30];
+    double nxt_u[5];
     if (i > is) {
 #pragma unroll
       for (int e = 0; e < 30; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
       io.uload(i - 1, nxt_u);
     }
-    double dl[5];
+    R dl[5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      double ad = cur_s[r * 5] * dp[0];
+      R ad = cur_s[r * 5] * dp[0];
 #pragma unroll
       for (int k = 1; k < 5; ++k) ad += cur_s[r * 5 + k] * dp[k];
       dl[r] = cur_s[25 + r] - ad;
     }
 #pragma unroll
     for (int r = 0; r < 5; ++r) dp[r] = dl[r];
-    io.ustore(i, cur_u, dp);
+    store(i, cur_u);
     if (i > is) {
 #pragma unroll
       for (int e = 0; e < 30; ++e) cur_s[e] = nxt_s[e];
@@ -1944,51 +1977,59 @@ __device__ __forceinline__ void implicit_column(IO& io, double* sm, double cos_t
 // correction corr is zero (its computation is commented out there).  Each
 // 3x3 block is inverted as its adjugate over its determinant, the closed form
 // a fixed-size 3x3 inverse takes.  Scratch per level: (A c)_i (9) and
-// delta_i (3).  IO and arguments as for implicit_column; sm holds the two
-// face blocks (18 doubles) and the prefetched w (5) and du (3) of a level.
+// delta_i (3).  IO and arguments as for implicit_column; the shared slices
+// hold the two face blocks (18 entries of sa) and the prefetched w (5) and
+// du (3) of a level (sp).
 template <class IO>
-__device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, double cos_theta,
-                                                        double sin_theta, double d2, double d3,
-                                                        const double* x1f, const double* x1v,
-                                                        const double* dx1f, int is, int ie,
-                                                        double dt, double gamma, double grav) {
+__device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Real* sa, double* sp, int ss,
+                                                        double cos_theta, double sin_theta,
+                                                        double d2, double d3, const double* x1f,
+                                                        const double* x1v, const double* dx1f,
+                                                        int is, int ie, double dt, double gamma,
+                                                        double grav) {
+  using R = typename IO::Real;
+  using ColCell = exo::EXO_KNS::ColCell<R>;
   constexpr int P[3] = {IDN, IVX, IEN};
   const double s = sin_theta;
-  const double gm1 = (gamma - 1.) * 1. / 1.;
-  const double gp = (gm1 + 1.) / gm1;
-  const double rdt = 1. / dt;
+  const R gm1 = R((gamma - 1.) * 1. / 1.);
+  const R gp = (gm1 + R(1)) / gm1;
+  const R gam = R(gamma);
+#if EXO_MIXED
+  const R grv = R(grav);
+#endif
+  const R rdt = R(1. / dt);
   auto cell = [&](const double* w) {
     ColCell c;
-    c.rho = w[IDN];
-    c.v1 = w[IVX];
-    c.v2 = w[IVY] + w[IVZ] * cos_theta;
-    c.v3 = w[IVZ] * sin_theta;
-    c.p = w[IPR];
+    c.rho = R(w[IDN]);
+    c.v1 = R(w[IVX]);
+    c.v2 = R(w[IVY] + w[IVZ] * cos_theta);
+    c.v3 = R(w[IVZ] * sin_theta);
+    c.p = R(w[IPR]);
     c.s2 = c.v1 * c.v1 + c.v2 * c.v2 + c.v3 * c.v3;
 #if EXO_MIXED
-    c.hr = gp * c.p * (1. / c.rho);
+    c.hr = gp * c.p * (R(1) / c.rho);
 #else
     c.hr = gp * c.p / c.rho;
 #endif
     return c;
   };
-  auto AMs = [&](int slot, int r, int q) -> double& { return sm[slot * 9 + r * 3 + q]; };
+  auto AMs = [&](int slot, int r, int q) -> R& { return sa[(slot * 9 + r * 3 + q) * ss]; };
   auto face = [&](const ColCell& lo, const ColCell& hi, int slot) {
-    double A[5][5];
-    abs_jacobian(lo, hi, gm1, gamma, A);
+    R A[5][5];
+    abs_jacobian(lo, hi, gm1, gam, A);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int q = 0; q < 3; ++q) AMs(slot, r, q) = A[P[r]][P[q]];
   };
-  double* pw = sm + 18;
-  double* pdu = sm + 23;
+  auto pw = [&](int n) -> double& { return sp[n * ss]; };
+  auto pdu = [&](int m) -> double& { return sp[(5 + m) * ss]; };
   auto prefetch = [&](int iw, int idu) {
 #pragma unroll
-    for (int n = 0; n < 5; ++n) cp_async8(pw + n, io.wptr(iw, n));
+    for (int n = 0; n < 5; ++n) cp_async8(&pw(n), io.wptr(iw, n));
     if (idu >= 0) {
 #pragma unroll
-      for (int m = 0; m < 3; ++m) cp_async8(pdu + m, io.duptr(idu, P[m]));
+      for (int m = 0; m < 3; ++m) cp_async8(&pdu(m), io.duptr(idu, P[m]));
     }
     cp_async_commit();
   };
@@ -1999,16 +2040,16 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
   ColCell c0 = cell(raw);
   prefetch(is + 1, is);
   face(cm, c0, 0);
-  double Ap[3][3];  // (A c)_{i-1}
-  double dp[3];     // delta_{i-1}
+  R Ap[3][3];  // (A c)_{i-1}
+  R dp[3];     // delta_{i-1}
   int cur = 0;
   for (int i = is; i <= ie; ++i) {
     cp_async_wait_all();
     double rhs[3];
 #pragma unroll
-    for (int n = 0; n < 5; ++n) raw[n] = pw[n];
+    for (int n = 0; n < 5; ++n) raw[n] = pw(n);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) rhs[m] = pdu[m];
+    for (int m = 0; m < 3; ++m) rhs[m] = pdu(m);
     ColCell cp = cell(raw);
     prefetch(i + 2, i < ie ? i + 1 : -1);
     const int nxt = cur ^ 1;
@@ -2017,31 +2058,32 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
     const double aright = d2 * d3 * x1f[i + 1] * x1f[i + 1] * s;
     const double vol = dx1f[i] * d2 * d3 * x1v[i] * x1v[i] * s;
 #if EXO_MIXED
-    const double i2v = 0.5 / vol, bl = aleft * i2v, cr = aright * i2v, dd = (aright - aleft) * i2v;
+    const double i2v = 0.5 / vol;
+    const R bl = R(aleft * i2v), cr = R(aright * i2v), dd = R((aright - aleft) * i2v);
 #endif
     const bool first = (i == is), last = (i == ie);
-    double t[3][3], cc[3][3], x[3];
-    unroll<3>([&](auto R) {
-      constexpr int r = decltype(R)::value;
+    R t[3][3], cc[3][3], x[3];
+    unroll<3>([&](auto Row) {
+      constexpr int r = decltype(Row)::value;
       constexpr int pr = P[r];
-      double brow[3];
+      R brow[3];
       unroll<3>([&](auto Q) {
         constexpr int q = decltype(Q)::value;
         constexpr int pq = P[q];
-        const double am = AMs(cur, r, q), ap = AMs(nxt, r, q);
+        const R am = AMs(cur, r, q), ap = AMs(nxt, r, q);
         // Phi << 0,0,0, grav,0,0, 0,grav,0 and Bnd = diag(1,-1,1)
         constexpr bool phi = (r == 1 && q == 0) || (r == 2 && q == 1);
 #if EXO_MIXED
-        double a = am * bl + ap * cr;
+        R a = am * bl + ap * cr;
         if constexpr (fj_nz(pr, pq)) a += dd * fj_entry<pr, pq>(c0, gm1);
         if constexpr (r == q) a += rdt;
-        if constexpr (phi) a -= grav;
-        double bm = am;
+        if constexpr (phi) a -= grv;
+        R bm = am;
         if constexpr (fj_nz(pr, pq)) bm += fj_entry<pr, pq>(cm, gm1);
-        double b = -bm * bl;
-        double cmv = ap;
+        R b = -bm * bl;
+        R cmv = ap;
         if constexpr (fj_nz(pr, pq)) cmv -= fj_entry<pr, pq>(cp, gm1);
-        double c = -cmv * cr;
+        R c = -cmv * cr;
         if (first) a += (q == 1) ? -b : b;
         if (last) a += (q == 1) ? -c : c;
 #else
@@ -2064,19 +2106,19 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
         cc[r][q] = c;
       });
 #if EXO_MIXED
-      x[r] = rhs[r] * rdt;
+      x[r] = R(rhs[r]) * rdt;
 #else
       x[r] = rhs[r] / dt;
 #endif
       if (!first) {
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-          double ba = brow[0] * Ap[0][q];
+          R ba = brow[0] * Ap[0][q];
 #pragma unroll
           for (int k = 1; k < 3; ++k) ba += brow[k] * Ap[k][q];
           t[r][q] = t[r][q] - ba;
         }
-        double bd = brow[0] * dp[0];
+        R bd = brow[0] * dp[0];
 #pragma unroll
         for (int k = 1; k < 3; ++k) bd += brow[k] * dp[k];
         x[r] = x[r] - bd;
@@ -2088,11 +2130,11 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
       const int i1 = (i0 + 1) % 3, i2 = (i0 + 2) % 3, j1 = (j0 + 1) % 3, j2 = (j0 + 2) % 3;
       return t[i1][j1] * t[i2][j2] - t[i1][j2] * t[i2][j1];
     };
-    double B[3][3];
+    R B[3][3];
     {
-      const double c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
-      const double det = c00 * t[0][0] + c10 * t[1][0] + c20 * t[2][0];
-      const double id = 1.0 / det;
+      const R c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
+      const R det = c00 * t[0][0] + c10 * t[1][0] + c20 * t[2][0];
+      const R id = R(1) / det;
       B[0][0] = c00 * id;
       B[0][1] = c10 * id;
       B[0][2] = c20 * id;
@@ -2104,7 +2146,7 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
     // delta_i = B x, (A c)_i = B c_i
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      double acc = B[r][0] * x[0];
+      R acc = B[r][0] * x[0];
 #pragma unroll
       for (int k = 1; k < 3; ++k) acc += B[r][k] * x[k];
       dp[r] = acc;
@@ -2113,7 +2155,7 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        double acc = B[r][0] * cc[0][q];
+        R acc = B[r][0] * cc[0][q];
 #pragma unroll
         for (int k = 1; k < 3; ++k) acc += B[r][k] * cc[k][q];
         Ap[r][q] = acc;
@@ -2150,14 +2192,15 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, double* sm, doub
   }
 #pragma unroll 1
   for (int i = ie - 1; i >= is; --i) {
-    double cs[12], u[5];
+    R cs[12];
+    double u[5];
 #pragma unroll
     for (int e = 0; e < 12; ++e) cs[e] = io.scr(i - is, e);
     io.uload(i, u);
-    double dl[3];
+    R dl[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      double ad = cs[r * 3] * dp[0];
+      R ad = cs[r * 3] * dp[0];
 #pragma unroll
       for (int k = 1; k < 3; ++k) ad += cs[r * 3 + k] * dp[k];
       dl[r] = cs[9 + r] - ad;
@@ -2234,13 +2277,44 @@ constexpr int IMPL_MAX_THREADS = 128;
 #else
 #define EXO_IMPL_BOUNDS __launch_bounds__(IMPL_MAX_THREADS, EXO_IMPL_MINB)
 #endif
-// each thread's doubles are contiguous (60, or 85 with (A c)_{i-1} kept
-// there), threads IMPL_SM_STRIDE doubles apart: an odd stride keeps a
-// half-warp's 8-byte accesses on distinct banks
+// FP64 solve: each thread's doubles are contiguous (60, or 85 with
+// (A c)_{i-1} kept there), threads IMPL_SM_STRIDE doubles apart: an odd
+// stride keeps a half-warp's 8-byte accesses on distinct banks.
+// FP32 solve: structure of arrays, the 10 prefetch doubles of every thread
+// first, then the 50 FP32 face-block entries, entry e of thread t at
+// [e * threads + t], so a warp's accesses are consecutive words.
 constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : (EXO_IMPL_BWD_SMEM ? 71 : 61);
+template <class R>
+__host__ __device__ constexpr int impl_slice_doubles() {
+  return sizeof(R) == 4 ? 10 + 50 / 2 : IMPL_SM_STRIDE;
+}
 // per block: the threads' slices, then x1f (nc1+1), x1v (nc1), dx1f (nc1)
-constexpr size_t impl_smem(int threads, int nc1) {
-  return ((size_t)IMPL_SM_STRIDE * threads + 3 * (size_t)(nc1 + 1)) * sizeof(double);
+template <class R>
+__host__ __device__ constexpr size_t impl_smem(int threads, int nc1) {
+  return ((size_t)impl_slice_doubles<R>() * threads + 3 * (size_t)(nc1 + 1)) * sizeof(double);
+}
+// this thread's slices of the block's shared memory (arguments sa, sp, ss of
+// implicit_column and implicit_column_partial)
+template <class R>
+struct ImplSlices {
+  R* sa;
+  double* sp;
+  int ss;
+};
+template <class R>
+__device__ __forceinline__ ImplSlices<R> impl_slices(double* ism, bool full) {
+  if constexpr (sizeof(R) == 4) {
+    const int nt = (int)blockDim.x, t = (int)threadIdx.x;
+    return {reinterpret_cast<R*>(ism + 10 * nt) + t, ism + t, nt};
+  } else {
+    double* sm = ism + threadIdx.x * IMPL_SM_STRIDE;
+    return {sm, sm + (full ? 50 : 18), 1};
+  }
+}
+// where the block's copy of the radial geometry starts
+template <class R>
+__device__ __forceinline__ double* impl_radial(double* ism) {
+  return ism + blockDim.x * impl_slice_doubles<R>();
 }
 // the largest dynamic shared memory a launch may ask for
 constexpr int IMPL_SMEM_MAX = 160 * 1024;
@@ -2271,12 +2345,14 @@ __device__ __forceinline__ void stage_radial(double* sg, int nc1, const double* 
 // A column of the stepping context: primitives and update from the state
 // arrays, the corrected update added to u (with the AirParcel round trip on
 // the last stage).
+template <class R>
 struct StepColumnIO {
+  using Real = R;
   const double* wc;
   const double* duc;
   double* uc;
   size_t vs;       // stride between variables
-  double* scr0;    // scratch of this column: [level][entry][32 lanes] per warp of columns
+  R* scr0;         // scratch of this column: [level][entry][32 lanes] per warp of columns
   int stage;            // < 0: write the corrected update into du, leave u alone
   double Rd, gamma;
   double* duw;          // du of this column, for stage < 0
@@ -2286,7 +2362,7 @@ struct StepColumnIO {
   }
   __device__ __forceinline__ const double* wptr(int i, int n) const { return wc + n * vs + i; }
   __device__ __forceinline__ const double* duptr(int i, int n) const { return duc + n * vs + i; }
-  __device__ __forceinline__ double& scr(int lev, int e) const {
+  __device__ __forceinline__ R& scr(int lev, int e) const {
     return scr0[(lev * 30 + e) * 32];
   }
   static constexpr bool kLoadsU = true;
@@ -2316,6 +2392,7 @@ struct StepColumnIO {
 // stage 0..2: a stage of the step (dt = beta_stage * the CFL step, u += du);
 // stage -1: ImplicitSolver::SolveImplicit3D alone (dt given, du corrected in
 // place)
+template <class R>
 __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, int stage,
                                                double dt_given = 0.) {
   extern __shared__ double ism[];
@@ -2326,23 +2403,26 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const double* x1f;
   const double* x1v;
   const double* dx1f;
-  stage_radial(ism + blockDim.x * IMPL_SM_STRIDE, v.nc1, v.x1f, v.x1v, v.dx1f, x1f, x1v, dx1f);
+  stage_radial(impl_radial<R>(ism), v.nc1, v.x1f, v.x1v, v.dx1f, x1f, x1v, dx1f);
   if (col >= ncol) return;
   const int j = v.js + col % v.N;
   const int k = v.ks + (col / v.N) % v.N;
   const int p = col / (v.N * v.N);
   const double dt = stage < 0 ? dt_given : rk_beta(stage) * v.sc->dt;
   const size_t base = idx(v, p, 0, k, j, 0);
-  // scratch in blocks of 32 columns: a warp's 32 entries are 256 contiguous bytes
-  double* scr0 = v.scratch + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
-  StepColumnIO io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
-                  v.du + base};
-  if (v.implicit_flag & 8)
-    implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
-                    geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), x1f,
-                    x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+  // scratch in blocks of 32 columns: a warp's 32 entries are 128 (FP32) or
+  // 256 (FP64) contiguous bytes
+  R* scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
+  StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
+                     v.du + base};
+  const bool full = (v.implicit_flag & 8) != 0;
+  const ImplSlices<R> sl = impl_slices<R>(ism, full);
+  if (full)
+    implicit_column(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j), geo(v, GSINC, p, k, j),
+                    geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
+                    dt, v.gamma, v.grav);
   else
-    implicit_column_partial(io, ism + threadIdx.x * IMPL_SM_STRIDE, geo(v, GCOSC, p, k, j),
+    implicit_column_partial(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
                             geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
                             geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma,
                             v.grav);
@@ -2505,11 +2585,12 @@ __global__ void EXO_UPD_BOUNDS kb_update(Batch bt, int stage) {
   update_block<T>(sv, b, stage);
 }
 
+template <class R>
 __global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage, double dt_given) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
-  implicit_block(sv, b, stage, dt_given);
+  implicit_block<R>(sv, b, stage, dt_given);
 }
 
 __global__ void kb_roundtrip(Batch bt) {
@@ -2545,6 +2626,25 @@ inline int check_launch() {
 
 inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// the implicit kernel of a precision: FP32 blocks for
+// EXO_PREC_MIXED_F32_SOLVE, FP64 for EXO_PREC_MIXED and the FP64 build
+template <class R>
+inline void launch_kb_implicit(unsigned blocks, int threads, int nc1, cudaStream_t st, Batch b,
+                               int stage, double dt_given) {
+  kb_implicit<R><<<blocks, threads, impl_smem<R>(threads, nc1), st>>>(b, stage, dt_given);
+}
+inline void launch_kb_implicit(int precision, unsigned blocks, int threads, int nc1,
+                               cudaStream_t st, Batch b, int stage, double dt_given) {
+#if EXO_MIXED
+  if (precision == EXO_PREC_MIXED_F32_SOLVE) {
+    launch_kb_implicit<float>(blocks, threads, nc1, st, b, stage, dt_given);
+    return;
+  }
+#endif
+  (void)precision;
+  launch_kb_implicit<double>(blocks, threads, nc1, st, b, stage, dt_given);
+}
+
 }  // namespace
 
 // The single-atmosphere launches run the batched kernels on a batch of one
@@ -2561,8 +2661,13 @@ inline unsigned member_block_count(const DevView& v, int kind) {
 bool x23_lines() { return EXO_X23_LINES != 0; }
 
 int prepare_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(kb_implicit, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       IMPL_SMEM_MAX);
+  cudaError_t e = cudaFuncSetAttribute(kb_implicit<double>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, IMPL_SMEM_MAX);
+#if EXO_MIXED
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kb_implicit<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             IMPL_SMEM_MAX);
+#endif
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(kb_flux_x1<EXO_FLUX_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              X1_SMEM_MAX);
@@ -2608,17 +2713,15 @@ int launch_update(const DevView& v, int stage, void* stream) {
 
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
-  kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
-                impl_smem(v.tiles[BK_IMPLICIT], v.nc1), (cudaStream_t)stream>>>(
-      one(v, BK_IMPLICIT), stage, 0.);
+  launch_kb_implicit(v.precision, member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT], v.nc1,
+                     (cudaStream_t)stream, one(v, BK_IMPLICIT), stage, 0.);
   return check_launch();
 }
 
 int launch_implicit_du(const DevView& v, double dt, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
-  kb_implicit<<<member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT],
-                impl_smem(v.tiles[BK_IMPLICIT], v.nc1), (cudaStream_t)stream>>>(
-      one(v, BK_IMPLICIT), -1, dt);
+  launch_kb_implicit(v.precision, member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT], v.nc1,
+                     (cudaStream_t)stream, one(v, BK_IMPLICIT), -1, dt);
   return check_launch();
 }
 
@@ -2665,8 +2768,8 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
       if ((rc = check_launch())) return rc;
     }
     if (pl.total[BK_IMPLICIT]) {
-      kb_implicit<<<pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT],
-                    impl_smem(pl.threads[BK_IMPLICIT], pl.max_nc1), st>>>(B(BK_IMPLICIT), s, 0.);
+      launch_kb_implicit(pl.precision, pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT],
+                         pl.max_nc1, st, B(BK_IMPLICIT), s, 0.);
       if ((rc = check_launch())) return rc;
     }
     if (s == 2) {

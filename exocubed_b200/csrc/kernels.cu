@@ -21,6 +21,7 @@ namespace {
 // A column of exo_implicit_columns: w [5][L+6] and du [5][L] of this column,
 // the corrected update written back into du.
 struct HookColumnIO {
+  using Real = double;
   const double* wc;
   double* duc;
   int nc1, L;
@@ -54,17 +55,18 @@ __global__ void EXO_IMPL_BOUNDS k_implicit_columns(
   const int col = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int nc1 = L + 2 * G;
   const double *sx1f, *sx1v, *sdx1f;
-  stage_radial(ism + blockDim.x * IMPL_SM_STRIDE, nc1, x1f, x1v, dx1f, sx1f, sx1v, sdx1f);
+  stage_radial(impl_radial<double>(ism), nc1, x1f, x1v, dx1f, sx1f, sx1v, sdx1f);
   if (col >= ncol) return;
   HookColumnIO io{w + (size_t)col * 5 * nc1, du + (size_t)col * 5 * L, nc1, L, scratch + col,
                   (size_t)ncol};
   const double* g4 = colgeo + (size_t)col * 4;
+  const ImplSlices<double> sl = impl_slices<double>(ism, full != 0);
   if (full)
-    implicit_column(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3], sx1f,
-                    sx1v, sdx1f, G, G + L - 1, dt, gamma, grav);
+    implicit_column(io, sl.sa, sl.sp, sl.ss, g4[0], g4[1], g4[2], g4[3], sx1f, sx1v, sdx1f, G,
+                    G + L - 1, dt, gamma, grav);
   else
-    implicit_column_partial(io, ism + threadIdx.x * IMPL_SM_STRIDE, g4[0], g4[1], g4[2], g4[3],
-                            sx1f, sx1v, sdx1f, G, G + L - 1, dt, gamma, grav);
+    implicit_column_partial(io, sl.sa, sl.sp, sl.ss, g4[0], g4[1], g4[2], g4[3], sx1f, sx1v,
+                            sdx1f, G, G + L - 1, dt, gamma, grav);
 }
 
 __global__ void k_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma,
@@ -205,7 +207,7 @@ int launch_implicit_columns(int ncol, int L, const double* w, double* du, const 
                             double gamma, double grav, double* scratch, void* stream, int full) {
   if (ncol <= 0) return 0;
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
-                              fp64::impl_smem(fp64::IMPL_THREADS, L + 2 * G),
+                              fp64::impl_smem<double>(fp64::IMPL_THREADS, L + 2 * G),
                               (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch, full);
   return fp64::check_launch();
@@ -257,7 +259,7 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
   }
   if (ncol <= 0) return 0;
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
-                              fp64::impl_smem(fp64::IMPL_THREADS, L + 2 * G),
+                              fp64::impl_smem<double>(fp64::IMPL_THREADS, L + 2 * G),
                               (cudaStream_t)stream>>>(
       ncol, L, w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, scratch, 1);
   e = cudaGetLastError();

@@ -60,7 +60,8 @@ def poisson_arrivals(rate, n, seed=0):
 class Server:
     """Continuous-batching server over one Ensemble.
 
-    precision      EXO_PREC_MIXED or EXO_PREC_FP64 (every member the same)
+    precision      EXO_PREC_MIXED, EXO_PREC_MIXED_F32_SOLVE or EXO_PREC_FP64 (every
+                   member the same)
     capacity       member slots
     budget_bytes   device memory the members may hold together
     max_chunk      steps launched between two admission checks (a chunk never

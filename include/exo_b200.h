@@ -58,9 +58,15 @@ enum {
 
 /* arithmetic of the flux path */
 enum {
-  EXO_PREC_FP64 = 0,  /* everything in FP64 */
-  EXO_PREC_MIXED = 1  /* FP32 reconstruction, Riemann flux and flux divergence;
-                         FP64 decomposition, implicit solve and RK accumulation */
+  EXO_PREC_FP64 = 0,            /* everything in FP64 */
+  EXO_PREC_MIXED = 1,           /* FP32 reconstruction, x2/x3 Riemann fluxes and
+                                   their divergence; FP64 decomposition, x1
+                                   (radial) fluxes and their divergence, implicit
+                                   solve, state and RK accumulation */
+  EXO_PREC_MIXED_F32_SOLVE = 2  /* EXO_PREC_MIXED with the implicit solve's blocks,
+                                   their factorisation and its back-substitution
+                                   factors in FP32 (faster solve, larger error;
+                                   state and corrected update stay FP64) */
 };
 
 /* Coriolis source (a user explicit source of the reference's examples):

@@ -2,6 +2,7 @@
 its stated distributions and profile, and the footprint the admission
 ledger charges is the sum of the member's device arrays."""
 import numpy as np
+import pytest
 
 from exocubed_b200 import _native as nat
 from exocubed_b200 import workloads as W
@@ -42,5 +43,9 @@ def test_footprint_counts_member_arrays():
     mix = footprint(dict(cfg, precision=nat.EXO_PREC_MIXED))
     assert f64 >= 7 * cells * 8      # u, w, u1, du, three flux arrays
     assert mix > f64                 # plus the FP32 primitive and flux copies
+    # FP32 implicit blocks take the same arrays (the solve's scratch is sized for FP64)
+    assert footprint(dict(cfg, precision=nat.EXO_PREC_MIXED_F32_SOLVE)) == mix
+    with pytest.raises(nat.ExoError):
+        footprint(dict(cfg, precision=3))
     big = footprint(dict(cfg, N=96, L=96))
     assert big > 50 * f64

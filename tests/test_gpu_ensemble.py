@@ -41,7 +41,8 @@ def _alone(cfg, w, nsteps):
         return a.conserved(), a.time
 
 
-@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED,
+                                       nat.EXO_PREC_MIXED_F32_SOLVE])
 def test_members_equal_alone_and_in_the_mix(precision):
     members = _members(precision)
     ens = Ensemble(precision=precision, capacity=16)

@@ -76,7 +76,8 @@ def test_hs94_mixed_close_to_oracle(oracle_mod):
     assert g.invalid() == 0
 
 
-@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED,
+                                       nat.EXO_PREC_MIXED_F32_SOLVE])
 def test_forced_and_unforced_members_in_one_batch(precision):
     cfgs = [dict(W.hs94_config(N=8, L=20, cfl=0.4), precision=precision),
             dict(W.dry_atmosphere_config(N=10, L=8, rsolver=nat.EXO_RS_HLLC,

@@ -133,7 +133,8 @@ def test_partial_mixed_close_to_oracle(oracle_mod):
         assert e1[n] < 10 * e9[n] + 1e-6, (n, e1, e9)
 
 
-@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED,
+                                       nat.EXO_PREC_MIXED_F32_SOLVE])
 def test_partial_and_full_members_in_one_batch(precision):
     """A batch may mix members of both corrections: each member's result is
     the one it has alone."""
