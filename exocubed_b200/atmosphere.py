@@ -234,6 +234,15 @@ class CubedSphereAtmosphere:
         t = (ctypes.c_int * nat.EXO_TILE_COUNT)(*[int(x) for x in threads])
         nat.check(nat.lib().exo_set_tiles(self._ctx, t))
 
+    def autotune(self, cache=None):
+        """Set the fastest measured tile of every kernel for this configuration
+        (autotune.best_tiles: timed once on a throw-away context, then cached)
+        and return the tiles.  The arithmetic per cell does not change."""
+        from . import autotune
+        tiles = autotune.best_tiles(self.cfg, cache)
+        self.set_tiles(tiles)
+        return self.tiles
+
     def invalid(self):
         f = ctypes.c_int()
         nat.check(nat.lib().exo_check_state(self._ctx, ctypes.byref(f)))

@@ -66,7 +66,7 @@ class TileCache:
         d = os.path.dirname(self.path)
         if d:
             os.makedirs(d, exist_ok=True)
-        tmp = self.path + ".tmp"
+        tmp = f"{self.path}.{os.getpid()}.tmp"
         with open(tmp, "w") as f:
             json.dump({k: {str(kid): {str(t): ms for t, ms in v.items()} for kid, v in tab.items()}
                        for k, tab in self.tables.items()}, f, indent=1, sort_keys=True)

@@ -75,3 +75,21 @@ def test_autotune_measures_once_and_caches(tmp_path, monkeypatch):
     assert (tmp_path / "tiles.json").exists()
     monkeypatch.setattr(autotune, "measure", lambda *a, **k: pytest.fail("measured twice"))
     assert autotune.best_tiles(cfg, autotune.TileCache(str(tmp_path / "tiles.json"))) == tiles
+
+
+def test_atmosphere_autotune_sets_the_tuned_tiles(tmp_path):
+    cache = autotune.TileCache(str(tmp_path / "tiles.json"))
+    cfg = W.dry_atmosphere_config(N=12, L=16, precision=nat.EXO_PREC_MIXED)
+    state = W.dry_atmosphere_state(cfg, seed=3)
+    with CubedSphereAtmosphere(cfg) as a:
+        a.set_primitive(state)
+        a.step(2)
+        want = a.conserved()
+    with CubedSphereAtmosphere(cfg) as a:
+        tiles = a.autotune(cache)
+        assert tiles == a.tiles
+        for k, cand in autotune.CANDIDATES.items():
+            assert tiles[k] in cand
+        a.set_primitive(state)
+        a.step(2)
+        assert np.array_equal(a.conserved(), want)
