@@ -202,10 +202,18 @@ size_t decomposition_refs_doubles(const DevView& v) {
   return nq * (v.nc1 + 1) + 2 * nq * v.nc1 + 2 * nq;
 }
 
+// the column kernel's shared memory grows with L (the radial tables); the
+// attribute lets a launch go past the 48 KB default
+static cudaError_t allow_column_smem() {
+  return cudaFuncSetAttribute(fp64::k_implicit_columns,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, fp64::IMPL_SMEM_MAX);
+}
+
 int launch_implicit_columns(int ncol, int L, const double* w, double* du, const double* colgeo,
                             const double* x1f, const double* x1v, const double* dx1f, double dt,
                             double gamma, double grav, double* scratch, void* stream, int full) {
   if (ncol <= 0) return 0;
+  if (allow_column_smem() != cudaSuccess) return EXO_ERR_CUDA;
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
                               fp64::impl_smem<double>(fp64::IMPL_THREADS, L + 2 * G),
                               (cudaStream_t)stream>>>(
@@ -258,6 +266,11 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
     scratch = g_noalloc_addr[dev];
   }
   if (ncol <= 0) return 0;
+  e = allow_column_smem();
+  if (e != cudaSuccess) {
+    *err = std::string("cudaFuncSetAttribute(k_implicit_columns): ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
   fp64::k_implicit_columns<<<fp64::nblk(ncol, fp64::IMPL_THREADS), fp64::IMPL_THREADS,
                               fp64::impl_smem<double>(fp64::IMPL_THREADS, L + 2 * G),
                               (cudaStream_t)stream>>>(

@@ -11,7 +11,8 @@ from _columns import column_problem
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("ncol,L,dt", [(1, 12, 30.0), (257, 16, 400.0), (1000, 40, 1500.0)])
+@pytest.mark.parametrize("ncol,L,dt", [(1, 12, 30.0), (257, 16, 400.0), (1000, 40, 1500.0),
+                                       (70, 250, 200.0)])
 def test_implicit_columns_bitwise(oracle_mod, native, ncol, L, dt):
     torch = pytest.importorskip("torch")
     w, du, colgeo, x1f, x1v, dx1f, cfg = column_problem(oracle_mod, ncol, L, seed=ncol)
