@@ -295,6 +295,11 @@ int view_allocate(const exo_config& cfg, const HostTables& t, DevView& v,
   v.nc1 = t.nc1;
   v.nc2 = t.nc2;
   v.nc3 = t.nc3;
+  v.div_L = make_fastdiv((unsigned)v.L);
+  v.div_N = make_fastdiv((unsigned)v.N);
+  v.div_nc1 = make_fastdiv((unsigned)v.nc1);
+  v.div_nc2 = make_fastdiv((unsigned)v.nc2);
+  v.div_nc3 = make_fastdiv((unsigned)v.nc3);
   v.is = v.js = v.ks = G;
   v.ie = G + cfg.L - 1;
   v.je = v.ke = G + cfg.N - 1;

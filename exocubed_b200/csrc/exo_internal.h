@@ -102,10 +102,30 @@ struct DevScalars {
   long long ncycle;
 };
 
+// n / d for 0 <= n < 2^40 / (d - 1) by one 64-bit multiply and a shift,
+// m = ceil(2^40 / d): with n = q d + t, n m / 2^40 = q + t / d + n r / (d 2^40)
+// for some r < d, which stays below q + 1 in that range (the kernels' flat
+// indices are 32-bit and their divisors at most a few thousand)
+struct FastDiv {
+  unsigned long long m;
+#ifdef __CUDACC__
+  __host__ __device__
+#endif
+  unsigned operator()(unsigned n) const {
+    return (unsigned)(((unsigned long long)n * m) >> 40);
+  }
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f;
+  f.m = ((1ull << 40) + d - 1) / d;
+  return f;
+}
+
 // Sizes, parameters and device pointers of one atmosphere; passed by value
 // to every kernel.
 struct alignas(16) DevView {
   int N, L, nv, nc1, nc2, nc3;
+  FastDiv div_L, div_N, div_nc1, div_nc2, div_nc3;  // divisions by L, N, nc1, nc2, nc3
   int is, ie, js, je, ks, ke;
   int eqn, rsolver, implicit_flag, coriolis;
   int precision, forcing;

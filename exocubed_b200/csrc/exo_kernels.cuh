@@ -581,12 +581,13 @@ __device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, 
   const unsigned long long none = ~0ull;
   unsigned total = 6u * (unsigned)v.cells;
   if (tid >= total) return none;
-  unsigned i = tid % (unsigned)v.nc1;
-  unsigned r = tid / (unsigned)v.nc1;
-  int j = (int)(r % (unsigned)v.nc2);
-  r /= (unsigned)v.nc2;
-  int k = (int)(r % (unsigned)v.nc3);
-  int p = (int)(r / (unsigned)v.nc3);
+  unsigned r = v.div_nc1(tid);
+  unsigned i = tid - r * (unsigned)v.nc1;
+  unsigned r2 = v.div_nc2(r);
+  int j = (int)(r - r2 * (unsigned)v.nc2);
+  unsigned r3 = v.div_nc3(r2);
+  int k = (int)(r2 - r3 * (unsigned)v.nc3);
+  int p = (int)r3;
   bool kin = (k >= v.ks && k <= v.ke), jin = (j >= v.js && j <= v.je);
   if (!kin && !jin) return none;  // corner: never read on the path
   int ii = i;
@@ -1000,10 +1001,11 @@ __device__ __forceinline__ void flux_x23_lines(const DevView& v, unsigned blk) {
   if (tid >= 2 * nline) return;
   const int dir = tid < nline ? 1 : 2;
   unsigned r = dir == 1 ? tid : tid - nline;
-  const int i = v.is + (int)(r % L);
-  r /= L;
-  const int a = (int)(r % N);  // position across the line: k - ks (x2) or j - js (x3)
-  const int p = (int)(r / N);
+  const unsigned rl = v.div_L(r);
+  const int i = v.is + (int)(r - rl * L);
+  const unsigned rn = v.div_N(rl);
+  const int a = (int)(rl - rn * N);  // position across the line: k - ks (x2) or j - js (x3)
+  const int p = (int)rn;
   const int nv = v.nv;
   const size_t vs = v.cells;
   const long s = dir == 1 ? (long)v.nc1 : (long)v.nc1 * v.nc2;  // stride along the line
@@ -1087,12 +1089,11 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   const unsigned tid = blk * blockDim.x + threadIdx.x;
   const unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
-  const int i = v.is + (int)(tid % L);
-  unsigned r = tid / L;
-  const int j = v.js + (int)(r % N);
-  r /= N;
-  const int k = v.ks + (int)(r % N);
-  const int p = (int)(r / N);
+  const unsigned r1 = v.div_L(tid), r2 = v.div_N(r1), r3 = v.div_N(r2);
+  const int i = v.is + (int)(tid - r1 * L);
+  const int j = v.js + (int)(r1 - r2 * N);
+  const int k = v.ks + (int)(r2 - r3 * N);
+  const int p = (int)r3;
   const double wght = rk_beta(stage) * v.sc->dt;
   const bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
   const int nv = v.nv;
@@ -2477,12 +2478,11 @@ __device__ __forceinline__ void roundtrip_block(const DevView& v, unsigned blk) 
   unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
-  int i = v.is + (int)(tid % L);
-  unsigned r = tid / L;
-  int j = v.js + (int)(r % N);
-  r /= N;
-  int k = v.ks + (int)(r % N);
-  int p = (int)(r / N);
+  const unsigned r1 = v.div_L(tid), r2 = v.div_N(r1), r3 = v.div_N(r2);
+  int i = v.is + (int)(tid - r1 * L);
+  int j = v.js + (int)(r1 - r2 * N);
+  int k = v.ks + (int)(r2 - r3 * N);
+  int p = (int)r3;
   double uu[5];
   for (int n = 0; n < 5; ++n) uu[n] = v.u[idx(v, p, n, k, j, i)];
   airparcel_round_trip(uu, v.Rd, v.gamma);
@@ -2493,12 +2493,11 @@ __device__ __forceinline__ void p2c_block(const DevView& v, unsigned blk, const 
   unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned L = v.L, N = v.N;
   if (tid >= 6u * N * N * L) return;
-  int i = v.is + (int)(tid % L);
-  unsigned r = tid / L;
-  int j = v.js + (int)(r % N);
-  r /= N;
-  int k = v.ks + (int)(r % N);
-  int p = (int)(r / N);
+  const unsigned r1 = v.div_L(tid), r2 = v.div_N(r1), r3 = v.div_N(r2);
+  int i = v.is + (int)(tid - r1 * L);
+  int j = v.js + (int)(r1 - r2 * N);
+  int k = v.ks + (int)(r2 - r3 * N);
+  int p = (int)r3;
   double w[5], c[5];
   #pragma unroll
   for (int n = 0; n < 5; ++n) {
