@@ -160,8 +160,8 @@ static int one_stage(exo_ctx* c, int s, bool cfl) {
   int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
   if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return STEP(launch_update, v, s, c->stream); })))
     return rc;
-  if (implicit &&
-      (rc = timed(c, EXO_K_IMPLICIT, 1, [&] { return STEP(launch_implicit, v, s, c->stream); })))
+  if (implicit && (rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(v.precision),
+                              [&] { return STEP(launch_implicit, v, s, c->stream); })))
     return rc;
   return boundary_and_prim(c, s == 2 && cfl);
 }
@@ -866,7 +866,7 @@ int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, dou
   size_t bytes = c->state_elems * sizeof(double);
   CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->v.du, du_host, bytes, cudaMemcpyHostToDevice, c->stream));
-  int rc = timed(c, EXO_K_IMPLICIT, 1,
+  int rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(c->v.precision),
                  [&] { return STEP(launch_implicit_du, c->v, dt, c->stream); });
   if (rc) return fail(rc, "implicit launch failed");
   CK(cudaMemcpyAsync(du_host, c->v.du, bytes, cudaMemcpyDeviceToHost, c->stream));

@@ -138,7 +138,8 @@ int rebuild(exo_ensemble* e) {
   pl.max_nc1 = max_nc1;
   pl.precision = e->precision;
   // count the kernel nodes of one step
-  int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 + (tot[exo::BK_IMPLICIT] ? 1 : 0) + 1;
+  int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 +
+                      (tot[exo::BK_IMPLICIT] ? exo::implicit_launches(e->precision) : 0) + 1;
   e->launches_per_step = 3 * per_stage + (tot[exo::BK_ROUNDTRIP] ? 1 : 0) + 1 + 1;
   cudaGraph_t graph;
   ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));

@@ -102,6 +102,15 @@ struct DevScalars {
   long long ncycle;
 };
 
+// The implicit solve of the stepping context with FP32 blocks
+// (EXO_PREC_MIXED_F32_SOLVE) runs as two kernels, the forward sweep and the
+// back substitution, so that many more columns are resident in the
+// memory-bound back substitution (4 % faster at 6x192^2x96); with FP64
+// blocks one kernel does both (the split measured 3 % slower there).
+inline int implicit_launches(int precision) {
+  return precision == EXO_PREC_MIXED_F32_SOLVE ? 2 : 1;
+}
+
 // n / d for 0 <= n < 2^40 / (d - 1) by one 64-bit multiply and a shift,
 // m = ceil(2^40 / d): with n = q d + t, n m / 2^40 = q + t / d + n r / (d 2^40)
 // for some r < d, which stays below q + 1 in that range (the kernels' flat

@@ -1546,6 +1546,88 @@ __device__ __forceinline__ void lu_solve_rows(const R (&t)[5][5], const R (&idg)
   for (int r = 0; r < 5; ++r) y[r] = z[r];
 }
 
+// BackwardSubstitution of the full correction (forward_backward.hpp:90-126):
+// delta_i -= (A c)_i delta_{i+1} from level ie (delta_ie given in dp) down
+// to is, each corrected update stored through io.  kPipe: software-pipelined,
+// the next level's factors and state in flight while a level finishes (for
+// the few resident columns of the solve kernel); otherwise one level at a
+// time, leaving the latency to the many columns of the back-substitution
+// kernel.
+template <class IO, bool kPipe = true>
+__device__ __forceinline__ void implicit_backward_full(IO& io, int is, int ie,
+                                                       typename IO::Real* dp) {
+  using R = typename IO::Real;
+  auto store = [&](int i, const double* u) {
+    double d[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) d[n] = dp[n];
+    io.ustore(i, u, d);
+  };
+  if constexpr (!kPipe) {
+    {
+      double u[5];
+      io.uload(ie, u);
+      store(ie, u);
+    }
+#pragma unroll 1
+    for (int i = ie - 1; i >= is; --i) {
+      R cs[30];
+      double u[5];
+#pragma unroll
+      for (int e = 0; e < 30; ++e) cs[e] = io.scr(i - is, e);
+      io.uload(i, u);
+      R dl[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        R ad = cs[r * 5] * dp[0];
+#pragma unroll
+        for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
+        dl[r] = cs[25 + r] - ad;
+      }
+#pragma unroll
+      for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+      store(i, u);
+    }
+    return;
+  }
+  R cur_s[30];
+  double cur_u[5];
+  io.uload(ie, cur_u);
+  store(ie, cur_u);
+  if (ie > is) {
+#pragma unroll
+    for (int e = 0; e < 30; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
+    io.uload(ie - 1, cur_u);
+  }
+#pragma unroll 1
+  for (int i = ie - 1; i >= is; --i) {
+    R nxt_s[30];
+    double nxt_u[5];
+    if (i > is) {
+#pragma unroll
+      for (int e = 0; e < 30; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
+      io.uload(i - 1, nxt_u);
+    }
+    R dl[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      R ad = cur_s[r * 5] * dp[0];
+#pragma unroll
+      for (int k = 1; k < 5; ++k) ad += cur_s[r * 5 + k] * dp[k];
+      dl[r] = cur_s[25 + r] - ad;
+    }
+#pragma unroll
+    for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+    store(i, cur_u);
+    if (i > is) {
+#pragma unroll
+      for (int e = 0; e < 30; ++e) cur_s[e] = nxt_s[e];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) cur_u[n] = nxt_u[n];
+    }
+  }
+}
+
 // The vertical 5x5 block-tridiagonal correction of one radial column
 // (ImplicitSolver::SolveImplicit3D X1 branch, solve_implicit_3d.cpp:102-179,
 // with FullCorrection, full_correction.cpp:32-165, and ForwardSweep /
@@ -1573,7 +1655,9 @@ __device__ __forceinline__ void lu_solve_rows(const R (&t)[5][5], const R (&idg)
 //   sa, sp, ss       this thread's shared memory: entry e (0..49) of the two
 //                    face blocks at sa[e * ss], prefetch slot n (0..9) at
 //                    sp[n * ss]
-template <class IO>
+// kBwd false: the forward sweep only, with delta_ie stored as scratch
+// entries 25..29 of the last level (implicit_backward_full finishes it).
+template <class IO, bool kBwd = true>
 __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, double* sp, int ss,
                                                 double cos_theta, double sin_theta, double d2,
                                                 double d3, const double* x1f, const double* x1v,
@@ -1900,6 +1984,12 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
 #pragma unroll
       for (int r = 0; r < 5; ++r) io.scr(lev, 25 + r) = dp[r];
     }
+    if constexpr (!kBwd) {
+      if (last) {
+#pragma unroll
+        for (int r = 0; r < 5; ++r) io.scr(lev, 25 + r) = dp[r];
+      }
+    }
     cm = c0;
     c0 = cp;
     cur = nxt;
@@ -1907,6 +1997,7 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
   // the last level's prefetch (unused) must land before the back substitution
   // reuses this thread's slots of shared memory
   cp_async_wait_all();
+  if constexpr (!kBwd) return;
 #if EXO_IMPL_BWD_SMEM
   // back substitution: delta_i -= (A c)_i delta_{i+1}.  The factors and the
   // state of the next two levels are copied asynchronously into this
@@ -1959,50 +2050,7 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
   }
 }
 #else
-  // back substitution: delta_i -= (A c)_i delta_{i+1}, software-pipelined:
-  // the next level's scratch and state are in flight while this level ends
-  auto store = [&](int i, const double* u) {
-    double d[5];
-#pragma unroll
-    for (int n = 0; n < 5; ++n) d[n] = dp[n];
-    io.ustore(i, u, d);
-  };
-  R cur_s[30];
-  double cur_u[5];
-  io.uload(ie, cur_u);
-  store(ie, cur_u);
-  if (ie > is) {
-#pragma unroll
-    for (int e = 0; e < 30; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
-    io.uload(ie - 1, cur_u);
-  }
-#pragma unroll 1
-  for (int i = ie - 1; i >= is; --i) {
-    R nxt_s[30];
-    double nxt_u[5];
-    if (i > is) {
-#pragma unroll
-      for (int e = 0; e < 30; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
-      io.uload(i - 1, nxt_u);
-    }
-    R dl[5];
-#pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      R ad = cur_s[r * 5] * dp[0];
-#pragma unroll
-      for (int k = 1; k < 5; ++k) ad += cur_s[r * 5 + k] * dp[k];
-      dl[r] = cur_s[25 + r] - ad;
-    }
-#pragma unroll
-    for (int r = 0; r < 5; ++r) dp[r] = dl[r];
-    store(i, cur_u);
-    if (i > is) {
-#pragma unroll
-      for (int e = 0; e < 30; ++e) cur_s[e] = nxt_s[e];
-#pragma unroll
-      for (int n = 0; n < 5; ++n) cur_u[n] = nxt_u[n];
-    }
-  }
+  implicit_backward_full(io, is, ie, dp);
 }
 #endif
 #undef EXO_AP
@@ -2019,7 +2067,52 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
 // delta_i (3).  IO and arguments as for implicit_column; the shared slices
 // hold the two face blocks (18 entries of sa) and the prefetched w (5) and
 // du (3) of a level (sp).
+// BackwardSubstitution of the partial correction: delta_i -= (A c)_i
+// delta_{i+1} for (rho, m1, E) from level ie (delta_ie in dp) down to is;
+// the update of level i takes delta for rho, m1, E and the explicit du for
+// m2, m3.
 template <class IO>
+__device__ __forceinline__ void implicit_backward_partial(IO& io, int is, int ie,
+                                                          typename IO::Real* dp) {
+  using R = typename IO::Real;
+  auto store = [&](int i, const double* u) {
+    double dl[5];
+    dl[IDN] = dp[0];
+    dl[IVX] = dp[1];
+    dl[IVY] = *io.duptr(i, IVY);
+    dl[IVZ] = *io.duptr(i, IVZ);
+    dl[IEN] = dp[2];
+    io.ustore(i, u, dl);
+  };
+  {
+    double u_ie[5];
+    io.uload(ie, u_ie);
+    store(ie, u_ie);
+  }
+#pragma unroll 1
+  for (int i = ie - 1; i >= is; --i) {
+    R cs[12];
+    double u[5];
+#pragma unroll
+    for (int e = 0; e < 12; ++e) cs[e] = io.scr(i - is, e);
+    io.uload(i, u);
+    R dl[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      R ad = cs[r * 3] * dp[0];
+#pragma unroll
+      for (int k = 1; k < 3; ++k) ad += cs[r * 3 + k] * dp[k];
+      dl[r] = cs[9 + r] - ad;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) dp[r] = dl[r];
+    store(i, u);
+  }
+}
+
+// kBwd false: the forward sweep only, with delta_ie stored as scratch
+// entries 9..11 of the last level (implicit_backward_partial finishes it).
+template <class IO, bool kBwd = true>
 __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Real* sa, double* sp, int ss,
                                                         double cos_theta, double sin_theta,
                                                         double d2, double d3, const double* x1f,
@@ -2214,46 +2307,19 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Rea
 #pragma unroll
       for (int r = 0; r < 3; ++r) io.scr(lev, 9 + r) = dp[r];
     }
+    if constexpr (!kBwd) {
+      if (last) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) io.scr(i - is, 9 + r) = dp[r];
+      }
+    }
     cm = c0;
     c0 = cp;
     cur = nxt;
   }
   cp_async_wait_all();  // the last level's prefetch (unused) lands before the slice is reused
-  // back substitution: delta_i -= (A c)_i delta_{i+1}; the update of level i
-  // takes delta for rho, m1, E and the explicit du for m2, m3
-  auto store = [&](int i, const double* u) {
-    double dl[5];
-    dl[IDN] = dp[0];
-    dl[IVX] = dp[1];
-    dl[IVY] = *io.duptr(i, IVY);
-    dl[IVZ] = *io.duptr(i, IVZ);
-    dl[IEN] = dp[2];
-    io.ustore(i, u, dl);
-  };
-  {
-    double u_ie[5];
-    io.uload(ie, u_ie);
-    store(ie, u_ie);
-  }
-#pragma unroll 1
-  for (int i = ie - 1; i >= is; --i) {
-    R cs[12];
-    double u[5];
-#pragma unroll
-    for (int e = 0; e < 12; ++e) cs[e] = io.scr(i - is, e);
-    io.uload(i, u);
-    R dl[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      R ad = cs[r * 3] * dp[0];
-#pragma unroll
-      for (int k = 1; k < 3; ++k) ad += cs[r * 3 + k] * dp[k];
-      dl[r] = cs[9 + r] - ad;
-    }
-#pragma unroll
-    for (int r = 0; r < 3; ++r) dp[r] = dl[r];
-    store(i, u);
-  }
+  if constexpr (!kBwd) return;
+  implicit_backward_partial(io, is, ie, dp);
 }
 
 // UpdateAllConserved on the last stage with NVAPOR = NCLOUD = 0: the
@@ -2462,15 +2528,47 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
                      v.du + base};
   const bool full = (v.implicit_flag & 8) != 0;
   const ImplSlices<R> sl = impl_slices<R>(ism, full);
+  using IO = StepColumnIO<R>;
+  // FP32 blocks: the back substitution is kb_implicit_bwd's
+  constexpr bool kBwd = sizeof(R) == 8;
   if (full)
-    implicit_column(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j), geo(v, GSINC, p, k, j),
-                    geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
-                    dt, v.gamma, v.grav);
+    implicit_column<IO, kBwd>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
+                                         geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
+                                         geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
+                                         dt, v.gamma, v.grav);
   else
-    implicit_column_partial(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
-                            geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
-                            geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma,
-                            v.grav);
+    implicit_column_partial<IO, kBwd>(io, sl.sa, sl.sp, sl.ss,
+                                                 geo(v, GCOSC, p, k, j), geo(v, GSINC, p, k, j),
+                                                 geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j),
+                                                 x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+}
+
+// The back substitution of a column whose forward sweep implicit_block ran
+// with FP32 blocks: no shared memory, few registers, so many columns are
+// resident while the factors stream back in.
+template <class R>
+__device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned blk, int stage) {
+  const int ncol = 6 * v.N * v.N;
+  const int col = (int)(blk * blockDim.x + threadIdx.x);
+  if (col >= ncol) return;
+  const int j = v.js + col % v.N;
+  const int k = v.ks + (col / v.N) % v.N;
+  const int p = col / (v.N * v.N);
+  const size_t base = idx(v, p, 0, k, j, 0);
+  R* scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
+  StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
+                     v.du + base};
+  if (v.implicit_flag & 8) {
+    R dp[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
+    implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
+  } else {
+    R dp[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) dp[r] = io.scr(v.L - 1, 9 + r);
+    implicit_backward_partial(io, v.is, v.ie, dp);
+  }
 }
 
 // last-stage round trip when the implicit solver is off
@@ -2636,6 +2734,18 @@ __global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage, double dt_given
   implicit_block<R>(sv, b, stage, dt_given);
 }
 
+// 128 registers: 16 warps per SM (96 spills)
+#ifndef EXO_IMPL_BWD_MAXNREG
+#define EXO_IMPL_BWD_MAXNREG 128
+#endif
+template <class R>
+__global__ void __maxnreg__(EXO_IMPL_BWD_MAXNREG) kb_implicit_bwd(Batch bt, int stage) {
+  __shared__ __align__(16) DevView sv;
+  unsigned b = batch_enter(bt, sv);
+  if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
+  implicit_bwd_block<R>(sv, b, stage);
+}
+
 __global__ void kb_roundtrip(Batch bt) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
@@ -2675,6 +2785,7 @@ template <class R>
 inline void launch_kb_implicit(unsigned blocks, int threads, int nc1, cudaStream_t st, Batch b,
                                int stage, double dt_given) {
   kb_implicit<R><<<blocks, threads, impl_smem<R>(threads, nc1), st>>>(b, stage, dt_given);
+  if constexpr (sizeof(R) == 4) kb_implicit_bwd<R><<<blocks, threads, 0, st>>>(b, stage);
 }
 inline void launch_kb_implicit(int precision, unsigned blocks, int threads, int nc1,
                                cudaStream_t st, Batch b, int stage, double dt_given) {
