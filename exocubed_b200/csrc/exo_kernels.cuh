@@ -2543,31 +2543,134 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
                                                  x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
 }
 
+// levels per shared-memory chunk of the back-substitution kernel (a power of
+// two: the tile's element index is split with shifts)
+constexpr int BWD_CHUNK = 4;
+static_assert((BWD_CHUNK & (BWD_CHUNK - 1)) == 0 && BWD_CHUNK == 4, "the tile index uses e >> 2");
+__host__ __device__ constexpr size_t impl_bwd_smem(int threads) {
+  return ((size_t)5 * threads * (BWD_CHUNK + 1) + threads) * sizeof(double);
+}
 // The back substitution of a column whose forward sweep implicit_block ran
 // with FP32 blocks: no shared memory, few registers, so many columns are
 // resident while the factors stream back in.
 template <class R>
 __device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned blk, int stage) {
   const int ncol = 6 * v.N * v.N;
-  const int col = (int)(blk * blockDim.x + threadIdx.x);
-  if (col >= ncol) return;
-  const int j = v.js + col % v.N;
-  const int k = v.ks + (col / v.N) % v.N;
-  const int p = col / (v.N * v.N);
-  const size_t base = idx(v, p, 0, k, j, 0);
-  R* scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
+  const int T = (int)blockDim.x, t = (int)threadIdx.x;
+  const int col0 = (int)blk * T, col = col0 + t;
+  const bool active = col < ncol;
+  const bool full = (v.implicit_flag & 8) != 0;
+  size_t base = 0;
+  R* scr0 = nullptr;
+  if (active) {
+    const int j = v.js + col % v.N;
+    const int k = v.ks + (col / v.N) % v.N;
+    const int p = col / (v.N * v.N);
+    base = idx(v, p, 0, k, j, 0);
+    scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
+  }
   StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
                      v.du + base};
-  if (v.implicit_flag & 8) {
-    R dp[5];
+  R dp[5] = {R(0), R(0), R(0), R(0), R(0)};
+  if (active) {
+    if (full) {
 #pragma unroll
-    for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
-    implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
-  } else {
-    R dp[3];
+      for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
+    } else {
 #pragma unroll
-    for (int r = 0; r < 3; ++r) dp[r] = io.scr(v.L - 1, 9 + r);
-    implicit_backward_partial(io, v.is, v.ie, dp);
+      for (int r = 0; r < 3; ++r) dp[r] = io.scr(v.L - 1, 9 + r);
+    }
+  }
+  if (stage < 0) {  // SolveImplicit3D alone: du corrected in place, column by column
+    if (!active) return;
+    if (full) implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
+    else implicit_backward_partial(io, v.is, v.ie, dp);
+    return;
+  }
+  // The stepping form: the block's columns move through BWD_CHUNK levels at a
+  // time.  u of those levels is copied into shared memory by the whole block
+  // (four consecutive lanes read one column's four levels: a 32-byte run per
+  // column instead of 32 scattered 8-byte loads per level), updated there by
+  // each column's thread, and copied back the same way.
+  // Tile: u[n][c][l] at ((n * T + c) * (BWD_CHUNK + 1) + l), padded so that
+  // a half-warp's 8-byte accesses of one level fall on distinct banks; then
+  // the column bases.
+  extern __shared__ double bsm[];
+  constexpr int CP = BWD_CHUNK + 1;
+  double* tile = bsm;
+  long long* cbase = reinterpret_cast<long long*>(bsm + 5 * T * CP);
+  cbase[t] = active ? (long long)base : 0;
+  __syncthreads();
+  const int ncb = min(T, ncol - col0);
+  const int lgT = __ffs(T) - 1;  // T is a power of two
+  const size_t vs = v.cells;
+  double* const u = v.u;
+  for (int hi = v.ie; hi >= v.is; hi -= BWD_CHUNK) {
+    const int lo = max(v.is, hi - BWD_CHUNK + 1);
+    for (int e = t; e < 5 * BWD_CHUNK * T; e += T) {
+      const int l = e & (BWD_CHUNK - 1), c = (e >> 2) & (T - 1), n = e >> (2 + lgT);
+      if (c < ncb && lo + l <= hi) tile[(n * T + c) * CP + l] = u[cbase[c] + n * vs + lo + l];
+    }
+    __syncthreads();
+    if (active) {
+      for (int i = hi; i >= lo; --i) {
+        if (i < v.ie) {
+          if (full) {
+            R cs[30];
+#pragma unroll
+            for (int e = 0; e < 30; ++e) cs[e] = io.scr(i - v.is, e);
+            R dl[5];
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+              R ad = cs[r * 5] * dp[0];
+#pragma unroll
+              for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
+              dl[r] = cs[25 + r] - ad;
+            }
+#pragma unroll
+            for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+          } else {
+            R cs[12];
+#pragma unroll
+            for (int e = 0; e < 12; ++e) cs[e] = io.scr(i - v.is, e);
+            R dl[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+              R ad = cs[r * 3] * dp[0];
+#pragma unroll
+              for (int k = 1; k < 3; ++k) ad += cs[r * 3 + k] * dp[k];
+              dl[r] = cs[9 + r] - ad;
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r) dp[r] = dl[r];
+          }
+        }
+        double d[5];
+        if (full) {
+#pragma unroll
+          for (int n = 0; n < 5; ++n) d[n] = dp[n];
+        } else {
+          d[IDN] = dp[0];
+          d[IVX] = dp[1];
+          d[IVY] = *io.duptr(i, IVY);
+          d[IVZ] = *io.duptr(i, IVZ);
+          d[IEN] = dp[2];
+        }
+        // StepColumnIO::ustore with u in the tile
+        double uu[5];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) uu[n] = tile[(n * T + t) * CP + (i - lo)] + 1. * d[n];
+        if (stage == 2) airparcel_round_trip(uu, v.Rd, v.gamma);
+#pragma unroll
+        for (int n = 0; n < 5; ++n) tile[(n * T + t) * CP + (i - lo)] = uu[n];
+      }
+    }
+    __syncthreads();
+    for (int e = t; e < 5 * BWD_CHUNK * T; e += T) {
+      const int l = e & (BWD_CHUNK - 1), c = (e >> 2) & (T - 1), n = e >> (2 + lgT);
+      if (c < ncb && lo + l <= hi) u[cbase[c] + n * vs + lo + l] = tile[(n * T + c) * CP + l];
+    }
+    __syncthreads();
   }
 }
 
@@ -2785,7 +2888,8 @@ template <class R>
 inline void launch_kb_implicit(unsigned blocks, int threads, int nc1, cudaStream_t st, Batch b,
                                int stage, double dt_given) {
   kb_implicit<R><<<blocks, threads, impl_smem<R>(threads, nc1), st>>>(b, stage, dt_given);
-  if constexpr (sizeof(R) == 4) kb_implicit_bwd<R><<<blocks, threads, 0, st>>>(b, stage);
+  if constexpr (sizeof(R) == 4)
+    kb_implicit_bwd<R><<<blocks, threads, impl_bwd_smem(threads), st>>>(b, stage);
 }
 inline void launch_kb_implicit(int precision, unsigned blocks, int threads, int nc1,
                                cudaStream_t st, Batch b, int stage, double dt_given) {
