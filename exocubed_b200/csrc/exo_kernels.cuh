@@ -2576,7 +2576,9 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const bool full = (v.implicit_flag & 8) != 0;
   const ImplSlices<R> sl = impl_slices<R>(ism, full);
   using IO = StepColumnIO<R>;
-  // FP32 blocks: the back substitution is kb_implicit_bwd's
+  // FP32 blocks: the back substitution of the full correction is
+  // kb_implicit_bwd's (the lighter partial one stays here: split, it measured
+  // slower)
   constexpr bool kBwd = sizeof(R) == 8;
   if (full)
     implicit_column<IO, kBwd>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
@@ -2584,7 +2586,7 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
                                          geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
                                          dt, v.gamma, v.grav);
   else
-    implicit_column_partial<IO, kBwd>(io, sl.sa, sl.sp, sl.ss,
+    implicit_column_partial<IO, true>(io, sl.sa, sl.sp, sl.ss,
                                                  geo(v, GCOSC, p, k, j), geo(v, GSINC, p, k, j),
                                                  geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j),
                                                  x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
@@ -2597,16 +2599,15 @@ static_assert((BWD_CHUNK & (BWD_CHUNK - 1)) == 0 && BWD_CHUNK == 4, "the tile in
 __host__ __device__ constexpr size_t impl_bwd_smem(int threads) {
   return ((size_t)5 * threads * (BWD_CHUNK + 1) + threads) * sizeof(double);
 }
-// The back substitution of a column whose forward sweep implicit_block ran
-// with FP32 blocks: no shared memory, few registers, so many columns are
-// resident while the factors stream back in.
+// The back substitution of the full correction of a column whose forward
+// sweep implicit_block ran with FP32 blocks: few registers, so many columns
+// are resident while the factors stream back in.
 template <class R>
 __device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned blk, int stage) {
   const int ncol = 6 * v.N * v.N;
   const int T = (int)blockDim.x, t = (int)threadIdx.x;
   const int col0 = (int)blk * T, col = col0 + t;
   const bool active = col < ncol;
-  const bool full = (v.implicit_flag & 8) != 0;
   size_t base = 0;
   R* scr0 = nullptr;
   if (active) {
@@ -2618,20 +2619,13 @@ __device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned bl
   }
   StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
                      v.du + base};
-  R dp[5] = {R(0), R(0), R(0), R(0), R(0)};
+  R dp[5] = {R(0), R(0), R(0), R(0), R(0)};  // delta_ie, stored by the forward sweep
   if (active) {
-    if (full) {
 #pragma unroll
-      for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
-    } else {
-#pragma unroll
-      for (int r = 0; r < 3; ++r) dp[r] = io.scr(v.L - 1, 9 + r);
-    }
+    for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
   }
   if (stage < 0) {  // SolveImplicit3D alone: du corrected in place, column by column
-    if (!active) return;
-    if (full) implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
-    else implicit_backward_partial(io, v.is, v.ie, dp);
+    if (active) implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
     return;
   }
   // The stepping form: the block's columns move through BWD_CHUNK levels at a
@@ -2662,51 +2656,25 @@ __device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned bl
     if (active) {
       for (int i = hi; i >= lo; --i) {
         if (i < v.ie) {
-          if (full) {
-            R cs[30];
+          R cs[30];
 #pragma unroll
-            for (int e = 0; e < 30; ++e) cs[e] = io.scr(i - v.is, e);
-            R dl[5];
+          for (int e = 0; e < 30; ++e) cs[e] = io.scr(i - v.is, e);
+          R dl[5];
 #pragma unroll
-            for (int r = 0; r < 5; ++r) {
-              R ad = cs[r * 5] * dp[0];
+          for (int r = 0; r < 5; ++r) {
+            R ad = cs[r * 5] * dp[0];
 #pragma unroll
-              for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
-              dl[r] = cs[25 + r] - ad;
-            }
-#pragma unroll
-            for (int r = 0; r < 5; ++r) dp[r] = dl[r];
-          } else {
-            R cs[12];
-#pragma unroll
-            for (int e = 0; e < 12; ++e) cs[e] = io.scr(i - v.is, e);
-            R dl[3];
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-              R ad = cs[r * 3] * dp[0];
-#pragma unroll
-              for (int k = 1; k < 3; ++k) ad += cs[r * 3 + k] * dp[k];
-              dl[r] = cs[9 + r] - ad;
-            }
-#pragma unroll
-            for (int r = 0; r < 3; ++r) dp[r] = dl[r];
+            for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
+            dl[r] = cs[25 + r] - ad;
           }
-        }
-        double d[5];
-        if (full) {
 #pragma unroll
-          for (int n = 0; n < 5; ++n) d[n] = dp[n];
-        } else {
-          d[IDN] = dp[0];
-          d[IVX] = dp[1];
-          d[IVY] = *io.duptr(i, IVY);
-          d[IVZ] = *io.duptr(i, IVZ);
-          d[IEN] = dp[2];
+          for (int r = 0; r < 5; ++r) dp[r] = dl[r];
         }
         // StepColumnIO::ustore with u in the tile
         double uu[5];
 #pragma unroll
-        for (int n = 0; n < 5; ++n) uu[n] = tile[(n * T + t) * CP + (i - lo)] + 1. * d[n];
+        for (int n = 0; n < 5; ++n)
+          uu[n] = tile[(n * T + t) * CP + (i - lo)] + 1. * (double)dp[n];
         if (stage == 2) airparcel_round_trip(uu, v.Rd, v.gamma);
 #pragma unroll
         for (int n = 0; n < 5; ++n) tile[(n * T + t) * CP + (i - lo)] = uu[n];
@@ -2892,7 +2860,8 @@ template <class R>
 __global__ void __maxnreg__(EXO_IMPL_BWD_MAXNREG) kb_implicit_bwd(Batch bt, int stage) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
-  if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1)) return;
+  // members with the partial correction finished in kb_implicit
+  if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1) || !(sv.implicit_flag & 8)) return;
   implicit_bwd_block<R>(sv, b, stage);
 }
 
