@@ -249,6 +249,16 @@ def alg_bytes_per_cell(kernel, precision, implicit_flag=9):
             "other": 0}[kernel]
 
 
+def traffic_key(kernel, precision, implicit_flag=9):
+    """Key of a kernel's ncu-measured DRAM bytes per cell in profiles/traffic.json."""
+    key = f"{kernel}:{'mixed' if precision in (1, 2) else 'fp64'}"
+    if kernel == "implicit" and precision == 2:
+        key += "_f32_solve"
+    if kernel == "implicit" and not implicit_flag & 8:
+        key += ":partial"
+    return key
+
+
 def measure_path(cfg, state, steps, warmup, pg, local, sample_clocks, tune=True):
     """Device-timed steps of one atmosphere with the state resident (launch
     tiles autotuned before the clock starts unless tune is False)."""
@@ -431,12 +441,7 @@ def run_ours(args):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        key = f"{dom}:{'mixed' if prec in (1, 2) else 'fp64'}"
-        if dom == "implicit" and prec == 2:
-            key += "_f32_solve"
-        if dom == "implicit" and not iflag & 8:
-            key += ":partial"
-        tr = json.load(open(tp)).get(key)
+        tr = json.load(open(tp)).get(traffic_key(dom, prec, iflag))
         if tr:  # DRAM bytes per cell measured by ncu, scaled to this launch
             traffic = tr["bytes_per_cell"] * cells
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
