@@ -111,17 +111,21 @@ inline int implicit_launches(int precision) {
   return precision == EXO_PREC_MIXED_F32_SOLVE ? 2 : 1;
 }
 
-// n / d for 0 <= n < 2^40 / (d - 1) by one 64-bit multiply and a shift,
-// m = ceil(2^40 / d): with n = q d + t, n m / 2^40 = q + t / d + n r / (d 2^40)
-// for some r < d, which stays below q + 1 in that range (the kernels' flat
-// indices are 32-bit and their divisors at most a few thousand)
+// n / d for 0 <= n < 2^40 / (d - 1) as floor(n m / 2^40), m = ceil(2^40 / d):
+// with n = q d + t, n m / 2^40 = q + t / d + n r / (d 2^40) for some r < d,
+// which stays below q + 1 in that range (the kernels' flat indices are
+// 32-bit and their divisors at most a few thousand).  n m needs up to 72
+// bits (m < 2^41), so it is formed from the two 32-bit halves of m, each
+// product within 64 bits: floor(n m / 2^40) = (n mh + floor(n ml / 2^32)) >> 8.
 struct FastDiv {
   unsigned long long m;
 #ifdef __CUDACC__
   __host__ __device__
 #endif
   unsigned operator()(unsigned n) const {
-    return (unsigned)(((unsigned long long)n * m) >> 40);
+    const unsigned long long lo = (unsigned long long)n * (unsigned)(m & 0xffffffffull);
+    const unsigned long long hi = (unsigned long long)n * (unsigned)(m >> 32);
+    return (unsigned)((hi + (lo >> 32)) >> 8);
   }
 };
 inline FastDiv make_fastdiv(unsigned d) {

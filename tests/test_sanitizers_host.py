@@ -41,3 +41,8 @@ def test_oracle_under_sanitizers(tmp_path):
     out = _build_and_run(tmp_path, "oracle", ["oracle/exo_oracle.cpp",
                                               "tests/sanitize/oracle_driver.cpp"])
     assert "oracle: ok" in out
+
+
+def test_fastdiv_exact_under_sanitizers(tmp_path):
+    out = _build_and_run(tmp_path, "fastdiv", ["tests/sanitize/fastdiv_driver.cpp"])
+    assert "fastdiv: ok" in out
