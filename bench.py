@@ -90,13 +90,16 @@ def _workload(name):
     raise ValueError(name)
 
 
-def make_state(cfg, seed):
+def make_state(cfg, seed, geometry=None):
+    """Seeded initial primitives of a workload; geometry: None (the product
+    library's cell geometry) or the oracle's (CPU legs, which must not load
+    the product library)."""
     from exocubed_b200 import workloads as W
     if cfg["eqn"] == 0:
-        return W.shallow_water_state(cfg, seed=seed)
+        return W.shallow_water_state(cfg, seed=seed, geometry=geometry)
     if cfg.get("forcing", 0) == 1:
-        return W.hs94_state(cfg, seed=seed)
-    return W.dry_atmosphere_state(cfg, seed=seed)
+        return W.hs94_state(cfg, seed=seed, geometry=geometry)
+    return W.dry_atmosphere_state(cfg, seed=seed, geometry=geometry)
 
 
 def cells_of(cfg):
@@ -203,12 +206,14 @@ def member_seeds(rank, n):
 
 # ---------------------------------------------------------- CPU baseline --
 def cpu_worker(args):
-    """Runs in a fresh process: times the oracle on all host cores."""
+    """Runs in a fresh process: times the oracle on all host cores.  The
+    state is generated on the oracle's own mesh, so this process never loads
+    the product library."""
     import numpy as np  # noqa: F401
     from oracle import oracle
     cfg, _ = workload_config(args.workload)
     o = oracle.Oracle(cfg)
-    o.set_primitive(make_state(cfg, 0))
+    o.set_primitive(make_state(cfg, 0, geometry=oracle.cell_geometry))
     o.step(args.cpu_warmup)
     t0 = time.perf_counter()
     o.step(args.cpu_steps)
@@ -246,6 +251,22 @@ def alg_bytes_per_cell(kernel, precision, implicit_flag=9):
     # the x1 fluxes are FP64 in both builds (5 values of 8 bytes per cell)
     return {"flux_x1": 40 + 40, "flux_x23": x23, "update": 120 + 40 + 10 * t + 80,
             "implicit": 160 + factors, "prim_ghost": 80 + (20 if mixed else 0),
+            "other": 0}[kernel]
+
+
+def state_bytes_per_cell(kernel, precision):
+    """Compulsory bytes per interior cell and launch: the state arrays the
+    kernel must read or write, each once (u, u1, du, w in FP64; the FP32
+    primitive copy where the mixed x2/x3 sweep reads nothing else).  Face
+    fluxes, the implicit solve's factor scratch, FP32 flux copies, halos and
+    tables are implementation traffic and are not counted (the 320 B per
+    cell-update rule of the step applied to one kernel)."""
+    mixed = precision in (1, 2)
+    return {"flux_x1": 40,                        # w
+            "flux_x23": 20 if mixed else 40,      # w32 / w
+            "update": 160,                        # u, u1, w read; du (or u) written
+            "implicit": 160,                      # w, du, u read; u written
+            "prim_ghost": 80,                     # u read; w written
             "other": 0}[kernel]
 
 
@@ -435,9 +456,11 @@ def run_ours(args):
     n_l, t_l = prof[dom]
     avg_ms = t_l / max(n_l, 1)
     iflag = cfg.get("implicit_flag", 9)
-    alg_bytes = alg_bytes_per_cell(dom, prec, iflag) * cells
+    alg_bytes = state_bytes_per_cell(dom, prec) * cells
+    all_bytes = alg_bytes_per_cell(dom, prec, iflag) * cells
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    achieved_all = all_bytes / (avg_ms / 1e3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -496,6 +519,13 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": dom,
                      "peak_kind": peak_kind,
+                     "bytes_per_cell": state_bytes_per_cell(dom, prec),
+                     "ms_per_launch": avg_ms,
+                     "with_intermediates": {
+                         "bytes_per_cell": alg_bytes_per_cell(dom, prec, iflag),
+                         "achieved": achieved_all, "frac": achieved_all / peak,
+                         "note": "adds the kernel's face fluxes, factor scratch and FP32 "
+                                 "copies to its state bytes"},
                      "step_frac": value / world * BYTES_PER_CELL_UPDATE / 1e9 / peak},
         "kernel_share": shares,
         "cpu_baseline": extra.get("cpu_baseline"),
@@ -717,27 +747,32 @@ def run_accuracy(args):
 
 
 def run_reference(args):
+    """The reference arm: the oracle (the reference's algorithm restated in
+    C++, FP64, OpenMP on all host threads) on the same workload.  It times
+    the --steps steps after the --warmup warm-up steps it reports (or, with
+    --ref-steps, that many) in a process that never loads the product
+    library; under torchrun only rank 0 runs."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cfg, desc = workload_config(args.workload, args.precision)
-    steps, warm = min(args.steps, args.ref_steps), min(args.warmup, 1)
+    cfg, desc = workload_config(args.workload, 0)
+    steps = args.steps if args.ref_steps <= 0 else min(args.steps, args.ref_steps)
+    warm = args.warmup
     r = run_cpu(args.workload, steps, warm)
     v = r["cells"] * r["steps"] / r["seconds"]
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": r["steps"], "warmup": warm,
         "ms_per_step": r["seconds"] / r["steps"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "cells_per_step": r["cells"]},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": r["threads"],
                          "kind": "port",
                          "sample": f"{r['steps']} full FP64 step(s) of the workload after "
-                                   f"{warm} warm-up step(s) (of the {args.steps} + {args.warmup} "
-                                   "requested: a bounded sample of the same rate); the reference "
-                                   "cannot be built here, its C++ restatement (oracle/) runs "
-                                   "with OpenMP on all host threads"},
+                                   f"{warm} warm-up step(s); the reference cannot be built "
+                                   "here, its C++ restatement (oracle/) runs with OpenMP on "
+                                   "all host threads, on a state generated on its own mesh"},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -768,9 +803,9 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=8,
                     help="requests of the serving sample in the bench line (0: none)")
     ap.add_argument("--serve-rate", type=float, default=100.0)
-    ap.add_argument("--ref-steps", type=int, default=2,
-                    help="full steps the reference arm times at most (its bounded sample)")
-    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--ref-steps", type=int, default=0,
+                    help="full steps the reference arm times at most (0: all of --steps)")
+    ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-worker", action="store_true")

@@ -706,21 +706,27 @@ static int read_scalars(exo_ctx* c, const exo::DevScalars* src, exo::DevScalars*
   return EXO_OK;
 }
 
-// copy u, w and the clock: to the redo copy (save) or back (!save)
+// copy u, w, the FP32 primitive copy w32 (mixed builds: the flux kernels of
+// the next stage read it) and the clock: to the redo copy (save) or back
+// (!save)
 static int redo_copy(exo_ctx* c, bool save) {
   const size_t b = c->state_elems * sizeof(double);
   double* keep_u = c->redo_state;
   double* keep_w = c->redo_state + c->state_elems;
+  float* keep_w32 = reinterpret_cast<float*>(c->redo_state + 2 * c->state_elems);
+  const size_t b32 = c->state_elems * sizeof(float);
   auto cp = [&](void* dst, const void* src, size_t n) {
     return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, c->stream);
   };
   if (save) {
     CK(cp(keep_u, c->v.u, b));
     CK(cp(keep_w, c->v.w, b));
+    if (c->v.w32) CK(cp(keep_w32, c->v.w32, b32));
     CK(cp(c->redo_sc, c->v.sc, sizeof(exo::DevScalars)));
   } else {
     CK(cp(c->v.u, keep_u, b));
     CK(cp(c->v.w, keep_w, b));
+    if (c->v.w32) CK(cp(c->v.w32, keep_w32, b32));
     CK(cp(c->v.sc, c->redo_sc, sizeof(exo::DevScalars)));
   }
   return EXO_OK;
@@ -758,7 +764,9 @@ int exo_set_max_redo(exo_ctx* c, int max_redo) {
   if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
   if (max_redo < 0) return fail(EXO_ERR_ARG, "max_redo < 0");
   if (max_redo > 0 && !c->redo_state) {
-    CK(cudaMalloc((void**)&c->redo_state, 2 * c->state_elems * sizeof(double)));
+    // u and w, then room for w32 (half a double array) when the build keeps one
+    size_t words = 2 * c->state_elems + (c->v.w32 ? (c->state_elems + 1) / 2 : 0);
+    CK(cudaMalloc((void**)&c->redo_state, words * sizeof(double)));
     c->owned.push_back(c->redo_state);
     CK(cudaMalloc((void**)&c->redo_sc, sizeof(exo::DevScalars)));
     c->owned.push_back(c->redo_sc);

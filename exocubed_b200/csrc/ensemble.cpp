@@ -306,7 +306,11 @@ int admit(exo_ensemble* e, const exo_config* cfg, const double* w_host, const vo
       return efail(EXO_ERR_CUDA, "initialising the member failed");
     }
     ce = cudaStreamSynchronize(e->stream);
-    if (ce != cudaSuccess) return cuda_efail(ce, "exo_ensemble_add");
+    if (ce != cudaSuccess) {
+      for (void* p : m->owned) cudaFreeAsync(p, e->stream);
+      delete m;
+      return cuda_efail(ce, "exo_ensemble_add");
+    }
     e->launches += 4;
   }
   e->slots[free_slot] = m;

@@ -247,8 +247,13 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+  if (e != cudaSuccess) {
     *err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= 64) {
+    *err = "device index " + std::to_string(dev) +
+           " is not supported by the no-alloc scratch table (devices 0..63)";
     return EXO_ERR_CUDA;
   }
   double* scratch;

@@ -44,6 +44,7 @@ class Record:
     cells: int = 0
     steps: int = 0
     valid: bool = True
+    rejected: bool = False  # could not be admitted even with the device empty
     result: np.ndarray = None
 
     @property
@@ -116,6 +117,15 @@ class Server:
                 r = queue[0]
                 cfg = dict(r.cfg, precision=self.precision)
                 slot = self.ens.try_add(cfg, r.w)
+                if slot is None and not active:
+                    # refused with nothing else on the device (its memory
+                    # could not be had): it never fits, so it is rejected
+                    # rather than waited for
+                    queue.popleft()
+                    rec = recs[r.rid]
+                    rec.rejected, rec.valid = True, False
+                    rec.admitted = rec.done = now()
+                    continue
                 if slot is None:
                     break
                 queue.popleft()
@@ -181,7 +191,12 @@ def served_one_at_a_time(requests, precision=nat.EXO_PREC_FP64, keep_results=Fal
 
 def summarize(records):
     """p50/p99 latency (seconds), throughput (requests/s and cell-updates/s)
-    over a finished run."""
+    over a finished run; rejected requests are counted apart and take no
+    part in the latency and throughput figures."""
+    rejected = sum(1 for r in records if r.rejected)
+    records = [r for r in records if not r.rejected]
+    if not records:
+        return {"requests": 0, "rejected": rejected}
     lat = np.array([r.latency for r in records])
     span = max(r.done for r in records) - min(r.arrival for r in records)
     cu = sum(r.cells * r.steps for r in records)
@@ -189,4 +204,4 @@ def summarize(records):
             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
             "max_s": float(lat.max()), "span_s": float(span),
             "requests_per_s": len(records) / span, "cell_updates_per_s": cu / span,
-            "all_valid": all(r.valid for r in records)}
+            "all_valid": all(r.valid for r in records), "rejected": rejected}

@@ -15,9 +15,13 @@ shapes, sizes and value distributions of the configurations:
                   winds sigma 5 m/s per lat-lon component.
 
 Every generator takes a numpy PCG64 seed and returns the primitive array
-(6, nvar, N+6, N+6, L+6) with the interior filled (ghosts are zero).
+(6, nvar, N+6, N+6, L+6) with the interior filled (ghosts are zero).  The
+cell geometry comes from the product library (`cell_geometry`) unless a
+`geometry` callable with the same result is given: the CPU reference leg of
+the benchmark passes the oracle's, so that it never loads the product.
 """
 import math
+import types
 
 import numpy as np
 from scipy.special import lpmv
@@ -26,6 +30,16 @@ from . import _native as nat
 from .atmosphere import cell_geometry, make_config
 
 G = nat.NGHOST
+
+
+def _resolve(cfg, geometry):
+    """(attribute view of cfg, geometry function).  Without a geometry
+    function the configuration is completed with the library's defaults
+    (make_config) and the library's geometry is used; with one, a dict is
+    read as given."""
+    if geometry is None:
+        return (make_config(**cfg) if isinstance(cfg, dict) else cfg), cell_geometry
+    return (types.SimpleNamespace(**cfg) if isinstance(cfg, dict) else cfg), geometry
 
 
 def shallow_water_config(N=48, **kw):
@@ -74,10 +88,10 @@ def _solid_body_uv(lat, lon, u0, axis):
     return (v * east).sum(0), (v * north).sum(0)
 
 
-def shallow_water_state(cfg, seed=0):
-    cfg = make_config(**cfg) if isinstance(cfg, dict) else cfg
-    N, L = cfg.N, cfg.L
-    lat, lon, m, _ = cell_geometry(cfg)
+def shallow_water_state(cfg, seed=0, geometry=None):
+    c, geo = _resolve(cfg, geometry)
+    N, L = c.N, c.L
+    lat, lon, m, _ = geo(cfg)
     rng = np.random.Generator(np.random.PCG64(seed))
     base = 2.94e4
     d = _real_sph_harm_field(lat, lon, 8, rng)
@@ -96,13 +110,14 @@ def shallow_water_state(cfg, seed=0):
     return w
 
 
-def dry_atmosphere_state(cfg, seed=0, T0=250., ps=1e5, temp_sigma=1.0, wind_sigma=5.0):
-    cfg = make_config(**cfg) if isinstance(cfg, dict) else cfg
-    N, L = cfg.N, cfg.L
-    Rd, g = cfg.Rd, -cfg.grav
-    lat, lon, m, x1v = cell_geometry(cfg)
+def dry_atmosphere_state(cfg, seed=0, T0=250., ps=1e5, temp_sigma=1.0, wind_sigma=5.0,
+                         geometry=None):
+    c, geo = _resolve(cfg, geometry)
+    N, L = c.N, c.L
+    Rd, g = c.Rd, -c.grav
+    lat, lon, m, x1v = geo(cfg)
     rng = np.random.Generator(np.random.PCG64(seed))
-    z = x1v - cfg.x1min
+    z = x1v - c.x1min
     p = ps * np.exp(-g * z / (Rd * T0))
     T = T0 + temp_sigma * rng.standard_normal((6, N, N, L))
     U = wind_sigma * rng.standard_normal((6, N, N, L))
@@ -169,15 +184,15 @@ def ensemble_member_config(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_R
 
 
 def ensemble_member(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
-                    temp_sigma=1.0, wind_sigma=5.0, **kw):
+                    temp_sigma=1.0, wind_sigma=5.0, geometry=None, **kw):
     """One forward-model run of the batched ensemble: (config dict, primitive
     array) for ensemble_member_config(seed); temperature and wind noise as in
     dry_atmosphere_state, drawn from a generator seeded by (seed, 1)."""
     cfg, prof = ensemble_member_config(seed, precision, rsolver, **kw)
-    c = make_config(**cfg)
+    c, geo = _resolve(cfg, geometry)
     N, L, Rd, g = c.N, c.L, c.Rd, -c.grav
     rng = np.random.Generator(np.random.PCG64([seed, 1]))
-    lat, lon, m, x1v = cell_geometry(c)
+    lat, lon, m, x1v = geo(cfg)
     T0, p = _adiabat_isothermal(x1v - c.x1min, prof["Ts"], prof["Ttop"], g, Rd, c.gamma,
                                 prof["ps"])
     T = T0[None, None, None, :] + temp_sigma * rng.standard_normal((6, N, N, L))
@@ -212,18 +227,18 @@ def hs94_config(N=40, L=40, precision=nat.EXO_PREC_FP64, **kw):
     return cfg
 
 
-def hs94_state(cfg, seed=0, z_iso=2.e4, wind_sigma=10.):
+def hs94_state(cfg, seed=0, z_iso=2.e4, wind_sigma=10., geometry=None):
     """MeshBlock::ProblemGenerator of hs94.cpp:246-291 restated: a dry adiabat
     from (Ts, p0) up to z_iso, isothermal above (Ttop = Ts + grav z_iso / cp),
     and wind noise of wind_sigma m/s in v2 and v3 of the adiabatic cells; the
     isothermal cells of a column keep the noise of its top adiabatic cell, as
     the reference's level loop leaves them.  Noise from a PCG64 generator."""
-    c = make_config(**cfg) if isinstance(cfg, dict) else cfg
+    c, geo = _resolve(cfg, geometry)
     N, L, Rd, g = c.N, c.L, c.Rd, -c.grav
     cp = c.gamma / (c.gamma - 1.) * Rd
     Ts, p0 = c.hs_Ts, c.hs_p0
     Ttop = Ts - g * z_iso / cp
-    _, _, _, x1v = cell_geometry(c)
+    _, _, _, x1v = geo(cfg)
     z = x1v - c.x1min
     T, p = _adiabat_isothermal(z, Ts, Ttop, g, Rd, c.gamma, p0)
     rng = np.random.Generator(np.random.PCG64(seed))

@@ -2025,6 +2025,53 @@ void ora_get_mesh(void* h, int panel, double* x1f, double* x2f, double* x3f) {
   std::memcpy(x3f, o.pg[panel].x3f.data(), o.pg[panel].x3f.size() * sizeof(double));
 }
 
+// Cell-centre latitude, longitude and the (east, north) -> (v2, v3) velocity
+// coefficients of the interior cells, plus the interior x1v: GetLatLon and
+// GetVyVz (cubed_sphere.cpp:78-91, 149-162) on the mesh this oracle builds.
+// Used to generate seeded initial states without the product library.
+// lat, lon: [6][N][N]; uv_to_v23: [6][N][N][4] = (dv2/dU, dv2/dV, dv3/dU,
+// dv3/dV); x1v: [L].  Any pointer may be NULL.
+int ora_cell_geometry(const exo_config* cfg, double* lat, double* lon, double* uv_to_v23,
+                      double* x1v) {
+  if (!cfg || cfg->N < 2 || cfg->L < 1) return 1;
+  Oracle o;
+  o.cfg = *cfg;
+  o.N = cfg->N;
+  o.L = cfg->L;
+  o.nc1 = cfg->L + 2 * G;
+  o.nc2 = o.nc3 = cfg->N + 2 * G;
+  o.is = o.js = o.ks = G;
+  o.ie = G + cfg->L - 1;
+  o.je = o.ke = G + cfg->N - 1;
+  build_mesh(o);
+  const int N = cfg->N;
+  for (int p = 0; p < 6; ++p)
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j) {
+        size_t q = ((size_t)p * N + k) * N + j;
+        double dX = tan(o.pg[p].x2v[G + j]), dY = tan(o.pg[p].x3v[G + k]);
+        double la, lo;
+        rll_from_xyp(dY, -dX, p, lo, la);
+        if (lat) lat[q] = la;
+        // the longitude runs the other way round in GetLatLon
+        if (lon) lon[q] = 2.0 * M_PI - lo;
+        if (uv_to_v23) {
+          // VecTransABPFromRLL applied to unit east and north winds; the east
+          // component flips with the longitude
+          double a2, a3, b2, b3;
+          vec_abp_from_rll(dX, dY, p + 1, 1.0, 0.0, &a2, &a3);
+          vec_abp_from_rll(dX, dY, p + 1, 0.0, 1.0, &b2, &b3);
+          uv_to_v23[4 * q + 0] = -a2;
+          uv_to_v23[4 * q + 1] = b2;
+          uv_to_v23[4 * q + 2] = -a3;
+          uv_to_v23[4 * q + 3] = b3;
+        }
+      }
+  if (x1v)
+    for (int i = 0; i < cfg->L; ++i) x1v[i] = o.x1v[G + i];
+  return 0;
+}
+
 // FullCorrection (full != 0) or PartialCorrection over a batch of columns:
 // w [ncol][5][L+6], du [ncol][5][L] (in/out), colgeo [ncol][4] = (cos, sin,
 // dx2f_ang, dx3f_ang)

@@ -72,6 +72,8 @@ def lib():
         L.ora_calculate_fluxes.argtypes = [p]
         L.ora_step.argtypes = [p, i, d]
         L.ora_get_mesh.argtypes = [p, i, dp, dp, dp]
+        L.ora_cell_geometry.restype = i
+        L.ora_cell_geometry.argtypes = [ctypes.POINTER(ExoConfig), dp, dp, dp, dp]
         L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
         L.ora_correction_columns.argtypes = [i, i, i, dp, dp, dp, dp, dp, dp, d, d, d]
         L.ora_solve_implicit_3d.argtypes = [p, dp, dp, d]
@@ -94,6 +96,21 @@ def to_struct(cfg):
     for k, v in cfg.items():
         setattr(s, k, v)
     return s
+
+
+def cell_geometry(cfg):
+    """(lat, lon, uv_to_v23, x1v) of the interior cells from the oracle's own
+    mesh (GetLatLon / GetVyVz, cubed_sphere.cpp:78-162): the geometry that
+    seeded initial states need, without the product library."""
+    c = to_struct(cfg)
+    N, L = c.N, c.L
+    lat = np.empty((6, N, N))
+    lon = np.empty((6, N, N))
+    m = np.empty((6, N, N, 4))
+    x1v = np.empty(L)
+    if lib().ora_cell_geometry(ctypes.byref(c), _ptr(lat), _ptr(lon), _ptr(m), _ptr(x1v)):
+        raise ValueError("oracle rejected the configuration")
+    return lat, lon, m, x1v
 
 
 class Oracle:

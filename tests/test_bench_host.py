@@ -52,3 +52,57 @@ def test_measured_traffic_for_every_dominant_kernel(precision, flag):
         # measured bytes stay near the algorithmic count (no hidden re-reads)
         alg = bench.alg_bytes_per_cell(kernel, precision, flag)
         assert 0.8 * alg < entry["bytes_per_cell"] < 1.6 * alg, (kernel, entry, alg)
+
+
+def test_state_bytes_follow_the_step_rule():
+    # the state arrays each kernel reads or writes once; no scratch or copies
+    assert bench.state_bytes_per_cell("implicit", 1) == 160
+    assert bench.state_bytes_per_cell("implicit", 0) == 160
+    assert bench.state_bytes_per_cell("update", 1) == 160
+    assert bench.state_bytes_per_cell("flux_x23", 1) == 20
+    assert bench.state_bytes_per_cell("prim_ghost", 0) == 80
+    for k in ("flux_x1", "flux_x23", "update", "implicit", "prim_ghost"):
+        for p in (0, 1, 2):
+            assert bench.state_bytes_per_cell(k, p) <= bench.alg_bytes_per_cell(k, p)
+
+
+def test_reference_leg_never_loads_the_product_library():
+    """The CPU leg (bench.py --impl reference, cpu_baseline) builds its state
+    on the oracle's mesh and steps the oracle; the product library must not
+    be mapped into that process."""
+    import subprocess
+    import sys
+    code = (
+        "import sys, types, json\n"
+        f"sys.path.insert(0, {ROOT!r})\n"
+        "import bench\n"
+        "a = types.SimpleNamespace(workload='c1', cpu_warmup=0, cpu_steps=1)\n"
+        "bench.cpu_worker(a)\n"
+        "print(json.dumps({'mapped': 'libexo_b200' in open('/proc/self/maps').read()}))\n")
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                       check=True, timeout=600)
+    lines = [json.loads(x) for x in r.stdout.strip().splitlines()]
+    assert lines[0]["steps"] == 1 and lines[0]["cells"] == 6 * 48 * 48 * 3
+    assert lines[-1]["mapped"] is False
+
+
+@pytest.mark.parametrize("N", [6, 8, 48])
+def test_oracle_geometry_is_the_library_geometry(N, native):
+    """Seeded states generated on the oracle's mesh equal those generated on
+    the library's, bit for bit, so both arms start from the same state."""
+    import numpy as np
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.atmosphere import cell_geometry
+    from oracle import oracle
+    cfg = W.dry_atmosphere_config(N=N, L=7)
+    for a, b in zip(oracle.cell_geometry(cfg), cell_geometry(cfg)):
+        assert np.array_equal(a, b)
+    for seed in (0, 3):
+        c, w_ora = W.ensemble_member(seed, geometry=oracle.cell_geometry)
+        _, w_lib = W.ensemble_member(seed)
+        assert np.array_equal(w_ora, w_lib)
+    sw = W.shallow_water_config(N=N)
+    assert np.array_equal(W.shallow_water_state(sw, 1, geometry=oracle.cell_geometry),
+                          W.shallow_water_state(sw, 1))

@@ -18,8 +18,14 @@ def _cfg(**kw):
     return dict(W.dry_atmosphere_config(N=8, L=12, rsolver=nat.EXO_RS_HLLC), **kw)
 
 
-def test_fixed_step_redone_with_half_steps():
-    cfg = _cfg()
+PRECISIONS = [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED, nat.EXO_PREC_MIXED_F32_SOLVE]
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_fixed_step_redone_with_half_steps(precision):
+    # in the mixed builds the retaken step must also start from the kept FP32
+    # primitive copy, not from the failed step's
+    cfg = _cfg(precision=precision)
     state = W.dry_atmosphere_state(cfg, seed=3)
     with CubedSphereAtmosphere(cfg) as a:
         a.set_primitive(state)
@@ -42,8 +48,9 @@ def test_fixed_step_redone_with_half_steps():
         assert c.invalid() == 1
 
 
-def test_cfl_step_redone_with_half_steps():
-    cfg = _cfg(cfl=1.5)
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_cfl_step_redone_with_half_steps(precision):
+    cfg = _cfg(cfl=1.5, precision=precision)
     state = W.dry_atmosphere_state(cfg, seed=3)
     with CubedSphereAtmosphere(cfg) as a:
         a.set_primitive(state)
