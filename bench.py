@@ -280,6 +280,15 @@ def traffic_key(kernel, precision, implicit_flag=9):
     return key
 
 
+def alu_peaks():
+    """FP64 and FP32 FMA rates of this GPU (exo_measure_fma_peak), measured
+    in the same run, before any timed region."""
+    from exocubed_b200 import _native as nat
+    f64, f32 = nat.fma_peak(True), nat.fma_peak(False)
+    return {"fp64_flops_per_s": f64, "fp32_flops_per_s": f32,
+            "how": "independent FMA chains on every SM, best of 3 event-timed launches"}
+
+
 def measure_path(cfg, state, steps, warmup, pg, local, sample_clocks, tune=True):
     """Device-timed steps of one atmosphere with the state resident (launch
     tiles autotuned before the clock starts unless tune is False)."""
@@ -436,6 +445,7 @@ def run_ours(args):
     cells = cells_of(cfg)
 
     tune = not args.no_autotune
+    alu = alu_peaks()
     main = measure_path(cfg, state, args.steps, args.warmup, pg, local, rank == 0, tune)
     ms_e2e, nbytes = measure_e2e(cfg, state, args.steps, pg, tune)
     plain = None
@@ -462,11 +472,14 @@ def run_ours(args):
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     achieved_all = all_bytes / (avg_ms / 1e3) / 1e9
     traffic = None
+    fp64_flops = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         tr = json.load(open(tp)).get(traffic_key(dom, prec, iflag))
         if tr:  # DRAM bytes per cell measured by ncu, scaled to this launch
             traffic = tr["bytes_per_cell"] * cells
+            if tr.get("fp64_flops_per_cell"):  # ncu: dadd + dmul + 2 dfma per cell
+                fp64_flops = tr["fp64_flops_per_cell"] * cells
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
 
     extra = {}
@@ -526,7 +539,10 @@ def run_ours(args):
                          "achieved": achieved_all, "frac": achieved_all / peak,
                          "note": "adds the kernel's face fluxes, factor scratch and FP32 "
                                  "copies to its state bytes"},
-                     "step_frac": value / world * BYTES_PER_CELL_UPDATE / 1e9 / peak},
+                     "step_frac": value / world * BYTES_PER_CELL_UPDATE / 1e9 / peak,
+                     "alu_peaks": alu,
+                     "fp64_pipe_frac": (fp64_flops / (avg_ms / 1e3) / alu["fp64_flops_per_s"]
+                                        if fp64_flops and alu else None)},
         "kernel_share": shares,
         "cpu_baseline": extra.get("cpu_baseline"),
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",

@@ -44,6 +44,7 @@ EXPORTED = [
     "exo_checkpoint_bytes", "exo_checkpoint_save", "exo_checkpoint_load",
     "exo_ensemble_checkpoint_bytes", "exo_ensemble_checkpoint_save",
     "exo_ensemble_add_checkpoint", "exo_set_max_redo", "exo_redo_count",
+    "exo_measure_fma_peak",
 ]
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
 
@@ -154,6 +155,8 @@ def lib():
     L.exo_ensemble_check_state.argtypes = [p, i, ctypes.POINTER(i)]
     L.exo_set_max_redo.argtypes = [p, i]
     L.exo_redo_count.argtypes = [p, ctypes.POINTER(ctypes.c_int64)]
+    L.exo_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_double)]
     L.exo_checkpoint_bytes.argtypes = [p, ctypes.POINTER(sz)]
     L.exo_checkpoint_save.argtypes = [p, p, sz]
     L.exo_checkpoint_load.argtypes = [p, p, sz]
@@ -191,3 +194,11 @@ def checkpoint_header(image):
     return {"magic": bytes(h.magic), "version": h.version, "values": h.values,
             "time": h.time, "dt": h.dt, "ncycle": h.ncycle, "invalid": h.invalid,
             "cfg": h.cfg.as_dict()}
+
+
+def fma_peak(fp64=True, repeats=3):
+    """Best FMA rate (flops/s) of the current device in FP64 or FP32
+    (exo_measure_fma_peak)."""
+    out = ctypes.c_double()
+    check(lib().exo_measure_fma_peak(int(bool(fp64)), int(repeats), ctypes.byref(out)))
+    return out.value

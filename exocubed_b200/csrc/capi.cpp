@@ -1089,6 +1089,14 @@ int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
   return EXO_OK;
 }
 
+int exo_measure_fma_peak(int fp64, int repeats, double* flops_per_s) {
+  if (!flops_per_s || repeats < 1) return fail(EXO_ERR_ARG, "flops_per_s NULL or repeats < 1");
+  std::string err;
+  int rc = exo::measure_fma_peak(fp64 != 0, repeats, flops_per_s, &err);
+  if (rc) return fail(rc, err);
+  return EXO_OK;
+}
+
 int exo_weno5(int n, const double* a, const double* b, const double* c, const double* d,
               const double* e, double* out, void* stream) {
   if (n < 0 || !a || !b || !c || !d || !e || !out) return fail(EXO_ERR_ARG, "bad argument");

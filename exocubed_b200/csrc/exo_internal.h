@@ -264,6 +264,8 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
                                     const double* colgeo, const double* x1f, const double* x1v,
                                     const double* dx1f, double dt, double gamma, double grav,
                                     void* stream, std::string* err);
+// peaks.cu: best FMA rate (flops/s) of independent chains on all SMs
+int measure_fma_peak(bool fp64, int repeats, double* flops_per_s, std::string* err);
 
 
 // checkpoint.cpp: images of one atmosphere (exo_checkpoint_header, u, w)

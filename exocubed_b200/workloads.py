@@ -156,20 +156,13 @@ def _adiabat_isothermal(z, Ts, Ttop, g, Rd, gamma, ps):
     return T, p
 
 
-def ensemble_member_config(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
-                           ps=1e5, ptop=1e3, Rd=287.):
-    """Configuration of one forward-model run of the batched ensemble.
-    N ~ U{24,32,48,64,96}, L ~ U{32,48,64,96}, surface temperature
-    U[150,400] K, top temperature U[100,250] K (at most the surface's),
-    gravity U[3,25] m/s^2, gamma U[1.3,1.67]; the model top sits where the
-    profile reaches ptop.  Returns (config dict, profile parameters)."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    N = int(rng.choice(ENSEMBLE_N))
-    L = int(rng.choice(ENSEMBLE_L))
-    Ts = rng.uniform(150., 400.)
-    Ttop = min(rng.uniform(100., 250.), Ts)
-    g = rng.uniform(3., 25.)
-    gamma = rng.uniform(1.3, 1.67)
+def member_config(N, L, Ts, Ttop, g, gamma, precision=nat.EXO_PREC_MIXED,
+                  rsolver=nat.EXO_RS_LMARS, ps=1e5, ptop=1e3, Rd=287.):
+    """Configuration of one forward-model atmosphere with the given profile
+    parameters: dry adiabat from (Ts, ps) up to T = Ttop, isothermal above;
+    the model top sits where the profile reaches ptop.  Returns (config
+    dict, profile parameters)."""
+    Ttop = min(Ttop, Ts)
     cp = gamma / (gamma - 1.) * Rd
     zt = (Ts - Ttop) / (g / cp)
     pt = ps * (Ttop / Ts) ** (cp / Rd)
@@ -183,12 +176,27 @@ def ensemble_member_config(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_R
     return cfg, dict(Ts=Ts, Ttop=Ttop, ps=ps)
 
 
-def ensemble_member(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
-                    temp_sigma=1.0, wind_sigma=5.0, geometry=None, **kw):
-    """One forward-model run of the batched ensemble: (config dict, primitive
-    array) for ensemble_member_config(seed); temperature and wind noise as in
-    dry_atmosphere_state, drawn from a generator seeded by (seed, 1)."""
-    cfg, prof = ensemble_member_config(seed, precision, rsolver, **kw)
+def ensemble_member_config(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
+                           ps=1e5, ptop=1e3, Rd=287.):
+    """Configuration of one forward-model run of the batched ensemble.
+    N ~ U{24,32,48,64,96}, L ~ U{32,48,64,96}, surface temperature
+    U[150,400] K, top temperature U[100,250] K (at most the surface's),
+    gravity U[3,25] m/s^2, gamma U[1.3,1.67]; member_config places the
+    model top.  Returns (config dict, profile parameters)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    N = int(rng.choice(ENSEMBLE_N))
+    L = int(rng.choice(ENSEMBLE_L))
+    Ts = rng.uniform(150., 400.)
+    Ttop = min(rng.uniform(100., 250.), Ts)
+    g = rng.uniform(3., 25.)
+    gamma = rng.uniform(1.3, 1.67)
+    return member_config(N, L, Ts, Ttop, g, gamma, precision, rsolver, ps, ptop, Rd)
+
+
+def member_state(cfg, prof, seed, temp_sigma=1.0, wind_sigma=5.0, geometry=None):
+    """Primitive initial state of a member_config atmosphere: the profile
+    plus temperature and wind noise as in dry_atmosphere_state, drawn from a
+    generator seeded by (seed, 1)."""
     c, geo = _resolve(cfg, geometry)
     N, L, Rd, g = c.N, c.L, c.Rd, -c.grav
     rng = np.random.Generator(np.random.PCG64([seed, 1]))
@@ -204,7 +212,15 @@ def ensemble_member(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS
     w[:, 0][sl] = p[None, None, None, :] / (Rd * T)
     w[:, 2][sl] = m[..., 0, None] * U + m[..., 1, None] * V
     w[:, 3][sl] = m[..., 2, None] * U + m[..., 3, None] * V
-    return cfg, w
+    return w
+
+
+def ensemble_member(seed, precision=nat.EXO_PREC_MIXED, rsolver=nat.EXO_RS_LMARS,
+                    temp_sigma=1.0, wind_sigma=5.0, geometry=None, **kw):
+    """One forward-model run of the batched ensemble: (config dict, primitive
+    array) for ensemble_member_config(seed)."""
+    cfg, prof = ensemble_member_config(seed, precision, rsolver, **kw)
+    return cfg, member_state(cfg, prof, seed, temp_sigma, wind_sigma, geometry)
 
 
 def hs94_config(N=40, L=40, precision=nat.EXO_PREC_FP64, **kw):

@@ -387,7 +387,8 @@ int exo_ensemble_get_stream(exo_ensemble* ens, void** stream);
 
 /* The main loop's redo of failed steps (main.cpp.in:126-157,
    src/mesh_redo.cpp:12-46): with max_redo > 0 every exo_step step first
-   keeps a device copy of u, w and the clock; a step that leaves the state
+   keeps a device copy of u, w (with the FP32 primitive copy of the mixed
+   builds) and the clock; a step that leaves the state
    invalid (rho or p negative or not finite, exo_check_state) is taken again
    from that copy with half the time step (half the fixed dt when one is
    given), as often as needed.  As in the reference the budget counts redos
@@ -396,7 +397,8 @@ int exo_ensemble_get_stream(exo_ensemble* ens, void** stream);
    A step that starts from an invalid state returns EXO_ERR_NONFINITE at
    once.  Each step then waits for the device once (the flag read); the
    default 0, the reference's, keeps steps asynchronous.  The first call with
-   max_redo > 0 allocates the copy (2 x the state). */
+   max_redo > 0 allocates the copy (2 x the state, 2.5 x in the mixed
+   builds). */
 int exo_set_max_redo(exo_ctx* ctx, int max_redo);
 /* Redos taken so far. */
 int exo_redo_count(exo_ctx* ctx, int64_t* redos);
@@ -444,6 +446,17 @@ int exo_checkpoint_load(exo_ctx* ctx, const void* image, size_t bytes);
 int exo_ensemble_checkpoint_bytes(exo_ensemble* ens, int slot, size_t* bytes);
 int exo_ensemble_checkpoint_save(exo_ensemble* ens, int slot, void* image, size_t bytes);
 int exo_ensemble_add_checkpoint(exo_ensemble* ens, const void* image, size_t bytes, int* slot);
+
+/* --------------------------------------------------------- measurement */
+
+/* Arithmetic ceiling of the current device: the rate of fused multiply-adds
+   (2 flops each) that a kernel of independent FMA chains in FP64 (fp64 = 1)
+   or FP32 (fp64 = 0) reaches on all SMs, timed with CUDA events on the
+   default stream after one warm-up launch; *flops_per_s receives the best of
+   `repeats` launches.  No counterpart in the reference (its only instrument
+   is the zone-cycles print of src/mesh_destroy.cpp:43-63): it gives the
+   roofline of the step's FP64-issue-bound kernels a measured denominator. */
+int exo_measure_fma_peak(int fp64, int repeats, double* flops_per_s);
 
 #ifdef __cplusplus
 }

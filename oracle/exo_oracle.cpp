@@ -219,6 +219,10 @@ struct Oracle {
   double dt, time;
   int64_t ncycle;
   int invalid;
+  // panel ghost syncs per boundary update: 1, or 2 as the reference's
+  // cubed-sphere task list runs them (patches/24.time_integrator.patch:22-28,
+  // SEND_HYD2/RECV_HYD2/SETB_HYD2; patches/29.mesh.patch:19-86 at start-up)
+  int ghost_passes = 1;
   // ora_change_to_perturbation's column data for ora_restore_from_perturbation
   std::vector<double> dec_psf, dec_pres, dec_dens, dec_gam, dec_ent;
 
@@ -625,29 +629,39 @@ void pack_order(const std::vector<double>& a, int NN, int K, int J, int I,
 // One panel ghost exchange of the conserved variables: every panel packs
 // (LoadBoundaryBufferSameLevel -> CubedSphereUtility::PackData) for each of
 // its four sides and the neighbour unpacks into its ghost band in plain
-// (n,k,j,i) order.  With one block per panel the reference's second pass
-// (patches/24.time_integrator.patch:22-28) reads the same interior cells and
-// reproduces the first, so it is run once.
+// (n,k,j,i) order.  The interpolation reads only the sender's interior cells
+// (the G-wide band along the edge), so with one block per panel the
+// reference's second pass (patches/24.time_integrator.patch:22-28) writes
+// what the first wrote; Oracle::ghost_passes = 2 runs it to show that
+// (tests/test_oracle_properties.py), and 1 is the default.
+// The values panel p sends across its side s: its G-wide edge band of the
+// conserved variables, interpolated onto the neighbour's ghost cells and
+// packed in the traversal order of that (panel, side)
+void pack_face(const Oracle& o, int p, int s, std::vector<double>& buf) {
+  int blockID = p + 1;
+  int ox2 = side_ox2(s), ox3 = side_ox3(s);
+  // source index ranges of a face neighbour (bvals_cc.cpp LoadBoundaryBufferSameLevel)
+  int si = o.is, ei = o.ie;
+  int sj = (ox2 > 0) ? (o.je - G + 1) : o.js;
+  int ej = (ox2 < 0) ? (o.js + G - 1) : o.je;
+  int sk = (ox3 > 0) ? (o.ke - G + 1) : o.ks;
+  int ek = (ox3 < 0) ? (o.ks + G - 1) : o.ke;
+  bool along_x2 = (ox3 != 0);
+  std::vector<double> tmp;
+  const double* src = &o.u[o.at(p, 0, 0, 0, 0)];
+  interpolate_edge(o, src, blockID, along_x2, kDinv[p][s], kTgSide[p][s], kNbrPanel[p][s], 0,
+                   o.NV - 1, si, ei, sj, ej, sk, ek, tmp);
+  int K = ek - sk + 1, J = ej - sj + 1, I = ei - si + 1;
+  pack_order(tmp, o.NV, K, J, I, kPackOrder[p][s], buf);
+}
+
 void ghost_exchange(Oracle& o) {
   int NV = o.NV;
 #pragma omp parallel for collapse(2)
   for (int p = 0; p < 6; ++p)
     for (int s = 0; s < 4; ++s) {
-      int blockID = p + 1;
-      int ox2 = side_ox2(s), ox3 = side_ox3(s);
-      // source index ranges of a face neighbour (bvals_cc.cpp LoadBoundaryBufferSameLevel)
-      int si = o.is, ei = o.ie;
-      int sj = (ox2 > 0) ? (o.je - G + 1) : o.js;
-      int ej = (ox2 < 0) ? (o.js + G - 1) : o.je;
-      int sk = (ox3 > 0) ? (o.ke - G + 1) : o.ks;
-      int ek = (ox3 < 0) ? (o.ks + G - 1) : o.ke;
-      bool along_x2 = (ox3 != 0);
-      std::vector<double> tmp, buf;
-      const double* src = &o.u[o.at(p, 0, 0, 0, 0)];
-      interpolate_edge(o, src, blockID, along_x2, kDinv[p][s], kTgSide[p][s],
-                       kNbrPanel[p][s], 0, NV - 1, si, ei, sj, ej, sk, ek, tmp);
-      int K = ek - sk + 1, J = ej - sj + 1, I = ei - si + 1;
-      pack_order(tmp, NV, K, J, I, kPackOrder[p][s], buf);
+      std::vector<double> buf;
+      pack_face(o, p, s, buf);
       // unpack into the target's ghost band (SetBoundarySameLevel)
       int t = kNbrPanel[p][s] - 1, ts = kNbrSide[p][s];
       int tox2 = side_ox2(ts), tox3 = side_ox3(ts);
@@ -1763,7 +1777,7 @@ double new_block_dt(Oracle& o) {
 
 // Conserved interior -> ghosts -> primitives -> x1 boundary
 void boundary_and_prim(Oracle& o) {
-  ghost_exchange(o);
+  for (int pass = 0; pass < o.ghost_passes; ++pass) ghost_exchange(o);
   cons_to_prim(o);
   reflect_x1(o);
 }
@@ -2015,6 +2029,88 @@ void ora_restore_from_perturbation(void* h, double* w, double* wl, double* wr) {
           }
         }
       }
+}
+
+// ---- exports that hold pieces of the restatement against the reference's
+// own sources compiled here (oracle/ref, tests/test_ref_pinned.py)
+void ora_vec_abp_from_rll(double X, double Y, int blockID, double U, double V, double* out) {
+  vec_abp_from_rll(X, Y, blockID, U, V, &out[0], &out[1]);
+}
+void ora_vec_rll_from_abp(double X, double Y, int blockID, double V2, double V3, double* out) {
+  vec_rll_from_abp(X, Y, blockID, V2, V3, &out[0], &out[1]);
+}
+void ora_rll_from_xyp(double dX, double dY, int nP, double* out) {
+  rll_from_xyp(dX, dY, nP, out[0], out[1]);
+}
+double ora_interp_loc(int loc_n, int N_blk, int k, int ghost) {
+  return interp_loc(loc_n, N_blk, k, ghost != 0);
+}
+// the connectivity tables, 6 x 4 each (sides Up, Down, Left, Right)
+void ora_panel_tables(int* nbr_panel, int* nbr_side, int* dinv, int* tgside, int* pack) {
+  for (int p = 0; p < 6; ++p)
+    for (int s = 0; s < 4; ++s) {
+      nbr_panel[p * 4 + s] = kNbrPanel[p][s];
+      nbr_side[p * 4 + s] = kNbrSide[p][s];
+      dinv[p * 4 + s] = kDinv[p][s];
+      tgside[p * 4 + s] = kTgSide[p][s];
+      pack[p * 4 + s] = kPackOrder[p][s];
+    }
+}
+// the radial face widths (ncells1), ghosts included
+void ora_get_dx1f(void* h, double* out) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  std::memcpy(out, o.dx1f.data(), o.dx1f.size() * sizeof(double));
+}
+// what panel p sends across side s from the current conserved state;
+// returns the number of values
+int ora_pack_face(void* h, int p, int s, double* buf) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  std::vector<double> b;
+  pack_face(o, p, s, b);
+  std::memcpy(buf, b.data(), b.size() * sizeof(double));
+  return (int)b.size();
+}
+// face 1/2/3 areas, volume and the three centre widths of cell (k, j, i)
+void ora_cell_geometry_at(void* h, int p, int k, int j, int i, double* out) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const PanelGeo& g = o.pg[p];
+  size_t q = o.kj(k, j);
+  out[0] = face1_area(o, g, k, j, i);
+  out[1] = face2_area(o, g, k, j, i);
+  out[2] = face3_area(o, g, k, j, i);
+  out[3] = cell_volume(o, g, k, j, i);
+  out[4] = o.dx1f[i];
+  out[5] = o.x1v[i] * g.dx2a[q];
+  out[6] = o.x1v[i] * g.dx3a[q];
+}
+// the face geometry the Riemann solve of direction ivx at (k, j) uses:
+// (cos, sin of the face metric, covariant projection angle, cell cosine)
+void ora_face_geo(void* h, int p, int k, int j, int ivx, double* out) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const PanelGeo& g = o.pg[p];
+  size_t q = o.kj(k, j);
+  if (ivx == IVY) { out[0] = g.cosf2[q]; out[1] = g.sinf2[q]; out[2] = g.cthp2[q]; }
+  else if (ivx == IVZ) { out[0] = g.cosf3[q]; out[1] = g.sinf3[q]; out[2] = g.cthp3[q]; }
+  else { out[0] = 0.; out[1] = 1.; out[2] = g.cthp1[q]; }
+  out[3] = g.cosc[q];
+}
+// the panel-edge face-state exchange on given x2 and x3 face states (whole
+// arrays of six panels), in place
+void ora_exchange_faces(void* h, double* L2, double* R2, double* L3, double* R3) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  size_t n = o.u.size() * sizeof(double);
+  std::memcpy(o.L3[1].data(), L2, n); std::memcpy(o.R3[1].data(), R2, n);
+  std::memcpy(o.L3[2].data(), L3, n); std::memcpy(o.R3[2].data(), R3, n);
+  exchange_face_states(o);
+  std::memcpy(L2, o.L3[1].data(), n); std::memcpy(R2, o.R3[1].data(), n);
+  std::memcpy(L3, o.L3[2].data(), n); std::memcpy(R3, o.R3[2].data(), n);
+}
+
+// 1 or 2 panel ghost syncs per boundary update (the reference runs 2)
+int ora_set_ghost_passes(void* h, int passes) {
+  if (passes < 1 || passes > 2) return 1;
+  static_cast<Oracle*>(h)->ghost_passes = passes;
+  return 0;
 }
 
 // geometry exports for the tests

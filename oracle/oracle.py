@@ -72,6 +72,21 @@ def lib():
         L.ora_calculate_fluxes.argtypes = [p]
         L.ora_step.argtypes = [p, i, d]
         L.ora_get_mesh.argtypes = [p, i, dp, dp, dp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.ora_vec_abp_from_rll.argtypes = [d, d, i, d, d, dp]
+        L.ora_vec_rll_from_abp.argtypes = [d, d, i, d, d, dp]
+        L.ora_rll_from_xyp.argtypes = [d, d, i, dp]
+        L.ora_interp_loc.restype = d
+        L.ora_interp_loc.argtypes = [i, i, i, i]
+        L.ora_panel_tables.argtypes = [ip] * 5
+        L.ora_get_dx1f.argtypes = [p, dp]
+        L.ora_pack_face.restype = i
+        L.ora_pack_face.argtypes = [p, i, i, dp]
+        L.ora_cell_geometry_at.argtypes = [p, i, i, i, i, dp]
+        L.ora_face_geo.argtypes = [p, i, i, i, i, dp]
+        L.ora_exchange_faces.argtypes = [p, dp, dp, dp, dp]
+        L.ora_set_ghost_passes.restype = i
+        L.ora_set_ghost_passes.argtypes = [p, i]
         L.ora_cell_geometry.restype = i
         L.ora_cell_geometry.argtypes = [ctypes.POINTER(ExoConfig), dp, dp, dp, dp]
         L.ora_riemann_face.argtypes = [i, i, i, d, dp, dp, dp, d, d, d, d]
@@ -129,6 +144,12 @@ class Oracle:
         if getattr(self, "_h", None):
             lib().ora_destroy(self._h)
             self._h = None
+
+    def set_ghost_passes(self, passes):
+        """1 panel ghost sync per boundary update, or 2 as the reference's
+        cubed-sphere task list runs them."""
+        if lib().ora_set_ghost_passes(self._h, int(passes)):
+            raise ValueError("passes must be 1 or 2")
 
     def set_primitive(self, w):
         w = np.ascontiguousarray(w, dtype=np.float64)
@@ -197,6 +218,35 @@ class Oracle:
         assert du.flags.c_contiguous and du.dtype == np.float64
         lib().ora_solve_implicit_3d(self._h, _ptr(du), _ptr(w), float(dt))
 
+    def dx1f(self):
+        out = np.zeros(self.cfg.L + 2 * NGHOST)
+        lib().ora_get_dx1f(self._h, _ptr(out))
+        return out
+
+    def pack_face(self, p, s):
+        """What panel p sends across side s (0 Up, 1 Down, 2 Left, 3 Right)
+        from the current conserved state."""
+        buf = np.zeros(self.nvar * 3 * (self.cfg.N + 6) * (self.cfg.L + 6))
+        n = lib().ora_pack_face(self._h, p, s, _ptr(buf))
+        return buf[:n]
+
+    def cell_geometry_at(self, p, k, j, i):
+        out = np.zeros(7)
+        lib().ora_cell_geometry_at(self._h, p, k, j, i, _ptr(out))
+        return out
+
+    def face_geo(self, p, k, j, ivx):
+        out = np.zeros(4)
+        lib().ora_face_geo(self._h, p, k, j, ivx, _ptr(out))
+        return out
+
+    def exchange_faces(self, L2, R2, L3, R3):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in (L2, R2, L3, R3)]
+        for a in arrs:
+            assert a.shape == self.shape
+        lib().ora_exchange_faces(self._h, *[_ptr(a) for a in arrs])
+        return arrs
+
     def mesh(self, panel):
         c = self.cfg
         x1f = np.empty(c.L + 2 * NGHOST + 1)
@@ -246,3 +296,33 @@ def implicit_columns(w, du, colgeo, x1f, x1v, dx1f, dt, gamma, grav, full=True):
                                  _ptr(np.ascontiguousarray(x1f)), _ptr(np.ascontiguousarray(x1v)),
                                  _ptr(np.ascontiguousarray(dx1f)), dt, gamma, grav)
     return out
+
+
+def panel_tables():
+    """(neighbour panel, arrival side, direction inversion, target side,
+    pack order), each 6 x 4 (sides Up, Down, Left, Right)."""
+    out = [np.zeros(24, dtype=np.int32) for _ in range(5)]
+    lib().ora_panel_tables(*[a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) for a in out])
+    return [a.reshape(6, 4) for a in out]
+
+
+def vec_abp_from_rll(X, Y, blockID, U, V):
+    out = np.zeros(2)
+    lib().ora_vec_abp_from_rll(X, Y, blockID, U, V, _ptr(out))
+    return out
+
+
+def vec_rll_from_abp(X, Y, blockID, V2, V3):
+    out = np.zeros(2)
+    lib().ora_vec_rll_from_abp(X, Y, blockID, V2, V3, _ptr(out))
+    return out
+
+
+def rll_from_xyp(dX, dY, nP):
+    out = np.zeros(2)
+    lib().ora_rll_from_xyp(dX, dY, nP, _ptr(out))
+    return out
+
+
+def interp_loc(loc_n, N_blk, k, ghost):
+    return lib().ora_interp_loc(loc_n, N_blk, k, int(bool(ghost)))

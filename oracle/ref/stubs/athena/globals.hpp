@@ -1,0 +1,7 @@
+// harness stand-in for Athena++'s globals.hpp
+#ifndef REF_STUB_GLOBALS_HPP_
+#define REF_STUB_GLOBALS_HPP_
+namespace Globals {
+static const int my_rank = 0, nranks = 1;
+}
+#endif

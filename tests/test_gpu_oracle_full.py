@@ -1,0 +1,110 @@
+"""The CUDA path against the CPU oracle at the configurations' own sizes and
+at the edges of the ensemble's parameter distribution.
+
+Tolerances (the decomposition's log, exp and pow may differ in the last bit
+between CUDA and glibc; everything else in the FP64 build is bit-exact, see
+test_gpu_parity.py):
+  * FP64 build: relative L2 of every conserved variable <= 1e-9 after 10
+    CFL steps of the C2 workload (6 x 96 x 96 x 64), and after 3 steps of
+    each extreme member; the CFL time step to 1e-9.
+  * mixed build: relative L2 of density and pressure <= 1e-6 after 3 steps
+    of each extreme member.
+"""
+import numpy as np
+import pytest
+
+from exocubed_b200 import _native as nat
+from exocubed_b200 import workloads as W
+from exocubed_b200.atmosphere import CubedSphereAtmosphere
+from exocubed_b200.ensemble import Ensemble
+
+pytestmark = pytest.mark.gpu
+
+
+def _pressure(u, gamma):
+    ke = 0.5 * (u[:, 1] ** 2 + u[:, 2] ** 2 + u[:, 3] ** 2) / u[:, 0]
+    return (gamma - 1.0) * (u[:, 4] - ke)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("rsolver", [nat.EXO_RS_LMARS, nat.EXO_RS_HLLC])
+def test_c2_fp64_ten_steps_against_oracle(oracle_mod, rsolver):
+    """C2 as specified: 6 x 96 x 96 x 64, WENO5, implicit_flag 9, seeded
+    isothermal state with temperature and wind noise, 10 CFL steps."""
+    cfg = W.dry_atmosphere_config(N=96, L=64, rsolver=rsolver)
+    state = W.dry_atmosphere_state(cfg, seed=0)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(state)
+    o.step(10)
+    with CubedSphereAtmosphere(cfg) as g:
+        g.set_primitive(state)
+        g.step(10)
+        ug = W.interior(g.conserved())
+        assert g.invalid() == 0
+        assert g.dt == pytest.approx(o.dt, rel=1e-9)
+        assert g.time == pytest.approx(o.time, rel=1e-9)
+    uo = W.interior(o.conserved())
+    for n in range(5):
+        assert _rel(ug[:, n], uo[:, n]) < 1e-9, (n, _rel(ug[:, n], uo[:, n]))
+
+
+# the corners of the member distribution: gamma 1.3 / 1.67, gravity 3 / 25,
+# surface temperature 150 / 400 K, top temperature 100 / 250 K (at most Ts)
+EXTREMES = [
+    dict(Ts=150., Ttop=100., g=3., gamma=1.3),
+    dict(Ts=400., Ttop=250., g=25., gamma=1.67),
+    dict(Ts=400., Ttop=100., g=3., gamma=1.67),
+    dict(Ts=150., Ttop=250., g=25., gamma=1.3),   # isothermal column (Ttop capped at Ts)
+]
+
+
+def _extreme(params, precision, N=8, L=16):
+    cfg, prof = W.member_config(N, L, precision=precision, **params)
+    return cfg, W.member_state(cfg, prof, seed=4)
+
+
+def _check(cfg, ug, o, precision):
+    uo = W.interior(o.conserved())
+    if precision == nat.EXO_PREC_FP64:
+        for n in range(5):
+            assert _rel(ug[:, n], uo[:, n]) < 1e-9, (n, _rel(ug[:, n], uo[:, n]))
+    else:
+        g = cfg["gamma"]
+        assert _rel(ug[:, 0], uo[:, 0]) < 1e-6
+        assert _rel(_pressure(ug, g), _pressure(uo, g)) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+@pytest.mark.parametrize("k", range(len(EXTREMES)))
+def test_member_extremes_against_oracle(oracle_mod, k, precision):
+    cfg, state = _extreme(EXTREMES[k], precision)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(state)
+    o.step(3)
+    with CubedSphereAtmosphere(cfg) as a:
+        a.set_primitive(state)
+        a.step(3)
+        assert a.invalid() == 0
+        assert a.dt == pytest.approx(o.dt, rel=1e-9 if precision == 0 else 1e-5)
+        _check(cfg, W.interior(a.conserved()), o, precision)
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_extremes_batched_against_oracle(oracle_mod, precision):
+    """All four extremes in one batched ensemble (uneven sizes), each member
+    against its own oracle run."""
+    members = [_extreme(p, precision, N=6 + 2 * k, L=12 + 4 * k)
+               for k, p in enumerate(EXTREMES)]
+    with Ensemble(precision=precision, capacity=8) as ens:
+        slots = [ens.add(c, w) for c, w in members]
+        ens.step(3)
+        got = [W.interior(ens.conserved(s)) for s in slots]
+        assert all(ens.invalid(s) == 0 for s in slots)
+    for (cfg, w), ug in zip(members, got):
+        o = oracle_mod.Oracle(cfg)
+        o.set_primitive(w)
+        o.step(3)
+        _check(cfg, ug, o, precision)

@@ -99,3 +99,29 @@ def test_oracle_decomposition_round_trip(oracle_mod):
     faces = (slice(None), slice(None), slice(3, -3), slice(3, -3), slice(3, -2))
     assert (wl[faces][:, 4] > 0).all() and (wr[faces][:, 4] > 0).all()
     assert (wl[faces][:, 0] > 0).all()
+
+
+@pytest.mark.parametrize("case", ["shallow", "dry_lmars", "dry_hllc_partial"])
+def test_second_ghost_pass_changes_nothing(oracle_mod, case):
+    """The reference syncs the panel ghosts twice per stage and at start-up
+    (patches/24.time_integrator.patch:22-28, patches/29.mesh.patch:19-86).
+    With one block per panel the second pass reads the same interior cells
+    as the first, so the oracle (and the CUDA path) run one pass: running
+    both passes leaves every value of the run, ghosts included, unchanged."""
+    if case == "shallow":
+        cfg = W.shallow_water_config(N=8)
+        state, steps = W.shallow_water_state(cfg, seed=2), 4
+    else:
+        rs, flag = (1, 9) if case == "dry_lmars" else (2, 1)
+        cfg = W.dry_atmosphere_config(N=8, L=10, rsolver=rs, implicit_flag=flag)
+        state, steps = W.dry_atmosphere_state(cfg, seed=2), 3
+    out = []
+    for passes in (1, 2):
+        o = oracle_mod.Oracle(cfg)
+        o.set_ghost_passes(passes)
+        o.set_primitive(state)
+        o.step(steps)
+        out.append((o.conserved(), o.primitive(), o.dt, o.time))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2] and out[0][3] == out[1][3]
