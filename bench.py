@@ -406,7 +406,104 @@ def accuracy(cfg, state, steps, precision=1, ref=None):
             "state_valid": invalid == 0}
 
 
-def serving_sample(rate, nreq, steps, fp64_baseline=True):
+ORACLE_RUN = os.path.join(ROOT, "tests", "golden", "oracle_c2_lmars.npz")
+
+
+def accuracy_vs_oracle(precisions=(0, 1, 2), path=ORACLE_RUN):
+    """The GPU paths against the oracle's own long run of the C2 workload
+    (6x96x96x64, LMARS, implicit_flag 9, seeded state 0; the oracle's first
+    CFL step held fixed; tests/golden/make_oracle_runs.py): relative L2 and
+    L-inf of each primitive variable on the run's 8192 sampled interior
+    cells after each of its checkpoints (10, 100, 1000 steps)."""
+    import numpy as np
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
+    if not os.path.exists(path):
+        return None
+    fx = np.load(path)
+    N, L, rs, seed = int(fx["N"]), int(fx["L"]), int(fx["rsolver"]), int(fx["seed"])
+    dt = float(fx["dt"])
+    idx = fx["cells"]
+    cfg = W.dry_atmosphere_config(N=N, L=L, rsolver=rs)
+    state = W.dry_atmosphere_state(cfg, seed=seed)
+    names = ["rho", "v1", "v2", "v3", "p"]
+    out = {"workload": f"exo3 dry ideal gas 6x{N}x{N}x{L} LMARS implicit(9), seeded state {seed}, "
+                       f"dt = {dt:.6g} s fixed (the oracle's first CFL step)",
+           "vs": "oracle (FP64 C++ restatement, its own run on the same seeded state)",
+           "cells_sampled": int(idx.shape[1]), "paths": {}}
+    for prec in precisions:
+        a = CubedSphereAtmosphere(dict(cfg, precision=prec))
+        a.set_primitive(state)
+        done, rows = 0, {}
+        for n in [int(x) for x in fx["checkpoints"]]:
+            a.step(n - done, dt)
+            done = n
+            w = a.primitive()
+            g = w[idx[0], :, idx[1], idx[2], idx[3]].T
+            o = fx[f"sample_{n}"]
+            rows[str(n)] = {
+                name: {"rel_l2": float(np.linalg.norm(g[q] - o[q]) / np.linalg.norm(o[q])),
+                       "linf": float(np.abs(g[q] - o[q]).max()),
+                       "rel_linf": float(np.abs(g[q] - o[q]).max() / np.abs(o[q]).max())}
+                for q, name in enumerate(names)}
+            rows[str(n)]["state_valid"] = a.invalid() == 0
+        a.close()
+        out["paths"][{0: "fp64", 1: "mixed", 2: "mixed_f32_solve"}[prec]] = rows
+    return out
+
+
+def measure_ensemble(members, prec, steps, warmup, pg=None, cache=None, tune=True):
+    """Device-timed batched steps of an ensemble (state resident): ms, launches, validity."""
+    import torch
+
+    from exocubed_b200.ensemble import Ensemble
+    ens = Ensemble(precision=prec, capacity=len(members))
+    slots = [ens.add(dict(c, precision=prec), w) for c, w in members]
+    tiles = ens.autotune(cache) if tune else ens.tiles
+    stream = torch.cuda.ExternalStream(ens.stream)
+    ens.step(warmup)
+    ens.synchronize()
+    l0 = ens.stats()["launches"]
+    barrier(pg)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(pg)
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    out = {"ms": ms, "launches": ens.stats()["launches"] - l0, "tiles": tiles,
+           "valid": all(ens.invalid(s) == 0 for s in slots)}
+    ens.close()
+    return out
+
+
+def ensemble_sample(nmembers, steps, warmup, cache=None):
+    """The C4 batched ensemble in the default line: nmembers atmospheres of
+    the member distribution, mixed precision and the plain FP64 path on the
+    same members, one graph-captured batched step per step."""
+    from exocubed_b200 import workloads as W
+    members = [W.ensemble_member(sd, precision=1) for sd in member_seeds(0, nmembers)]
+    cells = sum(cells_of(c) for c, _ in members)
+    mixed = measure_ensemble(members, 1, steps, warmup, cache=cache)
+    fp64 = measure_ensemble(members, 0, steps, warmup, cache=cache)
+    return {"members": nmembers, "cells_per_step": cells, "steps": steps, "warmup": warmup,
+            "workload": "batched ensemble of exo3 dry atmospheres, N in {24..96}, L in {32..96}, "
+                        "Ts 150-400 K, gravity 3-25, gamma 1.3-1.67, one graph launch per step",
+            "mixed": {"value": cells * steps / (mixed["ms"] / 1e3),
+                      "ms_per_step": mixed["ms"] / steps, "gpu_launches": mixed["launches"],
+                      "state_valid": mixed["valid"]},
+            "fp64": {"value": cells * steps / (fp64["ms"] / 1e3),
+                     "ms_per_step": fp64["ms"] / steps, "state_valid": fp64["valid"]},
+            "mixed_over_fp64": fp64["ms"] / mixed["ms"],
+            "tiles": "autotuned per kernel over the members (autotune.batch_tiles)"}
+
+
+def serving_sample(rate, nreq, steps, fp64_baseline=True, cache=None):
     """A short continuous-batching run (mixed) and, for the same requests,
     the plain FP64 path one request at a time."""
     from exocubed_b200 import autotune
@@ -418,7 +515,7 @@ def serving_sample(rate, nreq, steps, fp64_baseline=True):
     for n, a in enumerate(t_arr):
         cfg, w = W.ensemble_member(50_000 + n, precision=1)
         reqs.append(Request(n, cfg, w, float(a), steps))
-    cache = autotune.TileCache()
+    cache = cache if cache is not None else autotune.TileCache()
     autotune.batch_tiles([r.cfg for r in reqs], cache)  # measured before the clock starts
     srv = Server(precision=1, capacity=64, budget_bytes=150 * 10 ** 9, max_chunk=8,
                  tile_cache=cache)
@@ -490,9 +587,17 @@ def run_ours(args):
             extra["accuracy"] = accuracy(c0, state, args.accuracy_steps, prec, ref)
             if f32s is not None:
                 extra["accuracy_f32_solve"] = accuracy(c0, state, args.accuracy_steps, 2, ref)
+        if args.oracle_accuracy:
+            extra["accuracy_vs_oracle"] = accuracy_vs_oracle()
+        from exocubed_b200 import autotune
+        cache = autotune.TileCache()
+        if args.ensemble_members > 0:
+            extra["ensemble"] = ensemble_sample(args.ensemble_members, args.ensemble_steps,
+                                                3, cache)
         if args.serve_requests > 0:
             extra["serving"] = serving_sample(args.serve_rate, args.serve_requests,
-                                              args.serve_steps, not args.no_fp64_baseline)
+                                              args.serve_steps, not args.no_fp64_baseline,
+                                              cache)
         if not args.no_cpu_baseline:
             r = run_cpu(args.workload, args.cpu_steps, args.cpu_warmup)
             extra["cpu_baseline"] = {
@@ -553,7 +658,11 @@ def run_ours(args):
         "state_valid": main["invalid"] == 0,
     }
     if "accuracy" in extra:
-        line["accuracy"] = extra["accuracy"]
+        line["accuracy"] = dict(extra["accuracy"], vs="the plain FP64 GPU path on the same state")
+    if extra.get("accuracy_vs_oracle"):
+        line["accuracy_vs_oracle"] = extra["accuracy_vs_oracle"]
+    if "ensemble" in extra:
+        line["ensemble"] = extra["ensemble"]
     if "serving" in extra:
         line["serving"] = extra["serving"]
     print(json.dumps(line))
@@ -816,8 +925,13 @@ def main():
                     help="skip the leg with FP32 implicit blocks (--precision 2)")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="steps of the mixed-vs-FP64 error check in the bench line (0: none)")
-    ap.add_argument("--serve-requests", type=int, default=8,
+    ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests of the serving sample in the bench line (0: none)")
+    ap.add_argument("--no-oracle-accuracy", dest="oracle_accuracy", action="store_false",
+                    help="skip the 1000-step C2 comparison with the oracle's run")
+    ap.add_argument("--ensemble-members", type=int, default=64,
+                    help="members of the C4 ensemble sample in the bench line (0: none)")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--serve-rate", type=float, default=100.0)
     ap.add_argument("--ref-steps", type=int, default=0,
                     help="full steps the reference arm times at most (0: all of --steps)")

@@ -45,7 +45,12 @@ EXPORTED = [
     "exo_ensemble_checkpoint_bytes", "exo_ensemble_checkpoint_save",
     "exo_ensemble_add_checkpoint", "exo_set_max_redo", "exo_redo_count",
     "exo_measure_fma_peak",
+    "exo_panel_pack", "exo_save_lr3d", "exo_load_lr3d", "exo_lr3d_arrays",
+    "exo_synchronize_faces", "exo_conserved_to_primitive", "exo_primitive_to_conserved",
+    "exo_sound_speed", "exo_set_primitive_views", "exo_get_primitive_views",
+    "exo_get_conserved_views", "exo_solve_implicit_3d_views",
 ]
+EXO_DTYPE_F64 = 0
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
 
 
@@ -67,6 +72,35 @@ class ExoConfig(ctypes.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ArrayView(ctypes.Structure):
+    """exo_array_view of include/exo_b200.h: a strided (n, k, j, i) view."""
+    _fields_ = [
+        ("data", ctypes.c_void_p), ("dtype", ctypes.c_int),
+        ("nx4", ctypes.c_int), ("nx3", ctypes.c_int), ("nx2", ctypes.c_int), ("nx1", ctypes.c_int),
+        ("stride", ctypes.c_int64 * 4), ("device", ctypes.c_int),
+    ]
+
+
+def views_of(panels, device=-1):
+    """Six ArrayViews of six 4-D panel arrays: numpy arrays (host, any
+    strides) or, with device >= 0, (data_ptr, shape, element strides)
+    triples of device arrays."""
+    out = (ArrayView * 6)()
+    for p, a in enumerate(panels):
+        if device < 0:
+            assert a.dtype.itemsize == 8 and a.ndim == 4
+            ptr, shape, strides = a.ctypes.data, a.shape, [st // 8 for st in a.strides]
+        else:
+            ptr, shape, strides = a
+        out[p].data = ptr
+        out[p].dtype = EXO_DTYPE_F64
+        out[p].nx4, out[p].nx3, out[p].nx2, out[p].nx1 = shape
+        for q in range(4):
+            out[p].stride[q] = strides[q]
+        out[p].device = device
+    return out
 
 
 class CheckpointHeader(ctypes.Structure):
@@ -157,6 +191,19 @@ def lib():
     L.exo_redo_count.argtypes = [p, ctypes.POINTER(ctypes.c_int64)]
     L.exo_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_double)]
+    L.exo_panel_pack.argtypes = [p, p, p] + [i] * 8 + [ip, i, i, i, i, p]
+    L.exo_save_lr3d.argtypes = [p, p, p, i, i, i, i, i, i, p]
+    L.exo_load_lr3d.argtypes = [p, p, p, i, i, i, i, i, i, p]
+    L.exo_lr3d_arrays.argtypes = [p] + [ctypes.POINTER(p)] * 4
+    L.exo_synchronize_faces.argtypes = [p, p]
+    L.exo_conserved_to_primitive.argtypes = [p, p, p, i, i, i, i, i, i, p]
+    L.exo_primitive_to_conserved.argtypes = [p, p, p, i, i, i, i, i, i, p]
+    L.exo_sound_speed.argtypes = [p, i, p, p, p]
+    vp = ctypes.POINTER(ArrayView)
+    L.exo_set_primitive_views.argtypes = [p, vp]
+    L.exo_get_primitive_views.argtypes = [p, vp]
+    L.exo_get_conserved_views.argtypes = [p, vp]
+    L.exo_solve_implicit_3d_views.argtypes = [p, vp, vp, d]
     L.exo_checkpoint_bytes.argtypes = [p, ctypes.POINTER(sz)]
     L.exo_checkpoint_save.argtypes = [p, p, sz]
     L.exo_checkpoint_load.argtypes = [p, p, sz]

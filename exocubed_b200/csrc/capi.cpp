@@ -100,6 +100,9 @@ struct exo_ctx {
   int64_t redo_attempts = 0;
   double* redo_state = nullptr;
   exo::DevScalars* redo_sc = nullptr;
+  // face-state stores of the SaveLR3DValues / LoadLR3DValues hooks: x2 L, R,
+  // x3 L, R in the context's layout (allocated on first use)
+  double* lr3d = nullptr;
 };
 
 
@@ -160,7 +163,7 @@ static int one_stage(exo_ctx* c, int s, bool cfl) {
   int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
   if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return STEP(launch_update, v, s, c->stream); })))
     return rc;
-  if (implicit && (rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(v.precision),
+  if (implicit && (rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(v.implicit_flag),
                               [&] { return STEP(launch_implicit, v, s, c->stream); })))
     return rc;
   return boundary_and_prim(c, s == 2 && cfl);
@@ -874,7 +877,7 @@ int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, dou
   size_t bytes = c->state_elems * sizeof(double);
   CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->v.du, du_host, bytes, cudaMemcpyHostToDevice, c->stream));
-  int rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(c->v.precision),
+  int rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(c->v.implicit_flag),
                  [&] { return STEP(launch_implicit_du, c->v, dt, c->stream); });
   if (rc) return fail(rc, "implicit launch failed");
   CK(cudaMemcpyAsync(du_host, c->v.du, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -965,6 +968,7 @@ int exo_check_state(exo_ctx* c, int* invalid) {
   int zero = 0;
   CK(cudaMemcpyAsync(&c->v.sc->invalid, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (s.timeout) return fail(EXO_ERR_TIMEOUT, "a kernel's bounded wait for its bulk copies gave up");
   return EXO_OK;
 }
 
@@ -1095,6 +1099,276 @@ int exo_measure_fma_peak(int fp64, int repeats, double* flops_per_s) {
   int rc = exo::measure_fma_peak(fp64 != 0, repeats, flops_per_s, &err);
   if (rc) return fail(rc, err);
   return EXO_OK;
+}
+
+// ------------------------------------------------- panel-exchange hooks ----
+static cudaStream_t hook_stream(exo_ctx* c, void* stream) {
+  return stream ? (cudaStream_t)stream : c->stream;
+}
+
+int exo_panel_pack(exo_ctx* c, const double* src, double* buf, int sn, int en, int si, int ei,
+                   int sj, int ej, int sk, int ek, int* offset, int ox1, int ox2, int ox3,
+                   int panel, void* stream) {
+  if (!c || !src || !buf || !offset) return fail(EXO_ERR_ARG, "NULL argument");
+  const DevView& v = c->v;
+  if (panel < 0 || panel > 5) return fail(EXO_ERR_ARG, "panel must be 0..5");
+  if (sn < 0 || en >= v.nv || sn > en || si < 0 || ei >= v.nc1 || si > ei || sj < 0 ||
+      ej >= v.nc2 || sj > ej || sk < 0 || ek >= v.nc3 || sk > ek)
+    return fail(EXO_ERR_SHAPE, "index range outside the panel array");
+  cudaStream_t st = hook_stream(c, stream);
+  const bool face = ox1 == 0 && ((ox2 != 0) != (ox3 != 0));
+  if (!face) {
+    // corners and radial neighbours: PackDataR0, a plain copy of the range
+    const int64_t ss[4] = {(int64_t)v.nc3 * v.nc2 * v.nc1, (int64_t)v.nc2 * v.nc1, v.nc1, 1};
+    const int size[4] = {en - sn + 1, ek - sk + 1, ej - sj + 1, ei - si + 1};
+    const int64_t ds[4] = {(int64_t)size[1] * size[2] * size[3], (int64_t)size[2] * size[3],
+                           size[3], 1};
+    const double* s0 = src + (((size_t)sn * v.nc3 + sk) * v.nc2 + sj) * v.nc1 + si;
+    RK(exo::launch_view_copy(s0, ss, buf + *offset, ds, size, st));
+    *offset += size[0] * size[1] * size[2] * size[3];
+    return EXO_OK;
+  }
+  // a panel edge: the band LoadBoundaryBufferSameLevel hands to PackData
+  const int G = exo::G;
+  const int want_sj = ox2 > 0 ? v.je - G + 1 : v.js, want_ej = ox2 < 0 ? v.js + G - 1 : v.je;
+  const int want_sk = ox3 > 0 ? v.ke - G + 1 : v.ks, want_ek = ox3 < 0 ? v.ks + G - 1 : v.ke;
+  if (sn != 0 || en != v.nv - 1 || si != v.is || ei != v.ie || sj != want_sj || ej != want_ej ||
+      sk != want_sk || ek != want_ek)
+    return fail(EXO_ERR_SHAPE, "a panel-edge pack takes every variable and the G-wide edge band "
+                               "of the interior (one block per panel)");
+  const int side = ox2 < 0 ? 0 : ox2 > 0 ? 1 : ox3 < 0 ? 2 : 3;
+  int tp, ts;
+  exo::panel_neighbor(panel, side, &tp, &ts);
+  const int tox2 = ts == 0 ? -1 : ts == 1 ? 1 : 0, tox3 = ts == 2 ? -1 : ts == 3 ? 1 : 0;
+  const int rsj = tox2 < 0 ? v.js - G : tox2 > 0 ? v.je + 1 : v.js;
+  const int rsk = tox3 < 0 ? v.ks - G : tox3 > 0 ? v.ke + 1 : v.ks;
+  const int J = tox2 != 0 ? G : v.N, K = tox3 != 0 ? G : v.N;
+  RK(exo::launch_panel_pack(v, src, buf + *offset, tp, rsk, rsj, K, J, st));
+  *offset += v.nv * K * J * v.L;
+  return EXO_OK;
+}
+
+static int lr3d_ensure(exo_ctx* c) {
+  if (c->lr3d) return EXO_OK;
+  CK(cudaMalloc((void**)&c->lr3d, 4 * c->state_elems * sizeof(double)));
+  c->owned.push_back(c->lr3d);
+  CK(cudaMemsetAsync(c->lr3d, 0, 4 * c->state_elems * sizeof(double), c->stream));
+  return EXO_OK;
+}
+static double* lr3d_store(exo_ctx* c, int direction, bool right) {
+  return c->lr3d + ((size_t)(direction - 2) * 2 + (right ? 1 : 0)) * c->state_elems;
+}
+
+int exo_save_lr3d(exo_ctx* c, const double* L_row, const double* R_row, int direction, int panel,
+                  int k, int j, int il, int iu, void* stream) {
+  if (!c || !L_row || !R_row) return fail(EXO_ERR_ARG, "NULL argument");
+  const DevView& v = c->v;
+  if (direction != 2 && direction != 3) return fail(EXO_ERR_ARG, "direction must be 2 or 3");
+  if (panel < 0 || panel > 5 || k < 0 || k >= v.nc3 || j < 0 || j >= v.nc2 || il < 0 ||
+      iu >= v.nc1 || il > iu)
+    return fail(EXO_ERR_SHAPE, "row outside the arrays");
+  int rc = lr3d_ensure(c);
+  if (rc) return rc;
+  cudaStream_t st = hook_stream(c, stream);
+  const size_t w = (size_t)(iu - il + 1) * sizeof(double);
+  for (int side = 0; side < 2; ++side) {
+    double* dst = lr3d_store(c, direction, side == 1) + (((size_t)panel * v.nv * v.nc3 + k) * v.nc2 + j) * v.nc1 + il;
+    const double* srow = (side ? R_row : L_row) + il;
+    CK(cudaMemcpy2DAsync(dst, v.cells * sizeof(double), srow, v.nc1 * sizeof(double), w, v.nv,
+                         cudaMemcpyDefault, st));
+  }
+  return EXO_OK;
+}
+
+int exo_load_lr3d(exo_ctx* c, double* L_row, double* R_row, int direction, int panel, int k,
+                  int j, int il, int iu, void* stream) {
+  if (!c || !L_row || !R_row) return fail(EXO_ERR_ARG, "NULL argument");
+  const DevView& v = c->v;
+  if (direction != 2 && direction != 3) return fail(EXO_ERR_ARG, "direction must be 2 or 3");
+  if (panel < 0 || panel > 5 || k < 0 || k >= v.nc3 || j < 0 || j >= v.nc2 || il < 0 ||
+      iu >= v.nc1 || il > iu)
+    return fail(EXO_ERR_SHAPE, "row outside the arrays");
+  int rc = lr3d_ensure(c);
+  if (rc) return rc;
+  cudaStream_t st = hook_stream(c, stream);
+  const size_t w = (size_t)(iu - il + 1) * sizeof(double);
+  for (int side = 0; side < 2; ++side) {
+    const double* src = lr3d_store(c, direction, side == 1) + (((size_t)panel * v.nv * v.nc3 + k) * v.nc2 + j) * v.nc1 + il;
+    double* drow = (side ? R_row : L_row) + il;
+    CK(cudaMemcpy2DAsync(drow, v.nc1 * sizeof(double), src, v.cells * sizeof(double), w, v.nv,
+                         cudaMemcpyDefault, st));
+  }
+  return EXO_OK;
+}
+
+int exo_lr3d_arrays(exo_ctx* c, double** L2, double** R2, double** L3, double** R3) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = lr3d_ensure(c);
+  if (rc) return rc;
+  if (L2) *L2 = lr3d_store(c, 2, false);
+  if (R2) *R2 = lr3d_store(c, 2, true);
+  if (L3) *L3 = lr3d_store(c, 3, false);
+  if (R3) *R3 = lr3d_store(c, 3, true);
+  return EXO_OK;
+}
+
+int exo_synchronize_faces(exo_ctx* c, void* stream) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = lr3d_ensure(c);
+  if (rc) return rc;
+  RK(exo::launch_face_sync(c->v, lr3d_store(c, 2, false), lr3d_store(c, 2, true),
+                           lr3d_store(c, 3, false), lr3d_store(c, 3, true),
+                           hook_stream(c, stream)));
+  return EXO_OK;
+}
+
+// ------------------------------------------------- equation-of-state hooks --
+static int eos_range(exo_ctx* c, int to_prim, const double* in, double* out, int il, int iu,
+                     int jl, int ju, int kl, int ku, void* stream) {
+  if (!c || !in || !out) return fail(EXO_ERR_ARG, "NULL argument");
+  const DevView& v = c->v;
+  if (il < 0 || iu >= v.nc1 || jl < 0 || ju >= v.nc2 || kl < 0 || ku >= v.nc3)
+    return fail(EXO_ERR_SHAPE, "index range outside the arrays");
+  RK(exo::launch_eos_range(v, to_prim, in, out, il, iu, jl, ju, kl, ku, hook_stream(c, stream)));
+  return EXO_OK;
+}
+
+int exo_conserved_to_primitive(exo_ctx* c, const double* u, double* w, int il, int iu, int jl,
+                               int ju, int kl, int ku, void* stream) {
+  return eos_range(c, 1, u, w, il, iu, jl, ju, kl, ku, stream);
+}
+
+int exo_primitive_to_conserved(exo_ctx* c, const double* w, double* u, int il, int iu, int jl,
+                               int ju, int kl, int ku, void* stream) {
+  return eos_range(c, 0, w, u, il, iu, jl, ju, kl, ku, stream);
+}
+
+int exo_sound_speed(exo_ctx* c, int n, const double* prim, double* cs, void* stream) {
+  if (!c || n < 0 || (n > 0 && (!prim || !cs))) return fail(EXO_ERR_ARG, "bad argument");
+  RK(exo::launch_sound_speed(c->v, n, prim, cs, hook_stream(c, stream)));
+  return EXO_OK;
+}
+
+// ----------------------------------------------------------- array views --
+// Checks six panel views against the context's per-panel shape.
+static int check_views(exo_ctx* c, const exo_array_view* views) {
+  if (!views) return fail(EXO_ERR_ARG, "NULL views");
+  const DevView& v = c->v;
+  for (int p = 0; p < 6; ++p) {
+    const exo_array_view& a = views[p];
+    if (!a.data) return fail(EXO_ERR_ARG, "view without data");
+    if (a.dtype != EXO_DTYPE_F64) return fail(EXO_ERR_ARG, "views hold FP64 values");
+    if (a.nx4 != v.nv || a.nx3 != v.nc3 || a.nx2 != v.nc2 || a.nx1 != v.nc1)
+      return fail(EXO_ERR_SHAPE, "a panel view is (nvar, N+6, N+6, L+6)");
+    if (a.device >= 0 && a.device != c->device)
+      return fail(EXO_ERR_ARG, "device view on another GPU than the context's");
+  }
+  return EXO_OK;
+}
+
+// six panel views <-> the contiguous host staging array (whole-atmosphere layout)
+static int views_gather(exo_ctx* c, const exo_array_view* views, std::vector<double>& host) {
+  const DevView& v = c->v;
+  const size_t pan = (size_t)v.nv * v.cells;
+  host.resize(6 * pan);
+  const int size[4] = {v.nv, v.nc3, v.nc2, v.nc1};
+  const int64_t cs[4] = {(int64_t)v.nc3 * v.nc2 * v.nc1, (int64_t)v.nc2 * v.nc1, v.nc1, 1};
+  double* tmp = nullptr;
+  for (int p = 0; p < 6; ++p) {
+    const exo_array_view& a = views[p];
+    const double* d = static_cast<const double*>(a.data);
+    if (a.device < 0) {
+      double* out = host.data() + p * pan;
+      for (int n = 0; n < v.nv; ++n)
+        for (int k = 0; k < v.nc3; ++k)
+          for (int j = 0; j < v.nc2; ++j)
+            for (int i = 0; i < v.nc1; ++i)
+              *out++ = d[n * a.stride[0] + k * a.stride[1] + j * a.stride[2] + i * a.stride[3]];
+    } else {
+      if (!tmp) CK(cudaMalloc((void**)&tmp, pan * sizeof(double)));
+      int rc = exo::launch_view_copy(d, a.stride, tmp, cs, size, c->stream);
+      if (!rc && cudaMemcpyAsync(host.data() + p * pan, tmp, pan * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+        rc = EXO_ERR_CUDA;
+      if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = EXO_ERR_CUDA;
+      if (rc) {
+        cudaFree(tmp);
+        return fail(EXO_ERR_CUDA, "view gather failed");
+      }
+    }
+  }
+  if (tmp) cudaFree(tmp);
+  return EXO_OK;
+}
+
+static int views_scatter(exo_ctx* c, const std::vector<double>& host, const exo_array_view* views) {
+  const DevView& v = c->v;
+  const size_t pan = (size_t)v.nv * v.cells;
+  const int size[4] = {v.nv, v.nc3, v.nc2, v.nc1};
+  const int64_t cs[4] = {(int64_t)v.nc3 * v.nc2 * v.nc1, (int64_t)v.nc2 * v.nc1, v.nc1, 1};
+  double* tmp = nullptr;
+  for (int p = 0; p < 6; ++p) {
+    const exo_array_view& a = views[p];
+    double* d = static_cast<double*>(a.data);
+    if (a.device < 0) {
+      const double* in = host.data() + p * pan;
+      for (int n = 0; n < v.nv; ++n)
+        for (int k = 0; k < v.nc3; ++k)
+          for (int j = 0; j < v.nc2; ++j)
+            for (int i = 0; i < v.nc1; ++i)
+              d[n * a.stride[0] + k * a.stride[1] + j * a.stride[2] + i * a.stride[3]] = *in++;
+    } else {
+      if (!tmp) CK(cudaMalloc((void**)&tmp, pan * sizeof(double)));
+      int rc = cudaMemcpyAsync(tmp, host.data() + p * pan, pan * sizeof(double),
+                               cudaMemcpyHostToDevice, c->stream) == cudaSuccess ? 0 : EXO_ERR_CUDA;
+      if (!rc) rc = exo::launch_view_copy(tmp, cs, d, a.stride, size, c->stream);
+      if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = EXO_ERR_CUDA;
+      if (rc) {
+        cudaFree(tmp);
+        return fail(EXO_ERR_CUDA, "view scatter failed");
+      }
+    }
+  }
+  if (tmp) cudaFree(tmp);
+  return EXO_OK;
+}
+
+int exo_set_primitive_views(exo_ctx* c, const exo_array_view* w) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = check_views(c, w);
+  std::vector<double> h;
+  if (!rc) rc = views_gather(c, w, h);
+  return rc ? rc : exo_set_primitive(c, h.data());
+}
+
+int exo_get_primitive_views(exo_ctx* c, const exo_array_view* w) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = check_views(c, w);
+  if (rc) return rc;
+  std::vector<double> h(c->state_elems);
+  if ((rc = exo_get_primitive(c, h.data()))) return rc;
+  return views_scatter(c, h, w);
+}
+
+int exo_get_conserved_views(exo_ctx* c, const exo_array_view* u) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = check_views(c, u);
+  if (rc) return rc;
+  std::vector<double> h(c->state_elems);
+  if ((rc = exo_get_conserved(c, h.data()))) return rc;
+  return views_scatter(c, h, u);
+}
+
+int exo_solve_implicit_3d_views(exo_ctx* c, const exo_array_view* du, const exo_array_view* w,
+                                double dt) {
+  if (!c) return fail(EXO_ERR_ARG, "ctx is NULL");
+  int rc = check_views(c, du);
+  if (!rc) rc = check_views(c, w);
+  std::vector<double> hd, hw;
+  if (!rc) rc = views_gather(c, du, hd);
+  if (!rc) rc = views_gather(c, w, hw);
+  if (!rc) rc = exo_solve_implicit_3d(c, hd.data(), hw.data(), dt);
+  return rc ? rc : views_scatter(c, hd, du);
 }
 
 int exo_weno5(int n, const double* a, const double* b, const double* c, const double* d,

@@ -93,6 +93,7 @@ int rebuild(exo_ensemble* e) {
   std::vector<DevView> views;
   std::vector<unsigned> start((size_t)exo::BK_COUNT * (e->capacity + 1), 0);
   unsigned tot[exo::BK_COUNT] = {0, 0, 0, 0, 0, 0};
+  bool any_full = false;  // some member takes the 5x5 correction
   int max_nc1 = 1;
   int x1_threads = 32;
   size_t x1_smem = 8;
@@ -102,6 +103,8 @@ int rebuild(exo_ensemble* e) {
     views.push_back(m->v);
     for (int k = 0; k < exo::BK_COUNT; ++k) views.back().tiles[k] = e->tiles.t[k];
     max_nc1 = std::max(max_nc1, m->v.nc1);
+    if (m->v.eqn != EXO_EQN_SHALLOW_YZ && (m->v.implicit_flag & 1) && (m->v.implicit_flag & 8))
+      any_full = true;
     unsigned b[exo::BK_COUNT];
     exo::member_blocks(m->v, e->tiles.t, b);
     for (int k = 0; k < exo::BK_COUNT; ++k) {
@@ -137,9 +140,10 @@ int rebuild(exo_ensemble* e) {
   for (int k = 0; k < exo::BK_COUNT; ++k) pl.threads[k] = e->tiles.t[k];
   pl.max_nc1 = max_nc1;
   pl.precision = e->precision;
+  pl.any_full_correction = any_full;
   // count the kernel nodes of one step
   int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 +
-                      (tot[exo::BK_IMPLICIT] ? exo::implicit_launches(e->precision) : 0) + 1;
+                      (tot[exo::BK_IMPLICIT] ? (any_full ? 2 : 1) : 0) + 1;
   e->launches_per_step = 3 * per_stage + (tot[exo::BK_ROUNDTRIP] ? 1 : 0) + 1 + 1;
   cudaGraph_t graph;
   ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
@@ -444,6 +448,8 @@ int exo_ensemble_check_state(exo_ensemble* e, int slot, int* invalid) {
   int zero = 0;
   ECK(cudaMemcpyAsync(&m->v.sc->invalid, &zero, sizeof(int), cudaMemcpyHostToDevice, e->stream));
   ECK(cudaStreamSynchronize(e->stream));
+  if (s.timeout)
+    return efail(EXO_ERR_TIMEOUT, "a kernel's bounded wait for its bulk copies gave up");
   return EXO_OK;
 }
 

@@ -91,6 +91,9 @@ struct HostTables {
 
 // geometry.cpp
 bool build_tables(const exo_config& cfg, HostTables& t, std::string* err);
+// the panel (0-based) across side s (0 Up, 1 Down, 2 Left, 3 Right) of panel
+// p and the side of it that edge is (CubedSphere::TransformOX)
+void panel_neighbor(int p, int s, int* tp, int* ts);
 
 // Device-side scalars of one atmosphere (time step bookkeeping and flags).
 struct DevScalars {
@@ -98,18 +101,15 @@ struct DevScalars {
   double time;                     // simulated time
   unsigned long long dtmin_bits;   // running min of the CFL candidate (bits of a positive double)
   int invalid;                     // sticky: rho/p negative or NaN
-  int pad;
+  int timeout;                     // sticky: a kernel's bounded wait gave up
   long long ncycle;
 };
 
-// The implicit solve of the stepping context with FP32 blocks
-// (EXO_PREC_MIXED_F32_SOLVE) runs as two kernels, the forward sweep and the
-// back substitution, so that many more columns are resident in the
-// memory-bound back substitution (4 % faster at 6x192^2x96); with FP64
-// blocks one kernel does both (the split measured 3 % slower there).
-inline int implicit_launches(int precision) {
-  return precision == EXO_PREC_MIXED_F32_SOLVE ? 2 : 1;
-}
+// The implicit solve with the full (5x5) correction runs as two kernels,
+// the forward sweep (kb_implicit) and the back substitution
+// (kb_implicit_bwd, memory-bound, fed by bulk copies); the partial (3x3)
+// correction does both in kb_implicit.
+inline int implicit_launches(int implicit_flag) { return (implicit_flag & 8) ? 2 : 1; }
 
 // n / d for 0 <= n < 2^40 / (d - 1) as floor(n m / 2^40), m = ceil(2^40 / d):
 // with n = q d + t, n m / 2^40 = q + t / d + n r / (d 2^40) for some r < d,
@@ -183,6 +183,7 @@ struct BatchPlan {
   int threads[BK_COUNT];         // tiles of the other kernels
   int max_nc1;                   // largest nc1 of the members (radial tables in shared memory)
   int precision;                 // EXO_PREC_* of every member
+  bool any_full_correction;      // some member takes the 5x5 solve (kb_implicit_bwd runs)
 };
 // Threads per block ("tile") of each batched kernel by BatchKind.  BK_X1
 // takes one radial column per block (its size follows L) and ignores its
@@ -264,6 +265,16 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
                                     const double* colgeo, const double* x1f, const double* x1v,
                                     const double* dx1f, double dt, double gamma, double grav,
                                     void* stream, std::string* err);
+// kernels.cu: the boundary's panel and equation-of-state hooks (FP64)
+int launch_panel_pack(const DevView& v, const double* src, double* buf, int tp, int rsk, int rsj,
+                      int K, int J, void* stream);
+int launch_face_sync(const DevView& v, double* L2, double* R2, double* L3, double* R3,
+                     void* stream);
+int launch_eos_range(const DevView& v, int to_prim, const double* in, double* out, int il, int iu,
+                     int jl, int ju, int kl, int ku, void* stream);
+int launch_sound_speed(const DevView& v, int n, const double* prim, double* cs, void* stream);
+int launch_view_copy(const void* src, const int64_t* sstride, void* dst, const int64_t* dstride,
+                     const int* size, void* stream);
 // peaks.cu: best FMA rate (flops/s) of independent chains on all SMs
 int measure_fma_peak(bool fp64, int repeats, double* flops_per_s, std::string* err);
 

@@ -512,30 +512,27 @@ __device__ __forceinline__ void riemann(int rsolver, double gamma, int ivx, cons
 }
 
 // ----------------------------------------------------- k_prim_ghost ------
-// Conserved value of variable n at cell (p,k,j,i) where (k,j) is interior or
-// in a ghost band; vectors (IVY, IVZ) come back together.
-__device__ __forceinline__ void load_cons(const DevView& v, int p, int k, int j, int i,
-                                          bool interior, double* c) {
-  if (interior) {
-    #pragma unroll
-    for (int n = 0; n < 5; ++n) {
-      if (n >= v.nv) break;
-      c[n] = v.u[idx(v, p, n, k, j, i)];
-    }
-    return;
-  }
-  const GhostEntry& e = v.ghost[v.ghost_map[((size_t)p * v.nc3 + k) * v.nc2 + j]];
-  int sp = e.src_panel;
+// The conserved state a ghost-band cell gets from the neighbour panel
+// (CubedSphereUtility::PackData with InteprolateX2/X3, cubed_sphere_utility.
+// cpp:92-369, as the ghost table e precomputes it): linear interpolation
+// along the edge between two source cells, vectors (IVY, IVZ) raised,
+// rotated to the receiver's basis through latitude-longitude and lowered.
+// src is the source panel's (nv, nc3, nc2, nc1) array.
+__device__ __forceinline__ void ghost_interp(const DevView& v, const GhostEntry& e,
+                                             const double* src, int i, double* c) {
+  auto S = [&](int n, int k, int j) {
+    return src[(((size_t)n * v.nc3 + k) * v.nc2 + j) * v.nc1 + i];
+  };
   #pragma unroll
   for (int n = 0; n < 5; ++n) {
     if (n >= v.nv) break;
     if (n == IVY || n == IVZ) continue;
-    double v1 = v.u[idx(v, sp, n, e.k0, e.j0, i)];
-    double v2 = v.u[idx(v, sp, n, e.k1, e.j1, i)];
+    double v1 = S(n, e.k0, e.j0);
+    double v2 = S(n, e.k1, e.j1);
     c[n] = (e.A * v1 + e.B * v2) / e.C;
   }
-  double v1y = v.u[idx(v, sp, IVY, e.k0, e.j0, i)], v1z = v.u[idx(v, sp, IVZ, e.k0, e.j0, i)];
-  double v2y = v.u[idx(v, sp, IVY, e.k1, e.j1, i)], v2z = v.u[idx(v, sp, IVZ, e.k1, e.j1, i)];
+  double v1y = S(IVY, e.k0, e.j0), v1z = S(IVZ, e.k0, e.j0);
+  double v2y = S(IVY, e.k1, e.j1), v2z = S(IVZ, e.k1, e.j1);
   double vy = (e.A * v1y + e.B * v2y) / e.C;
   double vz = (e.A * v1z + e.B * v2z) / e.C;
   double sth = e.ss, cth = e.cs;
@@ -550,6 +547,22 @@ __device__ __forceinline__ void load_cons(const DevView& v, int p, int k, int j,
   vzt = vz;
   c[IVY] = vyt + vzt * e.ct;
   c[IVZ] = vzt + vyt * e.ct;
+}
+
+// Conserved value of variable n at cell (p,k,j,i) where (k,j) is interior or
+// in a ghost band; vectors (IVY, IVZ) come back together.
+__device__ __forceinline__ void load_cons(const DevView& v, int p, int k, int j, int i,
+                                          bool interior, double* c) {
+  if (interior) {
+    #pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= v.nv) break;
+      c[n] = v.u[idx(v, p, n, k, j, i)];
+    }
+    return;
+  }
+  const GhostEntry& e = v.ghost[v.ghost_map[((size_t)p * v.nc3 + k) * v.nc2 + j]];
+  ghost_interp(v, e, v.u + idx(v, e.src_panel, 0, 0, 0, 0), i, c);
 }
 
 // the CFL candidate of the block's cells is reduced in shared memory first,
@@ -2576,12 +2589,10 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const bool full = (v.implicit_flag & 8) != 0;
   const ImplSlices<R> sl = impl_slices<R>(ism, full);
   using IO = StepColumnIO<R>;
-  // FP32 blocks: the back substitution of the full correction is
-  // kb_implicit_bwd's (the lighter partial one stays here: split, it measured
-  // slower)
-  constexpr bool kBwd = sizeof(R) == 8;
+  // the back substitution of the full correction is kb_implicit_bwd's (the
+  // lighter partial one stays here: split, it measured slower)
   if (full)
-    implicit_column<IO, kBwd>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
+    implicit_column<IO, false>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
                                          geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
                                          geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
                                          dt, v.gamma, v.grav);
@@ -2592,80 +2603,181 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
                                                  x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
 }
 
-// levels per shared-memory chunk of the back-substitution kernel (a power of
-// two: the tile's element index is split with shifts)
-constexpr int BWD_CHUNK = 4;
-static_assert((BWD_CHUNK & (BWD_CHUNK - 1)) == 0 && BWD_CHUNK == 4, "the tile index uses e >> 2");
-__host__ __device__ constexpr size_t impl_bwd_smem(int threads) {
-  return ((size_t)5 * threads * (BWD_CHUNK + 1) + threads) * sizeof(double);
-}
-// The back substitution of the full correction of a column whose forward
-// sweep implicit_block ran with FP32 blocks: few registers, so many columns
-// are resident while the factors stream back in.
+// ---------------------------------------------------- kb_implicit_bwd ---
+// The back substitution of the full correction, delta_i -= (A c)_i
+// delta_{i+1} from the top level down, u += delta (with the AirParcel round
+// trip on the last stage), as a kernel of its own after the forward sweep
+// (kb_implicit, which leaves (A c)_i and delta_i of every level in scratch).
+// It streams 240 (FP64 factors) or 120 (FP32) bytes of scratch and 80 bytes
+// of u per cell and computes little, so it is built to keep HBM busy: one
+// warp per group of 32 columns, whose scratch is one contiguous run per
+// chunk of BWD_LEV levels ([group][level][entry][32]); the chunk below the
+// one being finished is already on its way into the other shared-memory
+// buffer, by one bulk TMA copy (cp.async.bulk, completion counted by an
+// mbarrier) for the factors and by 8-byte cp.async copies for u (four lanes
+// read one column's four levels: a 32-byte run per column and variable).
+// u is updated in the shared tile and written back the same way.
+constexpr int BWD_LEV = 4;  // levels per chunk
+// the shared memory of one warp: two buffers, each the factor chunk and the
+// u tile [5][32][BWD_LEV + 1] (padded: a warp's column-wise accesses of one
+// level fall on distinct banks), then the two mbarriers
 template <class R>
-__device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned blk, int stage) {
+__host__ __device__ constexpr size_t bwd_chunk_bytes() {
+  return (size_t)BWD_LEV * 30 * 32 * sizeof(R);
+}
+constexpr int BWD_TILE_DOUBLES = 5 * 32 * (BWD_LEV + 1);
+template <class R>
+__host__ __device__ constexpr size_t bwd_buffer_bytes() {
+  return bwd_chunk_bytes<R>() + BWD_TILE_DOUBLES * sizeof(double);
+}
+template <class R>
+__host__ __device__ constexpr size_t impl_bwd_smem() {
+  return 2 * bwd_buffer_bytes<R>() + 16;
+}
+static_assert(bwd_chunk_bytes<float>() % 16 == 0 && bwd_buffer_bytes<float>() % 16 == 0,
+              "bulk copies move multiples of 16 bytes to 16-byte aligned addresses");
+static_assert(bwd_chunk_bytes<double>() % 16 == 0 && bwd_buffer_bytes<double>() % 16 == 0,
+              "bulk copies move multiples of 16 bytes to 16-byte aligned addresses");
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(mb)), "r"(count)
+               : "memory");
+}
+// one arrival that also announces the bytes the bulk copy will complete
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mb)),
+               "r"(bytes)
+               : "memory");
+}
+// bulk copy global -> this CTA's shared memory, counted on mb (no multicast)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* mb) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(mb))
+      : "memory");
+}
+// Waits for phase `parity` of mb to complete, giving up once MBAR_WAIT_NS of
+// wall time (the %globaltimer clock) have passed: false after a timeout.
+constexpr unsigned long long MBAR_WAIT_NS = 100000000ull;  // 0.1 s
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long* mb, unsigned parity) {
+  const unsigned a = smem_u32(mb);
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > MBAR_WAIT_NS) return false;
+  }
+}
+
+template <class R>
+__device__ __forceinline__ void implicit_bwd_warp(const DevView& v, int group, int stage) {
+  extern __shared__ __align__(128) unsigned char bws[];
+  const int lane = (int)(threadIdx.x & 31);
   const int ncol = 6 * v.N * v.N;
-  const int T = (int)blockDim.x, t = (int)threadIdx.x;
-  const int col0 = (int)blk * T, col = col0 + t;
+  const int col0 = group * 32, col = col0 + lane;
   const bool active = col < ncol;
+  const int ncb = min(32, ncol - col0);
+  const int L = v.L;
+  const size_t vs = v.cells;
   size_t base = 0;
-  R* scr0 = nullptr;
   if (active) {
     const int j = v.js + col % v.N;
     const int k = v.ks + (col / v.N) % v.N;
     const int p = col / (v.N * v.N);
     base = idx(v, p, 0, k, j, 0);
-    scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
   }
-  StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
-                     v.du + base};
-  R dp[5] = {R(0), R(0), R(0), R(0), R(0)};  // delta_ie, stored by the forward sweep
-  if (active) {
-#pragma unroll
-    for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
+  // this column's scratch: entry e of level lev at sg[(lev * 30 + e) * 32 + lane]
+  const R* sg = reinterpret_cast<const R*>(v.scratch) + (size_t)group * L * 30 * 32;
+  unsigned long long* mb = reinterpret_cast<unsigned long long*>(bws + 2 * bwd_buffer_bytes<R>());
+  auto chunk_scr = [&](int b) { return reinterpret_cast<R*>(bws + b * bwd_buffer_bytes<R>()); };
+  auto chunk_tile = [&](int b) {
+    return reinterpret_cast<double*>(bws + b * bwd_buffer_bytes<R>() + bwd_chunk_bytes<R>());
+  };
+  if (lane == 0) {
+    mbar_init(&mb[0], 1);
+    mbar_init(&mb[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (stage < 0) {  // SolveImplicit3D alone: du corrected in place, column by column
-    if (active) implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
-    return;
-  }
-  // The stepping form: the block's columns move through BWD_CHUNK levels at a
-  // time.  u of those levels is copied into shared memory by the whole block
-  // (four consecutive lanes read one column's four levels: a 32-byte run per
-  // column instead of 32 scattered 8-byte loads per level), updated there by
-  // each column's thread, and copied back the same way.
-  // Tile: u[n][c][l] at ((n * T + c) * (BWD_CHUNK + 1) + l), padded so that
-  // a half-warp's 8-byte accesses of one level fall on distinct banks; then
-  // the column bases.
-  extern __shared__ double bsm[];
-  constexpr int CP = BWD_CHUNK + 1;
-  double* tile = bsm;
-  long long* cbase = reinterpret_cast<long long*>(bsm + 5 * T * CP);
-  cbase[t] = active ? (long long)base : 0;
-  __syncthreads();
-  const int ncb = min(T, ncol - col0);
-  const int lgT = __ffs(T) - 1;  // T is a power of two
-  const size_t vs = v.cells;
+  __syncwarp();
+  // the column bases of the group, for the tile copies
+  const long long cb_lane = active ? (long long)base : 0;
+  const int nch = (L + BWD_LEV - 1) / BWD_LEV;
   double* const u = v.u;
-  for (int hi = v.ie; hi >= v.is; hi -= BWD_CHUNK) {
-    const int lo = max(v.is, hi - BWD_CHUNK + 1);
-    for (int e = t; e < 5 * BWD_CHUNK * T; e += T) {
-      const int l = e & (BWD_CHUNK - 1), c = (e >> 2) & (T - 1), n = e >> (2 + lgT);
-      if (c < ncb && lo + l <= hi) tile[(n * T + c) * CP + l] = u[cbase[c] + n * vs + lo + l];
+  // chunk c holds levels [c * BWD_LEV, min(L, (c + 1) * BWD_LEV)) (level
+  // index i - is); a tile element e is (variable n, column c, level l)
+  auto issue = [&](int c, int b) {
+    const int lo = c * BWD_LEV, nl = min(L, lo + BWD_LEV) - lo;
+    if (lane == 0) {
+      const unsigned bytes = (unsigned)(nl * 30 * 32 * sizeof(R));
+      mbar_expect_tx(&mb[b], bytes);
+      bulk_g2s(chunk_scr(b), sg + (size_t)lo * 30 * 32, bytes, &mb[b]);
     }
-    __syncthreads();
+    double* tile = chunk_tile(b);
+    for (int e = lane; e < 5 * 32 * BWD_LEV; e += 32) {
+      const int l = e & (BWD_LEV - 1), cc = (e / BWD_LEV) & 31, n = e / (BWD_LEV * 32);
+      const long long cbase = __shfl_sync(0xffffffffu, cb_lane, cc);
+      if (cc < ncb && l < nl)
+        cp_async8(&tile[(n * 32 + cc) * (BWD_LEV + 1) + l], u + cbase + n * vs + v.is + lo + l);
+    }
+    cp_async_commit();
+  };
+  unsigned phases = 0u;   // bit b: the phase buffer b's mbarrier completes next
+  unsigned pending = 0u;  // bit b: buffer b's bulk copy is still outstanding
+  bool ok = true;
+  R dp[5] = {R(0), R(0), R(0), R(0), R(0)};
+  issue(nch - 1, 0);
+  pending |= 1u;
+  int b = 0;
+  for (int c = nch - 1; c >= 0; --c) {
+    if (c > 0) {
+      issue(c - 1, b ^ 1);
+      pending |= 1u << (b ^ 1);
+    }
+    // the factors of chunk c (bounded wait; the whole warp agrees) and its u tile
+    const bool got = mbar_wait(&mb[b], (phases >> b) & 1u);
+    if (!__all_sync(0xffffffffu, got)) {
+      ok = false;
+      break;
+    }
+    phases ^= 1u << b;
+    pending &= ~(1u << b);
+    if (c > 0) cp_async_wait_one();
+    else cp_async_wait_all();
+    __syncwarp();
+    const R* cs = chunk_scr(b);
+    double* tile = chunk_tile(b);
+    const int lo = c * BWD_LEV, nl = min(L, lo + BWD_LEV) - lo;
     if (active) {
-      for (int i = hi; i >= lo; --i) {
-        if (i < v.ie) {
-          R cs[30];
+      for (int l = nl - 1; l >= 0; --l) {
+        const int lev = lo + l;
+        const R* f = cs + (size_t)l * 30 * 32 + lane;
+        if (lev == L - 1) {
 #pragma unroll
-          for (int e = 0; e < 30; ++e) cs[e] = io.scr(i - v.is, e);
+          for (int r = 0; r < 5; ++r) dp[r] = f[(25 + r) * 32];  // delta_ie
+        } else {
           R dl[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
-            R ad = cs[r * 5] * dp[0];
+            R ad = f[(r * 5) * 32] * dp[0];
 #pragma unroll
-            for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
-            dl[r] = cs[25 + r] - ad;
+            for (int k = 1; k < 5; ++k) ad += f[(r * 5 + k) * 32] * dp[k];
+            dl[r] = f[(25 + r) * 32] - ad;
           }
 #pragma unroll
           for (int r = 0; r < 5; ++r) dp[r] = dl[r];
@@ -2674,19 +2786,48 @@ __device__ __forceinline__ void implicit_bwd_block(const DevView& v, unsigned bl
         double uu[5];
 #pragma unroll
         for (int n = 0; n < 5; ++n)
-          uu[n] = tile[(n * T + t) * CP + (i - lo)] + 1. * (double)dp[n];
+          uu[n] = tile[(n * 32 + lane) * (BWD_LEV + 1) + l] + 1. * (double)dp[n];
         if (stage == 2) airparcel_round_trip(uu, v.Rd, v.gamma);
 #pragma unroll
-        for (int n = 0; n < 5; ++n) tile[(n * T + t) * CP + (i - lo)] = uu[n];
+        for (int n = 0; n < 5; ++n) tile[(n * 32 + lane) * (BWD_LEV + 1) + l] = uu[n];
       }
     }
-    __syncthreads();
-    for (int e = t; e < 5 * BWD_CHUNK * T; e += T) {
-      const int l = e & (BWD_CHUNK - 1), c = (e >> 2) & (T - 1), n = e >> (2 + lgT);
-      if (c < ncb && lo + l <= hi) u[cbase[c] + n * vs + lo + l] = tile[(n * T + c) * CP + l];
+    __syncwarp();
+    for (int e = lane; e < 5 * 32 * BWD_LEV; e += 32) {
+      const int l = e & (BWD_LEV - 1), cc = (e / BWD_LEV) & 31, n = e / (BWD_LEV * 32);
+      const long long cbase = __shfl_sync(0xffffffffu, cb_lane, cc);
+      if (cc < ncb && l < nl)
+        u[cbase + n * vs + v.is + lo + l] = tile[(n * 32 + cc) * (BWD_LEV + 1) + l];
     }
-    __syncthreads();
+    __syncwarp();
+    b ^= 1;
   }
+  if (!ok) {
+    // a bulk copy did not complete in time: record it, and give every copy
+    // still outstanding a bounded wait before this warp's shared memory is
+    // released (the columns keep the forward sweep's state)
+    if (lane == 0) atomicOr(&v.sc->timeout, 1);
+    for (int bb = 0; bb < 2; ++bb)
+      if ((pending >> bb) & 1u) mbar_wait(&mb[bb], (phases >> bb) & 1u);
+    cp_async_wait_all();
+  }
+}
+
+// SolveImplicit3D alone (stage < 0): du corrected in place, column by column
+template <class R>
+__device__ __forceinline__ void implicit_bwd_du(const DevView& v, int col) {
+  if (col >= 6 * v.N * v.N) return;
+  const int j = v.js + col % v.N;
+  const int k = v.ks + (col / v.N) % v.N;
+  const int p = col / (v.N * v.N);
+  const size_t base = idx(v, p, 0, k, j, 0);
+  R* scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
+  StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, -1, v.Rd, v.gamma,
+                     v.du + base};
+  R dp[5];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) dp[r] = io.scr(v.L - 1, 25 + r);
+  implicit_backward_full<StepColumnIO<R>, false>(io, v.is, v.ie, dp);
 }
 
 // last-stage round trip when the implicit solver is off
@@ -2853,17 +2994,31 @@ __global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage, double dt_given
   implicit_block<R>(sv, b, stage, dt_given);
 }
 
-// 128 registers: 16 warps per SM (96 spills)
-#ifndef EXO_IMPL_BWD_MAXNREG
-#define EXO_IMPL_BWD_MAXNREG 128
-#endif
+// One warp per group of 32 columns: implicit block b of a member (its
+// columns b*T .. b*T+T-1 at T = the implicit tile) is T/32 blocks here.
 template <class R>
-__global__ void __maxnreg__(EXO_IMPL_BWD_MAXNREG) kb_implicit_bwd(Batch bt, int stage) {
+__global__ void __launch_bounds__(32) kb_implicit_bwd(Batch bt, int stage, int warps_per_iblock) {
   __shared__ __align__(16) DevView sv;
-  unsigned b = batch_enter(bt, sv);
+  const unsigned ib = blockIdx.x / (unsigned)warps_per_iblock;
+  {
+    static_assert(sizeof(DevView) % 16 == 0, "DevView is copied in 16-byte words");
+    const int m = batch_member(bt, ib);
+    const int4* src = reinterpret_cast<const int4*>(bt.views + m);
+    int4* dst = reinterpret_cast<int4*>(&sv);
+    for (int t = threadIdx.x; t < (int)(sizeof(DevView) / 16); t += blockDim.x) dst[t] = src[t];
+    __syncwarp();
+  }
+  const int m = batch_member(bt, ib);
+  const unsigned local = ib - bt.start[m];
   // members with the partial correction finished in kb_implicit
   if (sv.eqn == EXO_EQN_SHALLOW_YZ || !(sv.implicit_flag & 1) || !(sv.implicit_flag & 8)) return;
-  implicit_bwd_block<R>(sv, b, stage);
+  const int group = (int)(local * (unsigned)warps_per_iblock + blockIdx.x % (unsigned)warps_per_iblock);
+  if (group * 32 >= 6 * sv.N * sv.N) return;
+  if (stage < 0) {
+    implicit_bwd_du<R>(sv, group * 32 + (int)threadIdx.x);
+    return;
+  }
+  implicit_bwd_warp<R>(sv, group, stage);
 }
 
 __global__ void kb_roundtrip(Batch bt) {
@@ -2901,23 +3056,27 @@ inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // the implicit kernel of a precision: FP32 blocks for
 // EXO_PREC_MIXED_F32_SOLVE, FP64 for EXO_PREC_MIXED and the FP64 build
+// the forward sweep, then (when some member has the full correction) the
+// back substitution
 template <class R>
 inline void launch_kb_implicit(unsigned blocks, int threads, int nc1, cudaStream_t st, Batch b,
-                               int stage, double dt_given) {
+                               int stage, double dt_given, bool any_full) {
   kb_implicit<R><<<blocks, threads, impl_smem<R>(threads, nc1), st>>>(b, stage, dt_given);
-  if constexpr (sizeof(R) == 4)
-    kb_implicit_bwd<R><<<blocks, threads, impl_bwd_smem(threads), st>>>(b, stage);
+  if (any_full)
+    kb_implicit_bwd<R><<<blocks * (unsigned)(threads / 32), 32, impl_bwd_smem<R>(), st>>>(
+        b, stage, threads / 32);
 }
 inline void launch_kb_implicit(int precision, unsigned blocks, int threads, int nc1,
-                               cudaStream_t st, Batch b, int stage, double dt_given) {
+                               cudaStream_t st, Batch b, int stage, double dt_given,
+                               bool any_full) {
 #if EXO_MIXED
   if (precision == EXO_PREC_MIXED_F32_SOLVE) {
-    launch_kb_implicit<float>(blocks, threads, nc1, st, b, stage, dt_given);
+    launch_kb_implicit<float>(blocks, threads, nc1, st, b, stage, dt_given, any_full);
     return;
   }
 #endif
   (void)precision;
-  launch_kb_implicit<double>(blocks, threads, nc1, st, b, stage, dt_given);
+  launch_kb_implicit<double>(blocks, threads, nc1, st, b, stage, dt_given, any_full);
 }
 
 }  // namespace
@@ -2942,6 +3101,14 @@ int prepare_kernels() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(kb_implicit<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              IMPL_SMEM_MAX);
+#endif
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kb_implicit_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)impl_bwd_smem<double>());
+#if EXO_MIXED
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kb_implicit_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)impl_bwd_smem<float>());
 #endif
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(kb_flux_x1<EXO_FLUX_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2989,14 +3156,16 @@ int launch_update(const DevView& v, int stage, void* stream) {
 int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   launch_kb_implicit(v.precision, member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT], v.nc1,
-                     (cudaStream_t)stream, one(v, BK_IMPLICIT), stage, 0.);
+                     (cudaStream_t)stream, one(v, BK_IMPLICIT), stage, 0.,
+                     (v.implicit_flag & 8) != 0);
   return check_launch();
 }
 
 int launch_implicit_du(const DevView& v, double dt, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   launch_kb_implicit(v.precision, member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT], v.nc1,
-                     (cudaStream_t)stream, one(v, BK_IMPLICIT), -1, dt);
+                     (cudaStream_t)stream, one(v, BK_IMPLICIT), -1, dt,
+                     (v.implicit_flag & 8) != 0);
   return check_launch();
 }
 
@@ -3044,7 +3213,7 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
     }
     if (pl.total[BK_IMPLICIT]) {
       launch_kb_implicit(pl.precision, pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT],
-                         pl.max_nc1, st, B(BK_IMPLICIT), s, 0.);
+                         pl.max_nc1, st, B(BK_IMPLICIT), s, 0., pl.any_full_correction);
       if ((rc = check_launch())) return rc;
     }
     if (s == 2) {

@@ -401,6 +401,11 @@ static void build_edge_table(HostTables& t) {
     }
 }
 
+void panel_neighbor(int p, int s, int* tp, int* ts) {
+  *tp = kNbrPanel[p][s] - 1;
+  *ts = kNbrSide[p][s];
+}
+
 bool build_tables(const exo_config& cfg, HostTables& t, std::string* err) {
   if (cfg.N < 6 || (cfg.N % 2) != 0) {
     if (err) *err = "N must be even and >= 6 (one block per panel, even edge count)";

@@ -288,6 +288,177 @@ int launch_implicit_columns_noalloc(int ncol, int L, const double* w, double* du
   return 0;
 }
 
+namespace fp64 {
+namespace {
+
+// CubedSphereUtility::PackData of one face: panel src's edge band
+// interpolated onto the neighbour's ghost band (target panel tp, rows
+// [rsk, rsk+K) x [rsj, rsj+J)), packed in the band's plain (n, k, j, i) order
+// -- the order the receiver unpacks, which PackDataR0..R3 produce on the
+// sender's side
+__global__ void k_panel_pack(DevView v, const double* src, double* buf, int tp, int rsk, int rsj,
+                             int K, int J) {
+  const int L = v.L;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)K * J * L) return;
+  const int ii = (int)(tid % L);
+  const int r = (int)(tid / L);
+  const int jj = r % J, kk = r / J;
+  const int k = rsk + kk, j = rsj + jj, i = v.is + ii;
+  const GhostEntry& e = v.ghost[v.ghost_map[((size_t)tp * v.nc3 + k) * v.nc2 + j]];
+  double c[5];
+  ghost_interp(v, e, src, i, c);
+  for (int n = 0; n < v.nv; ++n) buf[(((size_t)n * K + kk) * J + jj) * L + ii] = c[n];
+}
+
+// The face position of along index `along` of a panel side: direction (1: x2
+// faces, 2: x3 faces) and (k, j)
+__device__ __forceinline__ void edge_face(const DevView& v, int side, int along, int& dir, int& k,
+                                          int& j) {
+  if (side == UP) { dir = 1; j = v.js; k = v.ks + along; }
+  else if (side == DOWN) { dir = 1; j = v.je + 1; k = v.ks + along; }
+  else if (side == LEFT) { dir = 2; k = v.ks; j = v.js + along; }
+  else { dir = 2; k = v.ke + 1; j = v.js + along; }
+}
+
+// CubedSphere::SynchronizeFluxesSend/Recv/Wait (cubed_sphere.cpp:289-688) on
+// the face-state stores: every receiving edge face takes the sender's
+// interior-side state (L at the sender's Down/Right edges, R at Up/Left),
+// rotated into the receiver's basis, as its outer state (L at the
+// receiver's Up/Left edges, R at Down/Right); faces i = is-1 .. ie+1.
+// Senders are never receivers of the same store, so one pass suffices.
+__global__ void k_face_sync(DevView v, double* L2, double* R2, double* L3, double* R3) {
+  const int ni = v.L + 2, N = v.N;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)6 * 4 * N * ni) return;
+  const int ii = (int)(tid % ni);
+  long long r = tid / ni;
+  const int b = (int)(r % N);
+  r /= N;
+  const int ts = (int)(r % 4), tp = (int)(r / 4);
+  const int i = v.is - 1 + ii;
+  const EdgeEntry& e = v.edge[((size_t)tp * 4 + ts) * N + b];
+  int sd, sk, sj, td, tk, tj;
+  edge_face(v, e.src_side, e.src_along, sd, sk, sj);
+  edge_face(v, ts, b, td, tk, tj);
+  const double* S = sd == 1 ? (e.src_side == DOWN ? L2 : R2) : (e.src_side == RIGHT ? L3 : R3);
+  double* D = td == 1 ? (ts == UP ? L2 : R2) : (ts == LEFT ? L3 : R3);
+  double st[5];
+  for (int n = 0; n < v.nv; ++n) st[n] = S[idx(v, e.src_panel, n, sk, sj, i)];
+  const double V2 = st[IVY], V3 = st[IVZ];
+  const double U = e.r[0] * V2 + e.r[1] * V3;
+  const double V = e.r[2] * V2 + e.r[3] * V3;
+  st[IVY] = e.q[0] * U + e.q[1] * V;
+  st[IVZ] = e.q[2] * U + e.q[3] * V;
+  for (int n = 0; n < v.nv; ++n) D[idx(v, tp, n, tk, tj, i)] = st[n];
+}
+
+// EquationOfState::ConservedToPrimitive (to_prim != 0) or PrimitiveToConserved
+// over cells [il, iu] x [jl, ju] x [kl, ku] of every panel (whole arrays in
+// the context's layout); an invalid density or pressure sets the sticky flag
+__global__ void k_eos_range(DevView v, int to_prim, const double* in, double* out, int il,
+                            int jl, int kl, int ni, int nj, int nk) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)6 * ni * nj * nk) return;
+  const int i = il + (int)(tid % ni);
+  long long r = tid / ni;
+  const int j = jl + (int)(r % nj);
+  r /= nj;
+  const int k = kl + (int)(r % nk);
+  const int p = (int)(r / nk);
+  double a[5], b[5];
+  for (int n = 0; n < v.nv; ++n) a[n] = in[idx(v, p, n, k, j, i)];
+  const double cth = geo(v, GCOSC, p, k, j);
+  if (to_prim) {
+    if (cons_to_prim(v, a, b, cth)) atomicOr(&v.sc->invalid, 1);
+  } else {
+    prim_to_cons(v, a, b, cth);
+  }
+  for (int n = 0; n < v.nv; ++n) out[idx(v, p, n, k, j, i)] = b[n];
+}
+
+// EquationOfState::SoundSpeed of n cells, prim (NHYDRO, n)
+__global__ void k_sound_speed(DevView v, int n, const double* prim, double* cs) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  double w[5];
+  for (int q = 0; q < v.nv; ++q) w[q] = prim[(size_t)q * n + m];
+  if (v.eqn == EXO_EQN_SHALLOW_YZ) {
+    cs[m] = sqrt(w[IDN]);
+  } else {
+    double fsig = 1., feps = 1.;
+    cs[m] = sqrt((1. + (v.gamma - 1) * feps / fsig) * w[IPR] / w[IDN]);
+  }
+}
+
+// element copy between two strided 4-D views of doubles (strides in elements)
+struct Strides4 {
+  long long s[4];
+};
+__global__ void k_view_copy(const double* src, Strides4 ss, double* dst, Strides4 ds, int n4,
+                            int n3, int n2, int n1) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)n4 * n3 * n2 * n1) return;
+  const int i = (int)(tid % n1);
+  long long r = tid / n1;
+  const int j = (int)(r % n2);
+  r /= n2;
+  const int k = (int)(r % n3);
+  const int n = (int)(r / n3);
+  dst[n * ds.s[0] + k * ds.s[1] + j * ds.s[2] + i * ds.s[3]] =
+      src[n * ss.s[0] + k * ss.s[1] + j * ss.s[2] + i * ss.s[3]];
+}
+
+}  // namespace
+}  // namespace fp64
+
+int launch_panel_pack(const DevView& v, const double* src, double* buf, int tp, int rsk, int rsj,
+                      int K, int J, void* stream) {
+  const long long n = (long long)K * J * v.L;
+  if (n <= 0) return 0;
+  fp64::k_panel_pack<<<fp64::nblk((size_t)n, 128), 128, 0, (cudaStream_t)stream>>>(
+      v, src, buf, tp, rsk, rsj, K, J);
+  return fp64::check_launch();
+}
+
+int launch_face_sync(const DevView& v, double* L2, double* R2, double* L3, double* R3,
+                     void* stream) {
+  const size_t n = (size_t)6 * 4 * v.N * (v.L + 2);
+  fp64::k_face_sync<<<fp64::nblk(n, 128), 128, 0, (cudaStream_t)stream>>>(v, L2, R2, L3, R3);
+  return fp64::check_launch();
+}
+
+int launch_eos_range(const DevView& v, int to_prim, const double* in, double* out, int il, int iu,
+                     int jl, int ju, int kl, int ku, void* stream) {
+  const int ni = iu - il + 1, nj = ju - jl + 1, nk = ku - kl + 1;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return 0;
+  const size_t n = (size_t)6 * ni * nj * nk;
+  fp64::k_eos_range<<<fp64::nblk(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      v, to_prim, in, out, il, jl, kl, ni, nj, nk);
+  return fp64::check_launch();
+}
+
+int launch_sound_speed(const DevView& v, int n, const double* prim, double* cs, void* stream) {
+  if (n <= 0) return 0;
+  fp64::k_sound_speed<<<fp64::nblk((size_t)n, 128), 128, 0, (cudaStream_t)stream>>>(v, n, prim,
+                                                                                     cs);
+  return fp64::check_launch();
+}
+
+int launch_view_copy(const void* src, const int64_t* sstride, void* dst, const int64_t* dstride,
+                     const int* size, void* stream) {
+  const size_t n = (size_t)size[0] * size[1] * size[2] * size[3];
+  if (n == 0) return 0;
+  fp64::Strides4 ss, ds;
+  for (int q = 0; q < 4; ++q) {
+    ss.s[q] = sstride[q];
+    ds.s[q] = dstride[q];
+  }
+  fp64::k_view_copy<<<fp64::nblk(n, 256), 256, 0, (cudaStream_t)stream>>>(
+      (const double*)src, ss, (double*)dst, ds, size[0], size[1], size[2], size[3]);
+  return fp64::check_launch();
+}
+
 int launch_riemann_rows(int rsolver, int eqn, int ivx, int n, double gamma, const double* wl,
                         const double* wr, double* flx, const double* cosf, const double* sinf,
                         const double* cthp, const double* cthc, void* stream) {

@@ -212,7 +212,10 @@ int exo_get_time(exo_ctx* ctx, double* time, int64_t* ncycle);
 
 /* Sticky device-side validity flag (MeshBlock::Impl::SetStateInvalid,
    src/snap/eos/ideal_moist_hydro.cpp:108,150): 1 if a density or pressure
-   went negative or NaN since the last call; the flag is cleared. */
+   went negative or NaN since the last call; the flag is cleared.  Returns
+   EXO_ERR_TIMEOUT (with *invalid set) once a kernel's bounded wait for its
+   bulk copies into shared memory has given up; that kernel left the state
+   of the columns it had not finished as the forward sweep left it. */
 int exo_check_state(exo_ctx* ctx, int* invalid);
 
 /* Block until the context's stream is idle. */
@@ -333,6 +336,88 @@ int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
    face value between the 2nd and 3rd argument (tests/test_weno.cpp:20-29). */
 int exo_weno5(int n, const double* a, const double* b, const double* c,
               const double* d, const double* e, double* out, void* stream);
+
+/* ------------------------------------------------- panel-exchange hooks */
+
+/* CubedSphereUtility::PackData (src/exo3/cubed_sphere_utility.hpp:10-12,
+   cubed_sphere_utility.cpp:370-619) for a context's panel: src is one
+   panel's array (NHYDRO, N+6, N+6, L+6) on the device, buf a device buffer
+   written from buf[*offset] on, *offset advanced by the values written.
+   Across a panel edge (ox1 = 0, exactly one of ox2, ox3 non-zero; the
+   ranges the G-wide interior band LoadBoundaryBufferSameLevel passes, every
+   variable) the band is interpolated onto the neighbour's ghost cells and
+   its vectors rotated into the neighbour's basis (InteprolateX2/X3), in the
+   order PackDataR0..R3 give, so the neighbour unpacks it in plain
+   (n, k, j, i) order; corners and radial neighbours are copied as
+   PackDataR0 does.  EXO_ERR_SHAPE for other ranges.  stream NULL: the
+   context's stream.  The reference's bound_lim > 0 (several blocks per
+   panel) has no counterpart: a context is one block per panel. */
+int exo_panel_pack(exo_ctx* ctx, const double* src, double* buf, int sn, int en, int si,
+                   int ei, int sj, int ej, int sk, int ek, int* offset, int ox1, int ox2,
+                   int ox3, int panel, void* stream);
+
+/* CubedSphere::SaveLR3DValues / LoadLR3DValues (src/exo3/cubed_sphere.hpp:
+   47-50, cubed_sphere.cpp:267-287): store and read back one row of x2
+   (direction 2) or x3 (direction 3) face states, L_row and R_row
+   [NHYDRO][L+6] (host or device memory), faces il..iu of row (k, j) of a
+   panel, in the context's face-state stores (device memory allocated on the
+   first call, four arrays of the state's size).  exo_lr3d_arrays returns
+   those stores (device pointers, the state's (panel, n, k, j, i) layout) for
+   callers that fill or read them whole. */
+int exo_save_lr3d(exo_ctx* ctx, const double* L_row, const double* R_row, int direction,
+                  int panel, int k, int j, int il, int iu, void* stream);
+int exo_load_lr3d(exo_ctx* ctx, double* L_row, double* R_row, int direction, int panel,
+                  int k, int j, int il, int iu, void* stream);
+int exo_lr3d_arrays(exo_ctx* ctx, double** L2, double** R2, double** L3, double** R3);
+/* CubedSphere::SynchronizeFluxesSend / Recv / Wait (cubed_sphere.cpp:
+   289-688) on the stores: at every panel-edge face (faces is-1..ie+1) the
+   neighbour's interior-side state, rotated into this panel's basis, becomes
+   the outer state (L at the Up/Left edges, R at Down/Right).  One kernel on
+   the device instead of MPI messages. */
+int exo_synchronize_faces(exo_ctx* ctx, void* stream);
+
+/* ---------------------------------------------- equation-of-state hooks */
+
+/* EquationOfState::ConservedToPrimitive / PrimitiveToConserved
+   (src/snap/eos/ideal_moist_hydro.cpp:77-196, shallow_yz_hydro.cpp:42-107)
+   on cells [il,iu] x [jl,ju] x [kl,ku] of every panel; u and w are device
+   arrays in the context's (panel, n, k, j, i) layout, ghosts included.
+   Covariant momenta become contravariant velocities with the cell metric as
+   in the reference; a negative or non-finite density or pressure sets the
+   sticky flag exo_check_state reads (SetStateInvalid). */
+int exo_conserved_to_primitive(exo_ctx* ctx, const double* u, double* w, int il, int iu,
+                               int jl, int ju, int kl, int ku, void* stream);
+int exo_primitive_to_conserved(exo_ctx* ctx, const double* w, double* u, int il, int iu,
+                               int jl, int ju, int kl, int ku, void* stream);
+/* EquationOfState::SoundSpeed (ideal_moist_hydro.cpp:226-238,
+   shallow_yz_hydro.cpp:103-107) of n cells: prim [NHYDRO][n] -> cs [n],
+   device arrays. */
+int exo_sound_speed(exo_ctx* ctx, int n, const double* prim, double* cs, void* stream);
+
+/* ---------------------------------------------------------- array views */
+
+/* A strided 4-D view of one panel's array, AthenaArray(n, k, j, i) order:
+   element (n,k,j,i) at data + n*stride[0] + k*stride[1] + j*stride[2] +
+   i*stride[3] (strides in elements, any sign).  device < 0: host memory;
+   otherwise the device memory of that CUDA device (the context's). */
+#define EXO_DTYPE_F64 0
+typedef struct exo_array_view {
+  void* data;
+  int dtype;              /* EXO_DTYPE_F64 */
+  int nx4, nx3, nx2, nx1; /* NHYDRO, N+6, N+6, L+6 */
+  int64_t stride[4];
+  int device;
+} exo_array_view;
+
+/* The whole-array entry points on six panel views (views[p] = panel p), the
+   reference's one AthenaArray per MeshBlock: exo_set_primitive,
+   exo_get_primitive, exo_get_conserved and exo_solve_implicit_3d (du in and
+   out, w in) with their arrays gathered from and scattered to the views. */
+int exo_set_primitive_views(exo_ctx* ctx, const exo_array_view* w);
+int exo_get_primitive_views(exo_ctx* ctx, const exo_array_view* w);
+int exo_get_conserved_views(exo_ctx* ctx, const exo_array_view* u);
+int exo_solve_implicit_3d_views(exo_ctx* ctx, const exo_array_view* du,
+                                const exo_array_view* w, double dt);
 
 /* ------------------------------------------------------------- ensembles */
 

@@ -2056,6 +2056,31 @@ void ora_panel_tables(int* nbr_panel, int* nbr_side, int* dinv, int* tgside, int
       pack[p * 4 + s] = kPackOrder[p][s];
     }
 }
+// ConservedToPrimitive (to_prim != 0) or PrimitiveToConserved over cells
+// [il,iu] x [jl,ju] x [kl,ku] of every panel, whole arrays; returns the
+// invalid flag of the cells converted
+int ora_eos_range(void* h, int to_prim, const double* in, double* out, int il, int iu, int jl,
+                  int ju, int kl, int ku) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  int invalid = 0;
+  for (int p = 0; p < 6; ++p)
+    for (int k = kl; k <= ku; ++k)
+      for (int j = jl; j <= ju; ++j) {
+        double cth = o.pg[p].cosc[o.kj(k, j)];
+        for (int i = il; i <= iu; ++i) {
+          double a[5] = {0, 0, 0, 0, 0}, b[5] = {0, 0, 0, 0, 0};
+          for (int n = 0; n < o.NV; ++n) a[n] = in[o.at(p, n, k, j, i)];
+          if (to_prim) cons_to_prim_cell(o, a, b, cth, &invalid);
+          else prim_to_cons_cell(o, a, b, cth);
+          for (int n = 0; n < o.NV; ++n) out[o.at(p, n, k, j, i)] = b[n];
+        }
+      }
+  return invalid;
+}
+double ora_sound_speed(void* h, const double* prim) {
+  return sound_speed(*static_cast<Oracle*>(h), prim);
+}
+
 // the radial face widths (ncells1), ghosts included
 void ora_get_dx1f(void* h, double* out) {
   Oracle& o = *static_cast<Oracle*>(h);

@@ -80,6 +80,10 @@ def lib():
         L.ora_interp_loc.argtypes = [i, i, i, i]
         L.ora_panel_tables.argtypes = [ip] * 5
         L.ora_get_dx1f.argtypes = [p, dp]
+        L.ora_eos_range.restype = i
+        L.ora_eos_range.argtypes = [p, i, dp, dp, i, i, i, i, i, i]
+        L.ora_sound_speed.restype = d
+        L.ora_sound_speed.argtypes = [p, dp]
         L.ora_pack_face.restype = i
         L.ora_pack_face.argtypes = [p, i, i, dp]
         L.ora_cell_geometry_at.argtypes = [p, i, i, i, i, dp]
@@ -217,6 +221,20 @@ class Oracle:
         w = np.ascontiguousarray(w, dtype=np.float64)
         assert du.flags.c_contiguous and du.dtype == np.float64
         lib().ora_solve_implicit_3d(self._h, _ptr(du), _ptr(w), float(dt))
+
+    def eos(self, to_prim, a, ranges):
+        """ConservedToPrimitive (to_prim) or PrimitiveToConserved of the whole
+        array a over ranges (il, iu, jl, ju, kl, ku); returns (out, invalid)
+        with out zero outside the ranges."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        out = np.zeros(self.shape)
+        inv = lib().ora_eos_range(self._h, int(bool(to_prim)), _ptr(a), _ptr(out), *ranges)
+        return out, inv
+
+    def sound_speed(self, prim):
+        w = np.zeros(5)
+        w[:len(prim)] = prim
+        return lib().ora_sound_speed(self._h, _ptr(w))
 
     def dx1f(self):
         out = np.zeros(self.cfg.L + 2 * NGHOST)
