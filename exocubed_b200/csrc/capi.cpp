@@ -455,10 +455,9 @@ void member_blocks(const DevView& v, const int* t, unsigned b[BK_COUNT]) {
   bool implicit = !shallow && (v.implicit_flag & 1);
   auto nb = [](size_t n, int th) { return (unsigned)((n + th - 1) / th); };
   b[BK_X1] = shallow ? 0u : nb((size_t)6 * v.N * v.N, t[BK_X1]);  // t[BK_X1] columns per block
-  // one thread per line of faces or per face, as the build chose
-  const bool lines = mixed_build(v.precision) ? mixed::x23_lines() : fp64::x23_lines();
-  b[BK_X23] = lines ? nb((size_t)2 * 6 * v.N * v.L, t[BK_X23])
-                    : nb((size_t)2 * 6 * v.N * (v.N + 1) * v.L, t[BK_X23]);
+  // tiles of faces, or one thread per line of faces or per face, as the build chose
+  b[BK_X23] = mixed_build(v.precision) ? mixed::x23_blocks(v, t[BK_X23])
+                                        : fp64::x23_blocks(v, t[BK_X23]);
   b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, t[BK_UPDATE]);
   b[BK_IMPLICIT] = implicit ? nb((size_t)6 * v.N * v.N, t[BK_IMPLICIT]) : 0u;  // thread per column
   b[BK_PRIM] = nb((size_t)6 * v.cells, t[BK_PRIM]);

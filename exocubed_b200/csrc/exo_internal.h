@@ -240,7 +240,8 @@ int view_refresh_self(DevView& v, void* stream, std::string* err);
   int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);          \
   int launch_batched_step(const BatchPlan& plan, void* stream);                     \
   int prepare_kernels();                                                            \
-  bool x23_lines();
+  bool x23_lines();                                                                 \
+  unsigned x23_blocks(const DevView& v, int tile);
 namespace fp64 { EXO_DECLARE_STEP_LAUNCHERS }
 namespace mixed { EXO_DECLARE_STEP_LAUNCHERS }
 #undef EXO_DECLARE_STEP_LAUNCHERS

@@ -31,8 +31,12 @@
 
 #include "exo_internal.h"
 
-// x2/x3 fluxes: 1 = one thread per line of faces (sliding stencil window),
-// 0 = one thread per face
+// x2/x3 fluxes: EXO_X23_TILES 1 = tiles staged through shared memory
+// (flux_x23_tile); otherwise EXO_X23_LINES 1 = one thread per line of faces
+// (sliding stencil window), 0 = one thread per face
+#ifndef EXO_X23_TILES
+#define EXO_X23_TILES 1
+#endif
 #ifndef EXO_X23_LINES
 #define EXO_X23_LINES EXO_MIXED
 #endif
@@ -1137,9 +1141,132 @@ __device__ __forceinline__ void flux_x23_lines(const DevView& v, unsigned blk) {
   }
 }
 
+// Tiles of faces staged through shared memory: a block of X23_THREADS
+// threads takes 32 consecutive radial indices i (one per lane, so every
+// global access of a warp is a coalesced row) of one line of one panel and
+// direction, and a chunk of x23_chunk<T>() faces along the line.
+//   0. the chunk's cells (with the three-cell halos of its stencils) are
+//      copied into shared memory, each cell once;
+//   1. one thread per cell computes both face values of the cell's WENO5
+//      reconstruction (the right-face value for the face above it, the
+//      left-face value for the face below; the mixed build shares the
+//      cell's smoothness indicators between the two, the FP64 build calls
+//      weno5 for each as the reference does);
+//   2. one thread per face takes the right-face value of the cell below
+//      and the left-face value of the cell above -- the neighbour panel's
+//      rotated state at a panel edge -- and solves the Riemann problem.
+// Each face gets the values and operations it gets in the per-face and
+// per-line kernels; phases 1 and 2 each keep few registers, so many warps
+// are resident.
+constexpr int X23_THREADS = 128;
+template <class T>
+__host__ __device__ constexpr int x23_chunk() {
+  return sizeof(T) == 4 ? 15 : 7;
+}
+// blocks of the tiled x2/x3 kernel for one atmosphere
+template <class T>
+__host__ __device__ constexpr unsigned x23_tile_blocks(int N, int L) {
+  return 2u * 6u * (unsigned)N * (unsigned)((L + 31) / 32) *
+         (unsigned)((N + 1 + x23_chunk<T>() - 1) / x23_chunk<T>());
+}
+
+template <class T>
+__device__ __forceinline__ void flux_x23_tile(const DevView& v, unsigned blk) {
+  constexpr int CF = x23_chunk<T>();   // faces of the chunk
+  constexpr int NC = CF + 1;           // cells reconstructed
+  constexpr int NIN = CF + 5;          // cells staged
+  __shared__ T sin_[5][NIN][32];
+  __shared__ T srec[2][5][NC][32];
+  const int N = v.N, L = v.L, nv = v.nv;
+  const unsigned nch = (unsigned)((N + 1 + CF - 1) / CF), nit = (unsigned)((L + 31) / 32);
+  unsigned r = blk;
+  const int chunk = (int)(r % nch);
+  r /= nch;
+  const int itile = (int)(r % nit);
+  r /= nit;
+  const int a = (int)(r % (unsigned)N);
+  r /= (unsigned)N;
+  const int p = (int)(r % 6u);
+  const int dir = (int)(r / 6u) + 1;
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+  constexpr int NW = X23_THREADS / 32;
+  const int il = itile * 32 + lane;   // radial index within the interior
+  const bool active = il < L;
+  const int i = v.is + il;
+  const size_t vs = v.cells;
+  const long s = dir == 1 ? (long)v.nc1 : (long)v.nc1 * v.nc2;  // stride along the line
+  const size_t base = dir == 1 ? idx(v, p, 0, v.ks + a, 0, i) : idx(v, p, 0, 0, v.js + a, i);
+  const T* __restrict__ W = prim_array<T>(v) + base;
+  const int c0 = dir == 1 ? v.js : v.ks, c1 = dir == 1 ? v.je : v.ke;
+  const int cb = c0 + chunk * CF;     // first face of the chunk
+  // 0. the cells cb-3 .. cb+CF+1 of the 32 lines (rows (variable, cell))
+  for (int row = warp; row < NIN * nv; row += NW) {
+    const int n = row / NIN, m = row % NIN;
+    const int c = cb - 3 + m;
+    T x = T(0);
+    if (active && c <= c1 + 3) x = __ldg(W + n * vs + (long)c * s);
+    sin_[n][m][lane] = x;
+  }
+  __syncthreads();
+  // 1. both face values of the cells cb-1 .. cb+CF-1
+  for (int mc = warp; mc < NC; mc += NW) {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
+      const T q0 = sin_[n][mc][lane], q1 = sin_[n][mc + 1][lane], q2 = sin_[n][mc + 2][lane];
+      const T q3 = sin_[n][mc + 3][lane], q4 = sin_[n][mc + 4][lane];
+#if EXO_X23_SHARED_BETA
+      const WenoCell<T> wc = weno_cell<T>(q0, q1, q2, q3, q4);
+      srec[0][n][mc][lane] = weno_right<T>(wc, q0, q1, q2, q3, q4);
+      srec[1][n][mc][lane] = weno_left<T>(wc, q0, q1, q2, q3, q4);
+#else
+      srec[0][n][mc][lane] = weno5<T>(q4, q3, q2, q1, q0);  // weno_r of the cell
+      srec[1][n][mc][lane] = weno5<T>(q0, q1, q2, q3, q4);  // weno_l of the cell
+#endif
+    }
+  }
+  __syncthreads();
+  if (!active) return;
+  // 2. the faces cb .. cb+CF-1 (up to c1+1)
+  T* F = flux_array<T>(v, dir);
+  for (int mf = warp; mf < CF; mf += NW) {
+    const int c = cb + mf;
+    if (c > c1 + 1) break;
+    T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
+      wl[n] = srec[0][n][mf][lane];
+      wr[n] = srec[1][n][mf + 1][lane];
+    }
+    const int k = dir == 1 ? v.ks + a : c;
+    const int j = dir == 1 ? c : v.js + a;
+    if (dir == 1) {
+      if (c == c0) edge_outer_state<T>(v, p, UP, a, i, wl);
+      else if (c == c1 + 1) edge_outer_state<T>(v, p, DOWN, a, i, wr);
+      FaceGeo<T> fg{T(geo(v, GCOSF2, p, k, j)), T(geo(v, GSINF2, p, k, j)),
+                    T(geo(v, GCTHP2, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+      riemann<T>(v.rsolver, v.gamma, IVY, fg, wl, wr, fx);
+    } else {
+      if (c == c0) edge_outer_state<T>(v, p, LEFT, a, i, wl);
+      else if (c == c1 + 1) edge_outer_state<T>(v, p, RIGHT, a, i, wr);
+      FaceGeo<T> fg{T(geo(v, GCOSF3, p, k, j)), T(geo(v, GSINF3, p, k, j)),
+                    T(geo(v, GCTHP3, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+      riemann<T>(v.rsolver, v.gamma, IVZ, fg, wl, wr, fx);
+    }
+    const size_t f0 = idx(v, p, 0, k, j, i);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      if (n >= nv) break;
+      F[f0 + n * vs] = fx[n];
+    }
+  }
+}
+
 template <class T>
 __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
-  if constexpr (EXO_X23_LINES) flux_x23_lines<T>(v, blk);
+  if constexpr (EXO_X23_TILES) flux_x23_tile<T>(v, blk);
+  else if constexpr (EXO_X23_LINES) flux_x23_lines<T>(v, blk);
   else flux_x23_faces<T>(v, blk);
 }
 
@@ -2959,10 +3086,12 @@ __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
 // the mixed build's sliding-window kernel: 168 registers (3 blocks of 128
 // threads per SM) measured 16 % faster than its natural 208 at 6x192^2x96;
 // the FP64 per-face kernel needs fewer
-#if !defined(EXO_X23_MAXNREG) && EXO_MIXED
+#if !defined(EXO_X23_MAXNREG) && EXO_MIXED && !EXO_X23_TILES
 #define EXO_X23_MAXNREG 168
 #endif
-#ifdef EXO_X23_MAXNREG
+#if EXO_X23_TILES
+#define EXO_X23_BOUNDS __launch_bounds__(X23_THREADS)
+#elif defined(EXO_X23_MAXNREG)
 #define EXO_X23_BOUNDS __maxnreg__(EXO_X23_MAXNREG)
 #else
 #define EXO_X23_BOUNDS
@@ -3086,6 +3215,9 @@ inline void launch_kb_implicit(int precision, unsigned blocks, int threads, int 
 // alone executes exactly the code it executes inside an ensemble.
 inline Batch one(const DevView& v, int kind) { return Batch{v.self, v.starts + 2 * kind, 1}; }
 
+// threads per block of the x2/x3 kernel: the tiled form is fixed at X23_THREADS
+inline int x23_threads(int tile) { return EXO_X23_TILES ? X23_THREADS : tile; }
+
 inline unsigned member_block_count(const DevView& v, int kind) {
   unsigned b[BK_COUNT];
   member_blocks(v, v.tiles, b);
@@ -3093,6 +3225,13 @@ inline unsigned member_block_count(const DevView& v, int kind) {
 }
 
 bool x23_lines() { return EXO_X23_LINES != 0; }
+
+unsigned x23_blocks(const DevView& v, int tile) {
+  if (EXO_X23_TILES) return x23_tile_blocks<EXO_FLUX_T>(v.N, v.L);
+  const size_t n = EXO_X23_LINES ? (size_t)2 * 6 * v.N * v.L
+                                 : (size_t)2 * 6 * v.N * (v.N + 1) * v.L;
+  return (unsigned)((n + tile - 1) / tile);
+}
 
 int prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(kb_implicit<double>,
@@ -3132,7 +3271,7 @@ int launch_flux_x1(const DevView& v, void* stream) {
 }
 
 int launch_flux_x23(const DevView& v, void* stream) {
-  kb_flux_x23<EXO_FLUX_T><<<member_block_count(v, BK_X23), v.tiles[BK_X23], 0,
+  kb_flux_x23<EXO_FLUX_T><<<member_block_count(v, BK_X23), x23_threads(v.tiles[BK_X23]), 0,
                             (cudaStream_t)stream>>>(
       one(v, BK_X23));
   return check_launch();
@@ -3203,7 +3342,8 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
       kb_flux_x1<EXO_FLUX_T><<<pl.total[BK_X1], pl.x1_threads, pl.x1_smem, st>>>(B(BK_X1));
       if ((rc = check_launch())) return rc;
     }
-    kb_flux_x23<EXO_FLUX_T><<<pl.total[BK_X23], pl.threads[BK_X23], 0, st>>>(B(BK_X23));
+    kb_flux_x23<EXO_FLUX_T><<<pl.total[BK_X23], x23_threads(pl.threads[BK_X23]), 0, st>>>(
+        B(BK_X23));
     if ((rc = check_launch())) return rc;
     kb_update<EXO_FLUX_T><<<pl.total[BK_UPDATE], pl.threads[BK_UPDATE], 0, st>>>(B(BK_UPDATE), s);
     if ((rc = check_launch())) return rc;
