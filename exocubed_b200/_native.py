@@ -48,7 +48,7 @@ EXPORTED = [
     "exo_panel_pack", "exo_save_lr3d", "exo_load_lr3d", "exo_lr3d_arrays",
     "exo_synchronize_faces", "exo_conserved_to_primitive", "exo_primitive_to_conserved",
     "exo_sound_speed", "exo_set_primitive_views", "exo_get_primitive_views",
-    "exo_get_conserved_views", "exo_solve_implicit_3d_views",
+    "exo_get_conserved_views", "exo_solve_implicit_3d_views", "exo_check_bounded_wait",
 ]
 EXO_DTYPE_F64 = 0
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
@@ -204,6 +204,7 @@ def lib():
     L.exo_get_primitive_views.argtypes = [p, vp]
     L.exo_get_conserved_views.argtypes = [p, vp]
     L.exo_solve_implicit_3d_views.argtypes = [p, vp, vp, d]
+    L.exo_check_bounded_wait.argtypes = [ctypes.POINTER(i), dp]
     L.exo_checkpoint_bytes.argtypes = [p, ctypes.POINTER(sz)]
     L.exo_checkpoint_save.argtypes = [p, p, sz]
     L.exo_checkpoint_load.argtypes = [p, p, sz]

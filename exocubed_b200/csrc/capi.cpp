@@ -1092,6 +1092,14 @@ int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
   return EXO_OK;
 }
 
+int exo_check_bounded_wait(int* gave_up, double* waited_ms) {
+  if (!gave_up || !waited_ms) return fail(EXO_ERR_ARG, "NULL argument");
+  std::string err;
+  int rc = exo::bounded_wait_selftest(gave_up, waited_ms, &err);
+  if (rc) return fail(rc, err);
+  return EXO_OK;
+}
+
 int exo_measure_fma_peak(int fp64, int repeats, double* flops_per_s) {
   if (!flops_per_s || repeats < 1) return fail(EXO_ERR_ARG, "flops_per_s NULL or repeats < 1");
   std::string err;

@@ -278,6 +278,8 @@ int launch_view_copy(const void* src, const int64_t* sstride, void* dst, const i
                      const int* size, void* stream);
 // peaks.cu: best FMA rate (flops/s) of independent chains on all SMs
 int measure_fma_peak(bool fp64, int repeats, double* flops_per_s, std::string* err);
+// peaks.cu: a bounded mbarrier wait that nothing completes, run once
+int bounded_wait_selftest(int* gave_up, double* waited_ms, std::string* err);
 
 
 // checkpoint.cpp: images of one atmosphere (exo_checkpoint_header, u, w)

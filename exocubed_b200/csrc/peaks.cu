@@ -6,6 +6,7 @@
 #include <string>
 
 #include "exo_internal.h"
+#include "exo_mbarrier.cuh"
 
 namespace exo {
 namespace {
@@ -76,7 +77,50 @@ int run(int repeats, double* out, std::string* err) {
   return EXO_OK;
 }
 
+// A wait that must give up: one warp waits on an mbarrier phase that
+// nothing completes (no arrival, no copy), through the same bounded wait
+// the back-substitution kernel uses for its bulk copies.
+__global__ void k_wait_selftest(int* gave_up, unsigned long long* waited_ns) {
+  __shared__ unsigned long long mb;
+  if (threadIdx.x == 0) {
+    mbar_init(&mb, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncwarp();
+  const unsigned long long t0 = global_ns();
+  const bool done = mbar_wait(&mb, 0u);
+  const unsigned long long t1 = global_ns();
+  if (threadIdx.x == 0) {
+    *gave_up = done ? 0 : 1;
+    *waited_ns = t1 - t0;
+  }
+}
+
 }  // namespace
+
+int bounded_wait_selftest(int* gave_up, double* waited_ms, std::string* err) {
+  int* g = nullptr;
+  unsigned long long* w = nullptr;
+  cudaError_t e = cudaMalloc((void**)&g, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&w, sizeof(unsigned long long));
+  if (e == cudaSuccess) {
+    k_wait_selftest<<<1, 32>>>(g, w);
+    e = cudaGetLastError();
+  }
+  int hg = -1;
+  unsigned long long hw = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&hg, g, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&hw, w, sizeof(hw), cudaMemcpyDeviceToHost);
+  if (g) cudaFree(g);
+  if (w) cudaFree(w);
+  if (e != cudaSuccess) {
+    *err = std::string("k_wait_selftest: ") + cudaGetErrorString(e);
+    return EXO_ERR_CUDA;
+  }
+  *gave_up = hg;
+  *waited_ms = hw * 1e-6;
+  return EXO_OK;
+}
 
 int measure_fma_peak(bool fp64, int repeats, double* flops_per_s, std::string* err) {
   return fp64 ? run<double>(repeats, flops_per_s, err) : run<float>(repeats, flops_per_s, err);

@@ -543,6 +543,14 @@ int exo_ensemble_add_checkpoint(exo_ensemble* ens, const void* image, size_t byt
    roofline of the step's FP64-issue-bound kernels a measured denominator. */
 int exo_measure_fma_peak(int fp64, int repeats, double* flops_per_s);
 
+/* Failure detection without a fault: one warp of a one-block kernel waits
+   on an mbarrier phase that nothing will complete, through the bounded
+   wait the library's kernels use for their bulk copies; it gives up after
+   0.1 s of wall time and returns.  *gave_up receives 1 (the wait ran out and
+   the kernel ended normally), *waited_ms how long it waited.  No
+   counterpart in the reference (its waits are MPI calls). */
+int exo_check_bounded_wait(int* gave_up, double* waited_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,3 +21,23 @@ def test_fma_peak_rejects_bad_arguments():
     out = ctypes.c_double()
     assert nat.lib().exo_measure_fma_peak(1, 0, ctypes.byref(out)) == nat.EXO_ERR_ARG
     assert nat.lib().exo_measure_fma_peak(1, 1, None) == nat.EXO_ERR_ARG
+
+
+def test_bounded_wait_gives_up_and_the_device_stays_usable():
+    """Failure detection without a fault: a wait on an mbarrier phase that
+    nothing completes (the bounded wait the back-substitution kernel uses for
+    its bulk copies) gives up after about 0.1 s and the kernel ends; the
+    device then runs a step as usual."""
+    import ctypes
+
+    from exocubed_b200 import workloads as W
+    from exocubed_b200.atmosphere import CubedSphereAtmosphere
+    gave_up, ms = ctypes.c_int(-1), ctypes.c_double()
+    nat.check(nat.lib().exo_check_bounded_wait(ctypes.byref(gave_up), ctypes.byref(ms)))
+    assert gave_up.value == 1
+    assert 90.0 <= ms.value < 2000.0, ms.value
+    cfg = W.dry_atmosphere_config(N=8, L=8)
+    with CubedSphereAtmosphere(cfg) as a:
+        a.set_primitive(W.dry_atmosphere_state(cfg, seed=1))
+        a.step(2)
+        assert a.invalid() == 0
