@@ -932,7 +932,9 @@ def main():
     ap.add_argument("--ensemble-members", type=int, default=64,
                     help="members of the C4 ensemble sample in the bench line (0: none)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
-    ap.add_argument("--serve-rate", type=float, default=100.0)
+    ap.add_argument("--serve-rate", type=float, default=2.0,
+                    help="arrival rate (req/s) of the serving sample: at 2 req/s the batching "
+                         "server keeps up with the stream and the one-at-a-time FP64 path does not")
     ap.add_argument("--ref-steps", type=int, default=0,
                     help="full steps the reference arm times at most (0: all of --steps)")
     ap.add_argument("--cpu-steps", type=int, default=3)

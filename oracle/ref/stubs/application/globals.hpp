@@ -1,0 +1,1 @@
+// harness stand-in: not used by the sources built here

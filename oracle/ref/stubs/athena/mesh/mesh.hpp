@@ -4,6 +4,8 @@
 #ifndef REF_STUB_MESH_HPP_
 #define REF_STUB_MESH_HPP_
 
+#include <memory>
+
 #include "../athena.hpp"
 #include "../bvals/bvals.hpp"
 
@@ -12,13 +14,17 @@ struct RegionSize {
   Real x1rat = 1.0, x2rat = 1.0, x3rat = 1.0;
 };
 
+class MeshBlock;
 class Mesh {
  public:
   bool multilevel = false;
+  // blocks of this process by gid (the harness has no local neighbours)
+  MeshBlock* FindMeshBlock(int) { return nullptr; }
 };
 
 class CubedSphere;
 class Microphysics;
+class Decomposition;
 
 class MeshBlock {
  public:
@@ -26,6 +32,7 @@ class MeshBlock {
   struct Impl {
     CubedSphere* pexo3 = nullptr;
     Microphysics* pmicro = nullptr;
+    std::shared_ptr<Decomposition> pdec;
   };
 
   Mesh* pmy_mesh = nullptr;

@@ -71,6 +71,57 @@ def ptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+_decomp = None
+
+
+def decomposition_lib():
+    """The reference's hydrostatic decomposition (change_to_perturbation.cpp,
+    decomposition.cpp) on one panel: oracle/_ref/libref_decomposition.so."""
+    global _decomp
+    if _decomp is None:
+        path = os.path.join(OUT, "libref_decomposition.so")
+        if not os.path.exists(path) and os.path.isdir(os.path.join(REF, "src")):
+            build()
+        L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        d, i, p = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.ref_decomp_create.restype = p
+        L.ref_decomp_create.argtypes = [i, i, d, d, d, dp, dp, dp, dp]
+        L.ref_decomp_destroy.argtypes = [p]
+        L.ref_change_to_perturbation.argtypes = [p, dp]
+        L.ref_restore_from_perturbation.argtypes = [p, dp, dp, dp, i, i, i, i]
+        _decomp = L
+    return _decomp
+
+
+class DecomposedPanel:
+    """One panel (MeshBlock) with the reference's Decomposition object."""
+
+    def __init__(self, N, L, gamma, Rd, grav, x1f, dx1f, x2f, x3f):
+        self.L_ = decomposition_lib()
+        self._keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (x1f, dx1f, x2f, x3f)]
+        self.h = self.L_.ref_decomp_create(N, L, gamma, Rd, grav, *[ptr(a) for a in self._keep])
+
+    def close(self):
+        if self.h:
+            self.L_.ref_decomp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def change_to_perturbation(self, w):
+        """w: one panel's primitives (5, N+6, N+6, L+6), changed in place."""
+        assert w.flags.c_contiguous and w.dtype == np.float64
+        self.L_.ref_change_to_perturbation(self.h, ptr(w))
+
+    def restore_from_perturbation(self, w, wl, wr, k, j, il, iu):
+        """w in place; wl, wr: face states of row (k, j), (5, L+6), in place."""
+        for a in (w, wl, wr):
+            assert a.flags.c_contiguous and a.dtype == np.float64
+        self.L_.ref_restore_from_perturbation(self.h, ptr(w), ptr(wl), ptr(wr), k, j, il, iu)
+
+
 class Sphere:
     """Six panels of one block each (MeshBlocks with the reference's
     GnomonicEquiangle, CubedSphere and Hydro objects) on a given mesh."""

@@ -24,10 +24,16 @@ inputs and require identical bits:
                                         LoadLR3DValues (face-state exchange)
   src/snap/riemann/lmars.cpp, hllc_transform.cpp, roe_shallow_yz.cpp,
   lmars_shallow_yz.cpp                  Hydro::RiemannSolver rows
+  src/snap/decomposition/change_to_perturbation.cpp, decomposition.cpp
+                                        ChangeToPerturbation (hydrostatic face
+                                        pressure, log-mean and isentropic
+                                        reference state, bottom entropy) and
+                                        RestoreFromPerturbation on one panel
 
 The stand-ins supply no arithmetic of their own except the equation of
 state's sound speed (ideal_moist_hydro.cpp with no vapour), which HLLC
-calls.  Through these pins and the GPU parity tests, the CUDA path is held
+calls, and the dry polytropic index 1 + (gamma - 1) feps / fsig of canoe's
+Thermodynamics, which the decomposition reads.  Through these pins and the GPU parity tests, the CUDA path is held
 to the same reference code.
 """
 import numpy as np
@@ -234,3 +240,40 @@ def test_face_state_exchange_bitwise(ref):
     # the exchange changed something (the edges were overwritten)
     assert not np.array_equal(want[0], arrs[0])
     sph.close()
+
+
+@pytest.mark.parametrize("rsolver,seed", [(1, 4), (2, 9)])
+def test_decomposition_bitwise(ref, rsolver, seed):
+    """ChangeToPerturbation and RestoreFromPerturbation of the reference
+    (one panel, reflecting radial boundaries, no vertical neighbours) against
+    the oracle's, panel by panel, on a seeded dry state."""
+    N, L = 8, 10
+    cfg = W.dry_atmosphere_config(N=N, L=L, rsolver=rsolver)
+    o = oracle.Oracle(cfg)
+    o.set_primitive(W.dry_atmosphere_state(cfg, seed=seed, geometry=oracle.cell_geometry))
+    w0 = o.primitive()
+    w_ora = w0.copy()
+    o.change_to_perturbation(w_ora)
+    rng = np.random.default_rng(seed)
+    wl = w_ora.copy() + rng.standard_normal(w_ora.shape) * 1e-3
+    wr = w_ora.copy() + rng.standard_normal(w_ora.shape) * 1e-3
+    wl_ora, wr_ora, w_back = wl.copy(), wr.copy(), w_ora.copy()
+    o.restore_from_perturbation(w_back, wl_ora, wr_ora)
+    x1f = o.mesh(0)[0]
+    for p in range(6):
+        _, x2f, x3f = o.mesh(p)
+        pan = reference.DecomposedPanel(N, L, cfg["gamma"], cfg["Rd"], cfg["grav"],
+                                        x1f, o.dx1f(), x2f, x3f)
+        wp = np.ascontiguousarray(w0[p])
+        pan.change_to_perturbation(wp)
+        inner = (slice(None), slice(G, G + N), slice(G, G + N), slice(None))
+        assert np.array_equal(wp[inner], w_ora[p][inner]), p
+        for k in range(G, G + N):
+            for j in range(G, G + N):
+                lrow = np.ascontiguousarray(wl[p, :, k, j, :])
+                rrow = np.ascontiguousarray(wr[p, :, k, j, :])
+                pan.restore_from_perturbation(wp, lrow, rrow, k, j, G, G + L)
+                assert np.array_equal(lrow[:, G:G + L + 1], wl_ora[p, :, k, j, G:G + L + 1])
+                assert np.array_equal(rrow[:, G:G + L + 1], wr_ora[p, :, k, j, G:G + L + 1])
+        assert np.array_equal(wp[inner], w_back[p][inner]), p
+        pan.close()
