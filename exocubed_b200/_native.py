@@ -86,8 +86,10 @@ class ArrayView(ctypes.Structure):
 def views_of(panels, device=-1):
     """Six ArrayViews of six 4-D panel arrays: numpy arrays (host, any
     strides) or, with device >= 0, (data_ptr, shape, element strides)
-    triples of device arrays."""
+    triples of device arrays.  The result holds a reference to the panels,
+    so a temporary list stays alive as long as the views do."""
     out = (ArrayView * 6)()
+    out._panels = list(panels)
     for p, a in enumerate(panels):
         if device < 0:
             assert a.dtype.itemsize == 8 and a.ndim == 4

@@ -163,21 +163,10 @@ static int one_stage(exo_ctx* c, int s, bool cfl) {
   int nup = (!shallow && !implicit && s == 2) ? 2 : 1;
   if ((rc = timed(c, EXO_K_UPDATE, nup, [&] { return STEP(launch_update, v, s, c->stream); })))
     return rc;
-  const bool dt = s == 2 && cfl;
-  if (implicit && exo::prims_from_bwd(v)) {
-    // the back substitution writes the primitives of the interior and radial
-    // ghost cells and the CFL candidates; the ghost bands follow
-    if (dt && (rc = timed(c, EXO_K_OTHER, 1, [&] { return STEP(launch_dt_reset, v, c->stream); })))
-      return rc;
-    if ((rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(v.implicit_flag),
-                    [&] { return STEP(launch_implicit, v, s, dt, c->stream); })))
-      return rc;
-    return timed(c, EXO_K_PRIM_GHOST, 1, [&] { return STEP(launch_aux, v, s, c->stream); });
-  }
-  if (implicit && (rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(v.implicit_flag),
-                              [&] { return STEP(launch_implicit, v, s, false, c->stream); })))
+  if (implicit && (rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(v.implicit_flag, v.precision),
+                              [&] { return STEP(launch_implicit, v, s, c->stream); })))
     return rc;
-  return boundary_and_prim(c, dt);
+  return boundary_and_prim(c, s == 2 && cfl);
 }
 
 static int one_step(exo_ctx* c, double dt_fixed) {
@@ -472,12 +461,7 @@ void member_blocks(const DevView& v, const int* t, unsigned b[BK_COUNT]) {
   b[BK_UPDATE] = nb((size_t)6 * v.N * v.N * v.L, t[BK_UPDATE]);
   b[BK_IMPLICIT] = implicit ? nb((size_t)6 * v.N * v.N, t[BK_IMPLICIT]) : 0u;  // thread per column
   b[BK_PRIM] = nb((size_t)6 * v.cells, t[BK_PRIM]);
-  // the auxiliary kernel: the round trip without the implicit solve, or the
-  // ghost bands when the back substitution writes the interior primitives
-  b[BK_ROUNDTRIP] = (!shallow && !implicit)
-                        ? nb((size_t)6 * v.N * v.N * v.L, t[BK_ROUNDTRIP])
-                        : prims_from_bwd(v) ? nb((size_t)6 * 4 * G * v.N * v.nc1, t[BK_ROUNDTRIP])
-                                            : 0u;
+  b[BK_ROUNDTRIP] = (!shallow && !implicit) ? nb((size_t)6 * v.N * v.N * v.L, t[BK_ROUNDTRIP]) : 0u;
 }
 
 int view_refresh_self(DevView& v, void* stream_v, std::string* err) {
@@ -892,7 +876,7 @@ int exo_solve_implicit_3d(exo_ctx* c, double* du_host, const double* w_host, dou
   size_t bytes = c->state_elems * sizeof(double);
   CK(cudaMemcpyAsync(c->v.w, w_host, bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->v.du, du_host, bytes, cudaMemcpyHostToDevice, c->stream));
-  int rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(c->v.implicit_flag),
+  int rc = timed(c, EXO_K_IMPLICIT, exo::implicit_launches(c->v.implicit_flag, c->v.precision),
                  [&] { return STEP(launch_implicit_du, c->v, dt, c->stream); });
   if (rc) return fail(rc, "implicit launch failed");
   CK(cudaMemcpyAsync(du_host, c->v.du, bytes, cudaMemcpyDeviceToHost, c->stream));

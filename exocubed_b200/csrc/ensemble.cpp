@@ -94,7 +94,6 @@ int rebuild(exo_ensemble* e) {
   std::vector<unsigned> start((size_t)exo::BK_COUNT * (e->capacity + 1), 0);
   unsigned tot[exo::BK_COUNT] = {0, 0, 0, 0, 0, 0};
   bool any_full = false;  // some member takes the 5x5 correction
-  bool any_bands = false;  // some member's primitives come from the back substitution
   int max_nc1 = 1;
   int x1_threads = 32;
   size_t x1_smem = 8;
@@ -106,7 +105,6 @@ int rebuild(exo_ensemble* e) {
     max_nc1 = std::max(max_nc1, m->v.nc1);
     if (m->v.eqn != EXO_EQN_SHALLOW_YZ && (m->v.implicit_flag & 1) && (m->v.implicit_flag & 8))
       any_full = true;
-    if (exo::prims_from_bwd(m->v)) any_bands = true;
     unsigned b[exo::BK_COUNT];
     exo::member_blocks(m->v, e->tiles.t, b);
     for (int k = 0; k < exo::BK_COUNT; ++k) {
@@ -143,13 +141,10 @@ int rebuild(exo_ensemble* e) {
   pl.max_nc1 = max_nc1;
   pl.precision = e->precision;
   pl.any_full_correction = any_full;
-  pl.any_bands = any_bands;
   // count the kernel nodes of one step
   int64_t per_stage = (tot[exo::BK_X1] ? 1 : 0) + 1 + 1 +
-                      (tot[exo::BK_IMPLICIT] ? (any_full ? 2 : 1) : 0) + 1;
-  // kb_aux: every stage with ghost bands to fill, else the last stage's round trip
-  const int64_t aux = tot[exo::BK_ROUNDTRIP] ? (any_bands ? 3 : 1) : 0;
-  e->launches_per_step = 3 * per_stage + aux + 1 + 1;
+                      (tot[exo::BK_IMPLICIT] ? (any_full && exo::split_bwd(e->precision) ? 2 : 1) : 0) + 1;
+  e->launches_per_step = 3 * per_stage + (tot[exo::BK_ROUNDTRIP] ? 1 : 0) + 1 + 1;
   cudaGraph_t graph;
   ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   int rc = exo::mixed_build(e->precision) ? exo::mixed::launch_batched_step(pl, e->stream)

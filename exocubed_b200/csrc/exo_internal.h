@@ -105,12 +105,6 @@ struct DevScalars {
   long long ncycle;
 };
 
-// The implicit solve with the full (5x5) correction runs as two kernels,
-// the forward sweep (kb_implicit) and the back substitution
-// (kb_implicit_bwd, memory-bound, fed by bulk copies); the partial (3x3)
-// correction does both in kb_implicit.
-inline int implicit_launches(int implicit_flag) { return (implicit_flag & 8) ? 2 : 1; }
-
 // n / d for 0 <= n < 2^40 / (d - 1) as floor(n m / 2^40), m = ceil(2^40 / d):
 // with n = q d + t, n m / 2^40 = q + t / d + n r / (d 2^40) for some r < d,
 // which stays below q + 1 in that range (the kernels' flat indices are
@@ -172,10 +166,6 @@ struct alignas(16) DevView {
 
 // A batched step: every member's DevView in device memory and, per kernel
 // kind, the first block of every member (start[k][n] = total blocks).
-// BK_ROUNDTRIP's block table serves the auxiliary kernel kb_aux: the
-// last-stage AirParcel round trip of members without the implicit solve,
-// and every stage's panel-edge ghost bands of members whose primitives come
-// from the back substitution (prims_from_bwd)
 enum BatchKind { BK_X1 = 0, BK_X23, BK_UPDATE, BK_IMPLICIT, BK_PRIM, BK_ROUNDTRIP, BK_COUNT };
 struct BatchPlan {
   const DevView* views;          // device, n entries
@@ -188,8 +178,6 @@ struct BatchPlan {
   int max_nc1;                   // largest nc1 of the members (radial tables in shared memory)
   int precision;                 // EXO_PREC_* of every member
   bool any_full_correction;      // some member takes the 5x5 solve (kb_implicit_bwd runs)
-  bool any_bands;                // some member's primitives come from kb_implicit_bwd
-                                 // (kb_aux fills its ghost bands every stage)
 };
 // Threads per block ("tile") of each batched kernel by BatchKind.  BK_X1
 // takes one radial column per block (its size follows L) and ignores its
@@ -213,17 +201,14 @@ constexpr int X1_MAX_COLUMNS = 8;
 EXO_HD inline bool mixed_build(int precision) {
   return precision == EXO_PREC_MIXED || precision == EXO_PREC_MIXED_F32_SOLVE;
 }
-// The back substitution of the full correction (kb_implicit_bwd) writes the
-// primitives of the interior cells and of the radial ghost cells, the
-// invalid flag and the CFL candidate, from the corrected state it holds in
-// shared memory; the primitive kernel then fills only the panel-edge ghost
-// bands (kb_aux).  Needs three levels for the radial ghosts' mirrors.
-#ifndef EXO_BWD_PRIM
-#define EXO_BWD_PRIM 1
-#endif
-EXO_HD inline bool prims_from_bwd(const DevView& v) {
-  return EXO_BWD_PRIM && v.eqn != EXO_EQN_SHALLOW_YZ && (v.implicit_flag & 1) &&
-         (v.implicit_flag & 8) && v.L >= 3;
+// The implicit solve with the full (5x5) correction: FP64 blocks solve and
+// back-substitute each column in kb_implicit (a column's back substitution
+// overlaps other columns' forward sweeps); FP32 blocks run the forward sweep
+// in kb_implicit and the back substitution in kb_implicit_bwd (memory-bound,
+// fed by bulk copies).  The partial (3x3) correction does both in kb_implicit.
+EXO_HD inline bool split_bwd(int precision) { return precision == EXO_PREC_MIXED_F32_SOLVE; }
+inline int implicit_launches(int implicit_flag, int precision) {
+  return ((implicit_flag & 8) && split_bwd(precision)) ? 2 : 1;
 }
 EXO_HD inline int x1_column_doubles(const DevView& v) {
   int faces = v.nc1 + 1;
@@ -250,8 +235,7 @@ int view_refresh_self(DevView& v, void* stream, std::string* err);
   int launch_flux_x1(const DevView& v, void* stream);                                \
   int launch_flux_x23(const DevView& v, void* stream);                               \
   int launch_update(const DevView& v, int stage, void* stream);                      \
-  int launch_implicit(const DevView& v, int stage, bool compute_dt, void* stream);   \
-  int launch_aux(const DevView& v, int stage, void* stream);                         \
+  int launch_implicit(const DevView& v, int stage, void* stream);                    \
   int launch_implicit_du(const DevView& v, double dt, void* stream);                 \
   int launch_dt_reset(const DevView& v, void* stream);                               \
   int launch_dt_finalize(const DevView& v, double dt_fixed, bool advance_time, void* stream); \

@@ -594,43 +594,18 @@ __device__ __forceinline__ void block_min_atomic(unsigned long long* target, uns
   }
 }
 
-// Hydro::NewBlockTimeStep with patches/21.new_blockdt.patch:23-35 at an
-// interior cell with primitives w: the candidate as the bits of a
-// non-negative double, or ~0 when there is none
-__device__ __forceinline__ unsigned long long cfl_candidate(const DevView& v, const double* w,
-                                                            int p, int k, int j, int i) {
+__device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, unsigned tid,
+                                                              int compute_dt) {
   const unsigned long long none = ~0ull;
-  bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
-  double cs;
-  if (shallow) cs = sqrt(w[IDN]);
-  else {
-    double fsig = 1., feps = 1.;
-    cs = sqrt((1. + (v.gamma - 1) * feps / fsig) * w[IPR] / w[IDN]);
-  }
-  double dt1 = v.dx1f[i], dt2 = v.x1v[i] * geo(v, GDX2A, p, k, j);
-  double dt3 = v.x1v[i] * geo(v, GDX3A, p, k, j);
-  double speed1 = fmax(0., (fabs(w[IVX]) + cs));
-  double speed2 = fmax(0., (fabs(w[IVY]) + cs));
-  double speed3 = fmax(0., (fabs(w[IVZ]) + cs));
-  if ((v.implicit_flag & 1) && (v.N > 1)) dt1 /= v.cfl * fabs(w[IVX]);
-  else dt1 /= speed1;
-  if (v.implicit_flag & 2) dt2 /= v.cfl * fabs(w[IVY]);
-  else dt2 /= speed2;
-  if (v.implicit_flag & 4) dt3 /= v.cfl * fabs(w[IVZ]);
-  else dt3 /= speed3;
-  double m = fmin(dt2, dt3);
-  if (!shallow) m = fmin(dt1, m);
-  if (m >= 0.) return (unsigned long long)__double_as_longlong(m);
-  return none;
-}
-
-// primitives of cell (p,k,j,i), (k,j) interior or in a ghost band: ghost
-// interpolation or the interior conserved state, ConservedToPrimitive, the
-// radial reflection, w and (mixed) w32 written; for interior cells the
-// invalid flag and, when compute_dt, the CFL candidate (returned)
-__device__ __forceinline__ unsigned long long prim_cell(const DevView& v, int p, int k, int j,
-                                                        int i, int compute_dt) {
-  const unsigned long long none = ~0ull;
+  unsigned total = 6u * (unsigned)v.cells;
+  if (tid >= total) return none;
+  unsigned r = v.div_nc1(tid);
+  unsigned i = tid - r * (unsigned)v.nc1;
+  unsigned r2 = v.div_nc2(r);
+  int j = (int)(r - r2 * (unsigned)v.nc2);
+  unsigned r3 = v.div_nc3(r2);
+  int k = (int)(r2 - r3 * (unsigned)v.nc3);
+  int p = (int)r3;
   bool kin = (k >= v.ks && k <= v.ke), jin = (j >= v.js && j <= v.je);
   if (!kin && !jin) return none;  // corner: never read on the path
   int ii = i;
@@ -656,54 +631,37 @@ __device__ __forceinline__ unsigned long long prim_cell(const DevView& v, int p,
 #endif
   if (!(kin && jin) || mirror) return none;
   if (bad) atomicOr(&v.sc->invalid, 1);
-  if (compute_dt) return cfl_candidate(v, w, p, k, j, i);
+  if (compute_dt) {
+    // Hydro::NewBlockTimeStep with patches/21.new_blockdt.patch:23-35
+    bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
+    double cs;
+    if (shallow) cs = sqrt(w[IDN]);
+    else {
+      double fsig = 1., feps = 1.;
+      cs = sqrt((1. + (v.gamma - 1) * feps / fsig) * w[IPR] / w[IDN]);
+    }
+    double dt1 = v.dx1f[i], dt2 = v.x1v[i] * geo(v, GDX2A, p, k, j);
+    double dt3 = v.x1v[i] * geo(v, GDX3A, p, k, j);
+    double speed1 = fmax(0., (fabs(w[IVX]) + cs));
+    double speed2 = fmax(0., (fabs(w[IVY]) + cs));
+    double speed3 = fmax(0., (fabs(w[IVZ]) + cs));
+    if ((v.implicit_flag & 1) && (v.N > 1)) dt1 /= v.cfl * fabs(w[IVX]);
+    else dt1 /= speed1;
+    if (v.implicit_flag & 2) dt2 /= v.cfl * fabs(w[IVY]);
+    else dt2 /= speed2;
+    if (v.implicit_flag & 4) dt3 /= v.cfl * fabs(w[IVZ]);
+    else dt3 /= speed3;
+    double m = fmin(dt2, dt3);
+    if (!shallow) m = fmin(dt1, m);
+    if (m >= 0.) return (unsigned long long)__double_as_longlong(m);
+  }
   return none;
-}
-
-__device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, unsigned tid,
-                                                              int compute_dt) {
-  const unsigned long long none = ~0ull;
-  unsigned total = 6u * (unsigned)v.cells;
-  if (tid >= total) return none;
-  unsigned r = v.div_nc1(tid);
-  unsigned i = tid - r * (unsigned)v.nc1;
-  unsigned r2 = v.div_nc2(r);
-  int j = (int)(r - r2 * (unsigned)v.nc2);
-  unsigned r3 = v.div_nc3(r2);
-  int k = (int)(r2 - r3 * (unsigned)v.nc3);
-  int p = (int)r3;
-  return prim_cell(v, p, k, j, (int)i, compute_dt);
 }
 
 __device__ __forceinline__ void prim_ghost_block(const DevView& v, unsigned blk, int compute_dt) {
   unsigned tid = blk * blockDim.x + threadIdx.x;
   unsigned long long m = prim_ghost_cell(v, tid, compute_dt);
   if (compute_dt) block_min_atomic(&v.sc->dtmin_bits, m);
-}
-
-// cells of the panel-edge ghost bands (radial ghosts included): per panel
-// four bands of G x N x nc1 cells
-__host__ __device__ constexpr unsigned band_cells(int N, int nc1) {
-  return 6u * 4u * (unsigned)G * (unsigned)N * (unsigned)nc1;
-}
-// The primitives of the ghost bands alone, for members whose interior
-// primitives the back substitution wrote (prims_from_bwd)
-__device__ __forceinline__ void prim_bands_block(const DevView& v, unsigned blk) {
-  const unsigned tid = blk * blockDim.x + threadIdx.x;
-  const int N = v.N, nc1 = v.nc1;
-  if (tid >= band_cells(N, nc1)) return;
-  const unsigned per_band = (unsigned)G * N * nc1;
-  const unsigned q = tid / per_band, r = tid - q * per_band;  // q = panel * 4 + band
-  const int p = (int)(q >> 2), band = (int)(q & 3u);
-  const int g = (int)(r / ((unsigned)N * nc1));
-  const unsigned r2 = r - (unsigned)g * N * nc1;
-  const int a = (int)(r2 / (unsigned)nc1), i = (int)(r2 - (unsigned)a * nc1);
-  int k, j;
-  if (band == 0) { j = g; k = v.ks + a; }
-  else if (band == 1) { j = v.je + 1 + g; k = v.ks + a; }
-  else if (band == 2) { k = g; j = v.js + a; }
-  else { k = v.ke + 1 + g; j = v.js + a; }
-  prim_cell(v, p, k, j, i, 0);
 }
 
 // ------------------------------------------------------------ k_flux_x1 ---
@@ -2759,10 +2717,12 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const bool full = (v.implicit_flag & 8) != 0;
   const ImplSlices<R> sl = impl_slices<R>(ism, full);
   using IO = StepColumnIO<R>;
-  // the back substitution of the full correction is kb_implicit_bwd's (the
-  // lighter partial one stays here: split, it measured slower)
+  // FP32 blocks: the back substitution of the full correction is
+  // kb_implicit_bwd's (split_bwd; the lighter partial one stays here: split,
+  // it measured slower)
+  constexpr bool kBwd = sizeof(R) == 8;
   if (full)
-    implicit_column<IO, false>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
+    implicit_column<IO, kBwd>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
                                          geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
                                          geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
                                          dt, v.gamma, v.grav);
@@ -2777,9 +2737,9 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
 // The back substitution of the full correction, delta_i -= (A c)_i
 // delta_{i+1} from the top level down, u += delta (with the AirParcel round
 // trip on the last stage), as a kernel of its own after the forward sweep
-// (kb_implicit, which leaves (A c)_i and delta_i of every level in scratch).
-// It streams 240 (FP64 factors) or 120 (FP32) bytes of scratch and 80 bytes
-// of u per cell and computes little, so it is built to keep HBM busy: one
+// (kb_implicit, which leaves (A c)_i and delta_i of every level in scratch),
+// for FP32 blocks.  It streams 120 bytes of scratch and 80 bytes of u per
+// cell and computes little, so it is built to keep HBM busy: one
 // warp per group of 32 columns, whose scratch is one contiguous run per
 // chunk of BWD_LEV levels ([group][level][entry][32]); the chunk below the
 // one being finished is already on its way into the other shared-memory
@@ -2810,8 +2770,7 @@ static_assert(bwd_chunk_bytes<double>() % 16 == 0 && bwd_buffer_bytes<double>() 
               "bulk copies move multiples of 16 bytes to 16-byte aligned addresses");
 
 template <class R>
-__device__ __forceinline__ void implicit_bwd_warp(const DevView& v, int group, int stage,
-                                                  int compute_dt) {
+__device__ __forceinline__ void implicit_bwd_warp(const DevView& v, int group, int stage) {
   extern __shared__ __align__(128) unsigned char bws[];
   const int lane = (int)(threadIdx.x & 31);
   const int ncol = 6 * v.N * v.N;
@@ -2821,18 +2780,12 @@ __device__ __forceinline__ void implicit_bwd_warp(const DevView& v, int group, i
   const int L = v.L;
   const size_t vs = v.cells;
   size_t base = 0;
-  int cp = 0, ck = 0, cj = 0;  // the column's panel, k, j
   if (active) {
-    cj = v.js + col % v.N;
-    ck = v.ks + (col / v.N) % v.N;
-    cp = col / (v.N * v.N);
-    base = idx(v, cp, 0, ck, cj, 0);
+    const int j = v.js + col % v.N;
+    const int k = v.ks + (col / v.N) % v.N;
+    const int p = col / (v.N * v.N);
+    base = idx(v, p, 0, k, j, 0);
   }
-  // the primitives of the interior and radial ghost cells come from here
-  const bool prims = prims_from_bwd(v);
-  const double cth = active ? geo(v, GCOSC, cp, ck, cj) : 0.;
-  bool bad_any = false;
-  unsigned long long dt_min = ~0ull;
   // this column's scratch: entry e of level lev at sg[(lev * 30 + e) * 32 + lane]
   const R* sg = reinterpret_cast<const R*>(v.scratch) + (size_t)group * L * 30 * 32;
   unsigned long long* mb = reinterpret_cast<unsigned long long*>(bws + 2 * bwd_buffer_bytes<R>());
@@ -2931,65 +2884,7 @@ __device__ __forceinline__ void implicit_bwd_warp(const DevView& v, int group, i
         u[cbase + n * vs + v.is + lo + l] = tile[(n * 32 + cc) * (BWD_LEV + 1) + l];
     }
     __syncwarp();
-    if (prims) {
-      // ConservedToPrimitive of the chunk's corrected cells, in the tile
-      // (the primitive kernel's arithmetic, prim_cell); the radial ghost
-      // cells' reflected primitives go out directly
-      if (active) {
-        for (int l = 0; l < nl; ++l) {
-          const int i = v.is + lo + l;
-          double uu[5], w[5];
-#pragma unroll
-          for (int n = 0; n < 5; ++n) uu[n] = tile[(n * 32 + lane) * (BWD_LEV + 1) + l];
-          if (cons_to_prim(v, uu, w, cth)) bad_any = true;
-          if (compute_dt) {
-            const unsigned long long m = cfl_candidate(v, w, cp, ck, cj, i);
-            dt_min = m < dt_min ? m : dt_min;
-          }
-#pragma unroll
-          for (int n = 0; n < 5; ++n) tile[(n * 32 + lane) * (BWD_LEV + 1) + l] = w[n];
-          const int lev = lo + l;
-          for (int side = 0; side < 2; ++side) {
-            const bool hit = side == 0 ? lev <= 2 : lev >= L - 3;
-            if (!hit) continue;
-            const int im = side == 0 ? v.is - 1 - lev : 2 * v.ie + 1 - i;
-#pragma unroll
-            for (int n = 0; n < 5; ++n) {
-              const double x = n == IVX ? -w[n] : w[n];
-              v.w[base + n * vs + im] = x;
-#if EXO_MIXED
-              v.w32[base + n * vs + im] = (float)x;
-#endif
-            }
-          }
-        }
-      }
-      __syncwarp();
-      for (int e = lane; e < 5 * 32 * BWD_LEV; e += 32) {
-        const int l = e & (BWD_LEV - 1), cc = (e / BWD_LEV) & 31, n = e / (BWD_LEV * 32);
-        const long long cbase = __shfl_sync(0xffffffffu, cb_lane, cc);
-        if (cc < ncb && l < nl) {
-          const double x = tile[(n * 32 + cc) * (BWD_LEV + 1) + l];
-          v.w[cbase + n * vs + v.is + lo + l] = x;
-#if EXO_MIXED
-          v.w32[cbase + n * vs + v.is + lo + l] = (float)x;
-#endif
-        }
-      }
-      __syncwarp();
-    }
     b ^= 1;
-  }
-  if (prims) {
-    if (__any_sync(0xffffffffu, bad_any) && lane == 0) atomicOr(&v.sc->invalid, 1);
-    if (compute_dt) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long y = __shfl_down_sync(0xffffffffu, dt_min, o);
-        dt_min = y < dt_min ? y : dt_min;
-      }
-      if (lane == 0 && dt_min != ~0ull) atomicMin(&v.sc->dtmin_bits, dt_min);
-    }
   }
   if (!ok) {
     // a bulk copy did not complete in time: record it, and give every copy
@@ -3125,12 +3020,9 @@ __device__ __forceinline__ unsigned batch_enter(const Batch& bt, DevView& sv) {
 #else
 #define EXO_PRIM_BOUNDS
 #endif
-// skip_bwd: members whose primitives come from the back substitution
-// (prims_from_bwd) are left to it and to kb_aux (the batched step)
-__global__ void EXO_PRIM_BOUNDS kb_prim_ghost(Batch bt, int compute_dt, int skip_bwd) {
+__global__ void EXO_PRIM_BOUNDS kb_prim_ghost(Batch bt, int compute_dt) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
-  if (skip_bwd && prims_from_bwd(sv)) return;
   prim_ghost_block(sv, b, compute_dt);
 }
 
@@ -3191,8 +3083,7 @@ __global__ void EXO_IMPL_BOUNDS kb_implicit(Batch bt, int stage, double dt_given
 // One warp per group of 32 columns: implicit block b of a member (its
 // columns b*T .. b*T+T-1 at T = the implicit tile) is T/32 blocks here.
 template <class R>
-__global__ void __launch_bounds__(32) kb_implicit_bwd(Batch bt, int stage, int warps_per_iblock,
-                                                      int compute_dt) {
+__global__ void __launch_bounds__(32) kb_implicit_bwd(Batch bt, int stage, int warps_per_iblock) {
   __shared__ __align__(16) DevView sv;
   const unsigned ib = blockIdx.x / (unsigned)warps_per_iblock;
   {
@@ -3213,22 +3104,14 @@ __global__ void __launch_bounds__(32) kb_implicit_bwd(Batch bt, int stage, int w
     implicit_bwd_du<R>(sv, group * 32 + (int)threadIdx.x);
     return;
   }
-  implicit_bwd_warp<R>(sv, group, stage, compute_dt);
+  implicit_bwd_warp<R>(sv, group, stage);
 }
 
-// The auxiliary kernel of the BK_ROUNDTRIP block table: the last stage's
-// AirParcel round trip of members without the implicit solve, and every
-// stage's panel-edge ghost bands of members whose interior primitives the
-// back substitution wrote (launched after it)
-__global__ void kb_aux(Batch bt, int stage) {
+__global__ void kb_roundtrip(Batch bt) {
   __shared__ __align__(16) DevView sv;
   unsigned b = batch_enter(bt, sv);
-  if (sv.eqn == EXO_EQN_SHALLOW_YZ) return;
-  if (!(sv.implicit_flag & 1)) {
-    if (stage == 2) roundtrip_block(sv, b);
-  } else if (prims_from_bwd(sv)) {
-    prim_bands_block(sv, b);
-  }
+  if (sv.eqn == EXO_EQN_SHALLOW_YZ || (sv.implicit_flag & 1)) return;
+  roundtrip_block(sv, b);
 }
 
 __global__ void k_p2c(DevView v, const double* wsrc) { p2c_block(v, blockIdx.x, wsrc); }
@@ -3263,24 +3146,25 @@ inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 // back substitution
 template <class R>
 inline void launch_kb_implicit(unsigned blocks, int threads, int nc1, cudaStream_t st, Batch b,
-                               int stage, double dt_given, bool any_full, int compute_dt) {
+                               int stage, double dt_given, bool any_full) {
   kb_implicit<R><<<blocks, threads, impl_smem<R>(threads, nc1), st>>>(b, stage, dt_given);
-  if (any_full)
-    kb_implicit_bwd<R><<<blocks * (unsigned)(threads / 32), 32, impl_bwd_smem<R>(), st>>>(
-        b, stage, threads / 32, compute_dt);
+  if constexpr (sizeof(R) == 4) {
+    if (any_full)
+      kb_implicit_bwd<R><<<blocks * (unsigned)(threads / 32), 32, impl_bwd_smem<R>(), st>>>(
+          b, stage, threads / 32);
+  }
 }
 inline void launch_kb_implicit(int precision, unsigned blocks, int threads, int nc1,
                                cudaStream_t st, Batch b, int stage, double dt_given,
-                               bool any_full, int compute_dt) {
+                               bool any_full) {
 #if EXO_MIXED
   if (precision == EXO_PREC_MIXED_F32_SOLVE) {
-    launch_kb_implicit<float>(blocks, threads, nc1, st, b, stage, dt_given, any_full,
-                              compute_dt);
+    launch_kb_implicit<float>(blocks, threads, nc1, st, b, stage, dt_given, any_full);
     return;
   }
 #endif
   (void)precision;
-  launch_kb_implicit<double>(blocks, threads, nc1, st, b, stage, dt_given, any_full, compute_dt);
+  launch_kb_implicit<double>(blocks, threads, nc1, st, b, stage, dt_given, any_full);
 }
 
 }  // namespace
@@ -3316,9 +3200,6 @@ int prepare_kernels() {
     e = cudaFuncSetAttribute(kb_implicit<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              IMPL_SMEM_MAX);
 #endif
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(kb_implicit_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)impl_bwd_smem<double>());
 #if EXO_MIXED
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(kb_implicit_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -3332,14 +3213,7 @@ int prepare_kernels() {
 
 int launch_prim_ghost(const DevView& v, bool compute_dt, void* stream) {
   kb_prim_ghost<<<member_block_count(v, BK_PRIM), v.tiles[BK_PRIM], 0, (cudaStream_t)stream>>>(
-      one(v, BK_PRIM), compute_dt ? 1 : 0, 0);
-  return check_launch();
-}
-
-int launch_aux(const DevView& v, int stage, void* stream) {
-  const unsigned nb = member_block_count(v, BK_ROUNDTRIP);
-  if (nb == 0) return 0;
-  kb_aux<<<nb, v.tiles[BK_ROUNDTRIP], 0, (cudaStream_t)stream>>>(one(v, BK_ROUNDTRIP), stage);
+      one(v, BK_PRIM), compute_dt ? 1 : 0);
   return check_launch();
 }
 
@@ -3365,16 +3239,20 @@ int launch_update(const DevView& v, int stage, void* stream) {
       one(v, BK_UPDATE), stage);
   int rc = check_launch();
   if (rc) return rc;
-  if (v.eqn != EXO_EQN_SHALLOW_YZ && !(v.implicit_flag & 1) && stage == 2)
-    rc = launch_aux(v, stage, stream);  // the AirParcel round trip
+  if (v.eqn != EXO_EQN_SHALLOW_YZ && !(v.implicit_flag & 1) && stage == 2) {
+    kb_roundtrip<<<member_block_count(v, BK_ROUNDTRIP), v.tiles[BK_ROUNDTRIP], 0,
+                   (cudaStream_t)stream>>>(
+        one(v, BK_ROUNDTRIP));
+    rc = check_launch();
+  }
   return rc;
 }
 
-int launch_implicit(const DevView& v, int stage, bool compute_dt, void* stream) {
+int launch_implicit(const DevView& v, int stage, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   launch_kb_implicit(v.precision, member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT], v.nc1,
                      (cudaStream_t)stream, one(v, BK_IMPLICIT), stage, 0.,
-                     (v.implicit_flag & 8) != 0, compute_dt ? 1 : 0);
+                     (v.implicit_flag & 8) != 0);
   return check_launch();
 }
 
@@ -3382,7 +3260,7 @@ int launch_implicit_du(const DevView& v, double dt, void* stream) {
   if (v.eqn == EXO_EQN_SHALLOW_YZ || !(v.implicit_flag & 1)) return 0;
   launch_kb_implicit(v.precision, member_block_count(v, BK_IMPLICIT), v.tiles[BK_IMPLICIT], v.nc1,
                      (cudaStream_t)stream, one(v, BK_IMPLICIT), -1, dt,
-                     (v.implicit_flag & 8) != 0, 0);
+                     (v.implicit_flag & 8) != 0);
   return check_launch();
 }
 
@@ -3425,22 +3303,20 @@ int launch_batched_step(const BatchPlan& pl, void* stream) {
     if ((rc = check_launch())) return rc;
     kb_update<EXO_FLUX_T><<<pl.total[BK_UPDATE], pl.threads[BK_UPDATE], 0, st>>>(B(BK_UPDATE), s);
     if ((rc = check_launch())) return rc;
-    if (s == 2) {  // before the back substitution, which adds CFL candidates
-      kb_dt_reset<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n);
+    if (s == 2 && pl.total[BK_ROUNDTRIP]) {
+      kb_roundtrip<<<pl.total[BK_ROUNDTRIP], pl.threads[BK_ROUNDTRIP], 0, st>>>(B(BK_ROUNDTRIP));
       if ((rc = check_launch())) return rc;
     }
     if (pl.total[BK_IMPLICIT]) {
       launch_kb_implicit(pl.precision, pl.total[BK_IMPLICIT], pl.threads[BK_IMPLICIT],
-                         pl.max_nc1, st, B(BK_IMPLICIT), s, 0., pl.any_full_correction,
-                         s == 2 ? 1 : 0);
+                         pl.max_nc1, st, B(BK_IMPLICIT), s, 0., pl.any_full_correction);
       if ((rc = check_launch())) return rc;
     }
-    if (pl.total[BK_ROUNDTRIP] && (s == 2 || pl.any_bands)) {
-      kb_aux<<<pl.total[BK_ROUNDTRIP], pl.threads[BK_ROUNDTRIP], 0, st>>>(B(BK_ROUNDTRIP), s);
+    if (s == 2) {
+      kb_dt_reset<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n);
       if ((rc = check_launch())) return rc;
     }
-    kb_prim_ghost<<<pl.total[BK_PRIM], pl.threads[BK_PRIM], 0, st>>>(B(BK_PRIM), s == 2 ? 1 : 0,
-                                                                     1);
+    kb_prim_ghost<<<pl.total[BK_PRIM], pl.threads[BK_PRIM], 0, st>>>(B(BK_PRIM), s == 2 ? 1 : 0);
     if ((rc = check_launch())) return rc;
   }
   kb_dt_finalize<<<nblk(pl.n, 128), 128, 0, st>>>(pl.views, pl.n, 1);

@@ -1,7 +1,8 @@
 """Generates tests/golden/oracle_c2_lmars.npz: a long run of the oracle on the
-C2 workload, the FP64 reference that the north star's accuracy bar is
-measured against (run from the repository root on the CPU, about half an
-hour on 8 cores: python tests/golden/make_oracle_runs.py).
+C2 workload, the FP64 reference that the mixed path's accuracy bar (1e-5
+relative L2 after 1000 steps) is measured against (run from the repository
+root on the CPU, about half an hour on 8 cores:
+python tests/golden/make_oracle_runs.py).
 
 Workload: the exo3 dry ideal-gas atmosphere, 6 panels x 96 x 96 x 64 levels,
 WENO5 + LMARS + the 5x5 implicit vertical solve (implicit_flag 9), SSPRK(3,3),
