@@ -193,11 +193,18 @@ __device__ __forceinline__ T weno_l(const S* q, long s, int c) {
 
 // ------------------------------------------------------------------ EOS ----
 // CubedSphereUtility::CovariantToContravariant (cubed_sphere_utility.hpp:22-31)
+// (the mixed build multiplies by one reciprocal instead of four divisions)
 __device__ __forceinline__ void cov_to_contra(double* a, double cth) {
   double v = a[IVY], w = a[IVZ];
   double sth2 = 1. - cth * cth;
+#if EXO_MIXED
+  const double is2 = 1. / sth2;
+  a[IVY] = (v - w * cth) * is2;
+  a[IVZ] = (w - v * cth) * is2;
+#else
   a[IVY] = v / sth2 - w * cth / sth2;
   a[IVZ] = -v * cth / sth2 + w / sth2;
+#endif
 }
 __device__ __forceinline__ void contra_to_cov(double* a, double cth) {
   double v = a[IVY], w = a[IVZ];
@@ -1142,6 +1149,21 @@ __device__ __forceinline__ void flux_x23_lines(const DevView& v, unsigned blk) {
   }
 }
 
+// asynchronous 8-byte global -> shared copies (the next level's inputs)
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
 // Tiles of faces staged through shared memory: a block of X23_THREADS
 // threads takes 32 consecutive radial indices i (one per lane, so every
 // global access of a warp is a coalesced row) of one line of one panel and
@@ -1164,11 +1186,18 @@ template <class T>
 __host__ __device__ constexpr int x23_chunk() {
   return sizeof(T) == 4 ? 15 : 7;
 }
+// EXO_X23_PIPE 1: a block walks its whole line of faces chunk by chunk,
+// the next chunk's cells copied into a ring of shared memory (cp.async)
+// while the current chunk is reconstructed and solved; the five halo cells
+// two chunks share are copied once.  0: one block per chunk.
+#ifndef EXO_X23_PIPE
+#define EXO_X23_PIPE 0
+#endif
 // blocks of the tiled x2/x3 kernel for one atmosphere
 template <class T>
 __host__ __device__ constexpr unsigned x23_tile_blocks(int N, int L) {
   return 2u * 6u * (unsigned)N * (unsigned)((L + 31) / 32) *
-         (unsigned)((N + 1 + x23_chunk<T>() - 1) / x23_chunk<T>());
+         (EXO_X23_PIPE ? 1u : (unsigned)((N + 1 + x23_chunk<T>() - 1) / x23_chunk<T>()));
 }
 
 template <class T>
@@ -1264,9 +1293,139 @@ __device__ __forceinline__ void flux_x23_tile(const DevView& v, unsigned blk) {
   }
 }
 
+// cp.async of 4 or 8 bytes, zero-filled when src_bytes is 0
+template <int B>
+__device__ __forceinline__ void cp_async_zfill(void* smem_dst, const void* gsrc, int src_bytes) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gsrc), "n"(B),
+               "r"(src_bytes)
+               : "memory");
+}
+
+// The x2/x3 faces of one line (32 radial indices of one row of one panel
+// and direction) chunk by chunk, with the same phases, values and
+// operations per face as flux_x23_tile.  Cell c of the line sits in ring
+// slot (c - c0 + 3) mod XR; the copies of chunk q + 1's new cells are in
+// flight while chunk q is finished.  Slots written for chunk q + 1 held
+// cells at least XR = 2 CF + 5 below them, which chunk q no longer reads;
+// the copies for chunk q + 2 start after the barrier that ends chunk q's
+// reconstruction.
+template <class T>
+__device__ __forceinline__ void flux_x23_pipe(const DevView& v, unsigned blk) {
+  constexpr int CF = x23_chunk<T>();
+  constexpr int NC = CF + 1;
+  constexpr int XR = 2 * CF + 5;
+  __shared__ __align__(16) T ring[5][XR][32];
+  __shared__ T srec[2][5][NC][32];
+  const int N = v.N, L = v.L, nv = v.nv;
+  const unsigned nit = (unsigned)((L + 31) / 32);
+  unsigned r = blk;
+  const int itile = (int)(r % nit);
+  r /= nit;
+  const int a = (int)(r % (unsigned)N);
+  r /= (unsigned)N;
+  const int p = (int)(r % 6u);
+  const int dir = (int)(r / 6u) + 1;
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+  constexpr int NW = X23_THREADS / 32;
+  const int il = itile * 32 + lane;
+  const bool active = il < L;
+  const int i = v.is + il;
+  const size_t vs = v.cells;
+  const long s = dir == 1 ? (long)v.nc1 : (long)v.nc1 * v.nc2;
+  const size_t base = dir == 1 ? idx(v, p, 0, v.ks + a, 0, active ? i : v.is)
+                               : idx(v, p, 0, 0, v.js + a, active ? i : v.is);
+  const T* __restrict__ W = prim_array<T>(v) + base;
+  const int c0 = dir == 1 ? v.js : v.ks, c1 = dir == 1 ? v.je : v.ke;
+  const int nch = (N + 1 + CF - 1) / CF;
+  // copies of cells [from, to] (line indices), rows (variable, cell) over the warps
+  auto issue = [&](int from, int to) {
+    const int nc = to - from + 1;
+    for (int row = warp; row < nc * nv; row += NW) {
+      const int n = row / nc, c = from + row % nc;
+      int slot = c - c0 + 3;
+      slot -= (slot >= XR) ? XR * (slot / XR) : 0;
+      const bool ok = active && c <= c1 + 3;
+      cp_async_zfill<sizeof(T)>(&ring[n][slot][lane], W + n * vs + (long)(ok ? c : c0) * s,
+                                ok ? (int)sizeof(T) : 0);
+    }
+    cp_async_commit();
+  };
+  issue(c0 - 3, c0 + CF + 1);
+  T* F = flux_array<T>(v, dir);
+  for (int q = 0; q < nch; ++q) {
+    const int cb = c0 + q * CF;
+    if (q + 1 < nch) {
+      issue(cb + CF + 2, cb + 2 * CF + 1);
+      cp_async_wait_one();
+    } else {
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    // 1. both face values of the cells cb-1 .. cb+CF-1
+    for (int mc = warp; mc < NC; mc += NW) {
+      int s0 = cb - 1 - c0 + 3 + mc - 2;  // slot of cell cb-1+mc-2
+      s0 -= (s0 >= XR) ? XR * (s0 / XR) : 0;
+      int sl[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) sl[m] = (s0 + m >= XR) ? s0 + m - XR : s0 + m;
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        if (n >= nv) break;
+        const T q0 = ring[n][sl[0]][lane], q1 = ring[n][sl[1]][lane], q2 = ring[n][sl[2]][lane];
+        const T q3 = ring[n][sl[3]][lane], q4 = ring[n][sl[4]][lane];
+#if EXO_X23_SHARED_BETA
+        const WenoCell<T> wc = weno_cell<T>(q0, q1, q2, q3, q4);
+        srec[0][n][mc][lane] = weno_right<T>(wc, q0, q1, q2, q3, q4);
+        srec[1][n][mc][lane] = weno_left<T>(wc, q0, q1, q2, q3, q4);
+#else
+        srec[0][n][mc][lane] = weno5<T>(q4, q3, q2, q1, q0);
+        srec[1][n][mc][lane] = weno5<T>(q0, q1, q2, q3, q4);
+#endif
+      }
+    }
+    __syncthreads();
+    if (!active) continue;
+    // 2. the faces cb .. cb+CF-1 (up to c1+1)
+    for (int mf = warp; mf < CF; mf += NW) {
+      const int c = cb + mf;
+      if (c > c1 + 1) break;
+      T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        if (n >= nv) break;
+        wl[n] = srec[0][n][mf][lane];
+        wr[n] = srec[1][n][mf + 1][lane];
+      }
+      const int k = dir == 1 ? v.ks + a : c;
+      const int j = dir == 1 ? c : v.js + a;
+      if (dir == 1) {
+        if (c == c0) edge_outer_state<T>(v, p, UP, a, i, wl);
+        else if (c == c1 + 1) edge_outer_state<T>(v, p, DOWN, a, i, wr);
+        FaceGeo<T> fg{T(geo(v, GCOSF2, p, k, j)), T(geo(v, GSINF2, p, k, j)),
+                      T(geo(v, GCTHP2, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+        riemann<T>(v.rsolver, v.gamma, IVY, fg, wl, wr, fx);
+      } else {
+        if (c == c0) edge_outer_state<T>(v, p, LEFT, a, i, wl);
+        else if (c == c1 + 1) edge_outer_state<T>(v, p, RIGHT, a, i, wr);
+        FaceGeo<T> fg{T(geo(v, GCOSF3, p, k, j)), T(geo(v, GSINF3, p, k, j)),
+                      T(geo(v, GCTHP3, p, k, j)), T(geo(v, GCOSC, p, k, j))};
+        riemann<T>(v.rsolver, v.gamma, IVZ, fg, wl, wr, fx);
+      }
+      const size_t f0 = idx(v, p, 0, k, j, i);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        if (n >= nv) break;
+        F[f0 + n * vs] = fx[n];
+      }
+    }
+  }
+}
+
 template <class T>
 __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
-  if constexpr (EXO_X23_TILES) flux_x23_tile<T>(v, blk);
+  if constexpr (EXO_X23_TILES && EXO_X23_PIPE) flux_x23_pipe<T>(v, blk);
+  else if constexpr (EXO_X23_TILES) flux_x23_tile<T>(v, blk);
   else if constexpr (EXO_X23_LINES) flux_x23_lines<T>(v, blk);
   else flux_x23_faces<T>(v, blk);
 }
@@ -1342,6 +1501,10 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   const double a3 = x1vi * dx2f3 * dx1fi;
   const double a3p = x1vi * dx2f3p * dx1fi;
   const double vol = dx1fi * d2 * d3 * x1vi * x1vi * s;
+  // the mixed build multiplies by reciprocals of the volume and the radius
+  // (one division each instead of eight; the FP64 build divides as the
+  // reference does)
+  [[maybe_unused]] const double ivol = 1. / vol, irad = 1. / x1vi;
   double du[5];
   // flux divergence in T (the x1 part in FP64 where its fluxes are); the
   // conserved state accumulates in FP64
@@ -1359,7 +1522,7 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
       T d23 = (A2p * f1r[n] - A2 * f1l[n]);
       d23 += (A3p * f2r[n] - A3 * f2l[n]);
       const double d1 = a1p * f0r[n] - a1 * f0l[n];
-      change = wght * ((d1 + (double)d23) / vol);
+      change = wght * ((d1 + (double)d23) * ivol);
     } else {
       T dflx = (A1p * f0r[n] - A1 * f0l[n]);
       dflx += (A2p * f1r[n] - A2 * f1l[n]);
@@ -1378,12 +1541,19 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   {
     const double cosine = G2(GCOSC, 0);
     const double sine2 = s * s;
+#if EXO_MIXED
+    const double x_ov_rD = (x1vi * dx3f2 * dx1fi * G2(GSINF2, 0) -
+                            x1vi * dx3f2p * dx1fi * G2(GSINF2, 1)) * ivol;
+    const double y_ov_rC = (x1vi * dx2f3 * dx1fi * G2(GSINF3, 0) -
+                            x1vi * dx2f3p * dx1fi * G2(GSINF3, v.nc2)) * ivol;
+#else
     const double x_ov_rD = (x1vi * dx3f2 * dx1fi * G2(GSINF2, 0) -
                             x1vi * dx3f2p * dx1fi * G2(GSINF2, 1)) / vol;
     const double y_ov_rC = (x1vi * dx2f3 * dx1fi * G2(GSINF3, 0) -
                             x1vi * dx2f3p * dx1fi * G2(GSINF3, v.nc2)) / vol;
+#endif
     const double rho = wv[IDN], v1 = wv[IVX], v2 = wv[IVY], v3 = wv[IVZ];
-    const double radius = x1vi;
+    [[maybe_unused]] const double radius = x1vi;
     double pr;
     const double v_2 = v2 + v3 * cosine;
     const double v_3 = v3 + v2 * cosine;
@@ -1391,12 +1561,22 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
       pr = 0.5 * rho * rho;
     } else {
       pr = wv[IPR];
+#if EXO_MIXED
+      double src1 = (2.0 * pr + rho * (v2 * v_2 + v3 * v_3)) * irad;
+#else
       double src1 = (2.0 * pr + rho * (v2 * v_2 + v3 * v_3)) / radius;
+#endif
       out[IVX] += wght * src1;
     }
+#if EXO_MIXED
+    double src2 = -x_ov_rD * (pr + rho * v3 * v3 * sine2) - rho * v1 * v_2 * irad;
+    out[IVY] += wght * src2;
+    double src3 = -y_ov_rC * (pr + rho * v2 * v2 * sine2) - rho * v1 * v_3 * irad;
+#else
     double src2 = -x_ov_rD * (pr + rho * v3 * v3 * sine2) - rho * v1 * v_2 / radius;
     out[IVY] += wght * src2;
     double src3 = -y_ov_rC * (pr + rho * v2 * v2 * sine2) - rho * v1 * v_3 / radius;
+#endif
     out[IVZ] += wght * src3;
     // constant gravity (patches/25.constant_acc.patch:35-53)
     if (v.grav != 0.) {
@@ -1558,21 +1738,6 @@ __device__ __forceinline__ R fj_entry(const ColCell<R>& c, R gm1) {
     else if constexpr (q == 3) return -gm1 * c.v3 * c.v1;
     else return (gm1 + 1) * c.v1;
   }
-}
-
-// asynchronous 8-byte global -> shared copies (the next level's inputs)
-__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_one() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
 // compile-time loops (the matrix entries live in registers, so every index
@@ -3046,7 +3211,9 @@ __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
 #if !defined(EXO_X23_MAXNREG) && EXO_MIXED && !EXO_X23_TILES
 #define EXO_X23_MAXNREG 168
 #endif
-#if EXO_X23_TILES
+#if EXO_X23_TILES && defined(EXO_X23_MINB)
+#define EXO_X23_BOUNDS __launch_bounds__(X23_THREADS, EXO_X23_MINB)
+#elif EXO_X23_TILES
 #define EXO_X23_BOUNDS __launch_bounds__(X23_THREADS)
 #elif defined(EXO_X23_MAXNREG)
 #define EXO_X23_BOUNDS __maxnreg__(EXO_X23_MAXNREG)
