@@ -1191,7 +1191,7 @@ __host__ __device__ constexpr int x23_chunk() {
 // while the current chunk is reconstructed and solved; the five halo cells
 // two chunks share are copied once.  0: one block per chunk.
 #ifndef EXO_X23_PIPE
-#define EXO_X23_PIPE 0
+#define EXO_X23_PIPE 1
 #endif
 // blocks of the tiled x2/x3 kernel for one atmosphere
 template <class T>
@@ -1981,6 +1981,132 @@ __device__ __forceinline__ void implicit_backward_full(IO& io, int is, int ie,
   }
 }
 
+// The back substitution of the stepping kernel's FP64 blocks (mixed build)
+// with the state u moved through shared memory by the warp: the warp's 32
+// columns go down BWD_TL levels at a time; each lane copies four levels of
+// a column for one variable in one 32-byte run (the per-lane accesses of
+// one level are 816 bytes apart, a sector each), the next chunk's copies in
+// flight while a chunk is corrected.  The factors are read per lane, one
+// level ahead, as in implicit_backward_full (they are contiguous across the
+// warp).  io.live: the lanes of the warp with a column.  wtile: 2 x 5 x 32 x
+// (BWD_TL + 1) doubles of shared memory for the warp alone.
+constexpr int BWD_TL = 4;
+__device__ __forceinline__ void airparcel_round_trip(double* u, double Rd, double gamma);
+// the stepping solve's shared doubles per thread
+constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : (EXO_IMPL_BWD_SMEM ? 71 : 61);
+static_assert(32 * IMPL_SM_STRIDE >= 2 * 5 * 32 * (BWD_TL + 1),
+              "the tiled back substitution's buffers fit in the warp's slices");
+template <class IO>
+__device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, double* dp,
+                                                        double* wtile) {
+  static_assert(BWD_TL == 4, "the lane -> (column, level) split below assumes 4 levels");
+  constexpr int TS = BWD_TL + 1;
+  constexpr int TW = 5 * 32 * TS;
+  const unsigned live = io.live;
+  const int lane = (int)(threadIdx.x & 31);
+  __syncwarp(live);
+  // lane copies level (lane & 3) of columns (lane >> 2) + 8 m, m = 0..3
+  // (in a warp with a column in every lane)
+  double* ub[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    ub[m] = reinterpret_cast<double*>(__shfl_sync(
+        live, reinterpret_cast<unsigned long long>(io.uc), ((lane >> 2) + 8 * m) & 31));
+  const int l = lane & 3;
+  const int nch = (ie - is + BWD_TL) / BWD_TL;
+  auto range = [&](int c, int& lo, int& hi) {
+    hi = ie - c * BWD_TL;
+    lo = max(is, hi - BWD_TL + 1);
+  };
+  // a warp with a column in every lane copies in 32-byte runs; the last warp
+  // of a member may have fewer, and there each lane copies its own column
+  const bool full = live == 0xffffffffu;
+  auto load = [&](int c) {
+    double* t = wtile + (c & 1) * TW;
+    int lo, hi;
+    range(c, lo, hi);
+    if (full) {
+      if (lo + l <= hi) {
+#pragma unroll
+        for (int e = 0; e < 20; ++e) {
+          const int m = e & 3, n = e >> 2;
+          cp_async8(&t[(n * 32 + (lane >> 2) + 8 * m) * TS + l], ub[m] + n * io.vs + lo + l);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 20; ++e) {
+        const int ll = e & 3, n = e >> 2;
+        if (lo + ll <= hi) cp_async8(&t[(n * 32 + lane) * TS + ll], io.uc + n * io.vs + lo + ll);
+      }
+    }
+    cp_async_commit();
+  };
+  load(0);
+  if (nch > 1) load(1);
+  using R = typename IO::Real;
+  R cur_s[30];
+  if (ie > is) {
+#pragma unroll
+    for (int e = 0; e < 30; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
+  }
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) cp_async_wait_one();
+    else cp_async_wait_all();
+    __syncwarp(live);
+    double* t = wtile + (c & 1) * TW;
+    int lo, hi;
+    range(c, lo, hi);
+    for (int i = hi; i >= lo; --i) {
+      if (i < ie) {
+        R nxt_s[30];
+        if (i > is) {
+#pragma unroll
+          for (int e = 0; e < 30; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
+        }
+        R dl[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+          R ad = cur_s[r * 5] * dp[0];
+#pragma unroll
+          for (int k = 1; k < 5; ++k) ad += cur_s[r * 5 + k] * dp[k];
+          dl[r] = cur_s[25 + r] - ad;
+        }
+#pragma unroll
+        for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+        if (i > is) {
+#pragma unroll
+          for (int e = 0; e < 30; ++e) cur_s[e] = nxt_s[e];
+        }
+      }
+      double uu[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) uu[n] = t[(n * 32 + lane) * TS + (i - lo)] + 1. * (double)dp[n];
+      if (io.stage == 2) airparcel_round_trip(uu, io.Rd, io.gamma);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) t[(n * 32 + lane) * TS + (i - lo)] = uu[n];
+    }
+    __syncwarp(live);
+    if (full) {
+      if (lo + l <= hi) {
+#pragma unroll
+        for (int e = 0; e < 20; ++e) {
+          const int m = e & 3, n = e >> 2;
+          ub[m][n * io.vs + lo + l] = t[(n * 32 + (lane >> 2) + 8 * m) * TS + l];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 20; ++e) {
+        const int ll = e & 3, n = e >> 2;
+        if (lo + ll <= hi) io.uc[n * io.vs + lo + ll] = t[(n * 32 + lane) * TS + ll];
+      }
+    }
+    __syncwarp(live);
+    if (c + 2 < nch) load(c + 2);
+  }
+}
+
 // The vertical 5x5 block-tridiagonal correction of one radial column
 // (ImplicitSolver::SolveImplicit3D X1 branch, solve_implicit_3d.cpp:102-179,
 // with FullCorrection, full_correction.cpp:32-165, and ForwardSweep /
@@ -2403,6 +2529,14 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
   }
 }
 #else
+  if constexpr (IO::kLoadsU && sizeof(R) == 8) {
+    if (io.stage >= 0) {
+      // the warp's 32 shared slices are free once every lane has finished
+      // its forward sweep
+      implicit_backward_tiled(io, is, ie, dp, sa - (threadIdx.x & 31) * IMPL_SM_STRIDE);
+      return;
+    }
+  }
   implicit_backward_full(io, is, ie, dp);
 }
 #endif
@@ -2742,12 +2876,12 @@ constexpr int IMPL_MAX_THREADS = 128;
 #define EXO_IMPL_BOUNDS __launch_bounds__(IMPL_MAX_THREADS, EXO_IMPL_MINB)
 #endif
 // FP64 solve: each thread's doubles are contiguous (60, or 85 with
-// (A c)_{i-1} kept there), threads IMPL_SM_STRIDE doubles apart: an odd
-// stride keeps a half-warp's 8-byte accesses on distinct banks.
+// (A c)_{i-1} kept there), threads IMPL_SM_STRIDE doubles apart (defined
+// with the back substitution): an odd stride keeps a half-warp's 8-byte
+// accesses on distinct banks.
 // FP32 solve: structure of arrays, the 10 prefetch doubles of every thread
 // first, then the 50 FP32 face-block entries, entry e of thread t at
 // [e * threads + t], so a warp's accesses are consecutive words.
-constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : (EXO_IMPL_BWD_SMEM ? 71 : 61);
 template <class R>
 __host__ __device__ constexpr int impl_slice_doubles() {
   return sizeof(R) == 4 ? 10 + 50 / 2 : IMPL_SM_STRIDE;
@@ -2830,6 +2964,7 @@ struct StepColumnIO {
     return scr0[(lev * 30 + e) * 32];
   }
   static constexpr bool kLoadsU = true;
+  unsigned live = 0xffffffffu;  // the lanes of the warp with a column
   __device__ __forceinline__ const double* uptr(int i, int n) const { return uc + n * vs + i; }
   __device__ __forceinline__ void uload(int i, double* u) const {
     if (stage < 0) return;
@@ -2868,6 +3003,7 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   const double* x1v;
   const double* dx1f;
   stage_radial(impl_radial<R>(ism), v.nc1, v.x1f, v.x1v, v.dx1f, x1f, x1v, dx1f);
+  const unsigned live = __ballot_sync(0xffffffffu, col < ncol);
   if (col >= ncol) return;
   const int j = v.js + col % v.N;
   const int k = v.ks + (col / v.N) % v.N;
@@ -2879,6 +3015,7 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
   R* scr0 = reinterpret_cast<R*>(v.scratch) + (size_t)(col >> 5) * v.L * 30 * 32 + (col & 31);
   StepColumnIO<R> io{v.w + base, v.du + base, v.u + base, v.cells, scr0, stage, v.Rd, v.gamma,
                      v.du + base};
+  io.live = live;
   const bool full = (v.implicit_flag & 8) != 0;
   const ImplSlices<R> sl = impl_slices<R>(ism, full);
   using IO = StepColumnIO<R>;
@@ -3210,6 +3347,12 @@ __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
 // the FP64 per-face kernel needs fewer
 #if !defined(EXO_X23_MAXNREG) && EXO_MIXED && !EXO_X23_TILES
 #define EXO_X23_MAXNREG 168
+#endif
+// the pipelined line kernel of the mixed build at 128 registers (4 blocks of
+// 128 threads per SM): 1.64 ms per launch at 6x192^2x96 against 1.75 at its
+// natural 148 and 1.91 for one block per chunk
+#if EXO_X23_TILES && EXO_X23_PIPE && EXO_MIXED && !defined(EXO_X23_MINB)
+#define EXO_X23_MINB 4
 #endif
 #if EXO_X23_TILES && defined(EXO_X23_MINB)
 #define EXO_X23_BOUNDS __launch_bounds__(X23_THREADS, EXO_X23_MINB)
