@@ -54,12 +54,6 @@
 #ifndef EXO_X23_SHARED_BETA
 #define EXO_X23_SHARED_BETA EXO_MIXED
 #endif
-// 1: the implicit solve's back substitution prefetches two levels through
-// shared memory (FP64: 3% faster at 6x192^2x96; mixed: 1% slower, since its
-// 204-register cap already keeps a level in flight)
-#ifndef EXO_IMPL_BWD_SMEM
-#define EXO_IMPL_BWD_SMEM (!EXO_MIXED)
-#endif
 // 1: the implicit solve keeps (A c)_{i-1} in shared memory instead of registers
 #ifndef EXO_IMPL_AP_SMEM
 #define EXO_IMPL_AP_SMEM 0
@@ -1993,13 +1987,18 @@ __device__ __forceinline__ void implicit_backward_full(IO& io, int is, int ie,
 constexpr int BWD_TL = 4;
 __device__ __forceinline__ void airparcel_round_trip(double* u, double Rd, double gamma);
 // the stepping solve's shared doubles per thread
-constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : (EXO_IMPL_BWD_SMEM ? 71 : 61);
+constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : 61;
 static_assert(32 * IMPL_SM_STRIDE >= 2 * 5 * 32 * (BWD_TL + 1),
               "the tiled back substitution's buffers fit in the warp's slices");
-template <class IO>
+// NB = 5: the full correction (30 factors per level, delta on every
+// variable); NB = 3: the partial one (12 factors per level, delta on rho,
+// m1 and E, the explicit du on m2 and m3, read per lane one level ahead).
+template <int NB, class IO>
 __device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, double* dp,
                                                         double* wtile) {
   static_assert(BWD_TL == 4, "the lane -> (column, level) split below assumes 4 levels");
+  static_assert(NB == 5 || NB == 3, "5x5 or 3x3 blocks");
+  constexpr int NF = NB * NB + NB;  // factors per level: (A c)_i and delta_i
   constexpr int TS = BWD_TL + 1;
   constexpr int TW = 5 * 32 * TS;
   const unsigned live = io.live;
@@ -2045,10 +2044,16 @@ __device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, 
   load(0);
   if (nch > 1) load(1);
   using R = typename IO::Real;
-  R cur_s[30];
+  R cur_s[NF];
   if (ie > is) {
 #pragma unroll
-    for (int e = 0; e < 30; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
+    for (int e = 0; e < NF; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
+  }
+  // the partial correction's explicit du of m2 and m3, one level ahead
+  double cur_du[2] = {0., 0.};
+  if constexpr (NB == 3) {
+    cur_du[0] = *io.duptr(ie, IVY);
+    cur_du[1] = *io.duptr(ie, IVZ);
   }
   for (int c = 0; c < nch; ++c) {
     if (c + 1 < nch) cp_async_wait_one();
@@ -2058,30 +2063,51 @@ __device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, 
     int lo, hi;
     range(c, lo, hi);
     for (int i = hi; i >= lo; --i) {
+      double nxt_du[2] = {0., 0.};
+      if constexpr (NB == 3) {
+        if (i > is) {
+          nxt_du[0] = *io.duptr(i - 1, IVY);
+          nxt_du[1] = *io.duptr(i - 1, IVZ);
+        }
+      }
       if (i < ie) {
-        R nxt_s[30];
+        R nxt_s[NF];
         if (i > is) {
 #pragma unroll
-          for (int e = 0; e < 30; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
+          for (int e = 0; e < NF; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
         }
-        R dl[5];
+        R dl[NB];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) {
-          R ad = cur_s[r * 5] * dp[0];
+        for (int r = 0; r < NB; ++r) {
+          R ad = cur_s[r * NB] * dp[0];
 #pragma unroll
-          for (int k = 1; k < 5; ++k) ad += cur_s[r * 5 + k] * dp[k];
-          dl[r] = cur_s[25 + r] - ad;
+          for (int k = 1; k < NB; ++k) ad += cur_s[r * NB + k] * dp[k];
+          dl[r] = cur_s[NB * NB + r] - ad;
         }
 #pragma unroll
-        for (int r = 0; r < 5; ++r) dp[r] = dl[r];
+        for (int r = 0; r < NB; ++r) dp[r] = dl[r];
         if (i > is) {
 #pragma unroll
-          for (int e = 0; e < 30; ++e) cur_s[e] = nxt_s[e];
+          for (int e = 0; e < NF; ++e) cur_s[e] = nxt_s[e];
         }
+      }
+      // the corrected update of every variable
+      double d[5];
+      if constexpr (NB == 5) {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) d[n] = dp[n];
+      } else {
+        d[IDN] = dp[0];
+        d[IVX] = dp[1];
+        d[IVY] = cur_du[0];
+        d[IVZ] = cur_du[1];
+        d[IEN] = dp[2];
+        cur_du[0] = nxt_du[0];
+        cur_du[1] = nxt_du[1];
       }
       double uu[5];
 #pragma unroll
-      for (int n = 0; n < 5; ++n) uu[n] = t[(n * 32 + lane) * TS + (i - lo)] + 1. * (double)dp[n];
+      for (int n = 0; n < 5; ++n) uu[n] = t[(n * 32 + lane) * TS + (i - lo)] + 1. * d[n];
       if (io.stage == 2) airparcel_round_trip(uu, io.Rd, io.gamma);
 #pragma unroll
       for (int n = 0; n < 5; ++n) t[(n * 32 + lane) * TS + (i - lo)] = uu[n];
@@ -2477,69 +2503,16 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
   // reuses this thread's slots of shared memory
   cp_async_wait_all();
   if constexpr (!kBwd) return;
-#if EXO_IMPL_BWD_SMEM
-  // back substitution: delta_i -= (A c)_i delta_{i+1}.  The factors and the
-  // state of the next two levels are copied asynchronously into this
-  // thread's shared memory (two slots of 35 doubles, free once the forward
-  // sweep is done) while a level is finished.
-  {
-    double u_ie[5];
-    io.uload(ie, u_ie);
-    io.ustore(ie, u_ie, dp);
-  }
-  static_assert(sizeof(R) == 8, "the FP32 solve keeps its back substitution in registers");
-  auto issue = [&](int i, int slot) {
-    double* d = sa + slot * 35;
-#pragma unroll
-    for (int e = 0; e < 30; ++e) cp_async8(d + e, &io.scr(i - is, e));
-    if (IO::kLoadsU) {
-#pragma unroll
-      for (int n = 0; n < 5; ++n) cp_async8(d + 30 + n, io.uptr(i, n));
-    }
-    cp_async_commit();
-  };
-  if (ie - 1 >= is) issue(ie - 1, 0);
-  if (ie - 2 >= is) issue(ie - 2, 1);
-  int slot = 0;
-#pragma unroll 1
-  for (int i = ie - 1; i >= is; --i) {
-    if (i - 1 >= is) cp_async_wait_one();
-    else cp_async_wait_all();
-    const double* d = sa + slot * 35;
-    double cs[30], cu[5];
-#pragma unroll
-    for (int e = 0; e < 30; ++e) cs[e] = d[e];
-    if (IO::kLoadsU) {
-#pragma unroll
-      for (int n = 0; n < 5; ++n) cu[n] = d[30 + n];
-    }
-    double dl[5];
-#pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      double ad = cs[r * 5] * dp[0];
-#pragma unroll
-      for (int k = 1; k < 5; ++k) ad += cs[r * 5 + k] * dp[k];
-      dl[r] = cs[25 + r] - ad;
-    }
-#pragma unroll
-    for (int r = 0; r < 5; ++r) dp[r] = dl[r];
-    io.ustore(i, cu, dp);
-    if (i - 2 >= is) issue(i - 2, slot);
-    slot ^= 1;
-  }
-}
-#else
   if constexpr (IO::kLoadsU && sizeof(R) == 8) {
     if (io.stage >= 0) {
       // the warp's 32 shared slices are free once every lane has finished
       // its forward sweep
-      implicit_backward_tiled(io, is, ie, dp, sa - (threadIdx.x & 31) * IMPL_SM_STRIDE);
+      implicit_backward_tiled<5>(io, is, ie, dp, sa - (threadIdx.x & 31) * IMPL_SM_STRIDE);
       return;
     }
   }
   implicit_backward_full(io, is, ie, dp);
 }
-#endif
 #undef EXO_AP
 
 // ImplicitSolver::PartialCorrection (partial_correction.cpp:26-173) of one
@@ -2806,6 +2779,12 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Rea
   }
   cp_async_wait_all();  // the last level's prefetch (unused) lands before the slice is reused
   if constexpr (!kBwd) return;
+  if constexpr (IO::kLoadsU && sizeof(R) == 8) {
+    if (io.stage >= 0) {
+      implicit_backward_tiled<3>(io, is, ie, dp, sa - (threadIdx.x & 31) * IMPL_SM_STRIDE);
+      return;
+    }
+  }
   implicit_backward_partial(io, is, ie, dp);
 }
 
@@ -2965,7 +2944,6 @@ struct StepColumnIO {
   }
   static constexpr bool kLoadsU = true;
   unsigned live = 0xffffffffu;  // the lanes of the warp with a column
-  __device__ __forceinline__ const double* uptr(int i, int n) const { return uc + n * vs + i; }
   __device__ __forceinline__ void uload(int i, double* u) const {
     if (stage < 0) return;
 #pragma unroll

@@ -39,7 +39,6 @@ struct HookColumnIO {
     return scr0[((size_t)lev * 30 + e) * nslot];
   }
   static constexpr bool kLoadsU = false;
-  __device__ __forceinline__ const double* uptr(int, int) const { return nullptr; }
   __device__ __forceinline__ void uload(int, double*) const {}
   __device__ __forceinline__ void ustore(int i, const double*, const double* dl) const {
 #pragma unroll
