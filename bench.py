@@ -324,10 +324,23 @@ def measure_path(cfg, state, steps, warmup, pg, local, sample_clocks, tune=True)
     g.synchronize()
     prof = g.profile_read()
     g.profile(False)
-    out = {"ms": max_over_ranks(pg, ms), "prof": prof, "launches": launches,
-           "clocks": clk, "invalid": g.invalid(), "tiles": tiles}
+    out = {"ms": max_over_ranks(pg, ms), "prof": prof, "prof_steps": min(steps, 5),
+           "launches": launches, "clocks": clk, "invalid": g.invalid(), "tiles": tiles}
     g.close()
     return out
+
+
+def launch_gaps(meas, steps):
+    """The captured step graph (the timed steps) against the same kernels
+    launched one by one between CUDA events (the profiled steps): the share
+    of the step outside the kernels, i.e. launch gaps a persistent kernel
+    could remove."""
+    graph = meas["ms"] / steps
+    kern = sum(v[1] for v in meas["prof"].values()) / max(meas["prof_steps"], 1)
+    return {"graph_ms_per_step": graph, "kernel_ms_per_step": kern,
+            "gap_frac": 1.0 - kern / graph,
+            "note": "per-kernel CUDA-event times of the same step summed, against the graph "
+                    "replay; a negative value means the events' own overhead exceeds the gaps"}
 
 
 def measure_e2e(cfg, state, steps, pg, tune=True):
@@ -649,6 +662,7 @@ def run_ours(args):
                      "fp64_pipe_frac": (fp64_flops / (avg_ms / 1e3) / alu["fp64_flops_per_s"]
                                         if fp64_flops and alu else None)},
         "kernel_share": shares,
+        "launch_gaps": launch_gaps(main, args.steps),
         "cpu_baseline": extra.get("cpu_baseline"),
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,

@@ -106,3 +106,16 @@ def test_oracle_geometry_is_the_library_geometry(N, native):
     sw = W.shallow_water_config(N=N)
     assert np.array_equal(W.shallow_water_state(sw, 1, geometry=oracle.cell_geometry),
                           W.shallow_water_state(sw, 1))
+
+
+def test_launch_gaps_from_graph_and_kernel_times():
+    """launch_gaps: the per-kernel event times of the profiled steps summed
+    per step, against the timed graph steps."""
+    import bench
+    meas = {"ms": 300.0, "prof_steps": 5,
+            "prof": {"implicit": (15, 60.0), "update": (15, 20.0), "other": (10, 0.5),
+                     "flux_x1": (15, 60.0), "flux_x23": (15, 5.0), "prim_ghost": (15, 2.0)}}
+    g = bench.launch_gaps(meas, 10)
+    assert g["graph_ms_per_step"] == 30.0
+    assert abs(g["kernel_ms_per_step"] - 147.5 / 5) < 1e-12
+    assert abs(g["gap_frac"] - (1 - 29.5 / 30.0)) < 1e-12

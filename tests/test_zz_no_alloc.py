@@ -61,14 +61,18 @@ def _solve(native, torch, arrays, cfg, dt, noalloc):
 
 def test_noalloc_matches_allocating_entry_point_twice(oracle_mod, native):
     torch = pytest.importorskip("torch")
+    # the last case fills the fixed array to its last whole column level:
+    # 4369 columns x 8 levels = NOALLOC_SCRATCH_DOUBLES // 30 column levels
+    assert 4369 * 8 == native.NOALLOC_SCRATCH_DOUBLES // 30
     cases = [(_columns(oracle_mod, 300, 40, seed=21), 900.0),
-             (_columns(oracle_mod, 120, 64, seed=22), 300.0)]
+             (_columns(oracle_mod, 120, 64, seed=22), 300.0),
+             (_columns(oracle_mod, 4369, 8, seed=23), 600.0)]
     for n, ((arrays, cfg), dt) in enumerate(cases):
         want, _ = _solve(native, torch, arrays, cfg, dt, noalloc=False)
         got, freed = _solve(native, torch, arrays, cfg, dt, noalloc=True)
         assert np.isfinite(got).all()
         assert np.array_equal(got, want), np.abs(got - want).max()
-        if n == 1:  # after the first call's one-time set-up: nothing is allocated
+        if n >= 1:  # after the first call's one-time set-up: nothing is allocated
             assert freed == 0
 
 
