@@ -210,9 +210,13 @@ EXO_HD inline bool split_bwd(int precision) { return precision == EXO_PREC_MIXED
 inline int implicit_launches(int implicit_flag, int precision) {
   return ((implicit_flag & 8) && split_bwd(precision)) ? 2 : 1;
 }
+// shared doubles of one x1 column: w [nv][nc1] and psf [nc1+1]; the mixed
+// build adds ln psf and the face densities [2][nc1+1] and the cells' two
+// WENO5 face values [2][nv][L+2] in FP32 (nv (L+2) doubles)
 EXO_HD inline int x1_column_doubles(const DevView& v) {
   int faces = v.nc1 + 1;
-  return v.nv * v.nc1 + (mixed_build(v.precision) ? 3 : 1) * faces;
+  return v.nv * v.nc1 +
+         (mixed_build(v.precision) ? 3 * faces + v.nv * (v.L + 2) : faces);
 }
 inline int x1_cols(const DevView& v) { return v.tiles[BK_X1] > 0 ? v.tiles[BK_X1] : 1; }
 inline size_t x1_smem_bytes(const DevView& v) {

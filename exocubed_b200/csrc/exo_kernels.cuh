@@ -54,6 +54,11 @@
 #ifndef EXO_X23_SHARED_BETA
 #define EXO_X23_SHARED_BETA EXO_MIXED
 #endif
+// 1: the same in the x1 kernel, whose cells' face values go through shared
+// memory (mixed build)
+#ifndef EXO_X1_SHARED_BETA
+#define EXO_X1_SHARED_BETA EXO_MIXED
+#endif
 // 1: the implicit solve keeps (A c)_{i-1} in shared memory instead of registers
 #ifndef EXO_IMPL_AP_SMEM
 #define EXO_IMPL_AP_SMEM 0
@@ -897,6 +902,35 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
   }
   using TF = X1Flux<T>;
   TF* F = flux_array<TF>(v, 0);
+#if EXO_X1_SHARED_BETA
+  // both face values of every cell is-1 .. ie+1, the cell's WENO5
+  // smoothness indicators computed once for the two (as the x2/x3 kernel
+  // does): rec [2][nv][L+2] floats of each column, after its psf arrays
+  const int ncell = L + 2;
+  auto REC = [&](int c) {
+    return reinterpret_cast<T*>(sm + (size_t)c * cstride + nv * nc1 + 3 * (nc1 + 1));
+  };
+  {
+    const float inv_nc = 1.f / (float)ncell;
+    for (int t = threadIdx.x; t < ncb * ncell; t += blockDim.x) {
+      int c, m;
+      divmod_small(t, ncell, inv_nc, c, m);
+      const int cell = v.is - 1 + m;
+      const double* wc = WC(c);
+      T* rec = REC(c);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        if (n >= nv) break;
+        const double* q = wc + n * nc1 + cell;
+        const T q0 = T(q[-2]), q1 = T(q[-1]), q2 = T(q[0]), q3 = T(q[1]), q4 = T(q[2]);
+        const WenoCell<T> wcl = weno_cell<T>(q0, q1, q2, q3, q4);
+        rec[n * ncell + m] = weno_right<T>(wcl, q0, q1, q2, q3, q4);
+        rec[(nv + n) * ncell + m] = weno_left<T>(wcl, q0, q1, q2, q3, q4);
+      }
+    }
+  }
+  __syncthreads();
+#endif
   const float inv_faces = 1.f / (float)(L + 1);
   for (int t = threadIdx.x; t < ncb * (L + 1); t += blockDim.x) {
     int c, f;
@@ -908,6 +942,17 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
     // perturbations are formed in FP64 above; WENO5 runs in T, the restore in
     // FP64 and the Riemann solve in TF
     TF wl[5], wr[5], fx[5] = {TF(0.), TF(0.), TF(0.), TF(0.), TF(0.)};
+#if EXO_X1_SHARED_BETA
+    {
+      const T* rec = REC(c);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        if (n >= nv) break;
+        wl[n] = TF(rec[n * ncell + f]);             // the upper face of cell i-1
+        wr[n] = TF(rec[(nv + n) * ncell + f + 1]);  // the lower face of cell i
+      }
+    }
+#else
     #pragma unroll
     for (int n = 0; n < 5; ++n) {
       if (n >= nv) break;
@@ -915,6 +960,7 @@ __device__ __forceinline__ void flux_x1_block(const DevView& v, unsigned blk) {
       wl[n] = TF(weno_r<T>(q, 1, i - 1));
       wr[n] = TF(weno_l<T>(q, 1, i));
     }
+#endif
     if (decomp) {
       // RestoreFromPerturbation (change_to_perturbation.cpp:159-222), in FP64
       double ps = psf[i];
@@ -2895,7 +2941,8 @@ __device__ __forceinline__ double* impl_radial(double* ism) {
 }
 // the largest dynamic shared memory a launch may ask for
 constexpr int IMPL_SMEM_MAX = 160 * 1024;
-constexpr int X1_SMEM_MAX = 160 * 1024;
+// the mixed x1 kernel's 8 columns of 250 levels take 212 KB
+constexpr int X1_SMEM_MAX = 224 * 1024;
 
 // copies the radial geometry of the member into shared memory (all threads
 // of the block take part; returns the shared copies)
