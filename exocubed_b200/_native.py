@@ -49,6 +49,7 @@ EXPORTED = [
     "exo_synchronize_faces", "exo_conserved_to_primitive", "exo_primitive_to_conserved",
     "exo_sound_speed", "exo_set_primitive_views", "exo_get_primitive_views",
     "exo_get_conserved_views", "exo_solve_implicit_3d_views", "exo_check_bounded_wait",
+    "exo_reciprocal",
 ]
 EXO_DTYPE_F64 = 0
 KERNELS = ["flux_x1", "flux_x23", "update", "implicit", "prim_ghost", "other"]
@@ -163,6 +164,7 @@ def lib():
     L.exo_get_flux.argtypes = [p, i, dp]
     L.exo_riemann.argtypes = [i, i, i, i, d, p, p, p, p, p, p, p, p]
     L.exo_weno5.argtypes = [i, p, p, p, p, p, p, p]
+    L.exo_reciprocal.argtypes = [i, i, p, p, p]
     L.exo_implicit_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
     L.exo_partial_correction_columns.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p, p]
     L.exo_implicit_columns_noalloc.argtypes = [i, i, p, p, p, p, p, p, d, d, d, p]

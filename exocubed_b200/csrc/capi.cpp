@@ -1378,6 +1378,15 @@ int exo_solve_implicit_3d_views(exo_ctx* c, const exo_array_view* du, const exo_
   return rc ? rc : views_scatter(c, hd, du);
 }
 
+int exo_reciprocal(int precision, int n, const double* x, double* out, void* stream) {
+  if (n < 0 || !x || !out) return fail(EXO_ERR_ARG, "bad argument");
+  if (precision < EXO_PREC_FP64 || precision > EXO_PREC_MIXED_F32_SOLVE)
+    return fail(EXO_ERR_ARG, "unknown precision");
+  RK(exo::mixed_build(precision) ? exo::mixed::launch_reciprocal(n, x, out, stream)
+                                 : exo::fp64::launch_reciprocal(n, x, out, stream));
+  return EXO_OK;
+}
+
 int exo_weno5(int n, const double* a, const double* b, const double* c, const double* d,
               const double* e, double* out, void* stream) {
   if (n < 0 || !a || !b || !c || !d || !e || !out) return fail(EXO_ERR_ARG, "bad argument");

@@ -247,7 +247,7 @@ int view_refresh_self(DevView& v, void* stream, std::string* err);
   int launch_p2c_interior(const DevView& v, const double* w_src, void* stream);          \
   int launch_batched_step(const BatchPlan& plan, void* stream);                     \
   int prepare_kernels();                                                            \
-  bool x23_lines();                                                                 \
+  int launch_reciprocal(int n, const double* x, double* out, void* stream);         \
   unsigned x23_blocks(const DevView& v, int tile);
 namespace fp64 { EXO_DECLARE_STEP_LAUNCHERS }
 namespace mixed { EXO_DECLARE_STEP_LAUNCHERS }

@@ -32,8 +32,9 @@
 #include "exo_internal.h"
 #include "exo_mbarrier.cuh"
 
-// x2/x3 fluxes: EXO_X23_TILES 1 = tiles staged through shared memory
-// (flux_x23_tile); otherwise EXO_X23_LINES 1 = one thread per line of faces
+// x2/x3 fluxes: EXO_X23_TILES 1 = a block per line of faces, cells staged
+// through shared memory (flux_x23_pipe); otherwise EXO_X23_LINES 1 = one
+// thread per line of faces
 // (sliding stencil window), 0 = one thread per face
 #ifndef EXO_X23_TILES
 #define EXO_X23_TILES 1
@@ -77,6 +78,30 @@ namespace {
 // 1e-7 of itself.
 __device__ __forceinline__ float abs_r(float x) { return fabsf(x); }
 __device__ __forceinline__ double abs_r(double x) { return fabs(x); }
+// EXO_IMPL_RCP_NR 1: the mixed build's FP64 implicit blocks take 1/x as PTX
+// rcp.approx.ftz.f64 refined by two Newton-Raphson steps, r <- r + r (1 - x r)
+// (Newton's method for 1/x: the relative error squares each step, so a
+// seed good to 2^-14 or better ends within an ulp or two of 1/x), instead of
+// the IEEE division sequence: 3.6 % less implicit time at 6x192^2x96, on
+// the LU pivots and the divisions of |A|.  The mixed build's primitive and
+// update kernels take their reciprocals (density, sin^2, volume, radius)
+// the same way.  The FP64 build divides.
+#ifndef EXO_IMPL_RCP_NR
+#define EXO_IMPL_RCP_NR 1
+#endif
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ float inv_r(float x) { return 1.f / x; }
+__device__ __forceinline__ double inv_r(double x) {
+  if constexpr (EXO_IMPL_RCP_NR && EXO_MIXED) return rcp_nr(x);
+  else return 1. / x;
+}
 __device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
 __device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
@@ -197,7 +222,7 @@ __device__ __forceinline__ void cov_to_contra(double* a, double cth) {
   double v = a[IVY], w = a[IVZ];
   double sth2 = 1. - cth * cth;
 #if EXO_MIXED
-  const double is2 = 1. / sth2;
+  const double is2 = inv_r(sth2);
   a[IVY] = (v - w * cth) * is2;
   a[IVZ] = (w - v * cth) * is2;
 #else
@@ -233,7 +258,7 @@ __device__ __forceinline__ int cons_to_prim(const DevView& v, const double* c, d
     double density = 0.;
     density += c[IDN];
     w[IDN] = density;
-    double di = 1. / density;
+    double di = inv_r(density);
     if ((w[IDN] < 0.) || isnan(w[IDN])) bad = 1;
     double fsig = 1., feps = 1.;
     w[IVX] = c[IVX] * di;
@@ -1204,12 +1229,12 @@ __device__ __forceinline__ void cp_async_wait_one() {
   asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
-// Tiles of faces staged through shared memory: a block of X23_THREADS
-// threads takes 32 consecutive radial indices i (one per lane, so every
-// global access of a warp is a coalesced row) of one line of one panel and
-// direction, and a chunk of x23_chunk<T>() faces along the line.
-//   0. the chunk's cells (with the three-cell halos of its stencils) are
-//      copied into shared memory, each cell once;
+// Faces staged through shared memory: a block of X23_THREADS threads takes
+// 32 consecutive radial indices i (one per lane, so every global access of a
+// warp is a coalesced row) of one line of one panel and direction, and walks
+// the line in chunks of x23_chunk<T>() faces:
+//   0. the chunk's cells (with the three-cell halos of its stencils) are in
+//      shared memory, each cell copied once;
 //   1. one thread per cell computes both face values of the cell's WENO5
 //      reconstruction (the right-face value for the face above it, the
 //      left-face value for the face below; the mixed build shares the
@@ -1226,111 +1251,10 @@ template <class T>
 __host__ __device__ constexpr int x23_chunk() {
   return sizeof(T) == 4 ? 15 : 7;
 }
-// EXO_X23_PIPE 1: a block walks its whole line of faces chunk by chunk,
-// the next chunk's cells copied into a ring of shared memory (cp.async)
-// while the current chunk is reconstructed and solved; the five halo cells
-// two chunks share are copied once.  0: one block per chunk.
-#ifndef EXO_X23_PIPE
-#define EXO_X23_PIPE 1
-#endif
-// blocks of the tiled x2/x3 kernel for one atmosphere
-template <class T>
+// blocks of the tiled x2/x3 kernel for one atmosphere: one per line of 32
+// radial indices of one row of one panel and direction
 __host__ __device__ constexpr unsigned x23_tile_blocks(int N, int L) {
-  return 2u * 6u * (unsigned)N * (unsigned)((L + 31) / 32) *
-         (EXO_X23_PIPE ? 1u : (unsigned)((N + 1 + x23_chunk<T>() - 1) / x23_chunk<T>()));
-}
-
-template <class T>
-__device__ __forceinline__ void flux_x23_tile(const DevView& v, unsigned blk) {
-  constexpr int CF = x23_chunk<T>();   // faces of the chunk
-  constexpr int NC = CF + 1;           // cells reconstructed
-  constexpr int NIN = CF + 5;          // cells staged
-  __shared__ T sin_[5][NIN][32];
-  __shared__ T srec[2][5][NC][32];
-  const int N = v.N, L = v.L, nv = v.nv;
-  const unsigned nch = (unsigned)((N + 1 + CF - 1) / CF), nit = (unsigned)((L + 31) / 32);
-  unsigned r = blk;
-  const int chunk = (int)(r % nch);
-  r /= nch;
-  const int itile = (int)(r % nit);
-  r /= nit;
-  const int a = (int)(r % (unsigned)N);
-  r /= (unsigned)N;
-  const int p = (int)(r % 6u);
-  const int dir = (int)(r / 6u) + 1;
-  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
-  constexpr int NW = X23_THREADS / 32;
-  const int il = itile * 32 + lane;   // radial index within the interior
-  const bool active = il < L;
-  const int i = v.is + il;
-  const size_t vs = v.cells;
-  const long s = dir == 1 ? (long)v.nc1 : (long)v.nc1 * v.nc2;  // stride along the line
-  const size_t base = dir == 1 ? idx(v, p, 0, v.ks + a, 0, i) : idx(v, p, 0, 0, v.js + a, i);
-  const T* __restrict__ W = prim_array<T>(v) + base;
-  const int c0 = dir == 1 ? v.js : v.ks, c1 = dir == 1 ? v.je : v.ke;
-  const int cb = c0 + chunk * CF;     // first face of the chunk
-  // 0. the cells cb-3 .. cb+CF+1 of the 32 lines (rows (variable, cell))
-  for (int row = warp; row < NIN * nv; row += NW) {
-    const int n = row / NIN, m = row % NIN;
-    const int c = cb - 3 + m;
-    T x = T(0);
-    if (active && c <= c1 + 3) x = __ldg(W + n * vs + (long)c * s);
-    sin_[n][m][lane] = x;
-  }
-  __syncthreads();
-  // 1. both face values of the cells cb-1 .. cb+CF-1
-  for (int mc = warp; mc < NC; mc += NW) {
-#pragma unroll
-    for (int n = 0; n < 5; ++n) {
-      if (n >= nv) break;
-      const T q0 = sin_[n][mc][lane], q1 = sin_[n][mc + 1][lane], q2 = sin_[n][mc + 2][lane];
-      const T q3 = sin_[n][mc + 3][lane], q4 = sin_[n][mc + 4][lane];
-#if EXO_X23_SHARED_BETA
-      const WenoCell<T> wc = weno_cell<T>(q0, q1, q2, q3, q4);
-      srec[0][n][mc][lane] = weno_right<T>(wc, q0, q1, q2, q3, q4);
-      srec[1][n][mc][lane] = weno_left<T>(wc, q0, q1, q2, q3, q4);
-#else
-      srec[0][n][mc][lane] = weno5<T>(q4, q3, q2, q1, q0);  // weno_r of the cell
-      srec[1][n][mc][lane] = weno5<T>(q0, q1, q2, q3, q4);  // weno_l of the cell
-#endif
-    }
-  }
-  __syncthreads();
-  if (!active) return;
-  // 2. the faces cb .. cb+CF-1 (up to c1+1)
-  T* F = flux_array<T>(v, dir);
-  for (int mf = warp; mf < CF; mf += NW) {
-    const int c = cb + mf;
-    if (c > c1 + 1) break;
-    T wl[5], wr[5], fx[5] = {T(0.), T(0.), T(0.), T(0.), T(0.)};
-#pragma unroll
-    for (int n = 0; n < 5; ++n) {
-      if (n >= nv) break;
-      wl[n] = srec[0][n][mf][lane];
-      wr[n] = srec[1][n][mf + 1][lane];
-    }
-    const int k = dir == 1 ? v.ks + a : c;
-    const int j = dir == 1 ? c : v.js + a;
-    if (dir == 1) {
-      if (c == c0) edge_outer_state<T>(v, p, UP, a, i, wl);
-      else if (c == c1 + 1) edge_outer_state<T>(v, p, DOWN, a, i, wr);
-      FaceGeo<T> fg{T(geo(v, GCOSF2, p, k, j)), T(geo(v, GSINF2, p, k, j)),
-                    T(geo(v, GCTHP2, p, k, j)), T(geo(v, GCOSC, p, k, j))};
-      riemann<T>(v.rsolver, v.gamma, IVY, fg, wl, wr, fx);
-    } else {
-      if (c == c0) edge_outer_state<T>(v, p, LEFT, a, i, wl);
-      else if (c == c1 + 1) edge_outer_state<T>(v, p, RIGHT, a, i, wr);
-      FaceGeo<T> fg{T(geo(v, GCOSF3, p, k, j)), T(geo(v, GSINF3, p, k, j)),
-                    T(geo(v, GCTHP3, p, k, j)), T(geo(v, GCOSC, p, k, j))};
-      riemann<T>(v.rsolver, v.gamma, IVZ, fg, wl, wr, fx);
-    }
-    const size_t f0 = idx(v, p, 0, k, j, i);
-#pragma unroll
-    for (int n = 0; n < 5; ++n) {
-      if (n >= nv) break;
-      F[f0 + n * vs] = fx[n];
-    }
-  }
+  return 2u * 6u * (unsigned)N * (unsigned)((L + 31) / 32);
 }
 
 // cp.async of 4 or 8 bytes, zero-filled when src_bytes is 0
@@ -1344,7 +1268,7 @@ __device__ __forceinline__ void cp_async_zfill(void* smem_dst, const void* gsrc,
 
 // The x2/x3 faces of one line (32 radial indices of one row of one panel
 // and direction) chunk by chunk, with the same phases, values and
-// operations per face as flux_x23_tile.  Cell c of the line sits in ring
+// operations per face as the per-face form.  Cell c of the line sits in ring
 // slot (c - c0 + 3) mod XR; the copies of chunk q + 1's new cells are in
 // flight while chunk q is finished.  Slots written for chunk q + 1 held
 // cells at least XR = 2 CF + 5 below them, which chunk q no longer reads;
@@ -1464,8 +1388,7 @@ __device__ __forceinline__ void flux_x23_pipe(const DevView& v, unsigned blk) {
 
 template <class T>
 __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
-  if constexpr (EXO_X23_TILES && EXO_X23_PIPE) flux_x23_pipe<T>(v, blk);
-  else if constexpr (EXO_X23_TILES) flux_x23_tile<T>(v, blk);
+  if constexpr (EXO_X23_TILES) flux_x23_pipe<T>(v, blk);
   else if constexpr (EXO_X23_LINES) flux_x23_lines<T>(v, blk);
   else flux_x23_faces<T>(v, blk);
 }
@@ -1544,7 +1467,7 @@ __device__ __forceinline__ void update_block(const DevView& v, unsigned blk, int
   // the mixed build multiplies by reciprocals of the volume and the radius
   // (one division each instead of eight; the FP64 build divides as the
   // reference does)
-  [[maybe_unused]] const double ivol = 1. / vol, irad = 1. / x1vi;
+  [[maybe_unused]] const double ivol = inv_r(vol), irad = inv_r(x1vi);
   double du[5];
   // flux divergence in T (the x1 part in FP64 where its fluxes are); the
   // conserved state accumulates in FP64
@@ -1819,9 +1742,14 @@ __device__ __forceinline__ void abs_jacobian(const ColCell<R>& L, const ColCell<
   } else {
     sqrtdl = sqrt_r(wl[IDN]);
     sqrtdr = sqrt_r(wr[IDN]);
-    isdlpdr = one / (sqrtdl + sqrtdr);
-    isl = isdlpdr / sqrtdl;
-    isr = isdlpdr / sqrtdr;
+    isdlpdr = inv_r(sqrtdl + sqrtdr);
+    if constexpr (EXO_IMPL_RCP_NR) {
+      isl = isdlpdr * inv_r(sqrtdl);
+      isr = isdlpdr * inv_r(sqrtdr);
+    } else {
+      isl = isdlpdr / sqrtdl;
+      isr = isdlpdr / sqrtdr;
+    }
   }
   R rr = sqrtdl * sqrtdr;
   R u = (sqrtdl * wl[IVX] + sqrtdr * wr[IVX]) * isdlpdr;
@@ -1841,14 +1769,16 @@ __device__ __forceinline__ void abs_jacobian(const ColCell<R>& L, const ColCell<
     cs = cs2 * ics;
     i2cshp = ics;  // times 1/(2 hp) below
   } else {
-    irr = one / rr;
+    irr = inv_r(rr);
     cs = sqrt_r(gamma * p * irr);
   }
   R hp = (gm1 + one) * inv_gm1 * p * irr;
   R h = hp + ke;
-  R ihp = one / hp, i2hp = half * ihp;
+  R ihp = inv_r(hp), i2hp = half * ihp;
   if constexpr (f32)
     i2cshp *= i2hp;
+  else if constexpr (EXO_IMPL_RCP_NR)
+    i2cshp = i2hp * inv_r(cs);
   else
     i2cshp = i2hp / cs;
   R au = abs_r(u), al = abs_r(u - cs) - au, ar = abs_r(u + cs) - au;
@@ -2437,7 +2367,7 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
           perm |= (unsigned)k << (3 * k);
         }
       }
-      idg[k] = R(1) / t[O[k]][k];
+      idg[k] = inv_r(t[O[k]][k]);
 #pragma unroll
       for (int r = k + 1; r < 5; ++r) {
         const R l = t[O[r]][k] * idg[k];
@@ -3376,7 +3306,7 @@ __global__ void EXO_X1_BOUNDS kb_flux_x1(Batch bt) {
 // the pipelined line kernel of the mixed build at 128 registers (4 blocks of
 // 128 threads per SM): 1.64 ms per launch at 6x192^2x96 against 1.75 at its
 // natural 148 and 1.91 for one block per chunk
-#if EXO_X23_TILES && EXO_X23_PIPE && EXO_MIXED && !defined(EXO_X23_MINB)
+#if EXO_X23_TILES && EXO_MIXED && !defined(EXO_X23_MINB)
 #define EXO_X23_MINB 4
 #endif
 #if EXO_X23_TILES && defined(EXO_X23_MINB)
@@ -3518,10 +3448,19 @@ inline unsigned member_block_count(const DevView& v, int kind) {
   return b[kind];
 }
 
-bool x23_lines() { return EXO_X23_LINES != 0; }
+// 1/x as this build's FP64 implicit blocks take it (inv_r), element-wise
+__global__ void k_reciprocal(int n, const double* x, double* out) {
+  const int m = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (m < n) out[m] = inv_r(x[m]);
+}
+int launch_reciprocal(int n, const double* x, double* out, void* stream) {
+  if (n <= 0) return 0;
+  k_reciprocal<<<nblk((size_t)n, 128), 128, 0, (cudaStream_t)stream>>>(n, x, out);
+  return check_launch();
+}
 
 unsigned x23_blocks(const DevView& v, int tile) {
-  if (EXO_X23_TILES) return x23_tile_blocks<EXO_FLUX_T>(v.N, v.L);
+  if (EXO_X23_TILES) return x23_tile_blocks(v.N, v.L);
   const size_t n = EXO_X23_LINES ? (size_t)2 * 6 * v.N * v.L
                                  : (size_t)2 * 6 * v.N * (v.N + 1) * v.L;
   return (unsigned)((n + tile - 1) / tile);

@@ -337,6 +337,12 @@ int exo_implicit_columns_noalloc(int ncol, int L, const double* w, double* du,
 int exo_weno5(int n, const double* a, const double* b, const double* c,
               const double* d, const double* e, double* out, void* stream);
 
+/* out[m] = 1/x[m] on device as the implicit solve's FP64 blocks of the given
+   precision compute it: an IEEE division in the FP64 build, a reciprocal
+   refined by Newton's method in the mixed build (within an ulp or two).  A
+   self-test of that arithmetic; x and out are device arrays of n doubles. */
+int exo_reciprocal(int precision, int n, const double* x, double* out, void* stream);
+
 /* ------------------------------------------------- panel-exchange hooks */
 
 /* CubedSphereUtility::PackData (src/exo3/cubed_sphere_utility.hpp:10-12,

@@ -41,3 +41,31 @@ def test_bounded_wait_gives_up_and_the_device_stays_usable():
         a.set_primitive(W.dry_atmosphere_state(cfg, seed=1))
         a.step(2)
         assert a.invalid() == 0
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_reciprocal_of_the_implicit_blocks(precision):
+    """1/x as the implicit solve's FP64 blocks take it: the FP64 build's IEEE
+    division equals numpy's bit for bit; the mixed build's reciprocal refined
+    by Newton's method stays within two ulps of it, for finite x of either
+    sign whose reciprocal is a normal number."""
+    import numpy as np
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(7)
+    x = np.concatenate([np.sign(rng.uniform(-1, 1, 20000)) * 10.0 ** rng.uniform(-300, 300, 20000),
+                        rng.uniform(0.5, 2.0, 20000), np.array([1.0, -1.0, 3.0, 0.1, 7e-301])])
+    xd = torch.from_numpy(x).cuda()
+    out = torch.empty_like(xd)
+    nat.check(nat.lib().exo_reciprocal(precision, x.size, xd.data_ptr(), out.data_ptr(), None))
+    torch.cuda.synchronize()
+    got, want = out.cpu().numpy(), 1.0 / x
+    if precision == nat.EXO_PREC_FP64:
+        assert np.array_equal(got, want)
+    else:
+        ulps = np.abs(got - want) / np.spacing(np.abs(want))
+        assert ulps.max() <= 2.0, ulps.max()
+
+
+def test_reciprocal_rejects_bad_arguments():
+    assert nat.lib().exo_reciprocal(1, -1, None, None, None) == nat.EXO_ERR_ARG
+    assert nat.lib().exo_reciprocal(7, 0, 1, 1, None) == nat.EXO_ERR_ARG
