@@ -1730,13 +1730,15 @@ __device__ __forceinline__ void abs_jacobian(const ColCell<R>& L, const ColCell<
   R wl[5] = {L.rho, L.v1, L.v2, L.v3, L.p};
   R wr[5] = {R_.rho, R_.v1, R_.v2, R_.v3, R_.p};
 #if EXO_MIXED
+  // FP32 blocks take the cells' sqrt(rho) and 1/sqrt(rho); the same scheme
+  // in FP64 (with a Newton-refined rsqrt) measured 0.5 % slower
   constexpr bool f32 = sizeof(R) == 4;
   const R one = R(1), half = R(0.5);
   R sqrtdl, sqrtdr, isl, isr, isdlpdr;
   if constexpr (f32) {
     sqrtdl = L.sq;
     sqrtdr = R_.sq;
-    isdlpdr = one / (sqrtdl + sqrtdr);
+    isdlpdr = inv_r(sqrtdl + sqrtdr);
     isl = isdlpdr * L.isq;
     isr = isdlpdr * R_.isq;
   } else {
@@ -2170,7 +2172,7 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
       c.sq = c.rho * c.isq;
       c.hr = gp * c.p * (c.isq * c.isq);
     } else {
-      c.hr = gp * c.p * (R(1) / c.rho);
+      c.hr = gp * c.p * inv_r(c.rho);
     }
 #else
     c.hr = gp * c.p / c.rho;
@@ -2580,7 +2582,7 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Rea
       c.sq = c.rho * c.isq;
       c.hr = gp * c.p * (c.isq * c.isq);
     } else {
-      c.hr = gp * c.p * (R(1) / c.rho);
+      c.hr = gp * c.p * inv_r(c.rho);
     }
 #else
     c.hr = gp * c.p / c.rho;
