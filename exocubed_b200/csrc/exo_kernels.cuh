@@ -1963,6 +1963,12 @@ __device__ __forceinline__ void implicit_backward_full(IO& io, int is, int ie,
 // warp).  io.live: the lanes of the warp with a column.  wtile: 2 x 5 x 32 x
 // (BWD_TL + 1) doubles of shared memory for the warp alone.
 constexpr int BWD_TL = 4;
+// levels of look-ahead of the factor loads (1 or 2): two in the FP64 build
+// (implicit 8.63 -> 8.39 ms per 6x192^2x96 launch), one in the mixed build,
+// where two measured 2.6 % slower
+#ifndef EXO_BWD_AHEAD
+#define EXO_BWD_AHEAD (EXO_MIXED ? 1 : 2)
+#endif
 __device__ __forceinline__ void airparcel_round_trip(double* u, double Rd, double gamma);
 // the stepping solve's shared doubles per thread
 constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : 61;
@@ -2022,10 +2028,19 @@ __device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, 
   load(0);
   if (nch > 1) load(1);
   using R = typename IO::Real;
-  R cur_s[NF];
+  // the factors of the next level (cur_s) and, with EXO_BWD_AHEAD 2, of the
+  // one after (ahd_s): their loads are in flight for two levels (the
+  // registers of the finished forward sweep are free)
+  R cur_s[NF], ahd_s[NF];
   if (ie > is) {
 #pragma unroll
     for (int e = 0; e < NF; ++e) cur_s[e] = io.scr(ie - 1 - is, e);
+  }
+  if constexpr (EXO_BWD_AHEAD == 2) {
+    if (ie - 1 > is) {
+#pragma unroll
+      for (int e = 0; e < NF; ++e) ahd_s[e] = io.scr(ie - 2 - is, e);
+    }
   }
   // the partial correction's explicit du of m2 and m3, one level ahead
   double cur_du[2] = {0., 0.};
@@ -2050,9 +2065,10 @@ __device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, 
       }
       if (i < ie) {
         R nxt_s[NF];
-        if (i > is) {
+        const int ahead = i - EXO_BWD_AHEAD;  // the level whose factors load now
+        if (ahead >= is) {
 #pragma unroll
-          for (int e = 0; e < NF; ++e) nxt_s[e] = io.scr(i - 1 - is, e);
+          for (int e = 0; e < NF; ++e) nxt_s[e] = io.scr(ahead - is, e);
         }
         R dl[NB];
 #pragma unroll
@@ -2064,7 +2080,13 @@ __device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, 
         }
 #pragma unroll
         for (int r = 0; r < NB; ++r) dp[r] = dl[r];
-        if (i > is) {
+        if constexpr (EXO_BWD_AHEAD == 2) {
+#pragma unroll
+          for (int e = 0; e < NF; ++e) {
+            cur_s[e] = ahd_s[e];
+            ahd_s[e] = nxt_s[e];
+          }
+        } else {
 #pragma unroll
           for (int e = 0; e < NF; ++e) cur_s[e] = nxt_s[e];
         }
