@@ -51,3 +51,27 @@ def test_chain_does_not_depend_on_batching():
         assert np.array_equal(a.par[t], b.par[t])
         assert np.array_equal(a.lnp[t], b.lnp[t])
     assert a.accept == b.accept
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_forward_model_against_the_oracle(oracle_mod, precision):
+    """A walker's forward model (the profile problem: build the atmosphere
+    from the parameters, step it, observe the level-mean temperatures) on the
+    GPU against the same model run by the oracle: FP64 to 1e-11 relative,
+    mixed to 1e-6."""
+    build, observe, nvalue = profile_problem(N=8, L=12, steps=3)
+    theta = np.array([[290., 210.], [260., 240.]])
+    fb = EnsembleForward(build, observe, nvalue, 3, precision=precision, capacity=2)
+    try:
+        got = fb(theta)
+    finally:
+        fb.close()
+    for n, p in enumerate(theta):
+        cfg, w = build(p)
+        o = oracle_mod.Oracle(dict(cfg, precision=0))
+        o.set_primitive(w)
+        o.step(3)
+        assert o.invalid() == 0
+        want = observe(cfg, o.primitive())
+        rel = np.abs(got[n] - want).max() / np.abs(want).max()
+        assert rel < (1e-11 if precision == nat.EXO_PREC_FP64 else 1e-6), (n, rel)

@@ -77,3 +77,27 @@ def test_wall_clock_serving_reports_latency():
     assert s["requests"] == len(reqs)
     assert 0 < s["p50_s"] <= s["p99_s"] <= s["max_s"]
     assert all(rec.admitted >= rec.arrival for rec in recs)
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_served_results_against_the_oracle(oracle_mod, precision):
+    """Every served request's conserved state after its steps against the
+    oracle's run of the same member: the FP64 path to 1e-9 relative L2 per
+    variable (only the last bits of log/exp/pow differ), the mixed path to
+    1e-5 in density and energy."""
+    reqs = _requests(precision, steps=3)[:4]
+    srv = Server(precision=precision, capacity=3, max_chunk=2, keep_results=True)
+    recs = srv.run(reqs, clock="steps")
+    srv.close()
+    for r, rec in zip(reqs, recs):
+        o = oracle_mod.Oracle(dict(r.cfg, precision=0))
+        o.set_primitive(r.w)
+        o.step(r.steps)
+        assert o.invalid() == 0 and rec.valid
+        got, want = W.interior(rec.result), W.interior(o.conserved())
+        for n in range(5):
+            rel = np.linalg.norm(got[:, n] - want[:, n]) / np.linalg.norm(want[:, n])
+            if precision == nat.EXO_PREC_FP64:
+                assert rel < 1e-9, (r.rid, n, rel)
+            elif n in (0, 4):
+                assert rel < 1e-5, (r.rid, n, rel)
