@@ -1963,6 +1963,9 @@ __device__ __forceinline__ void implicit_backward_full(IO& io, int is, int ie,
 // warp).  io.live: the lanes of the warp with a column.  wtile: 2 x 5 x 32 x
 // (BWD_TL + 1) doubles of shared memory for the warp alone.
 constexpr int BWD_TL = 4;
+// the two u tiles of a warp's back substitution (5 variables x 32 columns x
+// BWD_TL levels, padded)
+constexpr int WARP_TILE_DOUBLES = 2 * 5 * 32 * (BWD_TL + 1);
 // levels of look-ahead of the factor loads (1 or 2): two in the FP64 build
 // (implicit 8.63 -> 8.39 ms per 6x192^2x96 launch), one in the mixed build,
 // where two measured 2.6 % slower
@@ -1972,14 +1975,14 @@ constexpr int BWD_TL = 4;
 __device__ __forceinline__ void airparcel_round_trip(double* u, double Rd, double gamma);
 // the stepping solve's shared doubles per thread
 constexpr int IMPL_SM_STRIDE = EXO_IMPL_AP_SMEM ? 87 : 61;
-static_assert(32 * IMPL_SM_STRIDE >= 2 * 5 * 32 * (BWD_TL + 1),
+static_assert(32 * IMPL_SM_STRIDE >= WARP_TILE_DOUBLES,
               "the tiled back substitution's buffers fit in the warp's slices");
 // NB = 5: the full correction (30 factors per level, delta on every
 // variable); NB = 3: the partial one (12 factors per level, delta on rho,
 // m1 and E, the explicit du on m2 and m3, read per lane one level ahead).
 template <int NB, class IO>
-__device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie, double* dp,
-                                                        double* wtile) {
+__device__ __forceinline__ void implicit_backward_tiled(IO& io, int is, int ie,
+                                                        typename IO::Real* dp, double* wtile) {
   static_assert(BWD_TL == 4, "the lane -> (column, level) split below assumes 4 levels");
   static_assert(NB == 5 || NB == 3, "5x5 or 3x3 blocks");
   constexpr int NF = NB * NB + NB;  // factors per level: (A c)_i and delta_i
@@ -2167,7 +2170,8 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
                                                 double cos_theta, double sin_theta, double d2,
                                                 double d3, const double* x1f, const double* x1v,
                                                 const double* dx1f, int is, int ie, double dt,
-                                                double gamma, double grav) {
+                                                double gamma, double grav,
+                                                double* wt = nullptr) {
   using R = typename IO::Real;
   using ColCell = exo::EXO_KNS::ColCell<R>;
   const double s = sin_theta;
@@ -2505,9 +2509,9 @@ __device__ __forceinline__ void implicit_column(IO& io, typename IO::Real* sa, d
   if constexpr (!kBwd) return;
   if constexpr (IO::kLoadsU && sizeof(R) == 8) {
     if (io.stage >= 0) {
-      // the warp's 32 shared slices are free once every lane has finished
-      // its forward sweep
-      implicit_backward_tiled<5>(io, is, ie, dp, sa - (threadIdx.x & 31) * IMPL_SM_STRIDE);
+      // the warp's tiles (FP64 blocks: its 32 shared slices, free once every
+      // lane has finished its forward sweep)
+      implicit_backward_tiled<5>(io, is, ie, dp, wt);
       return;
     }
   }
@@ -2578,7 +2582,7 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Rea
                                                         double d2, double d3, const double* x1f,
                                                         const double* x1v, const double* dx1f,
                                                         int is, int ie, double dt, double gamma,
-                                                        double grav) {
+                                                        double grav, double* wt = nullptr) {
   using R = typename IO::Real;
   using ColCell = exo::EXO_KNS::ColCell<R>;
   constexpr int P[3] = {IDN, IVX, IEN};
@@ -2781,7 +2785,7 @@ __device__ __forceinline__ void implicit_column_partial(IO& io, typename IO::Rea
   if constexpr (!kBwd) return;
   if constexpr (IO::kLoadsU && sizeof(R) == 8) {
     if (io.stage >= 0) {
-      implicit_backward_tiled<3>(io, is, ie, dp, sa - (threadIdx.x & 31) * IMPL_SM_STRIDE);
+      implicit_backward_tiled<3>(io, is, ie, dp, wt);
       return;
     }
   }
@@ -2877,15 +2881,16 @@ struct ImplSlices {
   R* sa;
   double* sp;
   int ss;
+  double* wt;  // FP64 blocks: the warp's back-substitution tiles (WARP_TILE_DOUBLES)
 };
 template <class R>
 __device__ __forceinline__ ImplSlices<R> impl_slices(double* ism, bool full) {
   if constexpr (sizeof(R) == 4) {
     const int nt = (int)blockDim.x, t = (int)threadIdx.x;
-    return {reinterpret_cast<R*>(ism + 10 * nt) + t, ism + t, nt};
+    return {reinterpret_cast<R*>(ism + 10 * nt) + t, ism + t, nt, nullptr};
   } else {
     double* sm = ism + threadIdx.x * IMPL_SM_STRIDE;
-    return {sm, sm + (full ? 50 : 18), 1};
+    return {sm, sm + (full ? 50 : 18), 1, ism + (threadIdx.x & ~31u) * IMPL_SM_STRIDE};
   }
 }
 // where the block's copy of the radial geometry starts
@@ -3006,12 +3011,13 @@ __device__ __forceinline__ void implicit_block(const DevView& v, unsigned blk, i
     implicit_column<IO, kBwd>(io, sl.sa, sl.sp, sl.ss, geo(v, GCOSC, p, k, j),
                                          geo(v, GSINC, p, k, j), geo(v, GDX2A, p, k, j),
                                          geo(v, GDX3A, p, k, j), x1f, x1v, dx1f, v.is, v.ie,
-                                         dt, v.gamma, v.grav);
+                                         dt, v.gamma, v.grav, sl.wt);
   else
     implicit_column_partial<IO, true>(io, sl.sa, sl.sp, sl.ss,
                                                  geo(v, GCOSC, p, k, j), geo(v, GSINC, p, k, j),
                                                  geo(v, GDX2A, p, k, j), geo(v, GDX3A, p, k, j),
-                                                 x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav);
+                                                 x1f, x1v, dx1f, v.is, v.ie, dt, v.gamma, v.grav,
+                                                 sl.wt);
 }
 
 // ---------------------------------------------------- kb_implicit_bwd ---
