@@ -277,3 +277,74 @@ def test_decomposition_bitwise(ref, rsolver, seed):
                 assert np.array_equal(rrow[:, G:G + L + 1], wr_ora[p, :, k, j, G:G + L + 1])
         assert np.array_equal(wp[inner], w_back[p][inner]), p
         pan.close()
+
+
+def _unpack(buf, order, nv, K, J, I):
+    """The inverse of PackDataR0..R3 (oracle pack_order): the (n, k, j, i)
+    array a packed buffer was traversed from."""
+    if order in (0, 2):
+        a = buf.reshape(nv, K, J, I)
+        return a if order == 0 else a[:, ::-1, ::-1, :]
+    b = buf.reshape(nv, J, K, I).transpose(0, 2, 1, 3)
+    return b[:, :, ::-1, :] if order == 1 else b[:, ::-1, :, :]
+
+
+def _pack(a, order):
+    if order == 0:
+        return a.ravel()
+    if order == 2:
+        return a[:, ::-1, ::-1, :].ravel()
+    if order == 1:
+        return a[:, :, ::-1, :].transpose(0, 2, 1, 3).ravel()
+    return a[:, ::-1, :, :].transpose(0, 2, 1, 3).ravel()
+
+
+@pytest.mark.parametrize("N,nb", [(16, 2), (32, 4)])
+def test_multiblock_pack_data_equals_one_block_per_panel(ref, N, nb):
+    """Multi-block panels: with nb x nb blocks per panel, the
+    reference's own PackData (cubed_sphere_utility.cpp:92-369: N_blk the whole
+    panel edge, n_start the block's offset along it) sends, from every block
+    on a panel edge, exactly the slice of what one block per panel sends,
+    bit for bit, once the block's ghost cells along the edge hold the
+    neighbouring blocks' current values (the reference's second ghost pass).
+    So a run with blocks per panel gives the one-block-per-panel result, and
+    the one-block layout stands in for it.  Blocks are 8 cells wide here: the
+    reference tells a block's low-side band from its high-side band by
+    comparing the band's start with the other direction's end less NGHOST
+    (`sk < ej - NGHOST` in InteprolateX2), which for blocks of G + 1 = 4
+    cells or fewer treats a low-side band as a high-side one and reverses
+    its rows (a block-size limit of the reference, not of this layout)."""
+    L = 4
+    n = N // nb
+    level = 2 + int(np.log2(nb))
+    cfg = W.dry_atmosphere_config(N=N, L=L)
+    o = oracle.Oracle(cfg)
+    rng = np.random.default_rng(17 + nb)
+    o.set_conserved(_random_conserved(o, rng))
+    u = o.conserved()
+    nv, nc1 = u.shape[1], u.shape[4]
+    pack = oracle.panel_tables()[4]
+    for p in range(6):
+        for s in range(4):
+            ox2, ox3 = SIDE_OX[s]
+            order = int(pack[p][s])
+            K1, J1 = (N, G) if ox2 else (G, N)
+            whole = _unpack(o.pack_face(p, s), order, nv, K1, J1, L)
+            for b in range(nb):
+                bx = (0 if ox2 < 0 else nb - 1) if ox2 else b
+                by = (0 if ox3 < 0 else nb - 1) if ox3 else b
+                blk = np.ascontiguousarray(u[p][:, by * n:by * n + n + 2 * G,
+                                                 bx * n:bx * n + n + 2 * G, :])
+                sj = G + n - G if ox2 > 0 else G
+                ej = G + G - 1 if ox2 < 0 else G + n - 1
+                sk = G + n - G if ox3 > 0 else G
+                ek = G + G - 1 if ox3 < 0 else G + n - 1
+                buf = np.zeros(blk.size)
+                cnt = ref.ref_pack_data(reference.ptr(blk), nv, n + 2 * G, n + 2 * G, nc1, 0,
+                                        nv - 1, G, G + L - 1, sj, ej, sk, ek, 0, ox2, ox3,
+                                        (p % 2) * nb + bx, (p // 2) * nb + by, level,
+                                        reference.ptr(buf))
+                part = whole[:, b * n:(b + 1) * n] if ox2 else whole[:, :, b * n:(b + 1) * n]
+                want = _pack(np.ascontiguousarray(part), order)
+                assert cnt == want.size, (p, s, b, cnt, want.size)
+                assert np.array_equal(buf[:cnt], want), (p, s, b, np.abs(buf[:cnt] - want).max())
