@@ -625,6 +625,35 @@ __device__ __forceinline__ void block_min_atomic(unsigned long long* target, uns
   }
 }
 
+// Hydro::NewBlockTimeStep with patches/21.new_blockdt.patch:23-35 at an
+// interior cell with primitives w: the candidate as the bits of a
+// non-negative double, or ~0 when there is none
+__device__ __forceinline__ unsigned long long cfl_candidate(const DevView& v, const double* w,
+                                                            int p, int k, int j, int i) {
+  const bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
+  double cs;
+  if (shallow) cs = sqrt(w[IDN]);
+  else {
+    double fsig = 1., feps = 1.;
+    cs = sqrt((1. + (v.gamma - 1) * feps / fsig) * w[IPR] / w[IDN]);
+  }
+  double dt1 = v.dx1f[i], dt2 = v.x1v[i] * geo(v, GDX2A, p, k, j);
+  double dt3 = v.x1v[i] * geo(v, GDX3A, p, k, j);
+  double speed1 = fmax(0., (fabs(w[IVX]) + cs));
+  double speed2 = fmax(0., (fabs(w[IVY]) + cs));
+  double speed3 = fmax(0., (fabs(w[IVZ]) + cs));
+  if ((v.implicit_flag & 1) && (v.N > 1)) dt1 /= v.cfl * fabs(w[IVX]);
+  else dt1 /= speed1;
+  if (v.implicit_flag & 2) dt2 /= v.cfl * fabs(w[IVY]);
+  else dt2 /= speed2;
+  if (v.implicit_flag & 4) dt3 /= v.cfl * fabs(w[IVZ]);
+  else dt3 /= speed3;
+  double m = fmin(dt2, dt3);
+  if (!shallow) m = fmin(dt1, m);
+  if (m >= 0.) return (unsigned long long)__double_as_longlong(m);
+  return ~0ull;
+}
+
 __device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, unsigned tid,
                                                               int compute_dt) {
   const unsigned long long none = ~0ull;
@@ -662,32 +691,10 @@ __device__ __forceinline__ unsigned long long prim_ghost_cell(const DevView& v, 
 #endif
   if (!(kin && jin) || mirror) return none;
   if (bad) atomicOr(&v.sc->invalid, 1);
-  if (compute_dt) {
-    // Hydro::NewBlockTimeStep with patches/21.new_blockdt.patch:23-35
-    bool shallow = (v.eqn == EXO_EQN_SHALLOW_YZ);
-    double cs;
-    if (shallow) cs = sqrt(w[IDN]);
-    else {
-      double fsig = 1., feps = 1.;
-      cs = sqrt((1. + (v.gamma - 1) * feps / fsig) * w[IPR] / w[IDN]);
-    }
-    double dt1 = v.dx1f[i], dt2 = v.x1v[i] * geo(v, GDX2A, p, k, j);
-    double dt3 = v.x1v[i] * geo(v, GDX3A, p, k, j);
-    double speed1 = fmax(0., (fabs(w[IVX]) + cs));
-    double speed2 = fmax(0., (fabs(w[IVY]) + cs));
-    double speed3 = fmax(0., (fabs(w[IVZ]) + cs));
-    if ((v.implicit_flag & 1) && (v.N > 1)) dt1 /= v.cfl * fabs(w[IVX]);
-    else dt1 /= speed1;
-    if (v.implicit_flag & 2) dt2 /= v.cfl * fabs(w[IVY]);
-    else dt2 /= speed2;
-    if (v.implicit_flag & 4) dt3 /= v.cfl * fabs(w[IVZ]);
-    else dt3 /= speed3;
-    double m = fmin(dt2, dt3);
-    if (!shallow) m = fmin(dt1, m);
-    if (m >= 0.) return (unsigned long long)__double_as_longlong(m);
-  }
+  if (compute_dt) return cfl_candidate(v, w, p, k, j, (int)i);
   return none;
 }
+
 
 __device__ __forceinline__ void prim_ghost_block(const DevView& v, unsigned blk, int compute_dt) {
   unsigned tid = blk * blockDim.x + threadIdx.x;
