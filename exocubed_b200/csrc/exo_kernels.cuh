@@ -3485,7 +3485,8 @@ inline unsigned member_block_count(const DevView& v, int kind) {
   return b[kind];
 }
 
-// 1/x as this build's FP64 implicit blocks take it (inv_r), element-wise
+// 1/x as the FP64 implicit blocks of this compilation take it (inv_r),
+// element-wise
 __global__ void k_reciprocal(int n, const double* x, double* out) {
   const int m = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (m < n) out[m] = inv_r(x[m]);

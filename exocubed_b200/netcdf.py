@@ -12,7 +12,7 @@ vel3 [m/s].  Here a meshblock is a panel (gid = panel, at (lx2, lx3) =
 (panel % 2, panel // 2) of the 2 x 3 panel layout).
 
 The reference calls libnetcdf with NC_NETCDF4 (HDF5 storage); that library
-is not part of this build, so the files are written in the NetCDF classic
+is not linked here, so the files are written in the NetCDF classic
 format (the published CDF-1 layout: big-endian header of dimension,
 attribute and variable lists, then the fixed-size variables, then the
 records), which every NetCDF reader opens with the same dimensions,

@@ -1,8 +1,8 @@
 """Members and serving requests spread over ranks (exocubed_b200/multigpu.py)
 without a GPU: placement by footprint, and two gloo ranks on 127.0.0.1 that
 each advance their share with a stand-in ensemble and server, gathered on
-rank 0 in input order.  Unmeasured on more than one GPU (every GPU call of
-this build has one device); the placement and gather logic is what runs on
+rank 0 in input order.  Unmeasured on more than one GPU (the GPU machines
+at hand give one device); the placement and gather logic is what runs on
 the host here."""
 import os
 import socket

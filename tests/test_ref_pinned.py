@@ -301,7 +301,7 @@ def _pack(a, order):
 
 @pytest.mark.parametrize("N,nb", [(16, 2), (32, 4)])
 def test_multiblock_pack_data_equals_one_block_per_panel(ref, N, nb):
-    """Multi-block panels (SURVEY 8(f)1): with nb x nb blocks per panel, the
+    """Multi-block panels: with nb x nb blocks per panel, the
     reference's own PackData (cubed_sphere_utility.cpp:92-369: N_blk the whole
     panel edge, n_start the block's offset along it) sends, from every block
     on a panel edge, exactly the slice of what one block per panel sends,
