@@ -245,8 +245,8 @@ def run_cpu(workload, steps, warmup):
 def alg_bytes_per_cell(kernel, precision, implicit_flag=9):
     mixed = precision in (1, 2)
     t = 4 if mixed else 8
-    # mixed flux_x23: one thread per line of faces reads every cell once per direction
-    x23 = 10 * t + 10 * t if mixed else 5 * t + 10 * t
+    # flux_x23: a block per line of faces reads every cell once per direction
+    x23 = 10 * t + 10 * t
     factors = (30 if implicit_flag & 8 else 12) * (4 if precision == 2 else 8) * 2
     # the x1 fluxes are FP64 in both builds (5 values of 8 bytes per cell)
     return {"flux_x1": 40 + 40, "flux_x23": x23, "update": 120 + 40 + 10 * t + 80,
@@ -574,8 +574,10 @@ def run_ours(args):
     prof = main["prof"]
     dom = max((k for k in prof if k != "other"), key=lambda k: prof[k][1])
     n_l, t_l = prof[dom]
-    avg_ms = t_l / max(n_l, 1)
     iflag = cfg.get("implicit_flag", 9)
+    if dom == "implicit" and prec == 2 and iflag & 8:
+        n_l //= 2  # the FP32-block full solve is a forward and a backward launch
+    avg_ms = t_l / max(n_l, 1)
     alg_bytes = state_bytes_per_cell(dom, prec) * cells
     all_bytes = alg_bytes_per_cell(dom, prec, iflag) * cells
     peak, peak_kind = load_peaks()

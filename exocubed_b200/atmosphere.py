@@ -152,12 +152,18 @@ class CubedSphereAtmosphere:
         nat.check(nat.lib().exo_redo_count(self._ctx, ctypes.byref(n)))
         return n.value
 
-    def write_netcdf(self, basename, file_id="out2", number=0, directory="."):
-        """Primitive output in the reference's per-block NetCDF layout (one
-        file per panel; exocubed_b200.netcdf)."""
+    def write_netcdf(self, basename, file_id="out2", number=0, directory=".", blocks=1,
+                     combine=False):
+        """Primitive output in the reference's per-meshblock NetCDF layout
+        (exocubed_b200.netcdf): blocks x blocks files per panel; with
+        combine, joined into the one file the reference's CombineBlocks
+        leaves.  Returns the paths written."""
         from . import netcdf
-        return netcdf.write_prim_output(self.primitive(), lambda p: mesh(self.cfg, p), basename,
-                                        file_id, number, self.time, directory)
+        paths = netcdf.write_prim_output(self.primitive(), lambda p: mesh(self.cfg, p), basename,
+                                         file_id, number, self.time, directory, blocks)
+        if combine:
+            return [netcdf.combine_blocks(basename, file_id, number, directory)]
+        return paths
 
     def checkpoint(self):
         """The run's checkpoint image (numpy uint8 array): configuration,

@@ -61,6 +61,27 @@ def _num(blocks, block, key, default=None):
     return float(v)
 
 
+def meshblocks_per_edge(source):
+    """Meshblocks along a panel edge (<mesh> nx2 / 2 over <meshblock> nx2)
+    of an input file (a path or its text): the `blocks` of the NetCDF
+    output.  <meshblock> nx3 must equal nx2, and the count must divide the
+    panel and be a power of two (CubedSphere::FindBlockID,
+    src/exo3/cs_find_block_id.cpp:11-13, shifts by it)."""
+    text = source
+    if "\n" not in source and "<" not in source:
+        with open(source) as f:
+            text = f.read()
+    b = parse_inp(text)
+    N = int(_num(b, "mesh", "nx2")) // 2
+    bx2 = int(_num(b, "meshblock", "nx2", N))
+    bx3 = int(_num(b, "meshblock", "nx3", bx2))
+    nb = N // bx2 if bx2 else 0
+    if bx3 != bx2 or bx2 < 1 or N % bx2 or nb & (nb - 1):
+        raise ValueError(f"<meshblock> nx2 = {bx2}, nx3 = {bx3} do not cut a {N}^2 panel "
+                         f"into a power-of-two square of blocks")
+    return nb
+
+
 def config_from_inp(source, precision=nat.EXO_PREC_FP64, eqn=None, rsolver=None,
                     problem=None):
     """(config dict, notes) of an input file (a path or its text).  notes
@@ -83,8 +104,9 @@ def config_from_inp(source, precision=nat.EXO_PREC_FP64, eqn=None, rsolver=None,
     N = nx2 // 2
     bx2 = int(_num(b, "meshblock", "nx2", N))
     if bx2 < N:
-        notes.append(f"meshblocks of {bx2}^2 run as one {N}^2 block per panel "
-                     f"(multi-block ghost interpolation is not built)")
+        notes.append(f"meshblocks of {bx2}^2 step as one {N}^2 block per panel "
+                     f"(multi-block ghost interpolation is not built); output files "
+                     f"follow the {N // bx2} x {N // bx2} blocks (meshblocks_per_edge)")
     if eqn is None:
         eqn = nat.EXO_EQN_SHALLOW_YZ if problem in SHALLOW_PROBLEMS else nat.EXO_EQN_IDEAL
     shallow = eqn == nat.EXO_EQN_SHALLOW_YZ

@@ -23,7 +23,7 @@ def test_implicit_bytes_per_cell(precision, flag, want):
 def test_other_kernels_bytes_per_cell():
     assert bench.alg_bytes_per_cell("flux_x1", 1) == 80
     assert bench.alg_bytes_per_cell("flux_x23", 1) == 80
-    assert bench.alg_bytes_per_cell("flux_x23", 0) == 120
+    assert bench.alg_bytes_per_cell("flux_x23", 0) == 160
     assert bench.alg_bytes_per_cell("update", 1) == 280
     assert bench.alg_bytes_per_cell("update", 2) == 280
     assert bench.alg_bytes_per_cell("update", 0) == 320

@@ -126,10 +126,23 @@ def test_netcdf_output_of_a_run(tmp_path):
         a.set_primitive(W.dry_atmosphere_state(cfg, seed=0))
         a.step(2)
         paths = a.write_netcdf("exo3", "out2", 1, directory=str(tmp_path))
+        combined = a.write_netcdf("exo3", "out2", 2, directory=str(tmp_path), blocks=2,
+                                  combine=True)
         w = a.primitive()
         t = a.time
     f = netcdf_file(paths[2], "r", mmap=False)
     assert np.array_equal(f.variables["press"][0],
                           W.interior(w)[2, 4].transpose(2, 1, 0).astype(np.float32))
     assert f.variables["time"][0] == np.float32(t)
+    f.close()
+    # 2 x 2 meshblocks per panel joined into one file of the 2 x 3 panel layout
+    assert len(combined) == 1 and combined[0].endswith("exo3.out2.00002.nc")
+    f = netcdf_file(combined[0], "r", mmap=False)
+    press = f.variables["press"][0]
+    assert press.shape == (12, 16, 24)
+    wi = W.interior(w)
+    for p in range(6):
+        l2, l3 = p % 2, p // 2
+        assert np.array_equal(press[:, 8 * l2:8 * l2 + 8, 8 * l3:8 * l3 + 8],
+                              wi[p, 4].transpose(2, 1, 0).astype(np.float32))
     f.close()

@@ -7,7 +7,7 @@ import pytest
 
 from exocubed_b200 import _native as nat
 from exocubed_b200 import workloads as W
-from exocubed_b200.inp import config_from_inp, parse_inp
+from exocubed_b200.inp import config_from_inp, meshblocks_per_edge, parse_inp
 
 HS94_LIKE = """
 <comment>
@@ -111,3 +111,15 @@ def test_multi_block_and_unsupported_inputs():
         config_from_inp(HS94_LIKE.replace("xorder     = 5", "xorder     = 3"))
     with pytest.raises(ValueError):
         config_from_inp(HS94_LIKE.replace("nx3        = 120", "nx3        = 100"))
+
+
+def test_meshblocks_per_edge():
+    blocks20 = HS94_LIKE.replace("nx2        = 40\nnx3        = 40",
+                                 "nx2        = 20\nnx3        = 20")
+    assert meshblocks_per_edge(HS94_LIKE) == 1
+    assert meshblocks_per_edge(blocks20) == 2   # hs94-stable20.inp's 20 x 20 blocks
+    assert "(meshblocks_per_edge)" in config_from_inp(blocks20)[1][0]
+    for nx2, nx3 in ((20, 40), (8, 8), (30, 30)):   # not square / not a power of two
+        with pytest.raises(ValueError):
+            meshblocks_per_edge(HS94_LIKE.replace(
+                "nx2        = 40\nnx3        = 40", f"nx2        = {nx2}\nnx3        = {nx3}"))
