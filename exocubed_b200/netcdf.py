@@ -175,8 +175,11 @@ def write_prim_output(w, mesh, basename, file_id="out2", number=0, time=0.0, dir
     names = ["rho", "press", "vel1", "vel2", "vel3"] if nv == 5 else ["rho", "vel1", "vel2",
                                                                       "vel3"]
     index = {"rho": 0, "press": 4, "vel1": 1, "vel2": 2, "vel3": 3}
-    dims = [("time", None), ("x1", L), ("x1f", L + 1), ("x2", n), ("x2f", n + 1),
-            ("x3", n), ("x3f", n + 1)]
+    # a face dimension and its coordinate exist only where the block has
+    # more than one cell along the axis (netcdf.cpp:110-133)
+    dims = [("time", None), ("x1", L)] + ([("x1f", L + 1)] if L > 1 else []) + \
+        [("x2", n)] + ([("x2f", n + 1)] if n > 1 else []) + \
+        [("x3", n)] + ([("x3f", n + 1)] if n > 1 else [])
     gatts = {"NumFilesInSet": np.array([6 * nb * nb], dtype=np.int32)}
     faces = [mesh(p) for p in range(6)]
 
@@ -198,11 +201,15 @@ def write_prim_output(w, mesh, basename, file_id="out2", number=0, time=0.0, dir
         x3v = 0.5 * (x3f[1:] + x3f[:-1])
         variables = [("time", ["time"], {"axis": "T", "units": "s", "long_name": "time"},
                       np.array([time], dtype=np.float32))]
-        variables += [coord("x1", "Z", x1v, [1, L, 1, L]), coord("x1f", None, x1f, [0, L, 0, L]),
-                      coord("x2", "Y", x2v, [1, 2 * N, n * lx2 + 1, n * (lx2 + 1)]),
-                      coord("x2f", None, x2f, [0, 2 * N, n * lx2, n * (lx2 + 1)]),
-                      coord("x3", "X", x3v, [1, 3 * N, n * lx3 + 1, n * (lx3 + 1)]),
-                      coord("x3f", None, x3f, [0, 3 * N, n * lx3, n * (lx3 + 1)])]
+        variables.append(coord("x1", "Z", x1v, [1, L, 1, L]))
+        if L > 1:
+            variables.append(coord("x1f", None, x1f, [0, L, 0, L]))
+        variables.append(coord("x2", "Y", x2v, [1, 2 * N, n * lx2 + 1, n * (lx2 + 1)]))
+        if n > 1:
+            variables.append(coord("x2f", None, x2f, [0, 2 * N, n * lx2, n * (lx2 + 1)]))
+        variables.append(coord("x3", "X", x3v, [1, 3 * N, n * lx3 + 1, n * (lx3 + 1)]))
+        if n > 1:
+            variables.append(coord("x3f", None, x3f, [0, 3 * N, n * lx3, n * (lx3 + 1)]))
         for name in names:
             f = w[p, index[name], k0:k0 + n, j0:j0 + n, G:G + L]       # (k, j, i)
             data = np.transpose(f, (2, 1, 0))[None].astype(np.float32)  # (time, i, j, k)

@@ -181,3 +181,19 @@ def test_combine_blocks(tmp_path, oracle_mod, blocks):
     f.close()
     with pytest.raises(RuntimeError):
         nc.combine_blocks("hs", "out2", 1, directory=d)
+
+
+def test_single_level_has_no_x1_faces(tmp_path, oracle_mod):
+    # the writer defines x1f only where a block has more than one level
+    cfg = W.dry_atmosphere_config(N=6, L=1)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(W.dry_atmosphere_state(cfg, seed=0))
+    paths = nc.write_prim_output(o.primitive(), o.mesh, "t", directory=str(tmp_path))
+    f = netcdf_file(paths[0], "r", mmap=False)
+    assert "x1f" not in f.dimensions and "x1f" not in f.variables
+    assert f.variables["rho"].shape == (1, 1, 6, 6) and "x2f" in f.variables
+    f.close()
+    out = nc.combine_blocks("t", directory=str(tmp_path))
+    f = netcdf_file(out, "r", mmap=False)
+    assert f.variables["rho"].shape == (1, 1, 12, 18)
+    f.close()
