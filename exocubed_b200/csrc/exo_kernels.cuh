@@ -33,8 +33,8 @@
 #include "exo_mbarrier.cuh"
 
 // x2/x3 fluxes: EXO_X23_TILES 1 = a block per line of faces, cells staged
-// through shared memory (flux_x23_pipe); otherwise EXO_X23_LINES 1 = one
-// thread per line of faces
+// through shared memory (flux_x23_pipe), and one thread per face for grids
+// of few levels; otherwise EXO_X23_LINES 1 = one thread per line of faces
 // (sliding stencil window), 0 = one thread per face
 #ifndef EXO_X23_TILES
 #define EXO_X23_TILES 1
@@ -1062,8 +1062,8 @@ __device__ __forceinline__ void edge_outer_state(const DevView& v, int p, int si
   st[IVZ] = T(e.q[2]) * U + T(e.q[3]) * V;
 }
 
-// One thread per face (the FP64 build: its solvers need too many registers
-// to also hold a sliding stencil window).
+// One thread per face: grids of at most X23_FACES_MAX_L levels, where a
+// line of faces would leave most of its lanes idle.
 template <class T>
 __device__ __forceinline__ void flux_x23_faces(const DevView& v, unsigned blk) {
   unsigned tid = blk * blockDim.x + threadIdx.x;
@@ -1254,6 +1254,12 @@ __device__ __forceinline__ void cp_async_wait_one() {
 // per-line kernels; phases 1 and 2 each keep few registers, so many warps
 // are resident.
 constexpr int X23_THREADS = 128;
+// A line's 32 lanes are its radial indices, so a grid of few levels leaves
+// most lanes idle (3 of 32 busy at the exo2 shallow-water grid's 3
+// levels); up to this many levels the tiled build runs the per-face form
+// instead, with X23_THREADS threads a block.
+constexpr int X23_FACES_MAX_L = 8;
+__host__ __device__ constexpr bool x23_uses_lines(int L) { return L > X23_FACES_MAX_L; }
 template <class T>
 __host__ __device__ constexpr int x23_chunk() {
   return sizeof(T) == 4 ? 15 : 7;
@@ -1395,9 +1401,14 @@ __device__ __forceinline__ void flux_x23_pipe(const DevView& v, unsigned blk) {
 
 template <class T>
 __device__ __forceinline__ void flux_x23_block(const DevView& v, unsigned blk) {
-  if constexpr (EXO_X23_TILES) flux_x23_pipe<T>(v, blk);
-  else if constexpr (EXO_X23_LINES) flux_x23_lines<T>(v, blk);
-  else flux_x23_faces<T>(v, blk);
+  if constexpr (EXO_X23_TILES) {
+    if (x23_uses_lines(v.L)) flux_x23_pipe<T>(v, blk);
+    else flux_x23_faces<T>(v, blk);
+  } else if constexpr (EXO_X23_LINES) {
+    flux_x23_lines<T>(v, blk);
+  } else {
+    flux_x23_faces<T>(v, blk);
+  }
 }
 
 // --------------------------------------------------------------- k_update -
@@ -3498,9 +3509,10 @@ int launch_reciprocal(int n, const double* x, double* out, void* stream) {
 }
 
 unsigned x23_blocks(const DevView& v, int tile) {
-  if (EXO_X23_TILES) return x23_tile_blocks(v.N, v.L);
-  const size_t n = EXO_X23_LINES ? (size_t)2 * 6 * v.N * v.L
-                                 : (size_t)2 * 6 * v.N * (v.N + 1) * v.L;
+  const bool lines = EXO_X23_TILES ? x23_uses_lines(v.L) : (bool)EXO_X23_LINES;
+  if (EXO_X23_TILES && lines) return x23_tile_blocks(v.N, v.L);
+  if (EXO_X23_TILES) tile = X23_THREADS;  // the per-face form of the tiled build
+  const size_t n = lines ? (size_t)2 * 6 * v.N * v.L : (size_t)2 * 6 * v.N * (v.N + 1) * v.L;
   return (unsigned)((n + tile - 1) / tile);
 }
 

@@ -24,10 +24,11 @@ def pressure(u, gamma):
     return (gamma - 1.0) * (u[:, 4] - ke)
 
 
+@pytest.mark.parametrize("L", [6, 16])   # the per-face and the line form of x2/x3
 @pytest.mark.parametrize("precision", [nat.EXO_PREC_MIXED, nat.EXO_PREC_MIXED_F32_SOLVE])
 @pytest.mark.parametrize("rsolver", [1, 2])
-def test_mixed_dry_atmosphere_close_to_oracle(oracle_mod, rsolver, precision):
-    cfg = W.dry_atmosphere_config(N=12, L=16, rsolver=rsolver)
+def test_mixed_dry_atmosphere_close_to_oracle(oracle_mod, rsolver, precision, L):
+    cfg = W.dry_atmosphere_config(N=12, L=L, rsolver=rsolver)
     state = W.dry_atmosphere_state(cfg, seed=31)
     o = oracle_mod.Oracle(cfg)
     o.set_primitive(state)
