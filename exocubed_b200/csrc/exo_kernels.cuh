@@ -1062,8 +1062,8 @@ __device__ __forceinline__ void edge_outer_state(const DevView& v, int p, int si
   st[IVZ] = T(e.q[2]) * U + T(e.q[3]) * V;
 }
 
-// One thread per face: grids of at most X23_FACES_MAX_L levels, where a
-// line of faces would leave most of its lanes idle.
+// One thread per face: grids whose level count leaves too many of a line's
+// lanes idle (x23_uses_lines).
 template <class T>
 __device__ __forceinline__ void flux_x23_faces(const DevView& v, unsigned blk) {
   unsigned tid = blk * blockDim.x + threadIdx.x;
@@ -1254,12 +1254,19 @@ __device__ __forceinline__ void cp_async_wait_one() {
 // per-line kernels; phases 1 and 2 each keep few registers, so many warps
 // are resident.
 constexpr int X23_THREADS = 128;
-// A line's 32 lanes are its radial indices, so a grid of few levels leaves
-// most lanes idle (3 of 32 busy at the exo2 shallow-water grid's 3
-// levels); up to this many levels the tiled build runs the per-face form
-// instead, with X23_THREADS threads a block.
-constexpr int X23_FACES_MAX_L = 8;
-__host__ __device__ constexpr bool x23_uses_lines(int L) { return L > X23_FACES_MAX_L; }
+// A line's 32 lanes are its radial indices, so the line form keeps
+// L / (32 ceil(L / 32)) of its lanes busy: 3 of 32 at the exo2
+// shallow-water grid's 3 levels, 62.5 % at HS94's 40.  Below a busy
+// fraction the per-face form (X23_THREADS threads a block) is faster:
+// measured at 40 and 64 levels, the FP64 build's crossover lies near 85 %
+// (its line form is 16 % faster at 100 %, 2x slower at 62.5 %), the mixed
+// build's near 65 % (line form 1.7x faster at 100 %).
+#ifndef EXO_X23_LINE_BUSY_PCT
+#define EXO_X23_LINE_BUSY_PCT (EXO_MIXED ? 65 : 85)
+#endif
+__host__ __device__ constexpr bool x23_uses_lines(int L) {
+  return L * 100 >= EXO_X23_LINE_BUSY_PCT * 32 * ((L + 31) / 32);
+}
 template <class T>
 __host__ __device__ constexpr int x23_chunk() {
   return sizeof(T) == 4 ? 15 : 7;

@@ -15,11 +15,12 @@ pytestmark = pytest.mark.gpu
 
 
 def _members(precision):
-    """Uneven members: sizes, levels, solvers, gases and one shallow-water
-    sphere (fp64 only: its own equation set and variable count)."""
+    """Uneven members: sizes, levels (32 takes the x2/x3 line form, the
+    others the per-face form), solvers, gases and one shallow-water sphere
+    (fp64 only: its own equation set and variable count)."""
     out = []
     for n, (N, L, rs) in enumerate([(8, 12, nat.EXO_RS_LMARS), (12, 8, nat.EXO_RS_HLLC),
-                                    (6, 20, nat.EXO_RS_LMARS), (10, 16, nat.EXO_RS_HLLC)]):
+                                    (6, 32, nat.EXO_RS_LMARS), (10, 16, nat.EXO_RS_HLLC)]):
         cfg = W.dry_atmosphere_config(N=N, L=L, rsolver=rs, T0=200. + 20 * n,
                                       g=5. + 4 * n, gamma=1.3 + 0.1 * n, precision=precision)
         out.append((cfg, W.dry_atmosphere_state(cfg, seed=40 + n)))
