@@ -11,9 +11,10 @@
 // member of a batch (a single atmosphere is a batch of one):
 //   kb_flux_x1    per radial column: hydrostatic decomposition, WENO5 in x1,
 //                 restore, Riemann solve -> x1 face fluxes         (exo3 only)
-//   kb_flux_x23   per horizontal face: WENO5 on both sides; at panel edges the
-//                 outer state is the neighbour panel's own reconstruction,
-//                 rotated into this panel's basis; Riemann solve -> x2/x3 fluxes
+//   kb_flux_x23   per line of horizontal faces (per face on grids of few
+//                 levels): WENO5 on both sides; at panel edges the outer state
+//                 is the neighbour panel's own reconstruction, rotated into
+//                 this panel's basis; Riemann solve -> x2/x3 fluxes
 //   kb_update     per cell: RK register average, flux divergence, geometric
 //                 source, gravity / Coriolis -> u (exo2) or du (exo3)
 //   kb_implicit   per radial column: 5x5 block-tridiagonal vertical correction,
