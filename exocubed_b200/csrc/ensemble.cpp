@@ -95,27 +95,34 @@ int rebuild(exo_ensemble* e) {
   unsigned tot[exo::BK_COUNT] = {0, 0, 0, 0, 0, 0};
   bool any_full = false;  // some member takes the 5x5 correction
   int max_nc1 = 1;
+  // the x1 blocks' threads: the ensemble's columns per block at the deepest
+  // member; every member then takes as many columns as fill those threads
   int x1_threads = 32;
+  for (Member* m : e->slots) {
+    if (!m || m->v.eqn == EXO_EQN_SHALLOW_YZ) continue;
+    DevView tv = m->v;  // with the ensemble's tiles
+    for (int k = 0; k < exo::BK_COUNT; ++k) tv.tiles[k] = e->tiles.t[k];
+    x1_threads = std::max(x1_threads, exo::x1_threads(tv));
+  }
   size_t x1_smem = 8;
   for (Member* m : e->slots) {
     if (!m) continue;
     int idx = (int)views.size();
     views.push_back(m->v);
-    for (int k = 0; k < exo::BK_COUNT; ++k) views.back().tiles[k] = e->tiles.t[k];
+    DevView& mv = views.back();
+    for (int k = 0; k < exo::BK_COUNT; ++k) mv.tiles[k] = e->tiles.t[k];
+    if (mv.eqn != EXO_EQN_SHALLOW_YZ) {
+      mv.tiles[exo::BK_X1] = exo::x1_member_columns(mv, x1_threads, exo::X1_SMEM_MAX);
+      x1_smem = std::max(x1_smem, exo::x1_smem_bytes(mv));
+    }
     max_nc1 = std::max(max_nc1, m->v.nc1);
     if (m->v.eqn != EXO_EQN_SHALLOW_YZ && (m->v.implicit_flag & 1) && (m->v.implicit_flag & 8))
       any_full = true;
     unsigned b[exo::BK_COUNT];
-    exo::member_blocks(m->v, e->tiles.t, b);
+    exo::member_blocks(m->v, mv.tiles, b);
     for (int k = 0; k < exo::BK_COUNT; ++k) {
       start[(size_t)k * (e->capacity + 1) + idx] = tot[k];
       tot[k] += b[k];
-    }
-    if (m->v.eqn != EXO_EQN_SHALLOW_YZ) {
-      DevView tv = m->v;  // with the ensemble's tiles
-      for (int k = 0; k < exo::BK_COUNT; ++k) tv.tiles[k] = e->tiles.t[k];
-      x1_threads = std::max(x1_threads, exo::x1_threads(tv));
-      x1_smem = std::max(x1_smem, exo::x1_smem_bytes(tv));
     }
   }
   int n = (int)views.size();

@@ -192,6 +192,9 @@ bool valid_tiles(const int* t, std::string* err);
 // Shared memory per column: the primitives and the face pressures, and in
 // the mixed build ln psf and the face densities.
 constexpr int X1_MAX_COLUMNS = 8;
+// the x1 kernel's dynamic shared memory limit (the mixed build's 8 columns
+// of 250 levels take 212 KB)
+constexpr int X1_SMEM_MAX = 224 * 1024;
 #ifdef __CUDACC__
 #define EXO_HD __host__ __device__
 #else
@@ -226,6 +229,17 @@ inline size_t x1_smem_bytes(const DevView& v) {
 inline int x1_threads(const DevView& v) {
   int t = ((x1_cols(v) * (v.L + 1) + 31) / 32) * 32;
   return t > 1024 ? 1024 : t;
+}
+// Columns per block of a member of a batch whose x1 blocks run `threads`
+// threads: as many as the member's faces fill (a member with fewer levels
+// than the batch's deepest takes more columns per block rather than leave
+// threads idle), 1 to X1_MAX_COLUMNS, within the kernel's shared memory.
+inline int x1_member_columns(const DevView& v, int threads, size_t smem_max) {
+  int c = threads / (v.L + 1);
+  c = c < 1 ? 1 : (c > X1_MAX_COLUMNS ? X1_MAX_COLUMNS : c);
+  const size_t per = (size_t)x1_column_doubles(v) * sizeof(double);
+  while (c > 1 && (size_t)c * per > smem_max) --c;
+  return c;
 }
 // block counts of one member for the given tiles
 void member_blocks(const DevView& v, const int* tiles, unsigned blocks[BK_COUNT]);

@@ -2926,8 +2926,6 @@ __device__ __forceinline__ double* impl_radial(double* ism) {
 }
 // the largest dynamic shared memory a launch may ask for
 constexpr int IMPL_SMEM_MAX = 160 * 1024;
-// the mixed x1 kernel's 8 columns of 250 levels take 212 KB
-constexpr int X1_SMEM_MAX = 224 * 1024;
 
 // copies the radial geometry of the member into shared memory (all threads
 // of the block take part; returns the shared copies)
