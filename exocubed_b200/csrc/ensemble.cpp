@@ -105,8 +105,15 @@ int rebuild(exo_ensemble* e) {
     x1_threads = std::max(x1_threads, exo::x1_threads(tv));
   }
   size_t x1_smem = 8;
-  for (Member* m : e->slots) {
-    if (!m) continue;
+  // members in the batch deepest first: the blocks of a launch start in
+  // index order, so the columns with the longest vertical walks start
+  // first and the last wave holds short ones
+  std::vector<Member*> order;
+  for (Member* m : e->slots)
+    if (m) order.push_back(m);
+  std::stable_sort(order.begin(), order.end(),
+                   [](const Member* a, const Member* b) { return a->v.L > b->v.L; });
+  for (Member* m : order) {
     int idx = (int)views.size();
     views.push_back(m->v);
     DevView& mv = views.back();
