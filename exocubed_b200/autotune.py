@@ -26,9 +26,9 @@ from . import _native as nat
 CANDIDATES = {
     nat.EXO_K_FLUX_X1: (1, 2, 3, 4),     # radial columns per block
     nat.EXO_K_FLUX_X23: (128,),          # both x2/x3 forms run 128 threads a block
-    nat.EXO_K_UPDATE: (64, 128, 256),
+    nat.EXO_K_UPDATE: (32, 64, 128, 256),
     nat.EXO_K_IMPLICIT: (32, 64, 128),
-    nat.EXO_K_PRIM_GHOST: (128, 256, 512),
+    nat.EXO_K_PRIM_GHOST: (64, 128, 256, 512),
 }
 NTRIAL = max(len(c) for c in CANDIDATES.values())  # trials measure every kernel at once
 
