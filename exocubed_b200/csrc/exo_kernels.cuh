@@ -1254,7 +1254,10 @@ __device__ __forceinline__ void cp_async_wait_one() {
 // Each face gets the values and operations it gets in the per-face and
 // per-line kernels; phases 1 and 2 each keep few registers, so many warps
 // are resident.
-constexpr int X23_THREADS = 128;
+#ifndef EXO_X23_THREADS
+#define EXO_X23_THREADS 128
+#endif
+constexpr int X23_THREADS = EXO_X23_THREADS;
 // A line's 32 lanes are its radial indices, so the line form keeps
 // L / (32 ceil(L / 32)) of its lanes busy: 3 of 32 at the exo2
 // shallow-water grid's 3 levels, 62.5 % at HS94's 40.  Below a busy
