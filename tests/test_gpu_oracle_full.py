@@ -6,9 +6,10 @@ between CUDA and glibc; everything else in the FP64 build is bit-exact, see
 test_gpu_parity.py):
   * FP64 build: relative L2 of every conserved variable <= 1e-9 after 10
     CFL steps of the C2 workload (6 x 96 x 96 x 64), and after 3 steps of
-    each extreme member; the CFL time step to 1e-9.
+    each extreme member and of the headline workload (6 x 192 x 192 x 96);
+    the CFL time step to 1e-9.
   * mixed build: relative L2 of density and pressure <= 1e-6 after 3 steps
-    of each extreme member.
+    of each extreme member and of the headline workload.
 """
 import numpy as np
 import pytest
@@ -139,3 +140,36 @@ def test_c2_1000_steps_against_the_oracle_run():
             if bar is not None and not (row["rho"]["rel_l2"] < bar and row["p"]["rel_l2"] < bar):
                 failed.append((path, n, bar, row["rho"]["rel_l2"], row["p"]["rel_l2"]))
     assert not failed, failed
+
+
+@pytest.fixture(scope="module")
+def c3_oracle_run(oracle_mod):
+    """The headline workload (6 x 192 x 192 x 96, LMARS, implicit_flag 9,
+    seeded isothermal state with temperature and wind noise) stepped 3 CFL
+    steps by the oracle; about 15 s on 16 host threads."""
+    cfg = W.dry_atmosphere_config(N=192, L=96, rsolver=nat.EXO_RS_LMARS)
+    state = W.dry_atmosphere_state(cfg, seed=0)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(state)
+    o.step(3)
+    assert o.invalid() == 0
+    return dict(cfg=cfg, state=state, dt=o.dt, time=o.time, o=o)
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_c3_three_steps_against_oracle(c3_oracle_run, precision):
+    """The headline workload at its own size, both builds, against the same
+    oracle run: FP64 every conserved variable to 1e-9 relative L2 and the
+    time step to 1e-9; mixed density and pressure to 1e-6, the time step to
+    1e-5."""
+    r = c3_oracle_run
+    cfg = dict(r["cfg"], precision=precision)
+    with CubedSphereAtmosphere(cfg) as g:
+        g.set_primitive(r["state"])
+        g.step(3)
+        assert g.invalid() == 0
+        tol = 1e-9 if precision == nat.EXO_PREC_FP64 else 1e-5
+        assert g.dt == pytest.approx(r["dt"], rel=tol)
+        assert g.time == pytest.approx(r["time"], rel=tol)
+        ug = W.interior(g.conserved())
+    _check(cfg, ug, r["o"], precision)
