@@ -98,3 +98,28 @@ def test_forced_and_unforced_members_in_one_batch(precision):
         for slot, want in zip(slots, alone):
             assert np.array_equal(e.conserved(slot), want)
             assert e.invalid(slot) == 0
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_hs94_at_its_own_size(oracle_mod, precision):
+    """The Held-Suarez workload as its input file sets it up (6 x 40 x 40 x
+    40, HLLC, implicit_flag 1, CFL 0.9, forcing on), 5 CFL steps against the
+    oracle: FP64 every conserved variable to 1e-9 relative L2, mixed density
+    and total energy to 1e-6."""
+    cfg = W.hs94_config()
+    state = W.hs94_state(cfg, seed=0)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(state)
+    o.step(5)
+    assert o.invalid() == 0
+    with CubedSphereAtmosphere(dict(cfg, precision=precision)) as g:
+        g.set_primitive(state)
+        g.step(5)
+        assert g.invalid() == 0
+        assert g.dt == pytest.approx(o.dt, rel=1e-9 if precision == nat.EXO_PREC_FP64 else 1e-5)
+        ug = W.interior(g.conserved())
+    uo = W.interior(o.conserved())
+    vars_, tol = ((range(5), 1e-9) if precision == nat.EXO_PREC_FP64 else ((0, 4), 1e-6))
+    for n in vars_:
+        rel = np.linalg.norm(ug[:, n] - uo[:, n]) / np.linalg.norm(uo[:, n])
+        assert rel < tol, (n, rel)
