@@ -6,10 +6,11 @@ between CUDA and glibc; everything else in the FP64 build is bit-exact, see
 test_gpu_parity.py):
   * FP64 build: relative L2 of every conserved variable <= 1e-9 after 10
     CFL steps of the C2 workload (6 x 96 x 96 x 64), and after 3 steps of
-    each extreme member and of the headline workload (6 x 192 x 192 x 96);
-    the CFL time step to 1e-9.
+    each extreme member, of the headline workload (6 x 192 x 192 x 96) and
+    of four benchmarked ensemble members at their own sizes; the CFL time
+    step to 1e-9.
   * mixed build: relative L2 of density and pressure <= 1e-6 after 3 steps
-    of each extreme member and of the headline workload.
+    of the same runs.
 """
 import numpy as np
 import pytest
@@ -173,3 +174,34 @@ def test_c3_three_steps_against_oracle(c3_oracle_run, precision):
         assert g.time == pytest.approx(r["time"], rel=tol)
         ug = W.interior(g.conserved())
     _check(cfg, ug, r["o"], precision)
+
+
+@pytest.fixture(scope="module")
+def ensemble_oracle_runs(oracle_mod):
+    """The first four members of the benchmarked ensemble (seeds 0-3: N 96,
+    48, 96, 96; L 64, 64, 48, 32; gamma 1.34-1.60; gravity 3.4-23.9 m/s^2),
+    each stepped 3 CFL steps by the oracle at its own size."""
+    runs = []
+    for seed in range(4):
+        cfg, w = W.ensemble_member(seed, precision=nat.EXO_PREC_FP64)
+        o = oracle_mod.Oracle(cfg)
+        o.set_primitive(w)
+        o.step(3)
+        assert o.invalid() == 0
+        runs.append((cfg, w, o))
+    return runs
+
+
+@pytest.mark.parametrize("precision", [nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED])
+def test_ensemble_members_at_their_own_sizes_against_oracle(ensemble_oracle_runs, precision):
+    """Members of the benchmarked distribution, batched in one ensemble as the
+    benchmark runs them, each against its own oracle run (tolerances as for
+    the extremes)."""
+    with Ensemble(precision=precision, capacity=4) as ens:
+        slots = [ens.add(dict(cfg, precision=precision), w)
+                 for cfg, w, _ in ensemble_oracle_runs]
+        ens.step(3)
+        assert all(ens.invalid(s) == 0 for s in slots)
+        got = [W.interior(ens.conserved(s)) for s in slots]
+    for (cfg, _, o), ug in zip(ensemble_oracle_runs, got):
+        _check(cfg, ug, o, precision)
