@@ -205,3 +205,24 @@ def test_ensemble_members_at_their_own_sizes_against_oracle(ensemble_oracle_runs
         got = [W.interior(ens.conserved(s)) for s in slots]
     for (cfg, _, o), ug in zip(ensemble_oracle_runs, got):
         _check(cfg, ug, o, precision)
+
+
+def test_c3_hllc_partial_correction_against_oracle(oracle_mod):
+    """The headline grid with the other solver choices the benchmark reports:
+    HLLC and the partial 3x3 correction (implicit_flag 1), 3 CFL steps, the
+    FP64 and mixed builds against one oracle run (tolerances as above)."""
+    cfg = W.dry_atmosphere_config(N=192, L=96, rsolver=nat.EXO_RS_HLLC, implicit_flag=1)
+    state = W.dry_atmosphere_state(cfg, seed=1)
+    o = oracle_mod.Oracle(cfg)
+    o.set_primitive(state)
+    o.step(3)
+    assert o.invalid() == 0
+    for precision in (nat.EXO_PREC_FP64, nat.EXO_PREC_MIXED):
+        c = dict(cfg, precision=precision)
+        with CubedSphereAtmosphere(c) as g:
+            g.set_primitive(state)
+            g.step(3)
+            assert g.invalid() == 0
+            assert g.dt == pytest.approx(o.dt, rel=1e-9 if precision == nat.EXO_PREC_FP64 else 1e-5)
+            ug = W.interior(g.conserved())
+        _check(c, ug, o, precision)
